@@ -1,0 +1,242 @@
+/*
+ * nsegpu.h -- C-ABI of libnsegpu.so, the B200 (sm_100a) drop-in for the
+ * fractional-step hot path of DominikHenzel/vtkmakeCompare.
+ *
+ * Tier 1 and tier 2 are the reference's own Fortran subroutines, exported
+ * under gfortran's default mangling (lower case + trailing underscore), with
+ * every argument passed by reference exactly as the Fortran caller passes it.
+ * Arrays are the caller's host arrays in the reference layout:
+ *   padded field  REAL*8 (0:nx+1,0:ny+1,0:nz+1), column-major (x fastest)
+ *   cellvalue     REAL*8 (1:nx,1:ny,1:nz,1:4)
+ *   spectrum      COMPLEX*16 (0:nx/2,0:ny+1,0:nz+1), interleaved re,im
+ * Each call copies its inputs to the GPU, runs CUDA kernels and copies back
+ * exactly the entries the reference routine writes.  Legacy entry points
+ * return nothing (as in Fortran); on failure they print one line to stderr
+ * and record the error for nse_last_error().  There is no CPU fallback: a
+ * missing or unusable GPU is an error.
+ *
+ * Tier 3 is the resident API: the fields live in HBM across time steps and
+ * every function returns an nse_status.
+ *
+ * Not re-entrant per context; one host thread per context.
+ */
+#ifndef NSEGPU_H
+#define NSEGPU_H
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ------------------------------------------------------------------ status */
+typedef enum nse_status {
+  NSE_OK = 0,
+  NSE_ERR_ARG = 1,        /* bad dimension or argument */
+  NSE_ERR_CUDA = 2,       /* CUDA runtime error or no usable GPU */
+  NSE_ERR_NOMEM = 3,      /* device allocation failed */
+  NSE_ERR_NONFINITE = 4,  /* non-finite value detected in a field */
+  NSE_ERR_LIMIT = 5       /* size beyond a documented limit */
+} nse_status;
+
+const char* nse_last_error(void);
+int nse_last_status(void);
+void nse_clear_error(void);
+
+/* ------------------------------------------ tier 1: the drop-in files ---- */
+
+/* p2s_fftw2d.f:5 P2S(FP,FPT,NX,NY,NZ): per y-plane J=1..NY, real 2-D DFT of
+ * FP(0:NX-1,J,0:NZ-1), half spectrum scaled by 1/(NX*NZ) into
+ * FPT(0:NX/2,J,0:NZ-1).  Own radix kernels (no cuFFT/FFTW). */
+void p2s_(double* FP, double* FPT, const int* NX, const int* NY, const int* NZ);
+/* p2s_fftw2d.f:116 S2P(FPT,FP,NX,NY,NZ): inverse (unnormalised c2r) per plane,
+ * then FP(NX,J,:)=FP(0,J,:), FP(:,J,NZ)=FP(:,J,0). */
+void s2p_(double* FPT, double* FP, const int* NX, const int* NY, const int* NZ);
+
+/* tridiag.f:5 TRIDIAG(A,B,NN), :21 TRID2(A,B,M,N), :43 CTRIDIAG(A,B,NN):
+ * Thomas solves without pivoting; A(NN,3) is overwritten as in the reference. */
+void tridiag_(double* A, double* B, const int* NN);
+void trid2_(double* A, double* B, const int* M, const int* N);
+void ctridiag_(double* A, double* B, const int* NN);
+
+/* periodic_implicit.f:1 implicit_solver(SUX,nx,dx,dx12,Re,dt,ft,fb,eta,CUX),
+ * :47 TDMA(a,b,c,r,u,n), :67 cyclic(a,b,c,alpha,beta,r,x,n).  The NMAX=500
+ * static limit of the reference does not apply. */
+void implicit_solver_(double* SUX, const int* nx, const double* dx, const double* dx12,
+                      const double* Re, const double* dt, const double* ft,
+                      const double* fb, const double* eta, const double* CUX);
+void tdma_(const double* a, const double* b, const double* c, const double* r, double* u,
+           const int* n);
+void cyclic_(const double* a, const double* b, const double* c, const double* alpha,
+             const double* beta, const double* r, double* x, const int* n);
+
+/* mkp.f:9 MKP: projection step (divergence RHS, FFT Poisson, correction).
+ * ompnthreads is accepted and ignored. */
+void mkp_(double* p, double* u_temp, double* v_temp, double* w_temp, const double* dt,
+          const double* dx, const double* dy, const double* dz, const double* dx12,
+          const double* dy12, const double* dz12, const double* Re, const int* nx,
+          const int* ny, const int* nz, const void* ompnthreads, double* u_ta, double* v_ta,
+          double* w_ta, double* u_ep2, double* v_ep2, double* w_ep2, double* divu,
+          double* u, double* v, double* w, const double* xl, const double* zl);
+/* mkp.f:223 SPN, :263 SP0B, :293 PHIBC */
+void spn_(const int* NX, const int* NY, const int* NZ, const double* AC, const double* KXZ,
+          double* PHIT);
+void sp0b_(const int* NX, const int* NY, const int* NZ, const double* AC, double* PHIT);
+void phibc_(const int* NX, const int* NY, const int* NZ, double* PHI);
+
+/* set_levelset.f:1 set_levelset(nx,ny,nz,dx,dx12,dy12,dz12,phi0,phi,x,y,z,cellvalue):
+ * 2001 reinitialisation sweeps on the GPU, mask into cellvalue(:,:,:,1), and the
+ * ASCII files levelset.vtk / cellvalue1.vtk written as the reference does
+ * (set NSEGPU_NO_VTK=1 to skip the files). */
+void set_levelset_(const int* nx, const int* ny, const int* nz, const double* dx,
+                   const double* dx12, const double* dy12, const double* dz12,
+                   const double* phi0, double* phi, const double* x, const double* y,
+                   const double* z, double* cellvalue);
+/* set_levelset.f:202 readgrid3d(nx,ny,nz,phi0): reads structure.dat (host I/O) */
+void readgrid3d_(const int* nx, const int* ny, const int* nz, double* phi0);
+
+/* --------------------------- tier 2: step routines of nse_dominik.f ---- */
+void set_c_(const int* nx, const int* ny, const int* nz, double* x, double* x12, double* y,
+            double* y12, double* z, double* z12, double* dx, double* dx12, double* dy,
+            double* dy12, double* dz, double* dz12, const double* xl, const double* yl,
+            const double* zl);                                   /* nse_dominik.f:553 */
+void set_bc_(double* u, double* v, double* w, double* p, const int* nx, const int* ny,
+             const int* nz, double* T);                          /* nse_dominik.f:611 */
+void set_convect_(double* u, double* u_v, double* v, double* v_v, double* w, double* w_v,
+                  const double* dt, const int* nx, const int* ny, const int* nz,
+                  const double* dx, const double* dy, const double* dz, const double* dx12,
+                  const double* dy12, const double* dz12);     /* nse_dominik.f:757 */
+void set_convection_for_scalar_(double* u, double* v, double* w, const double* dt,
+                                const int* nx, const int* ny, const int* nz,
+                                const double* dx, const double* dy, const double* dz,
+                                const double* dx12, const double* dy12, const double* dz12,
+                                double* T, double* u_vT, double* rhoCp); /* :834 */
+void set_conduction_(double* u, double* u_d, double* v, double* v_d, double* w, double* w_d,
+                     const double* Re, const double* dt, const int* nx, const int* ny,
+                     const int* nz, const double* dx, const double* dy, const double* dz,
+                     const double* dx12, const double* dy12, const double* dz12); /* :888 */
+void set_diffusion_for_scalar_(const double* Re, const double* dt, const int* nx,
+                               const int* ny, const int* nz, const double* dx,
+                               const double* dy, const double* dz, const double* dx12,
+                               const double* dy12, const double* dz12, double* T,
+                               double* u_dT, const double* Sc, double* thc,
+                               double* rhoCp);                   /* :950 */
+void set_immersed_boundary_(const double* eta, const int* nx, const int* ny, const int* nz,
+                            const double* dt, double* u_l, double* v_l, double* w_l,
+                            const double* dx, const double* dy, const double* dz,
+                            double* T_l, double* cellvalue, double* u_ta, double* v_ta,
+                            double* w_ta, const int* l, double* cons_cell); /* :1011 */
+void set_explicit_(double* u_v, double* u_pre, double* u_d, double* u_a, double* v_v,
+                   double* v_pre, double* v_d, double* v_a, double* w_v, double* w_pre,
+                   double* w_d, double* w_a, double* u_l, double* v_l, double* w_l,
+                   const int* nx, const int* ny, const int* nz, const int* l); /* :1132 */
+void set_explicit_for_tempreture_(double* u_vT, double* u_dT, double* u_T, double* T_pre,
+                                  double* T_l, const int* nx, const int* ny, const int* nz,
+                                  const int* l);                  /* :1291 */
+void solve_u_temp_(double* u_a, double* v_a, double* w_a, const int* nx, const int* ny,
+                   const int* nz, const double* dx, const double* dy, const double* dz,
+                   const double* dx12, const double* dy12, const double* dz12,
+                   const double* Re, const double* dt, const double* eta,
+                   double* cellvalue, double* u, double* v, double* w); /* :1344 */
+void solve_t_(double* u_T, const int* nx, const int* ny, const int* nz, const double* dx,
+              const double* dy, const double* dz, const double* dx12, const double* dy12,
+              const double* dz12, const double* Re, const double* Sc, const double* dt,
+              double* rhoCp, double* thc, double* cellvalue, const double* eta); /* :1465 */
+/* single-line solvers nse_dominik.f:1505 implicit_uy, :1583 implicit_vy,
+ * :1725 implicit_Tx, :1784 implicit_Ty */
+void implicit_uy_(double* SUY, const int* ny, const double* dy, const double* dy12,
+                  const double* Re, const double* dt, const double* ft, const double* fb,
+                  const double* eta, const double* CUY);
+void implicit_vy_(double* SVY, const int* ny, const double* dy, const double* dy12,
+                  const double* Re, const double* dt, const double* ft, const double* fb,
+                  const double* eta, const double* CVY);
+void implicit_tx_(double* STX, const int* nx, const double* dx, const double* dx12,
+                  const double* Re, const double* Sc, const double* dt, const double* llx,
+                  const double* rrx, const double* ft, const double* fb, const double* eta,
+                  const double* CUX);
+void implicit_ty_(double* STY, const int* ny, const double* dy, const double* dy12,
+                  const double* Re, const double* Sc, const double* dt, const double* lly,
+                  const double* rry, const double* ft, const double* fb, const double* CUY,
+                  const double* eta);
+
+/* Extension (no counterpart in the reference): SET_C with the y faces
+ * y12(j) = y0 + yl/2 (1 + tanh(gamma(2j/ny-1))/tanh(gamma)), j=0..ny, the
+ * ghost spacing mirrored; gamma = 0 gives SET_C shifted by y0. */
+void nse_set_c_stretched(int nx, int ny, int nz, double* x, double* x12, double* y,
+                         double* y12, double* z, double* z12, double* dx, double* dx12,
+                         double* dy, double* dy12, double* dz, double* dz12, double xl,
+                         double yl, double zl, double y0, double gamma);
+
+/* ------------------------------------------------ tier 3: resident API ---- */
+typedef struct nse_config {
+  int nx, ny, nz;
+  double dt, Re, Sc, eta;
+  double xl, yl, zl;
+  double y0;            /* y origin (0 in the reference SET_C) */
+  double ystretch;      /* tanh stretching gamma in y; 0 = uniform (reference) */
+  double body_force;    /* x body force; 1.0 in the reference (nse_dominik.f:785) */
+  double heat_source;   /* volumetric heat source; 1.0 in the reference (:879) */
+  double t_bot, t_top;  /* wall temperatures at y=y0, y=y0+yl; 0 in the reference */
+  double t_solid;       /* temperature imposed in the solid; 0 in the reference */
+  double rho_cp, thc;   /* uniform rhoCp and conductivity; 1 in the reference */
+  int precision;        /* NSE_FP64 (plain) or NSE_MIXED */
+  int flags;
+} nse_config;
+
+enum { NSE_FP64 = 0, NSE_MIXED = 1 };
+
+/* field ids for upload/download (padded fields unless noted) */
+enum nse_field {
+  NSE_U = 0, NSE_V, NSE_W, NSE_P, NSE_T,
+  NSE_U_TA, NSE_V_TA, NSE_W_TA,
+  NSE_U_PRE, NSE_V_PRE, NSE_W_PRE, NSE_T_PRE,
+  NSE_DIVU, NSE_U_EP2, NSE_V_EP2, NSE_W_EP2,
+  NSE_PHI,          /* Poisson right-hand side / solution (padded) */
+  NSE_CELLVALUE,    /* (nx,ny,nz,4) mask, only column 1 is used on upload */
+  NSE_NUM_FIELDS
+};
+
+typedef struct nse_ctx nse_ctx;
+
+int nse_ctx_create(const nse_config* cfg, nse_ctx** out);
+int nse_ctx_destroy(nse_ctx* ctx);
+/* run subsequent work on this cudaStream_t (NULL = the context's own stream) */
+int nse_ctx_set_stream(nse_ctx* ctx, void* stream);
+int nse_ctx_upload(nse_ctx* ctx, int field, const double* host);
+int nse_ctx_download(nse_ctx* ctx, int field, double* host);
+/* grid arrays (each n+2 long) of the context, as SET_C / its stretched variant */
+int nse_ctx_grid(nse_ctx* ctx, double* x, double* x12, double* y, double* y12, double* z,
+                 double* z12, double* dx, double* dx12, double* dy, double* dy12,
+                 double* dz, double* dz12);
+/* step counter l of the reference loop (1 = first step: Euler start, masks built) */
+int nse_ctx_set_step(nse_ctx* ctx, int l);
+int nse_ctx_get_step(nse_ctx* ctx);
+/* copy u,v,w,T into the AB2 histories (nse_dominik.f:246-257) */
+int nse_start(nse_ctx* ctx);
+/* nsteps time steps (nse_dominik.f:290-446), asynchronous on the context stream */
+int nse_step(nse_ctx* ctx, int nsteps);
+/* MKP on the resident fields, reading u,v,w as u_temp (asynchronous) */
+int nse_project(nse_ctx* ctx);
+/* Poisson solve P2S->SPN->SP0B->S2P->PHIBC in place on the NSE_PHI field */
+int nse_poisson(nse_ctx* ctx);
+/* level set reinitialisation + mask from a padded phi0 (host) into the
+ * resident mask; phi_out (padded, host) may be NULL */
+int nse_levelset(nse_ctx* ctx, const double* phi0, double* phi_out, int nnn, double dtau,
+                 double width);
+/* FP64 device reductions: out[0]=max|divu|, out[1]=sum|u|dx, out[2]=sum|v|dy,
+ * out[3]=sum|w|dz, out[4]=sum T dx dy dz (all cells), out[5]=non-finite count */
+int nse_monitor(nse_ctx* ctx, double out[6]);
+int nse_sync(nse_ctx* ctx);
+/* Per-phase timing of the next max_steps steps with CUDA events on the
+ * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the
+ * summed milliseconds over the profiled steps; phases in launch order:
+ * set_bc, rhs, y-lines u/v/w, z-lines u/v/w, x-lines u/v/w, T y, T x, T z,
+ * set_bc(u_temp), fft x fwd, fft z fwd, spn+sp0b, fft z inv, fft x inv,
+ * phibc, correction (16 phases). */
+int nse_ctx_profile(nse_ctx* ctx, int max_steps);
+int nse_ctx_phase_times(nse_ctx* ctx, double* ms, int nphase, int* nsteps);
+/* number of kernel launches this process has issued through the library */
+long long nse_launch_count(void);
+
+#ifdef __cplusplus
+}
+#endif
+#endif

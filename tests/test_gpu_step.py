@@ -1,0 +1,199 @@
+"""Resident time step (nse_ctx_*) against the CPU oracle's restatement of the
+reference time loop, plus the known-answer and size-independent checks.
+
+Tolerance: velocity, pressure and temperature after N steps within 1e-10
+relative L2 of the oracle (the stencils and line solves round identically;
+the FFT transform differs at the 1e-15 level).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._helpers import oracle_grid, rel_l2
+from vtkmakecompare_b200 import solver as S
+from vtkmakecompare_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("u", "v", "w", "p", "T", "u_ta", "v_ta", "w_ta", "u_pre", "v_pre", "w_pre", "T_pre",
+         "divu", "u_ep2", "v_ep2", "w_ep2")
+
+
+def smooth_mask(g, center, radius, width):
+    """Smoothed-Heaviside mask of set_levelset.f:157-170 applied to the exact
+    signed distance (no reinitialisation)."""
+    phi = W.sphere_phi0(g, center, radius)[1:-1, 1:-1, 1:-1]
+    h = width * g["dx"][1:-1, None, None]
+    c = (np.sin(3.1415926535 * phi / 2.0 / h) + 1.0) / 2.0
+    c = np.where(phi >= h, 1.0, np.where(phi <= -h, 0.0, c))
+    return np.asfortranarray(c)
+
+
+def make_case(nx, ny, nz, seed=3, sphere=True, Re=3000.0, Pr=0.71, eta=1.0e4):
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = W.channel_state(g, seed)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    c1 = smooth_mask(g, (math.pi, 0.0, math.pi / 2), 0.6, 1.5) if sphere else np.zeros(
+        (nx, ny, nz), order="F")
+    par = dict(dt=dt, Re=Re, Sc=Pr, eta=eta, force=3.0 / Re, source=0.0, tbot=1.0, ttop=0.0,
+               tsolid=1.0 if sphere else 0.0)
+    return g, f, c1, par
+
+
+def run_oracle(g, f, c1, par, nsteps):
+    s = O.Solver(oracle_grid(g), par["dt"], par["Re"], par["Sc"], par["eta"],
+                 force=par["force"], source=par["source"], tbot=par["tbot"], ttop=par["ttop"],
+                 tsolid=par["tsolid"])
+    for k in ("u", "v", "w", "T"):
+        s.f[k][...] = f[k]
+    s.cellvalue[..., 0] = c1
+    s.start()
+    s.step(nsteps)
+    return s
+
+
+def make_ctx(g, f, c1, par):
+    cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                   g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0, body_force=par["force"],
+                   heat_source=par["source"], t_bot=par["tbot"], t_top=par["ttop"],
+                   t_solid=par["tsolid"])
+    ctx = S.Context(cfg)
+    for k in ("u", "v", "w", "T"):
+        ctx.upload(k, f[k])
+    ctx.upload("cellvalue", c1)
+    ctx.start()
+    return ctx
+
+
+def test_context_grid_matches_oracle_grid():
+    g = W.grid_arrays(24, 16, 12, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    og = O.Grid(24, 16, 12, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    for k in ("dx", "dy", "dz", "dx12", "dy12", "dz12", "y", "y12"):
+        assert np.array_equal(g[k], getattr(og, k)), k
+
+
+@pytest.mark.parametrize("n,sphere,steps", [((16, 12, 8), True, 3), ((32, 24, 16), True, 10),
+                                            ((24, 16, 20), False, 10)])
+def test_steps_match_oracle(n, sphere, steps):
+    g, f, c1, par = make_case(*n, sphere=sphere)
+    ref = run_oracle(g, f, c1, par, steps)
+    with make_ctx(g, f, c1, par) as ctx:
+        ctx.step(steps)
+        assert ctx.step_index == steps + 1
+        scale = max(1.0, np.abs(ref.f["u"]).max() / g["dx"][1])
+        for k in STATE:
+            got = ctx.download(k)
+            if k == "divu":  # both are round-off (~1e-13): compare absolutely
+                assert np.abs(got - ref.f[k]).max() < 1e-11 * scale
+                continue
+            err = rel_l2(got, ref.f[k])
+            assert err < 1e-10, (k, err)
+        mon = ctx.monitor()
+        assert mon["nonfinite"] == 0
+        assert mon["max_divu"] < 1e-12 * max(1.0, np.abs(ref.f["u"]).max() / g["dx"][1])
+
+
+def test_step_bitexact_without_projection_effects():
+    """With a zero velocity field and no body force the projection sees a zero
+    right-hand side; the temperature then evolves through stencils and line
+    solves only, which round identically to the oracle."""
+    nx, ny, nz = 16, 12, 10
+    g, f, c1, par = make_case(nx, ny, nz, sphere=True)
+    par["force"] = 0.0
+    for k in ("u", "v", "w"):
+        f[k][...] = 0.0
+    ref = run_oracle(g, f, c1, par, 2)
+    with make_ctx(g, f, c1, par) as ctx:
+        ctx.step(2)
+        T = ctx.download("T")
+        assert np.array_equal(T, ref.f["T"])
+
+
+def test_poiseuille_known_answer():
+    """check_convergence (nse_dominik.f:2875-2891): with body force 1 and the
+    reference's uniform grid the laminar profile -Re/2 y(y-yl) is steady.  The
+    discrete steady state (ghost u0 = -u1) is reproduced to round-off and is
+    within O(dy^2) of the analytic profile."""
+    nx, ny, nz, Re, yl, dt = 4, 64, 8, 20.0, 4.0, 1.0e-3
+    g = W.grid_arrays(nx, ny, nz, 0.25, yl, 4.0)
+    y = g["y"][1:-1]
+    dy = yl / ny
+    # discrete steady state of D2 u = -Re (force 1) with u0 = -u1, u(ny+1) = -u(ny)
+    A = np.zeros((ny, ny))
+    for j in range(ny):
+        A[j, j] = -2.0
+        if j > 0:
+            A[j, j - 1] = 1.0
+        if j < ny - 1:
+            A[j, j + 1] = 1.0
+    A[0, 0] -= 1.0
+    A[-1, -1] -= 1.0
+    us = np.linalg.solve(A / dy ** 2, -Re * np.ones(ny))
+    u = W.padded(g)
+    u[1:-1, 1:-1, 1:-1] = us[None, :, None]
+    cfg = S.Config(nx, ny, nz, dt, Re, 1.0, 0.0, 0.25, yl, 4.0)
+    with S.Context(cfg) as ctx:
+        ctx.upload("u", u)
+        ctx.start()
+        ctx.step(20)
+        got = ctx.download("u")[1:-1, 1:-1, 1:-1]
+        v = ctx.download("v")[1:-1, 1:-1, 1:-1]
+    assert np.abs(got - us[None, :, None]).max() < 1e-9 * us.max()
+    assert np.abs(v).max() < 1e-10
+    analytic = -Re / 2 * y * (y - yl)
+    assert np.abs(us - analytic).max() < Re * dy ** 2
+
+
+def laplacian(g, P):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    i, j, k = slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1)
+    dx, dy, dz = g["dx"], g["dy"], g["dz"]
+    dx12, dy12, dz12 = g["dx12"], g["dy12"], g["dz12"]
+    X = ((P[2:nx + 2, j, k] - P[i, j, k]) / dx12[1:nx + 1, None, None] -
+         (P[i, j, k] - P[0:nx, j, k]) / dx12[0:nx, None, None]) / dx[1:nx + 1, None, None]
+    Y = ((P[i, 2:ny + 2, k] - P[i, j, k]) / dy12[None, 1:ny + 1, None] -
+         (P[i, j, k] - P[i, 0:ny, k]) / dy12[None, 0:ny, None]) / dy[None, 1:ny + 1, None]
+    Z = ((P[i, j, 2:nz + 2] - P[i, j, k]) / dz12[None, None, 1:nz + 1] -
+         (P[i, j, k] - P[i, j, 0:nz]) / dz12[None, None, 0:nz]) / dz[None, None, 1:nz + 1]
+    return X + Y + Z
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (256, 192, 256)])
+def test_poisson_manufactured(n):
+    """P2S -> SPN -> SP0B -> S2P inverts the reference's 7-point operator
+    (solve_p stencil nse_dominik.f:1988-1993 with PHIBC ghosts): a random phi
+    with the SP0B gauge (plane mean at j=1 is zero) is recovered to 1e-12."""
+    nx, ny, nz = n
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    rng = np.random.default_rng(5)
+    phi = W.padded(g)
+    phi[1:-1, 1:-1, 1:-1] = rng.standard_normal((nx, ny, nz))
+    phi[1:-1, 1:-1, 1:-1] -= phi[1:-1, 1, 1:-1].mean()
+    O.phibc(nx, ny, nz, phi)
+    rhs = W.padded(g)
+    rhs[1:-1, 1:-1, 1:-1] = laplacian(g, phi)
+    rhs[1:nx + 1, 1:ny + 1, 0] = rhs[1:nx + 1, 1:ny + 1, nz]
+    rhs[0, 1:ny + 1, 1:nz + 1] = rhs[nx, 1:ny + 1, 1:nz + 1]
+    rhs[0, 1:ny + 1, 0] = rhs[nx, 1:ny + 1, nz]
+    cfg = S.Config(nx, ny, nz, 1.0, 1.0, 1.0, 0.0, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                   ystretch=2.0)
+    with S.Context(cfg) as ctx:
+        ctx.upload("phi", rhs)
+        ctx.poisson()
+        sol = ctx.download("phi")
+    I = (slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1))
+    assert rel_l2(sol[I], phi[I]) < 1e-12
+
+
+def test_full_size_step_properties():
+    """The benchmark workload at 256x192x256 (sphere, heat): one step keeps
+    every field finite and the projected velocity divergence-free."""
+    nx, ny, nz = 256, 192, 256
+    g, f, c1, par = make_case(nx, ny, nz, sphere=True)
+    with make_ctx(g, f, c1, par) as ctx:
+        ctx.step(2)
+        mon = ctx.monitor()
+    assert mon["nonfinite"] == 0
+    assert mon["max_divu"] < 1e-10

@@ -1,0 +1,1354 @@
+// runtime.cu -- host side of libnsegpu.so: error state, device work arena,
+// the reference-named legacy entry points (host arrays in, host arrays out)
+// and the resident context API (fields kept in HBM across steps).
+#include <ctype.h>
+#include <math.h>
+#include <stdarg.h>
+#include <stdlib.h>
+#include <string.h>
+
+#include <algorithm>
+#include <atomic>
+#include <string>
+#include <vector>
+
+#include "common.cuh"
+
+namespace nse {
+
+bool fft_size_ok(int n);  // k_fft.cu
+
+// ------------------------------------------------------------------ errors --
+static thread_local int g_status = NSE_OK;
+static thread_local char g_msg[512] = "";
+
+void set_error(int status, const char* fmt, ...) {
+  va_list ap;
+  va_start(ap, fmt);
+  vsnprintf(g_msg, sizeof(g_msg), fmt, ap);
+  va_end(ap);
+  g_status = status;
+  fprintf(stderr, "nsegpu: %s\n", g_msg);
+}
+
+bool cuda_ok(cudaError_t e, const char* what) {
+  if (e == cudaSuccess) return true;
+  set_error(e == cudaErrorMemoryAllocation ? NSE_ERR_NOMEM : NSE_ERR_CUDA, "%s: %s", what,
+            cudaGetErrorString(e));
+  return false;
+}
+
+bool DBuf::ensure(size_t n) {
+  if (n <= bytes && p) return true;
+  release();
+  if (n == 0) n = 16;
+  if (!NSE_CUDA(cudaMalloc(&p, n))) {
+    p = nullptr;
+    bytes = 0;
+    return false;
+  }
+  bytes = n;
+  return true;
+}
+void DBuf::release() {
+  if (p) cudaFree(p);
+  p = nullptr;
+  bytes = 0;
+}
+
+bool ensure_device() {
+  static int checked = 0;
+  static bool ok = false;
+  if (checked) {
+    if (!ok) set_error(NSE_ERR_CUDA, "no usable CUDA device (sm_100 required)");
+    return ok;
+  }
+  checked = 1;
+  int n = 0;
+  cudaError_t e = cudaGetDeviceCount(&n);
+  if (e != cudaSuccess || n == 0) {
+    set_error(NSE_ERR_CUDA, "no CUDA device available: %s", cudaGetErrorString(e));
+    ok = false;
+    return false;
+  }
+  int dev = 0, major = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&major, cudaDevAttrComputeCapabilityMajor, dev);
+  if (major != 10) {
+    set_error(NSE_ERR_CUDA, "device %d has compute capability %d.x; this library is built "
+              "for sm_100a only", dev, major);
+    ok = false;
+    return false;
+  }
+  ok = true;
+  return true;
+}
+
+static std::atomic<long long> g_launches{0};
+void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+
+DBuf& arena(int slot) {
+  static DBuf slots[48];
+  return slots[slot];
+}
+
+cudaStream_t legacy_stream() {
+  static cudaStream_t s = nullptr;
+  if (!s) cudaStreamCreateWithFlags(&s, cudaStreamNonBlocking);
+  return s;
+}
+
+static bool copy_box(double* dst, const double* src, const Dims& d, int i0, int i1, int j0,
+                     int j1, int k0, int k1, cudaMemcpyKind kind, cudaStream_t s) {
+  if (i0 == 0 && j0 == 0 && k0 == 0 && i1 == d.nx + 1 && j1 == d.ny + 1 && k1 == d.nz + 1)
+    return NSE_CUDA(cudaMemcpyAsync(dst, src, d.ntot * sizeof(double), kind, s));
+  cudaMemcpy3DParms p;
+  memset(&p, 0, sizeof(p));
+  size_t pitch = (size_t)(d.nx + 2) * sizeof(double);
+  p.srcPtr = make_cudaPitchedPtr((void*)src, pitch, d.nx + 2, d.ny + 2);
+  p.dstPtr = make_cudaPitchedPtr((void*)dst, pitch, d.nx + 2, d.ny + 2);
+  p.srcPos = make_cudaPos((size_t)i0 * sizeof(double), j0, k0);
+  p.dstPos = p.srcPos;
+  p.extent = make_cudaExtent((size_t)(i1 - i0 + 1) * sizeof(double), j1 - j0 + 1, k1 - k0 + 1);
+  p.kind = kind;
+  return NSE_CUDA(cudaMemcpy3DAsync(&p, s));
+}
+bool copy_box_d2h(double* host, const double* dev, const Dims& d, int i0, int i1, int j0,
+                  int j1, int k0, int k1, cudaStream_t s) {
+  return copy_box(host, dev, d, i0, i1, j0, j1, k0, k1, cudaMemcpyDeviceToHost, s);
+}
+bool copy_box_h2d(double* dev, const double* host, const Dims& d, int i0, int i1, int j0,
+                  int j1, int k0, int k1, cudaStream_t s) {
+  return copy_box(dev, host, d, i0, i1, j0, j1, k0, k1, cudaMemcpyHostToDevice, s);
+}
+
+// -------------------------------------------------------- legacy helpers --
+// A legacy call stages its arrays in arena slots; `Stage` hands them out.
+struct Stage {
+  int next = 0;
+  cudaStream_t s = legacy_stream();
+  bool ok = true;
+  double* alloc(size_t n) {
+    if (!ok) return nullptr;
+    DBuf& b = arena(next++);
+    if (!b.ensure(n * sizeof(double))) { ok = false; return nullptr; }
+    return b.as<double>();
+  }
+  double* up(const double* h, size_t n) {
+    double* d = alloc(n);
+    if (d && !NSE_CUDA(cudaMemcpyAsync(d, h, n * sizeof(double), cudaMemcpyHostToDevice, s)))
+      ok = false;
+    return ok ? d : nullptr;
+  }
+  bool down(double* h, const double* d, size_t n) {
+    if (!ok) return false;
+    if (!NSE_CUDA(cudaMemcpyAsync(h, d, n * sizeof(double), cudaMemcpyDeviceToHost, s)))
+      ok = false;
+    return ok;
+  }
+  bool finish() {
+    if (!ok) return false;
+    if (!NSE_CUDA(cudaGetLastError())) return false;
+    return NSE_CUDA(cudaStreamSynchronize(s));
+  }
+};
+
+static bool dims_ok(int nx, int ny, int nz, const char* who) {
+  if (nx < 1 || ny < 1 || nz < 1) {
+    set_error(NSE_ERR_ARG, "%s: bad dimensions nx=%d ny=%d nz=%d", who, nx, ny, nz);
+    return false;
+  }
+  return true;
+}
+
+}  // namespace nse
+
+using namespace nse;
+
+// =========================================================== C-ABI =========
+extern "C" {
+
+const char* nse_last_error(void) { return g_msg; }
+long long nse_launch_count(void) { return g_launches.load(); }
+int nse_last_status(void) { return g_status; }
+void nse_clear_error(void) {
+  g_status = NSE_OK;
+  g_msg[0] = 0;
+}
+
+// ------------------------------------------------------------ tridiag.f ----
+void tridiag_(double* A, double* B, const int* NN) {
+  if (!ensure_device()) return;
+  int n = *NN;
+  if (n < 1) { set_error(NSE_ERR_ARG, "tridiag: NN=%d", n); return; }
+  Stage st;
+  double* dA = st.up(A, 3 * (size_t)n);
+  double* dB = st.up(B, n);
+  if (!st.ok) return;
+  launch_tridiag(dA, dB, n, 1, st.s);
+  st.down(A, dA, 3 * (size_t)n);
+  st.down(B, dB, n);
+  st.finish();
+}
+
+void ctridiag_(double* A, double* B, const int* NN) {
+  if (!ensure_device()) return;
+  int n = *NN;
+  if (n < 1) { set_error(NSE_ERR_ARG, "ctridiag: NN=%d", n); return; }
+  Stage st;
+  double* dA = st.up(A, 3 * (size_t)n);
+  double* dB = st.up(B, 2 * (size_t)n);
+  if (!st.ok) return;
+  launch_tridiag(dA, dB, n, 2, st.s);
+  st.down(A, dA, 3 * (size_t)n);
+  st.down(B, dB, 2 * (size_t)n);
+  st.finish();
+}
+
+void trid2_(double* A, double* B, const int* M, const int* N) {
+  if (!ensure_device()) return;
+  int m = *M, n = *N;
+  if (m < 1 || n < 1) { set_error(NSE_ERR_ARG, "trid2: M=%d N=%d", m, n); return; }
+  Stage st;
+  double* dA = st.up(A, 3 * (size_t)n);
+  double* dAm = st.up(A, 3 * (size_t)n);
+  double* dB = st.up(B, (size_t)m * n);
+  if (!st.ok) return;
+  launch_trid2(dA, dAm, dB, m, n, st.s);
+  st.down(A, dAm, 3 * (size_t)n);
+  st.down(B, dB, (size_t)m * n);
+  st.finish();
+}
+
+// -------------------------------------------------- periodic_implicit.f ----
+void tdma_(const double* a, const double* b, const double* c, const double* r, double* u,
+           const int* n) {
+  if (!ensure_device()) return;
+  int m = *n;
+  if (m < 0) { set_error(NSE_ERR_ARG, "tdma: n=%d", m); return; }
+  size_t L = m + 2;
+  Stage st;
+  double *da = st.up(a, L), *db = st.up(b, L), *dc = st.up(c, L), *dr = st.up(r, L);
+  double *du = st.alloc(L), *dg = st.alloc(L);
+  if (!st.ok) return;
+  launch_tdma(da, db, dc, dr, du, dg, m, st.s);
+  st.down(u, du, L);
+  st.finish();
+}
+
+void cyclic_(const double* a, const double* b, const double* c, const double* alpha,
+             const double* beta, const double* r, double* x, const int* n) {
+  if (!ensure_device()) return;
+  int m = *n;
+  if (m < 0) { set_error(NSE_ERR_ARG, "cyclic: n=%d", m); return; }
+  size_t L = m + 2;
+  Stage st;
+  double *da = st.up(a, L), *db = st.up(b, L), *dc = st.up(c, L), *dr = st.up(r, L);
+  double *dx = st.alloc(L), *dbb = st.alloc(L), *dg = st.alloc(L), *dz = st.alloc(L);
+  if (!st.ok) return;
+  launch_cyclic_general(da, db, dc, *alpha, *beta, dr, dx, dbb, dg, dz, m, st.s);
+  st.down(x, dx, L);
+  st.finish();
+}
+
+// SUX is written on 0..nx+1 (cyclic writes x(0:n+1) although implicit_solver
+// declares SUX(0:nx); every caller of the reference passes an (0:n+1) array)
+void implicit_solver_(double* SUX, const int* nx, const double* dx, const double* dx12,
+                      const double* Re, const double* dt, const double* ft,
+                      const double* fb, const double* eta, const double* CUX) {
+  if (!ensure_device()) return;
+  int n = *nx;
+  if (n < 1) { set_error(NSE_ERR_ARG, "implicit_solver: nx=%d", n); return; }
+  size_t L = n + 2;
+  Stage st;
+  double* f = st.up(SUX, L);
+  double *ddx = st.up(dx, L), *ddx12 = st.up(dx12, L), *dcu = st.up(CUX, n);
+  double *g1 = st.alloc(L), *g2 = st.alloc(L);
+  if (!st.ok) return;
+  GridDev g{ddx, ddx, ddx, ddx12, ddx12, ddx12};
+  launch_single_cyc(f, g1, g2, 0, n, g, *Re, 1.0, *dt, *eta, *ft, *fb, dcu, nullptr, nullptr,
+                    st.s);
+  st.down(SUX, f, L);
+  st.finish();
+}
+
+// ----------------------------------------------- single y / T line solvers --
+void implicit_uy_(double* SUY, const int* ny, const double* dy, const double* dy12,
+                  const double* Re, const double* dt, const double* ft, const double* fb,
+                  const double* eta, const double* CUY) {
+  if (!ensure_device()) return;
+  int n = *ny;
+  if (n < 1) { set_error(NSE_ERR_ARG, "implicit_uy: ny=%d", n); return; }
+  size_t L = n + 2;
+  Stage st;
+  double* f = st.up(SUY, L);
+  double *ddy = st.up(dy, L), *ddy12 = st.up(dy12, L), *dcu = st.up(CUY, n);
+  double* lsc = st.alloc(L);
+  if (!st.ok) return;
+  GridDev g{ddy, ddy, ddy, ddy12, ddy12, ddy12};
+  launch_single_ul(f, lsc, 0, n, g, *Re, 1.0, *dt, *eta, *ft, *fb, dcu, nullptr, nullptr,
+                   st.s);
+  st.down(SUY, f, L);
+  st.finish();
+}
+
+// SVY is written on 0..ny (nse_dominik.f:1643-1645)
+void implicit_vy_(double* SVY, const int* ny, const double* dy, const double* dy12,
+                  const double* Re, const double* dt, const double* ft, const double* fb,
+                  const double* eta, const double* CVY) {
+  if (!ensure_device()) return;
+  int n = *ny;
+  if (n < 2) { set_error(NSE_ERR_ARG, "implicit_vy: ny=%d", n); return; }
+  size_t L = n + 2;
+  Stage st;
+  double* f = st.up(SVY, L);
+  double *ddy = st.up(dy, L), *ddy12 = st.up(dy12, L), *dcu = st.up(CVY, n);
+  double* lsc = st.alloc(L);
+  if (!st.ok) return;
+  GridDev g{ddy, ddy, ddy, ddy12, ddy12, ddy12};
+  launch_single_ul(f, lsc, 1, n, g, *Re, 1.0, *dt, *eta, *ft, *fb, dcu, nullptr, nullptr,
+                   st.s);
+  st.down(SVY, f, n + 1);
+  st.finish();
+}
+
+// STY is written on 1..ny (nse_dominik.f:1866-1868); lly/rry/CUY are (0:ny+1)
+void implicit_ty_(double* STY, const int* ny, const double* dy, const double* dy12,
+                  const double* Re, const double* Sc, const double* dt, const double* lly,
+                  const double* rry, const double* ft, const double* fb, const double* CUY,
+                  const double* eta) {
+  if (!ensure_device()) return;
+  int n = *ny;
+  if (n < 1) { set_error(NSE_ERR_ARG, "implicit_ty: ny=%d", n); return; }
+  size_t L = n + 2;
+  Stage st;
+  double* f = st.up(STY, L);
+  double *ddy = st.up(dy, L), *ddy12 = st.up(dy12, L);
+  double *dcu = st.up(CUY, L), *dll = st.up(lly, L), *drr = st.up(rry, L);
+  double* lsc = st.alloc(L);
+  if (!st.ok) return;
+  GridDev g{ddy, ddy, ddy, ddy12, ddy12, ddy12};
+  launch_single_ul(f, lsc, 2, n, g, *Re, *Sc, *dt, *eta, *ft, *fb, dcu, dll, drr, st.s);
+  st.down(STY + 1, f + 1, n);
+  st.finish();
+}
+
+// STX is written on 0..nx+1 by cyclic (nse_dominik.f:1779)
+void implicit_tx_(double* STX, const int* nx, const double* dx, const double* dx12,
+                  const double* Re, const double* Sc, const double* dt, const double* llx,
+                  const double* rrx, const double* ft, const double* fb, const double* eta,
+                  const double* CUX) {
+  if (!ensure_device()) return;
+  int n = *nx;
+  if (n < 1) { set_error(NSE_ERR_ARG, "implicit_tx: nx=%d", n); return; }
+  size_t L = n + 2;
+  Stage st;
+  double* f = st.up(STX, L);
+  double *ddx = st.up(dx, L), *ddx12 = st.up(dx12, L);
+  double *dcu = st.up(CUX, L), *dll = st.up(llx, L), *drr = st.up(rrx, L);
+  double *g1 = st.alloc(L), *g2 = st.alloc(L);
+  if (!st.ok) return;
+  GridDev g{ddx, ddx, ddx, ddx12, ddx12, ddx12};
+  launch_single_cyc(f, g1, g2, 1, n, g, *Re, *Sc, *dt, *eta, *ft, *fb, dcu, dll, drr, st.s);
+  st.down(STX, f, L);
+  st.finish();
+}
+
+// ------------------------------------------------------------- SET_C ------
+// grid setup (nse_dominik.f:553-607); O(n) host arithmetic, not a GPU path
+static void set_c_dir(int n, double L, double* X, double* X12, double* D, double* D12) {
+  for (int i = 0; i <= n + 1; ++i) {
+    X12[i] = L * (double)i / (double)n;
+    X[i] = L * ((double)i - 0.50) / (double)n;
+  }
+  for (int i = 0; i <= n; ++i) D12[i] = X[i + 1] - X[i];
+  D12[n + 1] = 2.0 * (X12[n + 1] - X[n + 1]);
+  for (int i = 1; i <= n + 1; ++i) D[i] = X12[i] - X12[i - 1];
+  D[0] = D[1];
+  D[n + 1] = D[n];
+}
+
+void set_c_(const int* nx, const int* ny, const int* nz, double* x, double* x12, double* y,
+            double* y12, double* z, double* z12, double* dx, double* dx12, double* dy,
+            double* dy12, double* dz, double* dz12, const double* xl, const double* yl,
+            const double* zl) {
+  set_c_dir(*nx, *xl, x, x12, dx, dx12);
+  set_c_dir(*ny, *yl, y, y12, dy, dy12);
+  set_c_dir(*nz, *zl, z, z12, dz, dz12);
+}
+
+// y faces y12(j) = y0 + yl/2 (1 + tanh(g(2j/ny-1))/tanh g) for j = 0..ny,
+// mirrored spacing in the ghost cells; x and z as SET_C
+void nse_set_c_stretched(int nx, int ny, int nz, double* x, double* x12, double* y,
+                         double* y12, double* z, double* z12, double* dx, double* dx12,
+                         double* dy, double* dy12, double* dz, double* dz12, double xl,
+                         double yl, double zl, double y0, double gamma) {
+  set_c_dir(nx, xl, x, x12, dx, dx12);
+  set_c_dir(nz, zl, z, z12, dz, dz12);
+  if (gamma == 0.0) {
+    set_c_dir(ny, yl, y, y12, dy, dy12);
+    for (int j = 0; j <= ny + 1; ++j) { y[j] += y0; y12[j] += y0; }
+    return;
+  }
+  double tg = tanh(gamma);
+  for (int j = 0; j <= ny; ++j)
+    y12[j] = y0 + 0.5 * yl * (1.0 + tanh(gamma * (2.0 * j / ny - 1.0)) / tg);
+  y12[ny + 1] = 2.0 * y12[ny] - y12[ny - 1];
+  for (int j = 1; j <= ny; ++j) y[j] = 0.5 * (y12[j - 1] + y12[j]);
+  y[0] = 2.0 * y12[0] - y[1];
+  y[ny + 1] = 2.0 * y12[ny] - y[ny];
+  for (int j = 0; j <= ny; ++j) dy12[j] = y[j + 1] - y[j];
+  dy12[ny + 1] = 2.0 * (y12[ny + 1] - y[ny + 1]);
+  for (int j = 1; j <= ny + 1; ++j) dy[j] = y12[j] - y12[j - 1];
+  dy[0] = dy[1];
+  dy[ny + 1] = dy[ny];
+}
+
+}  // extern "C"
+
+// grid arrays staged for one legacy call
+static bool stage_grid(Stage& st, int nx, int ny, int nz, const double* dx, const double* dy,
+                       const double* dz, const double* dx12, const double* dy12,
+                       const double* dz12, GridDev& g) {
+  g.dx = st.up(dx, nx + 2);
+  g.dy = st.up(dy, ny + 2);
+  g.dz = st.up(dz, nz + 2);
+  g.dx12 = dx12 ? st.up(dx12, nx + 2) : g.dx;
+  g.dy12 = dy12 ? st.up(dy12, ny + 2) : g.dy;
+  g.dz12 = dz12 ? st.up(dz12, nz + 2) : g.dz;
+  return st.ok;
+}
+
+extern "C" {
+
+// ----------------------------------------------------- tier-2 stencils ----
+void set_bc_(double* u, double* v, double* w, double* p, const int* nx, const int* ny,
+             const int* nz, double* T) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_bc")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  double *du = st.up(u, d.ntot), *dv = st.up(v, d.ntot), *dw = st.up(w, d.ntot);
+  double *dp = st.up(p, d.ntot), *dT = st.up(T, d.ntot);
+  if (!st.ok) return;
+  launch_set_bc(d, du, dv, dw, dp, dT, 0.0, 0.0, 31, st.s);
+  st.down(u, du, d.ntot); st.down(v, dv, d.ntot); st.down(w, dw, d.ntot);
+  st.down(p, dp, d.ntot); st.down(T, dT, d.ntot);
+  st.finish();
+}
+
+static bool down_interior(Stage& st, double* h, const double* dv, const Dims& d) {
+  if (!st.ok) return false;
+  if (!copy_box_d2h(h, dv, d, 1, d.nx, 1, d.ny, 1, d.nz, st.s)) st.ok = false;
+  return st.ok;
+}
+
+void set_convect_(double* u, double* u_v, double* v, double* v_v, double* w, double* w_v,
+                  const double* dt, const int* nx, const int* ny, const int* nz,
+                  const double* dx, const double* dy, const double* dz, const double* dx12,
+                  const double* dy12, const double* dz12) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_convect")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  double *du = st.up(u, d.ntot), *dv = st.up(v, d.ntot), *dw = st.up(w, d.ntot);
+  double *duv = st.alloc(d.ntot), *dvv = st.alloc(d.ntot), *dwv = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_convect(d, g, du, dv, dw, duv, dvv, dwv, *dt, 1.0, st.s);
+  down_interior(st, u_v, duv, d);
+  down_interior(st, v_v, dvv, d);
+  down_interior(st, w_v, dwv, d);
+  st.finish();
+}
+
+void set_convection_for_scalar_(double* u, double* v, double* w, const double* dt,
+                                const int* nx, const int* ny, const int* nz,
+                                const double* dx, const double* dy, const double* dz,
+                                const double* dx12, const double* dy12, const double* dz12,
+                                double* T, double* u_vT, double* rhoCp) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_convection_for_scalar")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  double *du = st.up(u, d.ntot), *dv = st.up(v, d.ntot), *dw = st.up(w, d.ntot);
+  double *dT = st.up(T, d.ntot), *dr = st.up(rhoCp, d.ntot), *dout = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_convect_scalar(d, g, du, dv, dw, dT, dr, dout, *dt, 1.0, st.s);
+  down_interior(st, u_vT, dout, d);
+  st.finish();
+}
+
+void set_conduction_(double* u, double* u_d, double* v, double* v_d, double* w, double* w_d,
+                     const double* Re, const double* dt, const int* nx, const int* ny,
+                     const int* nz, const double* dx, const double* dy, const double* dz,
+                     const double* dx12, const double* dy12, const double* dz12) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_conduction")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  double *du = st.up(u, d.ntot), *dv = st.up(v, d.ntot), *dw = st.up(w, d.ntot);
+  double *a = st.alloc(d.ntot), *b = st.alloc(d.ntot), *c = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_conduction(d, g, du, dv, dw, a, b, c, *Re, *dt, st.s);
+  down_interior(st, u_d, a, d);
+  down_interior(st, v_d, b, d);
+  down_interior(st, w_d, c, d);
+  st.finish();
+}
+
+void set_diffusion_for_scalar_(const double* Re, const double* dt, const int* nx,
+                               const int* ny, const int* nz, const double* dx,
+                               const double* dy, const double* dz, const double* dx12,
+                               const double* dy12, const double* dz12, double* T,
+                               double* u_dT, const double* Sc, double* thc, double* rhoCp) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_diffusion_for_scalar")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  double *dT = st.up(T, d.ntot), *dl = st.up(thc, d.ntot), *dr = st.up(rhoCp, d.ntot);
+  double* dout = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_diffusion_scalar(d, g, dT, dl, dr, dout, *Re, *Sc, *dt, st.s);
+  down_interior(st, u_dT, dout, d);
+  st.finish();
+}
+
+void set_immersed_boundary_(const double* eta, const int* nx, const int* ny, const int* nz,
+                            const double* dt, double* u_l, double* v_l, double* w_l,
+                            const double* dx, const double* dy, const double* dz,
+                            double* T_l, double* cellvalue, double* u_ta, double* v_ta,
+                            double* w_ta, const int* l, double* cons_cell) {
+  (void)dx; (void)dy; (void)dz;
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_immersed_boundary")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  double* dcv = st.up(cellvalue, 4 * (size_t)d.ncell);
+  double *a = st.up(u_ta, d.ntot), *b = st.up(v_ta, d.ntot), *c = st.up(w_ta, d.ntot);
+  double *ul = st.alloc(d.ntot), *vl = st.alloc(d.ntot), *wl = st.alloc(d.ntot);
+  double* tl = st.alloc(d.ntot);
+  if (!st.ok) return;
+  if (*l == 1) {
+    launch_build_face_masks(d, dcv, st.s);
+    st.down(cellvalue + d.ncell, dcv + d.ncell, 3 * (size_t)d.ncell);
+    *cons_cell = 0.0;
+  }
+  launch_ib_forcing(d, dcv, a, b, c, ul, vl, wl, tl, *eta, *dt, st.s);
+  down_interior(st, u_l, ul, d);
+  down_interior(st, v_l, vl, d);
+  down_interior(st, w_l, wl, d);
+  down_interior(st, T_l, tl, d);
+  st.finish();
+}
+
+void set_explicit_(double* u_v, double* u_pre, double* u_d, double* u_a, double* v_v,
+                   double* v_pre, double* v_d, double* v_a, double* w_v, double* w_pre,
+                   double* w_d, double* w_a, double* u_l, double* v_l, double* w_l,
+                   const int* nx, const int* ny, const int* nz, const int* l) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_explicit")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  size_t n = d.ntot;
+  double *uv = st.up(u_v, n), *up = st.up(u_pre, n), *ud = st.up(u_d, n), *ua = st.up(u_a, n);
+  double *vv = st.up(v_v, n), *vp = st.up(v_pre, n), *vd = st.up(v_d, n), *va = st.up(v_a, n);
+  double *wv = st.up(w_v, n), *wp = st.up(w_pre, n), *wd = st.up(w_d, n), *wa = st.up(w_a, n);
+  double *ul = st.up(u_l, n), *vl = st.up(v_l, n), *wl = st.up(w_l, n);
+  if (!st.ok) return;
+  launch_explicit(d, uv, up, ud, ua, vv, vp, vd, va, wv, wp, wd, wa, ul, vl, wl, *l, st.s);
+  st.down(u_a, ua, n); st.down(v_a, va, n); st.down(w_a, wa, n);
+  down_interior(st, u_pre, up, d);
+  down_interior(st, v_pre, vp, d);
+  down_interior(st, w_pre, wp, d);
+  st.finish();
+}
+
+void set_explicit_for_tempreture_(double* u_vT, double* u_dT, double* u_T, double* T_pre,
+                                  double* T_l, const int* nx, const int* ny, const int* nz,
+                                  const int* l) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_explicit_for_tempreture")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  size_t n = d.ntot;
+  double *vt = st.up(u_vT, n), *dtt = st.up(u_dT, n), *ut = st.up(u_T, n);
+  double *tp = st.up(T_pre, n), *tl = st.up(T_l, n);
+  if (!st.ok) return;
+  launch_explicit_T(d, vt, dtt, ut, tp, tl, *l, st.s);
+  st.down(u_T, ut, n);
+  down_interior(st, T_pre, tp, d);
+  st.finish();
+}
+
+void solve_u_temp_(double* u_a, double* v_a, double* w_a, const int* nx, const int* ny,
+                   const int* nz, const double* dx, const double* dy, const double* dz,
+                   const double* dx12, const double* dy12, const double* dz12,
+                   const double* Re, const double* dt, const double* eta,
+                   double* cellvalue, double* u, double* v, double* w) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "solve_u_temp")) return;
+  if (*ny < 2) { set_error(NSE_ERR_ARG, "solve_u_temp: ny=%d < 2", *ny); return; }
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  size_t n = d.ntot;
+  double *ua = st.up(u_a, n), *va = st.up(v_a, n), *wa = st.up(w_a, n);
+  double *du = st.up(u, n), *dv = st.up(v, n), *dw = st.up(w, n);
+  double* dcv = st.up(cellvalue, 4 * (size_t)d.ncell);
+  LineScratch sc{st.alloc(n), st.alloc(n)};
+  if (!st.ok) return;
+  double* fa[3] = {ua, va, wa};
+  double* fo[3] = {du, dv, dw};
+  for (int comp = 0; comp < 3; ++comp) {
+    const double* col = dcv + (size_t)(comp + 1) * d.ncell;
+    launch_penalize(d, fo[comp], fa[comp], col, *eta, *dt, 0.0, st.s);
+    launch_vel_line_col(d, g, fa[comp], col, 1, comp, *Re, *dt, *eta, sc, st.s);
+    launch_vel_line_col(d, g, fa[comp], col, 2, comp, *Re, *dt, *eta, sc, st.s);
+    launch_vel_line_col(d, g, fa[comp], col, 0, comp, *Re, *dt, *eta, sc, st.s);
+  }
+  st.down(u_a, ua, n); st.down(v_a, va, n); st.down(w_a, wa, n);
+  st.finish();
+}
+
+void solve_t_(double* u_T, const int* nx, const int* ny, const int* nz, const double* dx,
+              const double* dy, const double* dz, const double* dx12, const double* dy12,
+              const double* dz12, const double* Re, const double* Sc, const double* dt,
+              double* rhoCp, double* thc, double* cellvalue, const double* eta) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "solve_t")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  size_t n = d.ntot;
+  double *ut = st.up(u_T, n), *dr = st.up(rhoCp, n), *dl = st.up(thc, n);
+  double* dcv = st.up(cellvalue, d.ncell);
+  LineScratch sc{st.alloc(n), st.alloc(n)};
+  if (!st.ok) return;
+  launch_ysolve_T(d, g, ut, dcv, dr, dl, 1.0, 1.0, *Re, *Sc, *dt, *eta, 0.0, 0.0, sc, st.s);
+  launch_xsolve_T(d, g, ut, dcv, dr, dl, 1.0, 1.0, *Re, *Sc, *dt, *eta, sc, st.s);
+  launch_zsolve_T(d, g, ut, dcv, dr, dl, 1.0, 1.0, *Re, *Sc, *dt, *eta, sc, st.s);
+  down_interior(st, u_T, ut, d);
+  st.finish();
+}
+
+}  // extern "C"
+
+// ------------------------------------------------------ Poisson staging ----
+namespace nse {
+struct PoissonBufs {
+  DBuf spec, scr, AC, KXZ, twx, twz;
+  PoissonPlan pp;
+  bool build(int nx, int ny, int nz, const double* dx, const double* dy, const double* dz,
+             const double* dy12, double xl, double zl, cudaStream_t s) {
+    if (!fft_size_ok(nx) || !fft_size_ok(nz)) {
+      set_error(NSE_ERR_ARG, "FFT sizes nx=%d nz=%d must be products of 2, 3 and 5", nx, nz);
+      return false;
+    }
+    int H = nx / 2 + 1;
+    int Hp = (H + 7) / 8 * 8;
+    std::vector<double> AC(3 * (size_t)ny), KXZ((size_t)H * (nz + 1)), twx(2 * (size_t)nx),
+        twz(2 * (size_t)nz);
+    poisson_plan_tables(nx, ny, nz, dx, dy, dz, dy12, xl, zl, AC.data(), KXZ.data(),
+                        twx.data(), twz.data());
+    size_t nspec = (size_t)Hp * ny * nz;
+    if (!spec.ensure(2 * nspec * sizeof(double)) || !scr.ensure(nspec * sizeof(double)) ||
+        !this->AC.ensure(AC.size() * 8) || !this->KXZ.ensure(KXZ.size() * 8) ||
+        !this->twx.ensure(twx.size() * 8) || !this->twz.ensure(twz.size() * 8))
+      return false;
+    if (!NSE_CUDA(cudaMemcpyAsync(this->AC.p, AC.data(), AC.size() * 8, cudaMemcpyHostToDevice, s)) ||
+        !NSE_CUDA(cudaMemcpyAsync(this->KXZ.p, KXZ.data(), KXZ.size() * 8, cudaMemcpyHostToDevice, s)) ||
+        !NSE_CUDA(cudaMemcpyAsync(this->twx.p, twx.data(), twx.size() * 8, cudaMemcpyHostToDevice, s)) ||
+        !NSE_CUDA(cudaMemcpyAsync(this->twz.p, twz.data(), twz.size() * 8, cudaMemcpyHostToDevice, s)))
+      return false;
+    // the host vectors die here: wait for the copies
+    if (!NSE_CUDA(cudaStreamSynchronize(s))) return false;
+    pp.nx = nx; pp.ny = ny; pp.nz = nz; pp.H = H; pp.Hp = Hp;
+    pp.spec = spec.as<double>(); pp.scr = scr.as<double>();
+    pp.AC = this->AC.as<double>(); pp.KXZ = this->KXZ.as<double>();
+    pp.twx = this->twx.as<double>(); pp.twz = this->twz.as<double>();
+    return true;
+  }
+  void release() {
+    spec.release(); scr.release(); AC.release(); KXZ.release(); twx.release(); twz.release();
+  }
+};
+static PoissonBufs& legacy_poisson() {
+  static PoissonBufs pb;
+  return pb;
+}
+// reference-layout PHIT for legacy spn_/sp0b_ calls: plane-major with ghosts
+// is converted to the internal spectrum and back
+}  // namespace nse
+
+// single-thread SP0B on the reference PHIT layout (mkp.f:263-290), including
+// the ghost entries PHIT(0,0,0) = 0 and PHIT(0,NY+1,0) = PHIT(0,NY,0)
+__global__ void k_sp0b_phit(double2* col, long sj, int ny, const double* AC) {
+  if (blockIdx.x || threadIdx.x) return;
+  double2 Dn = col[sj * 1];
+  col[0] = make_double2(0.0, 0.0);
+  col[sj] = make_double2(0.0, 0.0);
+  double2 pm = make_double2(0.0, 0.0), pc = pm;
+  for (int J = 1; J <= ny - 1; ++J) {
+    double2 Dj = Dn;
+    Dn = col[sj * (J + 1)];
+    double a1 = AC[J - 1], a2 = AC[J - 1 + ny], a3 = AC[J - 1 + 2 * ny];
+    double2 pn = make_double2((Dj.x - a1 * pm.x - a2 * pc.x) / a3,
+                              (Dj.y - a1 * pm.y - a2 * pc.y) / a3);
+    col[sj * (J + 1)] = pn;
+    pm = pc;
+    pc = pn;
+  }
+  col[sj * (ny + 1)] = col[sj * ny];
+}
+
+extern "C" {
+
+// ------------------------------------------------------------ p2s / s2p ----
+void p2s_(double* FP, double* FPT, const int* NX, const int* NY, const int* NZ) {
+  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "p2s")) return;
+  int nx = *NX, ny = *NY, nz = *NZ;
+  Dims d = make_dims(nx, ny, nz);
+  Stage st;
+  std::vector<double> unit(std::max(nx, std::max(ny, nz)) + 2, 1.0);
+  PoissonBufs& pb = legacy_poisson();
+  if (!pb.build(nx, ny, nz, unit.data(), unit.data(), unit.data(), unit.data(), 1.0, 1.0, st.s))
+    return;
+  double* dfp = st.up(FP, d.ntot);
+  int H = nx / 2 + 1;
+  size_t nphit = 2 * (size_t)H * (ny + 2) * (nz + 2);
+  double* dphit = st.alloc(nphit);
+  if (!st.ok) return;
+  GridDev g{};
+  launch_fft_fwd_x(pb.pp, d, dfp, nullptr, nullptr, nullptr, g, 1.0, 0, st.s);
+  launch_fft_z(pb.pp, false, st.s);
+  launch_spec_to_phit(pb.pp, dphit, st.s);
+  // written entries: J = 1..NY, K = 0..NZ-1, all kx
+  size_t row = (size_t)H * 2 * sizeof(double);
+  NSE_CUDA(cudaMemcpy2DAsync(FPT + 2 * (size_t)H, row * (ny + 2), dphit + 2 * (size_t)H,
+                             row * (ny + 2), row * ny, nz, cudaMemcpyDeviceToHost, st.s));
+  st.finish();
+}
+
+void s2p_(double* FPT, double* FP, const int* NX, const int* NY, const int* NZ) {
+  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "s2p")) return;
+  int nx = *NX, ny = *NY, nz = *NZ;
+  Dims d = make_dims(nx, ny, nz);
+  Stage st;
+  std::vector<double> unit(std::max(nx, std::max(ny, nz)) + 2, 1.0);
+  PoissonBufs& pb = legacy_poisson();
+  if (!pb.build(nx, ny, nz, unit.data(), unit.data(), unit.data(), unit.data(), 1.0, 1.0, st.s))
+    return;
+  int H = nx / 2 + 1;
+  size_t nphit = 2 * (size_t)H * (ny + 2) * (nz + 2);
+  double* dphit = st.up(FPT, nphit);
+  double* dfp = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_phit_to_spec(pb.pp, dphit, st.s);
+  launch_fft_z(pb.pp, true, st.s);
+  launch_fft_inv_x(pb.pp, d, dfp, st.s);
+  // written entries: FP(0:NX, J, 0:NZ) for J = 1..NY
+  copy_box_d2h(FP, dfp, d, 0, nx, 1, ny, 0, nz, st.s);
+  st.finish();
+}
+
+// --------------------------------------------------- SPN / SP0B / PHIBC ----
+void spn_(const int* NX, const int* NY, const int* NZ, const double* AC, const double* KXZ,
+          double* PHIT) {
+  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "spn")) return;
+  int nx = *NX, ny = *NY, nz = *NZ;
+  Stage st;
+  int H = nx / 2 + 1;
+  int Hp = (H + 7) / 8 * 8;
+  size_t nphit = 2 * (size_t)H * (ny + 2) * (nz + 2);
+  double* dphit = st.up(PHIT, nphit);
+  double* dAC = st.up(AC, 3 * (size_t)ny);
+  double* dK = st.up(KXZ, (size_t)H * (nz + 1));
+  double* spec = st.alloc(2 * (size_t)Hp * ny * nz);
+  double* scr = st.alloc((size_t)Hp * ny * nz);
+  if (!st.ok) return;
+  PoissonPlan pp{};
+  pp.nx = nx; pp.ny = ny; pp.nz = nz; pp.H = H; pp.Hp = Hp;
+  pp.spec = spec; pp.scr = scr; pp.AC = dAC; pp.KXZ = dK;
+  launch_phit_to_spec(pp, dphit, st.s);
+  launch_spn(pp, true, false, st.s);
+  launch_spec_to_phit(pp, dphit, st.s);
+  size_t row = (size_t)H * 2 * sizeof(double);
+  NSE_CUDA(cudaMemcpy2DAsync(PHIT + 2 * (size_t)H, row * (ny + 2), dphit + 2 * (size_t)H,
+                             row * (ny + 2), row * ny, nz, cudaMemcpyDeviceToHost, st.s));
+  st.finish();
+}
+
+void sp0b_(const int* NX, const int* NY, const int* NZ, const double* AC, double* PHIT) {
+  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "sp0b")) return;
+  int nx = *NX, ny = *NY;
+  Stage st;
+  int H = nx / 2 + 1;
+  // the column PHIT(0, 0:NY+1, 0) (stride H complex)
+  double* col = st.alloc(2 * (size_t)H * (ny + 2));
+  double* dAC = st.up(AC, 3 * (size_t)ny);
+  if (!st.ok) return;
+  size_t row = (size_t)H * 2 * sizeof(double);
+  NSE_CUDA(cudaMemcpy2DAsync(col, row, PHIT, row, 2 * sizeof(double), ny + 2,
+                             cudaMemcpyHostToDevice, st.s));
+  count_launch();
+  k_sp0b_phit<<<1, 32, 0, st.s>>>(reinterpret_cast<double2*>(col), H, ny, dAC);
+  NSE_CUDA(cudaMemcpy2DAsync(PHIT, row, col, row, 2 * sizeof(double), ny + 2,
+                             cudaMemcpyDeviceToHost, st.s));
+  st.finish();
+}
+
+void phibc_(const int* NX, const int* NY, const int* NZ, double* PHI) {
+  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "phibc")) return;
+  Dims d = make_dims(*NX, *NY, *NZ);
+  Stage st;
+  double* dphi = st.up(PHI, d.ntot);
+  if (!st.ok) return;
+  launch_phibc(d, dphi, st.s);
+  st.down(PHI, dphi, d.ntot);
+  st.finish();
+}
+
+// ------------------------------------------------------------------ MKP ----
+void mkp_(double* p, double* u_temp, double* v_temp, double* w_temp, const double* dt,
+          const double* dx, const double* dy, const double* dz, const double* dx12,
+          const double* dy12, const double* dz12, const double* Re, const int* nx,
+          const int* ny, const int* nz, const void* ompnthreads, double* u_ta, double* v_ta,
+          double* w_ta, double* u_ep2, double* v_ep2, double* w_ep2, double* divu,
+          double* u, double* v, double* w, const double* xl, const double* zl) {
+  (void)Re; (void)ompnthreads;
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "mkp")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  PoissonBufs& pb = legacy_poisson();
+  if (!pb.build(d.nx, d.ny, d.nz, dx, dy, dz, dy12, *xl, *zl, st.s)) return;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  size_t n = d.ntot;
+  double *ut = st.up(u_temp, n), *vt = st.up(v_temp, n), *wt = st.up(w_temp, n);
+  double *dp = st.up(p, n), *a = st.up(u_ta, n), *b = st.up(v_ta, n), *c = st.up(w_ta, n);
+  double *du = st.alloc(n), *dv = st.alloc(n), *dw = st.alloc(n);
+  double *e1 = st.alloc(n), *e2 = st.alloc(n), *e3 = st.alloc(n), *dd = st.alloc(n);
+  double* phi = st.alloc(n);
+  if (!st.ok) return;
+  NSE_CUDA(cudaMemsetAsync(phi, 0, n * sizeof(double), st.s));
+  launch_fft_fwd_x(pb.pp, d, nullptr, ut, vt, wt, g, *dt, 1, st.s);
+  launch_fft_z(pb.pp, false, st.s);
+  launch_spn(pb.pp, true, true, st.s);
+  launch_fft_z(pb.pp, true, st.s);
+  launch_fft_inv_x(pb.pp, d, phi, st.s);
+  launch_phibc(d, phi, st.s);
+  launch_correct(d, g, phi, ut, vt, wt, dp, du, dv, dw, a, b, c, e1, e2, e3, dd, *dt, st.s);
+  int X = d.nx, Y = d.ny, Z = d.nz;
+  copy_box_d2h(u, du, d, 0, X, 0, Y, 0, Z, st.s);
+  copy_box_d2h(v, dv, d, 0, X, 0, Y, 0, Z, st.s);
+  copy_box_d2h(w, dw, d, 0, X, 0, Y, 0, Z, st.s);
+  copy_box_d2h(u_ta, a, d, 0, X, 0, Y, 0, Z, st.s);
+  copy_box_d2h(v_ta, b, d, 0, X, 0, Y, 0, Z, st.s);
+  copy_box_d2h(w_ta, c, d, 0, X, 0, Y, 0, Z, st.s);
+  down_interior(st, p, dp, d);
+  down_interior(st, u_ep2, e1, d);
+  down_interior(st, v_ep2, e2, d);
+  down_interior(st, w_ep2, e3, d);
+  down_interior(st, divu, dd, d);
+  st.finish();
+}
+
+// ---------------------------------------------------------- set_levelset ----
+// Fortran Ew.d edit descriptor (w = 15, d = 7): [-]0.ddddddd E+ee, right-justified
+static void fortran_e15_7(char* out, double v) {
+  char m[32];
+  if (v == 0.0 || !isfinite(v)) {
+    if (v == 0.0) snprintf(m, sizeof(m), "0.0000000E+00");
+    else snprintf(m, sizeof(m), "%s", isnan(v) ? "NaN" : (v > 0 ? "Infinity" : "-Infinity"));
+    snprintf(out, 32, "%15s", m);
+    return;
+  }
+  char t[32];
+  snprintf(t, sizeof(t), "%.6E", fabs(v));  // d.ddddddE+xx, 7 significant digits
+  int e = atoi(t + 9) + 1;
+  char digits[8] = {t[0], t[2], t[3], t[4], t[5], t[6], t[7], 0};
+  snprintf(m, sizeof(m), "%s0.%sE%c%02d", v < 0 ? "-" : "", digits, e < 0 ? '-' : '+',
+           e < 0 ? -e : e);
+  snprintf(out, 32, "%15s", m);
+}
+
+// legacy ASCII VTK STRUCTURED_GRID file of set_levelset.f:131-156 / :171-198
+static void write_vtk(const char* path, const char* scalars, int nx, int ny, int nz,
+                      const double* x, const double* y, const double* z, const double* val,
+                      long si, long sj, long sk, long off) {
+  FILE* f = fopen(path, "w");
+  if (!f) { set_error(NSE_ERR_ARG, "cannot write %s", path); return; }
+  fprintf(f, "# vtk DataFile Version 3.8.1\n3D structure of vessel\nASCII \n"
+             "DATASET STRUCTURED_GRID\nDIMENSIONS %4d%4d%4d\nPOINTS %9d float\n",
+          nx, ny, nz, nx * ny * nz);
+  char a[32], b[32], c[32];
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        fortran_e15_7(a, x[i]); fortran_e15_7(b, y[j]); fortran_e15_7(c, z[k]);
+        fprintf(f, "%s%s%s\n", a, b, c);
+      }
+  fprintf(f, "POINT_DATA %9d\n%s\nLOOKUP_TABLE default\n", nx * ny * nz, scalars);
+  for (int k = 1; k <= nz; ++k)
+    for (int j = 1; j <= ny; ++j)
+      for (int i = 1; i <= nx; ++i) {
+        fortran_e15_7(a, val[off + i * si + j * sj + k * sk]);
+        fprintf(f, "%s\n", a);
+      }
+  fclose(f);
+}
+
+static bool run_levelset(const Dims& d, const GridDev& g, const double* dphi0, double* dphi,
+                         double* dtmp, double* dcv1, int nnn, double dtau, double width,
+                         cudaStream_t s) {
+  if (!NSE_CUDA(cudaMemcpyAsync(dphi, dphi0, d.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s)))
+    return false;
+  double* cur = dphi;
+  double* nxt = dtmp;
+  for (int it = 0; it <= nnn; ++it) {
+    launch_levelset_iter(d, g, dphi0, cur, nxt, dtau, s);
+    launch_levelset_bc(d, nxt, s);
+    double* t = cur; cur = nxt; nxt = t;
+  }
+  if (cur != dphi &&
+      !NSE_CUDA(cudaMemcpyAsync(dphi, cur, d.ntot * sizeof(double), cudaMemcpyDeviceToDevice, s)))
+    return false;
+  launch_levelset_mask(d, g, dphi, dcv1, width, s);
+  return NSE_CUDA(cudaGetLastError());
+}
+
+void set_levelset_(const int* nx, const int* ny, const int* nz, const double* dx,
+                   const double* dx12, const double* dy12, const double* dz12,
+                   const double* phi0, double* phi, const double* x, const double* y,
+                   const double* z, double* cellvalue) {
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_levelset")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  g.dx = st.up(dx, d.nx + 2);
+  g.dx12 = st.up(dx12, d.nx + 2);
+  g.dy12 = st.up(dy12, d.ny + 2);
+  g.dz12 = st.up(dz12, d.nz + 2);
+  g.dy = g.dy12;
+  g.dz = g.dz12;
+  double* d0 = st.up(phi0, d.ntot);
+  double *dphi = st.alloc(d.ntot), *dtmp = st.alloc(d.ntot), *dcv = st.alloc(d.ncell);
+  if (!st.ok) return;
+  if (!run_levelset(d, g, d0, dphi, dtmp, dcv, 2000, 1.0e-3, 1.0, st.s)) return;
+  st.down(phi, dphi, d.ntot);
+  st.down(cellvalue, dcv, d.ncell);
+  if (!st.finish()) return;
+  const char* novtk = getenv("NSEGPU_NO_VTK");
+  if (!(novtk && novtk[0] == '1')) {
+    write_vtk("levelset.vtk", "SCALARS phi float64", d.nx, d.ny, d.nz, x, y, z, phi, 1, d.sx,
+              d.sy, 0);
+    write_vtk("cellvalue1.vtk", "SCALARS PHI float", d.nx, d.ny, d.nz, x, y, z, cellvalue, 1,
+              d.nx, (long)d.nx * d.ny, -(1 + d.nx + (long)d.nx * d.ny));
+  }
+}
+
+// list-directed read of structure.dat (set_levelset.f:202-214): four numbers
+// per record (x y z phi0), i fastest; Fortran D exponents are accepted
+void readgrid3d_(const int* nx, const int* ny, const int* nz, double* phi0) {
+  Dims d = make_dims(*nx, *ny, *nz);
+  FILE* f = fopen("structure.dat", "r");
+  if (!f) { set_error(NSE_ERR_ARG, "readgrid3d: cannot open structure.dat"); return; }
+  char tok[128];
+  auto next = [&](double& v) -> bool {
+    if (fscanf(f, " %127[^ \t\r\n,]", tok) != 1) return false;
+    for (char* c = tok; *c; ++c)
+      if (*c == 'd' || *c == 'D') *c = 'e';
+    v = strtod(tok, nullptr);
+    int ch = fgetc(f);
+    if (ch != ',' && ch != EOF) ungetc(ch, f);
+    return true;
+  };
+  for (int k = 1; k <= d.nz; ++k)
+    for (int j = 1; j <= d.ny; ++j)
+      for (int i = 1; i <= d.nx; ++i) {
+        double a, b, c, v;
+        if (!next(a) || !next(b) || !next(c) || !next(v)) {
+          fclose(f);
+          set_error(NSE_ERR_ARG, "readgrid3d: structure.dat ended at cell %d %d %d", i, j, k);
+          return;
+        }
+        phi0[d.P(i, j, k)] = v;
+      }
+  fclose(f);
+}
+
+}  // extern "C"
+
+// ============================================================ tier 3 =======
+struct nse_ctx {
+  nse_config cfg;
+  Dims d;
+  int l;
+  cudaStream_t own, stream;
+  std::vector<double> hx, hx12, hy, hy12, hz, hz12, hdx, hdx12, hdy, hdy12, hdz, hdz12;
+  DBuf grid;
+  GridDev g;
+  DBuf f[NSE_NUM_FIELDS];
+  DBuf ua, va, wa, uT, sa, sb, tmp, mon;
+  PoissonBufs pb;
+  // per-phase CUDA events of profiled steps: ev[step][phase boundary]
+  std::vector<cudaEvent_t> ev;
+  int prof_cap = 0, prof_n = 0;
+};
+
+// phases of one step, in launch order
+enum {
+  PH_BC = 0, PH_RHS, PH_YVEL, PH_ZVEL, PH_XVEL, PH_YT, PH_XT, PH_ZT, PH_BC2, PH_FFTX_F,
+  PH_FFTZ_F, PH_SPN, PH_FFTZ_I, PH_FFTX_I, PH_PHIBC, PH_CORRECT, PH_COUNT
+};
+
+static void mark(nse_ctx* x, int phase) {
+  if (x->prof_n >= x->prof_cap) return;
+  cudaEventRecord(x->ev[(size_t)x->prof_n * (PH_COUNT + 1) + phase], x->stream);
+}
+
+static double* F(nse_ctx* c, int id) { return c->f[id].as<double>(); }
+
+static int status_or(int fallback) { return g_status != NSE_OK ? g_status : fallback; }
+
+extern "C" {
+
+int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
+  nse_clear_error();
+  if (!cfg || !out) { set_error(NSE_ERR_ARG, "nse_ctx_create: null argument"); return NSE_ERR_ARG; }
+  *out = nullptr;
+  if (!ensure_device()) return NSE_ERR_CUDA;
+  const nse_config& c = *cfg;
+  if (c.nx < 2 || c.ny < 3 || c.nz < 2) {
+    set_error(NSE_ERR_ARG, "nse_ctx_create: need nx>=2, ny>=3, nz>=2 (got %d %d %d)", c.nx, c.ny, c.nz);
+    return NSE_ERR_ARG;
+  }
+  if (!fft_size_ok(c.nx) || !fft_size_ok(c.nz)) {
+    set_error(NSE_ERR_ARG, "nse_ctx_create: nx=%d, nz=%d must be products of 2, 3 and 5", c.nx, c.nz);
+    return NSE_ERR_ARG;
+  }
+  if (!(c.dt > 0) || !(c.Re > 0) || !(c.Sc > 0) || !(c.rho_cp > 0) || !(c.thc > 0)) {
+    set_error(NSE_ERR_ARG, "nse_ctx_create: dt, Re, Sc, rho_cp, thc must be positive");
+    return NSE_ERR_ARG;
+  }
+  if (c.precision != NSE_FP64) {
+    set_error(NSE_ERR_ARG, "nse_ctx_create: precision %d not available", c.precision);
+    return NSE_ERR_ARG;
+  }
+  nse_ctx* x = new nse_ctx();
+  x->cfg = c;
+  x->d = make_dims(c.nx, c.ny, c.nz);
+  x->l = 1;
+  cudaStreamCreateWithFlags(&x->own, cudaStreamNonBlocking);
+  x->stream = x->own;
+  int nx = c.nx, ny = c.ny, nz = c.nz;
+  auto V = [](int n) { return std::vector<double>(n + 2, 0.0); };
+  x->hx = V(nx); x->hx12 = V(nx); x->hdx = V(nx); x->hdx12 = V(nx);
+  x->hy = V(ny); x->hy12 = V(ny); x->hdy = V(ny); x->hdy12 = V(ny);
+  x->hz = V(nz); x->hz12 = V(nz); x->hdz = V(nz); x->hdz12 = V(nz);
+  nse_set_c_stretched(nx, ny, nz, x->hx.data(), x->hx12.data(), x->hy.data(), x->hy12.data(),
+                      x->hz.data(), x->hz12.data(), x->hdx.data(), x->hdx12.data(),
+                      x->hdy.data(), x->hdy12.data(), x->hdz.data(), x->hdz12.data(), c.xl,
+                      c.yl, c.zl, c.y0, c.ystretch);
+  size_t gtot = 2 * (size_t)(nx + 2) + 2 * (size_t)(ny + 2) + 2 * (size_t)(nz + 2);
+  bool ok = x->grid.ensure(gtot * sizeof(double));
+  if (ok) {
+    double* gp = x->grid.as<double>();
+    std::vector<double> all;
+    for (auto* v : {&x->hdx, &x->hdy, &x->hdz, &x->hdx12, &x->hdy12, &x->hdz12})
+      all.insert(all.end(), v->begin(), v->end());
+    ok = NSE_CUDA(cudaMemcpy(gp, all.data(), gtot * sizeof(double), cudaMemcpyHostToDevice));
+    x->g.dx = gp; gp += nx + 2;
+    x->g.dy = gp; gp += ny + 2;
+    x->g.dz = gp; gp += nz + 2;
+    x->g.dx12 = gp; gp += nx + 2;
+    x->g.dy12 = gp; gp += ny + 2;
+    x->g.dz12 = gp;
+  }
+  size_t fb = x->d.ntot * sizeof(double);
+  for (int id = 0; ok && id < NSE_NUM_FIELDS; ++id) {
+    size_t nb = (id == NSE_CELLVALUE) ? x->d.ncell * sizeof(double) : fb;
+    ok = x->f[id].ensure(nb) && NSE_CUDA(cudaMemset(x->f[id].p, 0, nb));
+  }
+  for (DBuf* b : {&x->ua, &x->va, &x->wa, &x->uT, &x->sa, &x->sb, &x->tmp})
+    ok = ok && b->ensure(fb) && NSE_CUDA(cudaMemset(b->p, 0, fb));
+  ok = ok && x->mon.ensure((6 + 6 * 592) * sizeof(double));
+  ok = ok && x->pb.build(nx, ny, nz, x->hdx.data(), x->hdy.data(), x->hdz.data(),
+                         x->hdy12.data(), c.xl, c.zl, x->own);
+  if (!ok) {
+    nse_ctx_destroy(x);
+    return status_or(NSE_ERR_NOMEM);
+  }
+  *out = x;
+  return NSE_OK;
+}
+
+int nse_ctx_destroy(nse_ctx* x) {
+  if (!x) return NSE_OK;
+  if (x->own) cudaStreamSynchronize(x->own);
+  for (auto& b : x->f) b.release();
+  for (DBuf* b : {&x->grid, &x->ua, &x->va, &x->wa, &x->uT, &x->sa, &x->sb, &x->tmp, &x->mon})
+    b->release();
+  x->pb.release();
+  for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
+  if (x->own) cudaStreamDestroy(x->own);
+  delete x;
+  return NSE_OK;
+}
+
+int nse_ctx_set_stream(nse_ctx* x, void* stream) {
+  if (!x) return NSE_ERR_ARG;
+  x->stream = stream ? (cudaStream_t)stream : x->own;
+  return NSE_OK;
+}
+
+int nse_ctx_upload(nse_ctx* x, int id, const double* host) {
+  if (!x || !host || id < 0 || id >= NSE_NUM_FIELDS) {
+    set_error(NSE_ERR_ARG, "nse_ctx_upload: bad argument (field %d)", id);
+    return NSE_ERR_ARG;
+  }
+  size_t n = (id == NSE_CELLVALUE) ? x->d.ncell : x->d.ntot;
+  if (!NSE_CUDA(cudaMemcpyAsync(x->f[id].p, host, n * sizeof(double), cudaMemcpyHostToDevice,
+                                x->stream)))
+    return status_or(NSE_ERR_CUDA);
+  return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_ctx_download(nse_ctx* x, int id, double* host) {
+  if (!x || !host || id < 0 || id >= NSE_NUM_FIELDS) {
+    set_error(NSE_ERR_ARG, "nse_ctx_download: bad argument (field %d)", id);
+    return NSE_ERR_ARG;
+  }
+  size_t n = (id == NSE_CELLVALUE) ? x->d.ncell : x->d.ntot;
+  if (!NSE_CUDA(cudaMemcpyAsync(host, x->f[id].p, n * sizeof(double), cudaMemcpyDeviceToHost,
+                                x->stream)))
+    return status_or(NSE_ERR_CUDA);
+  return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_ctx_grid(nse_ctx* x, double* xx, double* x12, double* y, double* y12, double* z,
+                 double* z12, double* dx, double* dx12, double* dy, double* dy12, double* dz,
+                 double* dz12) {
+  if (!x) return NSE_ERR_ARG;
+  auto cp = [](double* dst, const std::vector<double>& v) {
+    if (dst) memcpy(dst, v.data(), v.size() * sizeof(double));
+  };
+  cp(xx, x->hx); cp(x12, x->hx12); cp(y, x->hy); cp(y12, x->hy12); cp(z, x->hz); cp(z12, x->hz12);
+  cp(dx, x->hdx); cp(dx12, x->hdx12); cp(dy, x->hdy); cp(dy12, x->hdy12); cp(dz, x->hdz);
+  cp(dz12, x->hdz12);
+  return NSE_OK;
+}
+
+int nse_ctx_set_step(nse_ctx* x, int l) {
+  if (!x || l < 1) return NSE_ERR_ARG;
+  x->l = l;
+  return NSE_OK;
+}
+int nse_ctx_get_step(nse_ctx* x) { return x ? x->l : -1; }
+
+int nse_start(nse_ctx* x) {
+  if (!x) return NSE_ERR_ARG;
+  size_t fb = x->d.ntot * sizeof(double);
+  const int src[4] = {NSE_U, NSE_V, NSE_W, NSE_T};
+  const int dst[4] = {NSE_U_PRE, NSE_V_PRE, NSE_W_PRE, NSE_T_PRE};
+  for (int q = 0; q < 4; ++q)
+    if (!NSE_CUDA(cudaMemcpyAsync(x->f[dst[q]].p, x->f[src[q]].p, fb, cudaMemcpyDeviceToDevice,
+                                  x->stream)))
+      return status_or(NSE_ERR_CUDA);
+  return NSE_OK;
+}
+
+// MKP (mkp.f:9-220) with u_temp = (ut, vt, wt); writes u, v, w, p, u_ta,
+// u_ep2, divu of the context and leaves phi in the NSE_PHI field
+static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double* wt) {
+  const Dims& d = x->d;
+  cudaStream_t s = x->stream;
+  double* phi = F(x, NSE_PHI);
+  mark(x, PH_FFTX_F);
+  launch_fft_fwd_x(x->pb.pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s);
+  mark(x, PH_FFTZ_F);
+  launch_fft_z(x->pb.pp, false, s);
+  mark(x, PH_SPN);
+  launch_spn(x->pb.pp, true, true, s);
+  mark(x, PH_FFTZ_I);
+  launch_fft_z(x->pb.pp, true, s);
+  mark(x, PH_FFTX_I);
+  launch_fft_inv_x(x->pb.pp, d, phi, s);
+  mark(x, PH_PHIBC);
+  launch_phibc(d, phi, s);
+  mark(x, PH_CORRECT);
+  launch_correct(d, x->g, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V), F(x, NSE_W),
+                 F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA), F(x, NSE_U_EP2),
+                 F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU), x->cfg.dt, s);
+  mark(x, PH_COUNT);
+}
+
+int nse_project(nse_ctx* x) {
+  if (!x) return NSE_ERR_ARG;
+  size_t fb = x->d.ntot * sizeof(double);
+  cudaStream_t s = x->stream;
+  if (!NSE_CUDA(cudaMemcpyAsync(x->ua.p, x->f[NSE_U].p, fb, cudaMemcpyDeviceToDevice, s)) ||
+      !NSE_CUDA(cudaMemcpyAsync(x->va.p, x->f[NSE_V].p, fb, cudaMemcpyDeviceToDevice, s)) ||
+      !NSE_CUDA(cudaMemcpyAsync(x->wa.p, x->f[NSE_W].p, fb, cudaMemcpyDeviceToDevice, s)))
+    return status_or(NSE_ERR_CUDA);
+  ctx_mkp(x, x->ua.as<double>(), x->va.as<double>(), x->wa.as<double>());
+  return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_poisson(nse_ctx* x) {
+  if (!x) return NSE_ERR_ARG;
+  const Dims& d = x->d;
+  cudaStream_t s = x->stream;
+  double* phi = F(x, NSE_PHI);
+  launch_fft_fwd_x(x->pb.pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+  launch_fft_z(x->pb.pp, false, s);
+  launch_spn(x->pb.pp, true, true, s);
+  launch_fft_z(x->pb.pp, true, s);
+  launch_fft_inv_x(x->pb.pp, d, phi, s);
+  launch_phibc(d, phi, s);
+  return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+// one time step, nse_dominik.f:290-446
+static void ctx_step(nse_ctx* x) {
+  const Dims& d = x->d;
+  const nse_config& c = x->cfg;
+  cudaStream_t s = x->stream;
+  StepParams sp;
+  sp.dt = c.dt; sp.Re = c.Re; sp.Sc = c.Sc; sp.eta = c.eta;
+  sp.force = c.body_force; sp.source = c.heat_source;
+  sp.tbot = c.t_bot; sp.ttop = c.t_top; sp.tsolid = c.t_solid;
+  sp.rho_cp = c.rho_cp; sp.thc = c.thc; sp.l = x->l;
+  double *u = F(x, NSE_U), *v = F(x, NSE_V), *w = F(x, NSE_W), *p = F(x, NSE_P);
+  double* T = F(x, NSE_T);
+  const double* c1 = F(x, NSE_CELLVALUE);
+  double *ua = x->ua.as<double>(), *va = x->va.as<double>(), *wa = x->wa.as<double>();
+  double* uT = x->uT.as<double>();
+  LineScratch sc{x->sa.as<double>(), x->sb.as<double>()};
+  // :290 set_bc(u,v,w,p,T)
+  mark(x, PH_BC);
+  launch_set_bc(d, u, v, w, p, T, c.t_bot, c.t_top, 31, s);
+  mark(x, PH_RHS);
+  // :299-396 explicit terms, AB2, set_bc(u_a,...) and the penalised updates
+  launch_rhs_fused(d, x->g, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA),
+                   F(x, NSE_U_PRE), F(x, NSE_V_PRE), F(x, NSE_W_PRE), F(x, NSE_T_PRE), c1,
+                   ua, va, wa, uT, s);
+  // :397 solve_u_temp: per component y, z, x line solves
+  // (timed per direction: all y solves, then z, then x of the three fields;
+  // the fields are independent, so this order gives the same values as
+  // the reference's per-field y, z, x order)
+  double* fa[3] = {ua, va, wa};
+  mark(x, PH_YVEL);
+  for (int comp = 0; comp < 3; ++comp)
+    launch_ysolve_vel(d, x->g, fa[comp], c1, comp, c.Re, c.dt, c.eta, sc, s);
+  mark(x, PH_ZVEL);
+  for (int comp = 0; comp < 3; ++comp)
+    launch_zsolve_vel(d, x->g, fa[comp], c1, comp, c.Re, c.dt, c.eta, sc, s);
+  mark(x, PH_XVEL);
+  for (int comp = 0; comp < 3; ++comp)
+    launch_xsolve_vel(d, x->g, fa[comp], c1, comp, c.Re, c.dt, c.eta, sc, s);
+  // :419 solve_t: y, x, z
+  mark(x, PH_YT);
+  launch_ysolve_T(d, x->g, uT, c1, nullptr, nullptr, c.rho_cp, c.thc, c.Re, c.Sc, c.dt, c.eta,
+                  2.0 * c.t_bot, 2.0 * c.t_top, sc, s);
+  mark(x, PH_XT);
+  launch_xsolve_T(d, x->g, uT, c1, nullptr, nullptr, c.rho_cp, c.thc, c.Re, c.Sc, c.dt, c.eta,
+                  sc, s);
+  mark(x, PH_ZT);
+  launch_zsolve_T(d, x->g, uT, c1, nullptr, nullptr, c.rho_cp, c.thc, c.Re, c.Sc, c.dt, c.eta,
+                  sc, s);
+  // :429-437 T = u_T (interior); the ghosts are rewritten by the next set_bc
+  std::swap(x->f[NSE_T], x->uT);
+  T = F(x, NSE_T);
+  // :441 set_bc(u_temp,v_temp,w_temp,p,T)
+  mark(x, PH_BC2);
+  launch_set_bc(d, ua, va, wa, p, T, c.t_bot, c.t_top, 31, s);
+  // :446 MKP
+  ctx_mkp(x, ua, va, wa);
+  if (x->prof_n < x->prof_cap) x->prof_n++;
+  x->l += 1;
+}
+
+int nse_step(nse_ctx* x, int nsteps) {
+  if (!x || nsteps < 0) return NSE_ERR_ARG;
+  for (int n = 0; n < nsteps; ++n) {
+    ctx_step(x);
+    if (!NSE_CUDA(cudaGetLastError())) return status_or(NSE_ERR_CUDA);
+    if (x->cfg.flags & 1) {  // check for non-finite values after every step
+      double m[6];
+      int st = nse_monitor(x, m);
+      if (st != NSE_OK) return st;
+      if (m[5] > 0) {
+        set_error(NSE_ERR_NONFINITE, "nse_step: %g non-finite cells after step %d", m[5],
+                  x->l - 1);
+        return NSE_ERR_NONFINITE;
+      }
+    }
+  }
+  return NSE_OK;
+}
+
+int nse_levelset(nse_ctx* x, const double* phi0, double* phi_out, int nnn, double dtau,
+                 double width) {
+  if (!x || !phi0 || nnn < 0) return NSE_ERR_ARG;
+  const Dims& d = x->d;
+  cudaStream_t s = x->stream;
+  // phi0 staged in the tmp work buffer, phi computed in NSE_PHI with ua as
+  // the ping-pong buffer
+  if (!NSE_CUDA(cudaMemcpyAsync(x->tmp.p, phi0, d.ntot * sizeof(double), cudaMemcpyHostToDevice, s)))
+    return status_or(NSE_ERR_CUDA);
+  if (!run_levelset(d, x->g, x->tmp.as<double>(), F(x, NSE_PHI), x->ua.as<double>(),
+                    F(x, NSE_CELLVALUE), nnn, dtau, width, s))
+    return status_or(NSE_ERR_CUDA);
+  if (phi_out &&
+      !NSE_CUDA(cudaMemcpyAsync(phi_out, x->f[NSE_PHI].p, d.ntot * sizeof(double),
+                                cudaMemcpyDeviceToHost, s)))
+    return status_or(NSE_ERR_CUDA);
+  return NSE_CUDA(cudaStreamSynchronize(s)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_monitor(nse_ctx* x, double out[6]) {
+  if (!x || !out) return NSE_ERR_ARG;
+  double* m = x->mon.as<double>();
+  launch_monitor(x->d, x->g, F(x, NSE_U), F(x, NSE_V), F(x, NSE_W), F(x, NSE_T),
+                 F(x, NSE_DIVU), m, x->stream);
+  if (!NSE_CUDA(cudaMemcpyAsync(out, m, 6 * sizeof(double), cudaMemcpyDeviceToHost, x->stream)))
+    return status_or(NSE_ERR_CUDA);
+  return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_ctx_profile(nse_ctx* x, int max_steps) {
+  if (!x || max_steps < 0) return NSE_ERR_ARG;
+  if (!NSE_CUDA(cudaStreamSynchronize(x->stream))) return status_or(NSE_ERR_CUDA);
+  for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
+  x->ev.assign((size_t)max_steps * (PH_COUNT + 1), nullptr);
+  for (auto& e : x->ev)
+    if (!NSE_CUDA(cudaEventCreate(&e))) return status_or(NSE_ERR_CUDA);
+  x->prof_cap = max_steps;
+  x->prof_n = 0;
+  return NSE_OK;
+}
+
+int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
+  if (!x || !ms || nphase < PH_COUNT) return NSE_ERR_ARG;
+  if (!NSE_CUDA(cudaStreamSynchronize(x->stream))) return status_or(NSE_ERR_CUDA);
+  for (int p = 0; p < PH_COUNT; ++p) ms[p] = 0.0;
+  for (int st = 0; st < x->prof_n; ++st)
+    for (int p = 0; p < PH_COUNT; ++p) {
+      float t = 0.f;
+      cudaEvent_t a = x->ev[(size_t)st * (PH_COUNT + 1) + p];
+      cudaEvent_t b = x->ev[(size_t)st * (PH_COUNT + 1) + p + 1];
+      if (!NSE_CUDA(cudaEventElapsedTime(&t, a, b))) return status_or(NSE_ERR_CUDA);
+      ms[p] += t;
+    }
+  if (nsteps) *nsteps = x->prof_n;
+  x->prof_n = 0;
+  return NSE_OK;
+}
+
+int nse_sync(nse_ctx* x) {
+  if (!x) return NSE_ERR_ARG;
+  return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+}  // extern "C"

@@ -1,0 +1,182 @@
+"""Resident solver: the fields stay in HBM across time steps (nse_ctx_* C-ABI).
+
+`Context` owns one device context.  A step is the reference time-loop body
+(nse_dominik.f:290-446): boundary conditions, fused explicit right-hand side,
+penalised ADI line solves (u, v, w then T), and the FFT projection (MKP).
+"""
+import ctypes as C
+
+import numpy as np
+
+from . import NseError, check, lib
+
+FIELDS = ("u", "v", "w", "p", "T", "u_ta", "v_ta", "w_ta", "u_pre", "v_pre", "w_pre",
+          "T_pre", "divu", "u_ep2", "v_ep2", "w_ep2", "phi", "cellvalue")
+FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
+FP64, MIXED = 0, 1
+PHASES = ("set_bc", "rhs", "y_vel", "z_vel", "x_vel", "y_T", "x_T", "z_T", "set_bc_temp",
+          "fft_x_fwd", "fft_z_fwd", "spn", "fft_z_inv", "fft_x_inv", "phibc", "correct")
+FLAG_CHECK_FINITE = 1
+
+
+class Config(C.Structure):
+    """nse_config of include/nsegpu.h.  Defaults are the reference's values
+    (body force and heat source 1, walls and solid at T = 0, rhoCp = thc = 1,
+    uniform grid)."""
+
+    _fields_ = [("nx", C.c_int), ("ny", C.c_int), ("nz", C.c_int),
+                ("dt", C.c_double), ("Re", C.c_double), ("Sc", C.c_double),
+                ("eta", C.c_double), ("xl", C.c_double), ("yl", C.c_double),
+                ("zl", C.c_double), ("y0", C.c_double), ("ystretch", C.c_double),
+                ("body_force", C.c_double), ("heat_source", C.c_double),
+                ("t_bot", C.c_double), ("t_top", C.c_double), ("t_solid", C.c_double),
+                ("rho_cp", C.c_double), ("thc", C.c_double),
+                ("precision", C.c_int), ("flags", C.c_int)]
+
+    def __init__(self, nx, ny, nz, dt, Re, Sc, eta, xl, yl, zl, y0=0.0, ystretch=0.0,
+                 body_force=1.0, heat_source=1.0, t_bot=0.0, t_top=0.0, t_solid=0.0,
+                 rho_cp=1.0, thc=1.0, precision=FP64, flags=0):
+        super().__init__(nx, ny, nz, dt, Re, Sc, eta, xl, yl, zl, y0, ystretch, body_force,
+                         heat_source, t_bot, t_top, t_solid, rho_cp, thc, precision, flags)
+
+
+def _sig():
+    L = lib()
+    vp = C.c_void_p
+    L.nse_ctx_create.argtypes = [C.POINTER(Config), C.POINTER(vp)]
+    for n in ("nse_ctx_destroy", "nse_start", "nse_project", "nse_poisson", "nse_sync",
+              "nse_ctx_get_step"):
+        getattr(L, n).argtypes = [vp]
+    L.nse_ctx_set_stream.argtypes = [vp, vp]
+    L.nse_ctx_upload.argtypes = [vp, C.c_int, vp]
+    L.nse_ctx_download.argtypes = [vp, C.c_int, vp]
+    L.nse_ctx_set_step.argtypes = [vp, C.c_int]
+    L.nse_step.argtypes = [vp, C.c_int]
+    L.nse_monitor.argtypes = [vp, vp]
+    L.nse_levelset.argtypes = [vp, vp, vp, C.c_int, C.c_double, C.c_double]
+    L.nse_ctx_grid.argtypes = [vp] + [vp] * 12
+    L.nse_ctx_profile.argtypes = [vp, C.c_int]
+    L.nse_ctx_phase_times.argtypes = [vp, vp, C.c_int, vp]
+    L.nse_launch_count.restype = C.c_longlong
+    return L
+
+
+def launch_count():
+    """Kernel launches issued by libnsegpu.so in this process."""
+    return int(_sig().nse_launch_count())
+
+
+class Context:
+    def __init__(self, cfg: Config):
+        self.L = _sig()
+        self.cfg = cfg
+        h = C.c_void_p()
+        check(self.L.nse_ctx_create(C.byref(cfg), C.byref(h)))
+        self.h = h
+        n = cfg.nx, cfg.ny, cfg.nz
+        self.shape = (n[0] + 2, n[1] + 2, n[2] + 2)
+        self.grid = {k: np.zeros(m + 2) for k, m in
+                     (("x", n[0]), ("x12", n[0]), ("y", n[1]), ("y12", n[1]), ("z", n[2]),
+                      ("z12", n[2]), ("dx", n[0]), ("dx12", n[0]), ("dy", n[1]),
+                      ("dy12", n[1]), ("dz", n[2]), ("dz12", n[2]))}
+        g = self.grid
+        check(self.L.nse_ctx_grid(self.h, *[g[k].ctypes.data for k in
+                                            ("x", "x12", "y", "y12", "z", "z12", "dx", "dx12",
+                                             "dy", "dy12", "dz", "dz12")]))
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nse_ctx_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+    def _fshape(self, name):
+        c = self.cfg
+        return (c.nx, c.ny, c.nz) if name == "cellvalue" else self.shape
+
+    def upload(self, name, arr):
+        a = np.asfortranarray(arr, dtype=np.float64)
+        want = self._fshape(name)
+        if name == "cellvalue" and a.ndim == 4:
+            a = np.asfortranarray(a[..., 0])
+        if a.shape != want:
+            raise ValueError(f"{name}: shape {a.shape}, expected {want}")
+        check(self.L.nse_ctx_upload(self.h, FIELD_ID[name], a.ctypes.data))
+
+    def upload_ptr(self, name, ptr):
+        """Upload from a host address (e.g. a pinned torch buffer)."""
+        check(self.L.nse_ctx_upload(self.h, FIELD_ID[name], ptr))
+
+    def download(self, name, out=None):
+        if out is None:
+            out = np.zeros(self._fshape(name), order="F")
+        check(self.L.nse_ctx_download(self.h, FIELD_ID[name], out.ctypes.data))
+        return out
+
+    def download_ptr(self, name, ptr):
+        check(self.L.nse_ctx_download(self.h, FIELD_ID[name], ptr))
+
+    def set_stream(self, stream_handle):
+        check(self.L.nse_ctx_set_stream(self.h, stream_handle))
+
+    @property
+    def step_index(self):
+        return self.L.nse_ctx_get_step(self.h)
+
+    @step_index.setter
+    def step_index(self, l):
+        check(self.L.nse_ctx_set_step(self.h, int(l)))
+
+    def start(self):
+        check(self.L.nse_start(self.h))
+
+    def step(self, n=1):
+        check(self.L.nse_step(self.h, int(n)))
+
+    def project(self):
+        check(self.L.nse_project(self.h))
+
+    def poisson(self):
+        check(self.L.nse_poisson(self.h))
+
+    def sync(self):
+        check(self.L.nse_sync(self.h))
+
+    def levelset(self, phi0, nnn=2000, dtau=1.0e-3, width=1.0, want_phi=True):
+        a = np.asfortranarray(phi0, dtype=np.float64)
+        out = np.zeros(self.shape, order="F") if want_phi else None
+        check(self.L.nse_levelset(self.h, a.ctypes.data, out.ctypes.data if want_phi else None,
+                                  int(nnn), float(dtau), float(width)))
+        return out
+
+    def profile(self, max_steps):
+        """Record CUDA events around every phase of the next max_steps steps."""
+        check(self.L.nse_ctx_profile(self.h, int(max_steps)))
+
+    def phase_times(self):
+        """Summed milliseconds per phase over the profiled steps, and the step count."""
+        ms = np.zeros(len(PHASES))
+        n = C.c_int(0)
+        check(self.L.nse_ctx_phase_times(self.h, ms.ctypes.data, len(PHASES),
+                                         C.addressof(n)))
+        return dict(zip(PHASES, ms.tolist())), n.value
+
+    def monitor(self):
+        out = np.zeros(6)
+        check(self.L.nse_monitor(self.h, out.ctypes.data))
+        return {"max_divu": out[0], "u_int": out[1], "v_int": out[2], "w_int": out[3],
+                "T_int": out[4], "nonfinite": int(out[5])}
+
+
+__all__ = ["Config", "Context", "FIELDS", "FP64", "MIXED", "FLAG_CHECK_FINITE", "NseError"]
