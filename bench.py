@@ -1,0 +1,430 @@
+"""Benchmark: fractional time steps of the penalised channel with heat at
+256x192x256 (FP64) on B200, plus the FFT Poisson solve.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl ours|reference]
+
+One JSON line on rank 0.  `value` is whole-job time steps per second (the N
+ranks run independent replicas: weak scaling), timed with CUDA events on the
+solver's stream between barriers, max over ranks.  `e2e` is the same metric
+through the public C-ABI with host buffers: pinned-host upload of the job's
+inputs, K steps each followed by the device monitor read-back, and the
+download of the final state, all inside the timed region.
+
+--impl reference times the CPU restatement of the reference Fortran (the
+oracle; the Fortran itself cannot be built here) on all host cores for the
+same workload and prints the same line with "impl": "reference".
+"""
+import argparse
+import json
+import math
+import os
+import statistics
+import subprocess
+import sys
+import threading
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+import numpy as np  # noqa: E402
+
+METRIC = "NS steps/s & Poisson GB/s at 256x192x256: FP64 vs mixed, div<=1e-10, 1 B200"
+UNIT = "steps/s"
+NX, NY, NZ = 256, 192, 256
+RE, PR, ETA, WIDTH = 3000.0, 0.71, 1.0e4, 1.5
+SPHERE = ((math.pi, 0.0, math.pi / 2), 0.25)
+WORKLOAD = ("sphere256: channel 2pi x 2 x pi, y walls at -1,1 (tanh stretch 2), "
+            "256x192x256 cells, sphere R=0.25 at (pi,0,pi/2) by volume penalisation "
+            "(eta=1e4, smoothed Heaviside 1.5 dx), heat transfer (sphere T=1, walls T=0), "
+            "Re=3000, Pr=0.71, u=1.5(1-y^2)+N(0,0.05^2), CFL 0.5")
+
+
+def peaks():
+    try:
+        with open(os.path.join(ROOT, "MEASURED_PEAKS.json")) as f:
+            p = json.load(f)
+        return float(p["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+def dram_traffic():
+    """bytes per launch from the committed ncu summary profiles/dram_traffic.txt
+    (lines: '<phase> <bytes per launch>'), or {}"""
+    out = {}
+    try:
+        with open(os.path.join(ROOT, "profiles", "dram_traffic.txt")) as f:
+            for line in f:
+                parts = line.split()
+                if len(parts) >= 2 and not line.startswith("#"):
+                    out[parts[0]] = float(parts[1])
+    except OSError:
+        pass
+    return out
+
+
+# algorithmic bytes per launch of each phase's kernel (FP64, N interior cells,
+# Hs = (nx/2+1)*ny*nz spectral values of 16 B); launches per step in LAUNCHES
+def algorithmic_bytes(nx, ny, nz):
+    N = nx * ny * nz
+    Hs = (nx // 2 + 1) * ny * nz
+    return {
+        "rhs": 8 * N * 20,        # read u,v,w,T,u_ta x3,4 histories,mask; write u*,v*,w*,T*,4 histories
+        "y_vel": 8 * N * 3,       # read rhs + mask, write solution (per field)
+        "z_vel": 8 * N * 3,
+        "x_vel": 8 * N * 3,
+        "y_T": 8 * N * 3,
+        "x_T": 8 * N * 3,
+        "z_T": 8 * N * 3,
+        "fft_x_fwd": 8 * N * 3 + 16 * Hs,   # read u*,v*,w*, write half spectrum
+        "fft_z_fwd": 2 * 16 * Hs,
+        "spn": 2 * 16 * Hs,
+        "fft_z_inv": 2 * 16 * Hs,
+        "fft_x_inv": 16 * Hs + 8 * N,
+        "correct": 8 * N * 18,    # read phi,u*,v*,w*,u_ta x3; write u,v,w,p,ep2 x3,u_ta x3,divu
+    }
+
+
+LAUNCHES = {"set_bc": 1, "rhs": 1, "y_vel": 3, "z_vel": 3, "x_vel": 3, "y_T": 1, "x_T": 1,
+            "z_T": 1, "set_bc_temp": 1, "fft_x_fwd": 1, "fft_z_fwd": 1, "spn": 1,
+            "fft_z_inv": 1, "fft_x_inv": 1, "phibc": 2, "correct": 1}
+
+
+class Clocks:
+    """nvidia-smi samples (200 ms) while the timed region runs."""
+
+    def __init__(self, index):
+        self.index = index
+        self.samples = []
+        self.proc = None
+
+    def __enter__(self):
+        q = ("clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.hw_slowdown,"
+             "clocks_event_reasons.hw_thermal_slowdown,clocks_event_reasons.sw_thermal_slowdown,"
+             "clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", "-i", str(self.index), f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                 "-lms", "200"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self.thread = threading.Thread(target=self._read, daemon=True)
+            self.thread.start()
+        except OSError:
+            self.proc = None
+        time.sleep(0.3)
+        return self
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.samples.append([s.strip() for s in line.split(",")])
+
+    def __exit__(self, *a):
+        if self.proc:
+            time.sleep(0.25)
+            self.proc.terminate()
+            try:
+                self.proc.wait(timeout=5)
+            except Exception:
+                self.proc.kill()
+
+    def summary(self):
+        if not self.samples:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["unavailable"]}
+        sm = [float(s[0]) for s in self.samples if s[0].replace(".", "").isdigit()]
+        mx = [float(s[1]) for s in self.samples if s[1].replace(".", "").isdigit()]
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        reasons = sorted({names[i] for s in self.samples for i in range(4)
+                          if len(s) > 3 + i and s[3 + i].lower().startswith("active")})
+        return {"sm_mhz": statistics.median(sm) if sm else None,
+                "sm_max_mhz": max(mx) if mx else None, "reasons": reasons,
+                "samples": len(self.samples)}
+
+
+def build_case(S, W, torch):
+    """Context with the workload's initial state: level-set mask, projected field."""
+    g = W.grid_arrays(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = W.channel_state(g, seed=2024, t_bot=0.0, t_top=0.0)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    cfg = S.Config(NX, NY, NZ, dt, RE, PR, ETA, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                   ystretch=2.0, body_force=3.0 / RE, heat_source=0.0, t_bot=0.0, t_top=0.0,
+                   t_solid=1.0)
+    ctx = S.Context(cfg)
+    for k in ("u", "v", "w", "T"):
+        ctx.upload(k, f[k])
+    phi0 = W.sphere_phi0(g, *SPHERE)
+    t0 = time.perf_counter()
+    ctx.levelset(phi0, width=WIDTH, want_phi=False)
+    ls_s = time.perf_counter() - t0
+    ctx.project()
+    ctx.start()
+    ctx.sync()
+    return g, f, cfg, ctx, ls_s
+
+
+def run_ours(args, rank, world, local_rank):
+    import torch
+    import torch.distributed as dist
+    from vtkmakecompare_b200 import solver as S
+    from vtkmakecompare_b200 import workload as W
+
+    torch.cuda.set_device(local_rank)
+    dev = torch.device("cuda", local_rank)
+    g, f0, cfg, ctx, ls_s = build_case(S, W, torch)
+    stream = torch.cuda.Stream(device=dev)
+    ctx.set_stream(stream.cuda_stream)
+
+    def barrier():
+        if world > 1:
+            dist.barrier()
+
+    def max_over_ranks(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=dev)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
+
+    # ---------------------------------------------------- device-resident steps
+    with torch.cuda.stream(stream):
+        ctx.step(args.warmup)
+    torch.cuda.synchronize()
+    barrier()
+    ctx.profile(args.steps)
+    n0 = S.launch_count()
+    e0 = torch.cuda.Event(enable_timing=True)
+    e1 = torch.cuda.Event(enable_timing=True)
+    with Clocks(local_rank) as clk:
+        torch.cuda.synchronize()
+        barrier()
+        e0.record(stream)
+        ctx.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        barrier()
+    launches = S.launch_count() - n0
+    ms = e0.elapsed_time(e1)
+    phases, nprof = ctx.phase_times()
+    ms_max = max_over_ranks(ms)
+    mon = ctx.monitor()
+
+    # ---------------------------------------------------------- Poisson solve
+    ctx.upload("phi", W.poisson_rhs(g, 7))
+    with torch.cuda.stream(stream):
+        ctx.poisson()
+    torch.cuda.synchronize()
+    npois = max(5, args.steps)
+    p0 = torch.cuda.Event(enable_timing=True)
+    p1 = torch.cuda.Event(enable_timing=True)
+    barrier()
+    p0.record(stream)
+    for _ in range(npois):
+        ctx.poisson()
+    p1.record(stream)
+    torch.cuda.synchronize()
+    pms = max_over_ranks(p0.elapsed_time(p1)) / npois
+    Hs = (NX // 2 + 1) * NY * NZ
+    BP = 2 * 8 * NX * NY * NZ + 4 * 16 * Hs
+
+    # ------------------------------------------------------------------ e2e
+    # the job through the public API from pinned host buffers: upload the
+    # inputs (u, v, w, T, mask), K steps each followed by the monitor
+    # read-back, download of the final state (u, v, w, p, T)
+    shape = (NX + 2, NY + 2, NZ + 2)
+    pin = {k: torch.from_numpy(np.ascontiguousarray(f0[k].ravel(order="F"))).pin_memory()
+           for k in ("u", "v", "w", "T")}
+    c1 = ctx.download("cellvalue")
+    pin["cellvalue"] = torch.from_numpy(np.ascontiguousarray(c1.ravel(order="F"))).pin_memory()
+    outs = {k: torch.empty(int(np.prod(shape)), dtype=torch.float64).pin_memory()
+            for k in ("u", "v", "w", "p", "T")}
+    h2d = sum(t.numel() * 8 for t in pin.values())
+    d2h = sum(t.numel() * 8 for t in outs.values()) + 48 * args.steps
+    mon_ok = True
+
+    def job():
+        nonlocal mon_ok
+        for k, t in pin.items():
+            ctx.upload_ptr(k, t.data_ptr())
+        ctx.step_index = 1
+        ctx.start()
+        for _ in range(args.steps):
+            ctx.step(1)
+            m = ctx.monitor()
+            mon_ok = mon_ok and m["nonfinite"] == 0
+        for k, t in outs.items():
+            ctx.download_ptr(k, t.data_ptr())
+
+    job()  # warm
+    torch.cuda.synchronize()
+    barrier()
+    q0 = torch.cuda.Event(enable_timing=True)
+    q1 = torch.cuda.Event(enable_timing=True)
+    q0.record(stream)
+    job()
+    q1.record(stream)
+    torch.cuda.synchronize()
+    e2e_ms = max_over_ranks(q0.elapsed_time(q1))
+    barrier()
+
+    # ---------------------------------------------------------- CPU baseline
+    cpu = None
+    if rank == 0 and not args.no_cpu:
+        cpu = cpu_baseline(g, f0, c1, cfg, nsteps=args.cpu_steps)
+
+    if rank != 0:
+        ctx.close()
+        return None
+
+    # ------------------------------------------------------------- roofline
+    algo = algorithmic_bytes(NX, NY, NZ)
+    peak, peak_kind = peaks()
+    per_launch = {k: phases[k] / max(1, nprof) / LAUNCHES[k] for k in phases}
+    dominant = max((k for k in phases if k in algo), key=lambda k: phases[k])
+    t_launch_s = per_launch[dominant] / 1e3
+    achieved = algo[dominant] / t_launch_s / 1e9
+    traffic = dram_traffic().get(dominant)
+    steps_s = world * args.steps / (ms_max / 1e3)
+    line = {
+        "metric": METRIC,
+        "value": round(steps_s, 3),
+        "unit": UNIT,
+        "n_gpus": world,
+        "steps": args.steps,
+        "warmup": args.warmup,
+        "ms_per_step": round(ms_max / args.steps, 4),
+        "higher_is_better": True,
+        "scaling": "weak",
+        "vs_baseline": None,
+        "dtype": "f64",
+        "data": "synthetic (seeded channel flow + sphere level set; no dataset)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "precision": "fp64 plain",
+                   "parallelism": f"replicas x{world}",
+                   "l2": "inputs larger than L2 (16 resident FP64 fields of 103 MB)",
+                   "dt": cfg.dt},
+        "poisson": {"solves_per_s": round(world * 1e3 / pms, 2), "ms_per_solve": round(pms, 4),
+                    "algorithmic_bytes": BP, "gbs": round(BP / (pms / 1e3) / 1e9, 1),
+                    "frac_of_hbm": round(BP / (pms / 1e3) / 1e9 / peak, 4)},
+        "max_divu": mon["max_divu"],
+        "mixed_precision": None,
+        "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": UNIT,
+                "h2d_bytes_per_step": int(h2d / args.steps),
+                "d2h_bytes_per_step": int(d2h / args.steps),
+                "note": "job of K steps: pinned H2D of u,v,w,T,mask + K x (step + monitor "
+                        "read-back) + D2H of u,v,w,p,T"},
+        "roofline": {"bound": "hbm", "kernel": dominant, "achieved": round(achieved, 1),
+                     "peak": peak, "unit": "GB/s", "frac": round(achieved / peak, 4),
+                     "traffic": traffic, "peak_source": peak_kind,
+                     "algorithmic_bytes_per_launch": algo[dominant],
+                     "ms_per_launch": round(per_launch[dominant], 4)},
+        "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()},
+        "gpu_launches": int(launches),
+        "levelset_setup_s": round(ls_s, 3),
+        "clocks": clk.summary(),
+        "cpu_baseline": cpu,
+    }
+    ctx.close()
+    return line
+
+
+class _OGrid:
+    """grid dict -> the attribute object the oracle binding expects"""
+
+    def __init__(self, g):
+        self.__dict__.update(g)
+
+
+def cpu_baseline(g, f0, c1, cfg, nsteps=3):
+    """The oracle (C++ restatement of the reference, faithful mode with the
+    per-line dense matrix zeroing) on all host cores: `nsteps` full steps."""
+    from oracle import oracle as O
+    O.set_faithful(True)
+    s = O.Solver(_OGrid(g), cfg.dt, cfg.Re, cfg.Sc, cfg.eta, force=cfg.body_force,
+                 source=cfg.heat_source, tbot=cfg.t_bot, ttop=cfg.t_top, tsolid=cfg.t_solid)
+    for k in ("u", "v", "w", "T"):
+        s.f[k][...] = f0[k]
+    s.cellvalue[..., 0] = c1
+    s.start()
+    s.step(1)  # warm (first-touch of the 45 work arrays)
+    t0 = time.perf_counter()
+    s.step(nsteps)
+    el = time.perf_counter() - t0
+    return {"value": round(nsteps / el, 4), "unit": UNIT, "cores": O.num_threads(),
+            "kind": "port",
+            "sample": f"{nsteps} full FP64 time steps of the 256x192x256 workload "
+                      f"({el:.1f} s) after one warm step; oracle faithful mode"}
+
+
+def run_reference(args, rank, world):
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    from vtkmakecompare_b200 import workload as W
+    g = W.grid_arrays(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = W.channel_state(g, seed=2024, t_bot=0.0, t_top=0.0)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    phi = W.sphere_phi0(g, *SPHERE)[1:-1, 1:-1, 1:-1]
+    h = WIDTH * g["dx"][1:-1, None, None]
+    c1 = np.where(phi >= h, 1.0, np.where(phi <= -h, 0.0,
+                                          (np.sin(3.1415926535 * phi / 2 / h) + 1) / 2))
+    O.set_faithful(True)
+    s = O.Solver(_OGrid(g), dt, RE, PR, ETA, force=3.0 / RE, source=0.0, tbot=0.0,
+                 ttop=0.0, tsolid=1.0)
+    for k in ("u", "v", "w", "T"):
+        s.f[k][...] = f[k]
+    s.cellvalue[..., 0] = c1
+    s.start()
+    s.step(max(1, args.warmup))
+    t0 = time.perf_counter()
+    s.step(args.steps)
+    el = time.perf_counter() - t0
+    v = args.steps / el
+    return {
+        "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
+        "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * el / args.steps, 1),
+        "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
+        "data": "synthetic (seeded channel flow + sphere mask)",
+        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "precision": "fp64 plain"},
+        "impl": "reference",
+        "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": O.num_threads(),
+                         "kind": "port",
+                         "sample": f"{args.steps} full time steps after {max(1, args.warmup)} "
+                                   "warm steps; C++/OpenMP restatement of the reference "
+                                   "(the Fortran + FFTW build is not available here)"},
+        "e2e": {"value": round(v, 4), "unit": UNIT, "h2d_bytes_per_step": 0,
+                "d2h_bytes_per_step": 0},
+    }
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=20)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--cpu-steps", type=int, default=3)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local_rank = int(os.environ.get("LOCAL_RANK", "0"))
+    if args.warmup < 3 and args.impl == "ours":
+        args.warmup = 3
+    if args.impl == "reference":
+        line = run_reference(args, rank, world)
+    else:
+        if world > 1:
+            import datetime
+
+            import torch
+            import torch.distributed as dist
+            torch.cuda.set_device(local_rank)
+            dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+        line = run_ours(args, rank, world, local_rank)
+        if world > 1:
+            import torch.distributed as dist
+            dist.destroy_process_group()
+    if rank == 0 and line is not None:
+        print(json.dumps(line), flush=True)
+
+
+if __name__ == "__main__":
+    main()

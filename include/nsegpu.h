@@ -182,6 +182,12 @@ typedef struct nse_config {
 } nse_config;
 
 enum { NSE_FP64 = 0, NSE_MIXED = 1 };
+/* nse_config.flags bits */
+enum {
+  NSE_FLAG_CHECK_FINITE = 1, /* nse_step checks every step for non-finite values */
+  NSE_FLAG_EXACT = 4         /* resident step rounds every operation like the reference
+                                (no FMA, true divisions); default is the fast form */
+};
 
 /* field ids for upload/download (padded fields unless noted) */
 enum nse_field {

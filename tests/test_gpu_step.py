@@ -54,11 +54,11 @@ def run_oracle(g, f, c1, par, nsteps):
     return s
 
 
-def make_ctx(g, f, c1, par):
+def make_ctx(g, f, c1, par, exact=False):
     cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                    g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0, body_force=par["force"],
                    heat_source=par["source"], t_bot=par["tbot"], t_top=par["ttop"],
-                   t_solid=par["tsolid"])
+                   t_solid=par["tsolid"], flags=S.FLAG_EXACT if exact else 0)
     ctx = S.Context(cfg)
     for k in ("u", "v", "w", "T"):
         ctx.upload(k, f[k])
@@ -74,12 +74,13 @@ def test_context_grid_matches_oracle_grid():
         assert np.array_equal(g[k], getattr(og, k)), k
 
 
+@pytest.mark.parametrize("exact", [False, True])
 @pytest.mark.parametrize("n,sphere,steps", [((16, 12, 8), True, 3), ((32, 24, 16), True, 10),
-                                            ((24, 16, 20), False, 10)])
-def test_steps_match_oracle(n, sphere, steps):
+                                            ((24, 16, 20), False, 10), ((40, 33, 36), True, 4)])
+def test_steps_match_oracle(n, sphere, steps, exact):
     g, f, c1, par = make_case(*n, sphere=sphere)
     ref = run_oracle(g, f, c1, par, steps)
-    with make_ctx(g, f, c1, par) as ctx:
+    with make_ctx(g, f, c1, par, exact) as ctx:
         ctx.step(steps)
         assert ctx.step_index == steps + 1
         scale = max(1.0, np.abs(ref.f["u"]).max() / g["dx"][1])
@@ -105,7 +106,7 @@ def test_step_bitexact_without_projection_effects():
     for k in ("u", "v", "w"):
         f[k][...] = 0.0
     ref = run_oracle(g, f, c1, par, 2)
-    with make_ctx(g, f, c1, par) as ctx:
+    with make_ctx(g, f, c1, par, exact=True) as ctx:
         ctx.step(2)
         T = ctx.download("T")
         assert np.array_equal(T, ref.f["T"])

@@ -22,6 +22,9 @@ SOURCES = {
     "k_stencil.cu": ["--fmad=false"],
     "k_line.cu": ["--fmad=false"],
     "k_levelset.cu": ["--fmad=false"],
+    "k_lines_exact.cu": ["--fmad=false"],
+    "k_lines_fast.cu": [],
+    "k_rhs_fast.cu": [],
     "k_fft.cu": [],
 }
 
@@ -42,7 +45,7 @@ def _needs(obj, deps):
 
 def build(verbose=False, extra=()):
     os.makedirs(BUILD, exist_ok=True)
-    headers = [os.path.join(CSRC, "common.cuh"),
+    headers = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "k_lines.cuh"),
                os.path.join(HERE, "..", "include", "nsegpu.h")]
     jobs = []
     objs = []

@@ -43,6 +43,11 @@ struct GridDev {
   const double *dx, *dy, *dz, *dx12, *dy12, *dz12;
 };
 
+// reciprocals of the grid spacings (fast form of the resident step)
+struct GridRcp {
+  const double *rdx, *rdy, *rdz, *rdx12, *rdy12, *rdz12;
+};
+
 // physical parameters of one step
 struct StepParams {
   double dt, Re, Sc, eta;
@@ -123,6 +128,15 @@ void launch_rhs_fused(const Dims& d, const GridDev& g, const StepParams& sp,
                       double* u_pre, double* v_pre, double* w_pre, double* T_pre,
                       const double* c1, double* u_a, double* v_a, double* w_a,
                       double* u_T, cudaStream_t s);
+
+// same terms in the fast form (reciprocal metrics, FMA, mask-free cells skip
+// the immersed-boundary loads); k_rhs_fast.cu
+void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
+                     const double* u, const double* v, const double* w, const double* T,
+                     const double* u_ta, const double* v_ta, const double* w_ta,
+                     double* u_pre, double* v_pre, double* w_pre, double* T_pre,
+                     const double* c1, double* u_a, double* v_a, double* w_a, double* u_T,
+                     cudaStream_t s);
 
 // ADI line solves; mask is c1 (nx,ny,nz); comp: 0 u (c2), 1 v (c3), 2 w (c4)
 struct LineScratch {

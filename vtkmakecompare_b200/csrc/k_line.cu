@@ -18,7 +18,7 @@
 //    and a third sweep applies x - fact*z.
 // Consecutive threads own lines that are adjacent in x (y and z lines) so
 // loads are coalesced; x lines are contiguous per thread and rely on L1.
-#include "common.cuh"
+#include "k_lines.cuh"
 
 namespace nse {
 
@@ -45,50 +45,6 @@ struct MaskSrc {
     return (k < d.nz) ? (a + LD(m, c + (long)d.nx * d.ny)) * 0.50 : a;
   }
 };
-
-struct Row {
-  double lo, di, up;
-};
-
-// implicit_uy rows (nse_dominik.f:1524-1529)
-__device__ __forceinline__ Row row_uy(double beta, double alpha, double dy12m, double dy12c,
-                                      double dyc) {
-  Row r;
-  r.lo = -beta / alpha / dy12m / dyc;
-  r.di = 1.0 + beta / alpha * (1.0 / dy12c + 1.0 / dy12m) / dyc;
-  r.up = -beta / alpha / dy12c / dyc;
-  return r;
-}
-// implicit_vy rows (:1605-1610)
-__device__ __forceinline__ Row row_vy(double beta, double alpha, double dyc, double dyp,
-                                      double dy12c) {
-  Row r;
-  r.lo = -beta / alpha / dyc / dy12c;
-  r.di = 1.0 + beta / alpha * (1.0 / dyp + 1.0 / dyc) / dy12c;
-  r.up = -beta / alpha / dyp / dy12c;
-  return r;
-}
-// implicit_solver rows (periodic_implicit.f:28-33): a,b,c
-__device__ __forceinline__ Row row_cyc(double beta, double alpha, double dc, double dp,
-                                       double d12c) {
-  Row r;
-  r.lo = -beta / alpha / dc / d12c;
-  r.di = 1.0 + beta / alpha * (1.0 / dp + 1.0 / dc) / d12c;
-  r.up = -beta / alpha / dp / d12c;
-  return r;
-}
-// implicit_Ty / implicit_Tx harmonic-conductance rows (:1752-1770, :1811-1829)
-__device__ __forceinline__ Row row_T(double beta, double alpha, double dm, double dc,
-                                     double dp, double d12m, double d12c, double llm,
-                                     double llc, double llp, double rrc) {
-  double Hm = (dc + dm) / (dc / llc + dm / llm);
-  double Hp = (dp + dc) / (dp / llp + dc / llc);
-  Row r;
-  r.lo = -beta / alpha * Hm / d12m / dc / rrc;
-  r.di = 1.0 + beta / alpha * (Hp / d12c / dc + Hm / d12m / dc) / rrc;
-  r.up = -beta / alpha * Hp / d12c / dc / rrc;
-  return r;
-}
 
 // --------------------------------------------------------- UL (y) solver --
 // Rows 0..m; interior rows 1..m-1 come from rowfn(r); boundary rows:

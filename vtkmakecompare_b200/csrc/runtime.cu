@@ -13,10 +13,24 @@
 #include <vector>
 
 #include "common.cuh"
+#include "k_lines.cuh"
 
 namespace nse {
 
 bool fft_size_ok(int n);  // k_fft.cu
+void launch_line_table(int n, const double* D, const double* D12, const LineArgs& a, int kind,
+                       double* base, cudaStream_t s);
+void launch_line_flags(const Dims& d, const double* c1, int dir, int comp, int jtop,
+                       unsigned char* flags, cudaStream_t s);
+void launch_lines_exact(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
+                        const LineTab& tb, const int* slots, const double* ltab,
+                        cudaStream_t s);
+void launch_lines_fast(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
+                       const LineTab& tb, const int* slots, const double* ltab,
+                       cudaStream_t s);
+void launch_line_tables_masked(int dir, int kind, const Dims& d, const GridDev& g,
+                               const double* c1, const LineArgs& a, const int* ids, int count,
+                               double* out, cudaStream_t s);
 
 // ------------------------------------------------------------------ errors --
 static thread_local int g_status = NSE_OK;
@@ -988,13 +1002,136 @@ struct nse_ctx {
   std::vector<double> hx, hx12, hy, hy12, hz, hz12, hdx, hdx12, hdy, hdy12, hdz, hdz12;
   DBuf grid;
   GridDev g;
+  GridRcp rg;
   DBuf f[NSE_NUM_FIELDS];
   DBuf ua, va, wa, uT, sa, sb, tmp, mon;
   PoissonBufs pb;
   // per-phase CUDA events of profiled steps: ev[step][phase boundary]
   std::vector<cudaEvent_t> ev;
   int prof_cap = 0, prof_n = 0;
+  // tiled line solver: per-row tables of mask-free lines (7 tables: y UL_U,
+  // UL_V, UL_T; z CYC_VEL, CYC_T; x CYC_VEL, CYC_T) and per-line mask flags
+  DBuf ltab, lflags;
+  LineTab tab[7];
+  bool mask_dirty = true;
+  // per (direction, component): slot of every line (-1 = mask-free), the
+  // line ids of the masked lines and their coefficient tables
+  DBuf slots[3][4], ids[3][4], mtab[3][4];
+  int nmasked[3][4] = {};
 };
+
+enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
+
+static bool build_line_tables(nse_ctx* x) {
+  const Dims& d = x->d;
+  const nse_config& c = x->cfg;
+  int L = std::max(d.nx, std::max(d.ny, d.nz)) + 2;
+  size_t per = 10 * (size_t)L;
+  if (!x->ltab.ensure(7 * per * sizeof(double))) return false;
+  size_t nfl = 4 * ((size_t)d.nx * d.nz + (size_t)d.nx * d.ny + (size_t)d.ny * d.nz);
+  if (!x->lflags.ensure(nfl)) return false;
+  double* base = x->ltab.as<double>();
+  struct T { int n, kind; const double *D, *D12; bool temp; } spec[7] = {
+      {d.ny, LK_UL_U, x->g.dy, x->g.dy12, false}, {d.ny, LK_UL_V, x->g.dy, x->g.dy12, false},
+      {d.ny, LK_UL_T, x->g.dy, x->g.dy12, true},  {d.nz, LK_CYC_VEL, x->g.dz, x->g.dz12, false},
+      {d.nz, LK_CYC_T, x->g.dz, x->g.dz12, true}, {d.nx, LK_CYC_VEL, x->g.dx, x->g.dx12, false},
+      {d.nx, LK_CYC_T, x->g.dx, x->g.dx12, true}};
+  std::vector<double> dens(7);
+  for (int t = 0; t < 7; ++t) {
+    LineArgs a{};
+    a.beta = spec[t].temp ? c.dt / c.Re / c.Sc / 2.0 : c.dt / c.Re / 2.0;
+    a.dt = c.dt; a.eta = c.eta; a.r0 = c.rho_cp; a.l0 = c.thc;
+    double* b = base + t * per;
+    int Ln = spec[t].n + 2;
+    launch_line_table(spec[t].n, spec[t].D, spec[t].D12, a, spec[t].kind, b, x->own);
+    LineTab& tb = x->tab[t];
+    tb.l = b; tb.dm = b + Ln; tb.rdm = b + 2 * Ln; tb.up = b + 3 * Ln; tb.a = b + 4 * Ln;
+    tb.gam = b + 5 * Ln; tb.bet = b + 6 * Ln; tb.rbet = b + 7 * Ln; tb.z = b + 8 * Ln;
+    if (!NSE_CUDA(cudaMemcpyAsync(&dens[t], b + 9 * Ln, sizeof(double), cudaMemcpyDeviceToHost,
+                                  x->own)))
+      return false;
+  }
+  if (!NSE_CUDA(cudaStreamSynchronize(x->own))) return false;
+  for (int t = 0; t < 7; ++t) x->tab[t].den = dens[t];
+  return true;
+}
+
+// flags of lines touching the mask, per direction and component
+static unsigned char* flags_of(nse_ctx* x, int dir, int comp) {
+  const Dims& d = x->d;
+  unsigned char* f = x->lflags.as<unsigned char>();
+  size_t yz = (size_t)d.nx * d.nz, zz = (size_t)d.nx * d.ny, xz = (size_t)d.ny * d.nz;
+  if (dir == 1) return f + comp * yz;
+  if (dir == 2) return f + 4 * yz + comp * zz;
+  return f + 4 * yz + 4 * zz + comp * xz;
+}
+
+static int line_kind(int dir, int comp) {
+  if (dir == 1) return comp == 1 ? LK_UL_V : (comp == 3 ? LK_UL_T : LK_UL_U);
+  return comp == 3 ? LK_CYC_T : LK_CYC_VEL;
+}
+
+static LineArgs line_args(nse_ctx* x, int comp) {
+  const nse_config& c = x->cfg;
+  LineArgs a{};
+  a.beta = comp == 3 ? c.dt / c.Re / c.Sc / 2.0 : c.dt / c.Re / 2.0;
+  a.dt = c.dt; a.eta = c.eta; a.r0 = c.rho_cp; a.l0 = c.thc;
+  a.comp = comp;
+  a.jtop = comp == 1 ? x->d.ny - 1 : x->d.ny;
+  return a;
+}
+
+// after a mask change: flag the lines that touch the mask, give each of them
+// a slot and build its coefficient table (the mask is fixed between changes,
+// so the sweep is reused by every step)
+static bool refresh_line_flags(nse_ctx* x, cudaStream_t s) {
+  if (!x->mask_dirty) return true;
+  const Dims& d = x->d;
+  const double* c1 = x->f[NSE_CELLVALUE].as<double>();
+  for (int comp = 0; comp < 4; ++comp) {
+    int jtop = (comp == 1) ? d.ny - 1 : d.ny;
+    for (int dir = 0; dir < 3; ++dir)
+      launch_line_flags(d, c1, dir, comp, jtop, flags_of(x, dir, comp), s);
+  }
+  size_t nfl = 4 * ((size_t)d.nx * d.nz + (size_t)d.nx * d.ny + (size_t)d.ny * d.nz);
+  std::vector<unsigned char> hf(nfl);
+  if (!NSE_CUDA(cudaMemcpyAsync(hf.data(), x->lflags.p, nfl, cudaMemcpyDeviceToHost, s)) ||
+      !NSE_CUDA(cudaStreamSynchronize(s)))
+    return false;
+  for (int dir = 0; dir < 3; ++dir)
+    for (int comp = 0; comp < 4; ++comp) {
+      LineArgs a = line_args(x, comp);
+      long nlines = dir == 1 ? (long)d.nx * d.nz : (dir == 2 ? (long)d.nx * a.jtop
+                                                             : (long)a.jtop * d.nz);
+      const unsigned char* fl = hf.data() + (flags_of(x, dir, comp) - x->lflags.as<unsigned char>());
+      std::vector<int> slot(nlines), ids;
+      for (long t = 0; t < nlines; ++t) {
+        slot[t] = fl[t] ? (int)ids.size() : -1;
+        if (fl[t]) ids.push_back((int)t);
+      }
+      int kind = line_kind(dir, comp);
+      int n = dir == 0 ? d.nx : (dir == 1 ? d.ny : d.nz);
+      size_t stride = line_table_stride(kind, n);
+      x->nmasked[dir][comp] = (int)ids.size();
+      if (!x->slots[dir][comp].ensure(nlines * sizeof(int)) ||
+          !x->ids[dir][comp].ensure(std::max<size_t>(1, ids.size()) * sizeof(int)) ||
+          !x->mtab[dir][comp].ensure(std::max<size_t>(1, ids.size()) * stride * sizeof(double)))
+        return false;
+      if (!NSE_CUDA(cudaMemcpyAsync(x->slots[dir][comp].p, slot.data(), nlines * sizeof(int),
+                                    cudaMemcpyHostToDevice, s)))
+        return false;
+      if (!ids.empty() &&
+          !NSE_CUDA(cudaMemcpyAsync(x->ids[dir][comp].p, ids.data(), ids.size() * sizeof(int),
+                                    cudaMemcpyHostToDevice, s)))
+        return false;
+      launch_line_tables_masked(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
+                                (int)ids.size(), x->mtab[dir][comp].as<double>(), s);
+      // the host vectors die at the end of this iteration
+      if (!NSE_CUDA(cudaStreamSynchronize(s))) return false;
+    }
+  x->mask_dirty = false;
+  return true;
+}
 
 // phases of one step, in launch order
 enum {
@@ -1050,20 +1187,28 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
                       x->hz.data(), x->hz12.data(), x->hdx.data(), x->hdx12.data(),
                       x->hdy.data(), x->hdy12.data(), x->hdz.data(), x->hdz12.data(), c.xl,
                       c.yl, c.zl, c.y0, c.ystretch);
-  size_t gtot = 2 * (size_t)(nx + 2) + 2 * (size_t)(ny + 2) + 2 * (size_t)(nz + 2);
+  size_t gtot = 4 * (size_t)(nx + 2) + 4 * (size_t)(ny + 2) + 4 * (size_t)(nz + 2);
   bool ok = x->grid.ensure(gtot * sizeof(double));
   if (ok) {
     double* gp = x->grid.as<double>();
     std::vector<double> all;
     for (auto* v : {&x->hdx, &x->hdy, &x->hdz, &x->hdx12, &x->hdy12, &x->hdz12})
       all.insert(all.end(), v->begin(), v->end());
+    for (auto* v : {&x->hdx, &x->hdy, &x->hdz, &x->hdx12, &x->hdy12, &x->hdz12})
+      for (double e : *v) all.push_back(1.0 / e);
     ok = NSE_CUDA(cudaMemcpy(gp, all.data(), gtot * sizeof(double), cudaMemcpyHostToDevice));
     x->g.dx = gp; gp += nx + 2;
     x->g.dy = gp; gp += ny + 2;
     x->g.dz = gp; gp += nz + 2;
     x->g.dx12 = gp; gp += nx + 2;
     x->g.dy12 = gp; gp += ny + 2;
-    x->g.dz12 = gp;
+    x->g.dz12 = gp; gp += nz + 2;
+    x->rg.rdx = gp; gp += nx + 2;
+    x->rg.rdy = gp; gp += ny + 2;
+    x->rg.rdz = gp; gp += nz + 2;
+    x->rg.rdx12 = gp; gp += nx + 2;
+    x->rg.rdy12 = gp; gp += ny + 2;
+    x->rg.rdz12 = gp;
   }
   size_t fb = x->d.ntot * sizeof(double);
   for (int id = 0; ok && id < NSE_NUM_FIELDS; ++id) {
@@ -1075,6 +1220,7 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
   ok = ok && x->mon.ensure((6 + 6 * 592) * sizeof(double));
   ok = ok && x->pb.build(nx, ny, nz, x->hdx.data(), x->hdy.data(), x->hdz.data(),
                          x->hdy12.data(), c.xl, c.zl, x->own);
+  ok = ok && build_line_tables(x);
   if (!ok) {
     nse_ctx_destroy(x);
     return status_or(NSE_ERR_NOMEM);
@@ -1087,9 +1233,16 @@ int nse_ctx_destroy(nse_ctx* x) {
   if (!x) return NSE_OK;
   if (x->own) cudaStreamSynchronize(x->own);
   for (auto& b : x->f) b.release();
-  for (DBuf* b : {&x->grid, &x->ua, &x->va, &x->wa, &x->uT, &x->sa, &x->sb, &x->tmp, &x->mon})
+  for (DBuf* b : {&x->grid, &x->ua, &x->va, &x->wa, &x->uT, &x->sa, &x->sb, &x->tmp, &x->mon,
+                 &x->ltab, &x->lflags})
     b->release();
   x->pb.release();
+  for (int dir = 0; dir < 3; ++dir)
+    for (int comp = 0; comp < 4; ++comp) {
+      x->slots[dir][comp].release();
+      x->ids[dir][comp].release();
+      x->mtab[dir][comp].release();
+    }
   for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
   if (x->own) cudaStreamDestroy(x->own);
   delete x;
@@ -1108,6 +1261,7 @@ int nse_ctx_upload(nse_ctx* x, int id, const double* host) {
     return NSE_ERR_ARG;
   }
   size_t n = (id == NSE_CELLVALUE) ? x->d.ncell : x->d.ntot;
+  if (id == NSE_CELLVALUE) x->mask_dirty = true;
   if (!NSE_CUDA(cudaMemcpyAsync(x->f[id].p, host, n * sizeof(double), cudaMemcpyHostToDevice,
                                 x->stream)))
     return status_or(NSE_ERR_CUDA);
@@ -1230,33 +1384,43 @@ static void ctx_step(nse_ctx* x) {
   launch_set_bc(d, u, v, w, p, T, c.t_bot, c.t_top, 31, s);
   mark(x, PH_RHS);
   // :299-396 explicit terms, AB2, set_bc(u_a,...) and the penalised updates
-  launch_rhs_fused(d, x->g, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA),
-                   F(x, NSE_U_PRE), F(x, NSE_V_PRE), F(x, NSE_W_PRE), F(x, NSE_T_PRE), c1,
-                   ua, va, wa, uT, s);
+  if (c.flags & NSE_FLAG_EXACT)
+    launch_rhs_fused(d, x->g, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA),
+                     F(x, NSE_U_PRE), F(x, NSE_V_PRE), F(x, NSE_W_PRE), F(x, NSE_T_PRE), c1,
+                     ua, va, wa, uT, s);
+  else
+    launch_rhs_fast(d, x->g, x->rg, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA),
+                    F(x, NSE_W_TA), F(x, NSE_U_PRE), F(x, NSE_V_PRE), F(x, NSE_W_PRE),
+                    F(x, NSE_T_PRE), c1, ua, va, wa, uT, s);
   // :397 solve_u_temp: per component y, z, x line solves
   // (timed per direction: all y solves, then z, then x of the three fields;
   // the fields are independent, so this order gives the same values as
   // the reference's per-field y, z, x order)
+  refresh_line_flags(x, s);
+  const bool exact = (c.flags & NSE_FLAG_EXACT) != 0;
+  auto lines = exact ? launch_lines_exact : launch_lines_fast;
   double* fa[3] = {ua, va, wa};
+  auto run = [&](int dir, int comp, double* f, int tab, double ft, double fb) {
+    LineArgs la = line_args(x, comp);
+    la.ft = ft;
+    la.fb = fb;
+    lines(dir, line_kind(dir, comp), d, f, la, x->tab[tab], x->slots[dir][comp].as<int>(),
+          x->mtab[dir][comp].as<double>(), s);
+  };
   mark(x, PH_YVEL);
   for (int comp = 0; comp < 3; ++comp)
-    launch_ysolve_vel(d, x->g, fa[comp], c1, comp, c.Re, c.dt, c.eta, sc, s);
+    run(1, comp, fa[comp], comp == 1 ? TB_Y_V : TB_Y_U, 0.0, 0.0);
   mark(x, PH_ZVEL);
-  for (int comp = 0; comp < 3; ++comp)
-    launch_zsolve_vel(d, x->g, fa[comp], c1, comp, c.Re, c.dt, c.eta, sc, s);
+  for (int comp = 0; comp < 3; ++comp) run(2, comp, fa[comp], TB_Z_V, 0.0, 0.0);
   mark(x, PH_XVEL);
-  for (int comp = 0; comp < 3; ++comp)
-    launch_xsolve_vel(d, x->g, fa[comp], c1, comp, c.Re, c.dt, c.eta, sc, s);
+  for (int comp = 0; comp < 3; ++comp) run(0, comp, fa[comp], TB_X_V, 0.0, 0.0);
   // :419 solve_t: y, x, z
   mark(x, PH_YT);
-  launch_ysolve_T(d, x->g, uT, c1, nullptr, nullptr, c.rho_cp, c.thc, c.Re, c.Sc, c.dt, c.eta,
-                  2.0 * c.t_bot, 2.0 * c.t_top, sc, s);
+  run(1, 3, uT, TB_Y_T, 2.0 * c.t_bot, 2.0 * c.t_top);
   mark(x, PH_XT);
-  launch_xsolve_T(d, x->g, uT, c1, nullptr, nullptr, c.rho_cp, c.thc, c.Re, c.Sc, c.dt, c.eta,
-                  sc, s);
+  run(0, 3, uT, TB_X_T, 0.0, 0.0);
   mark(x, PH_ZT);
-  launch_zsolve_T(d, x->g, uT, c1, nullptr, nullptr, c.rho_cp, c.thc, c.Re, c.Sc, c.dt, c.eta,
-                  sc, s);
+  run(2, 3, uT, TB_Z_T, 0.0, 0.0);
   // :429-437 T = u_T (interior); the ghosts are rewritten by the next set_bc
   std::swap(x->f[NSE_T], x->uT);
   T = F(x, NSE_T);
@@ -1297,6 +1461,7 @@ int nse_levelset(nse_ctx* x, const double* phi0, double* phi_out, int nnn, doubl
   // the ping-pong buffer
   if (!NSE_CUDA(cudaMemcpyAsync(x->tmp.p, phi0, d.ntot * sizeof(double), cudaMemcpyHostToDevice, s)))
     return status_or(NSE_ERR_CUDA);
+  x->mask_dirty = true;
   if (!run_levelset(d, x->g, x->tmp.as<double>(), F(x, NSE_PHI), x->ua.as<double>(),
                     F(x, NSE_CELLVALUE), nnn, dtau, width, s))
     return status_or(NSE_ERR_CUDA);

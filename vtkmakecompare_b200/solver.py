@@ -17,6 +17,7 @@ FP64, MIXED = 0, 1
 PHASES = ("set_bc", "rhs", "y_vel", "z_vel", "x_vel", "y_T", "x_T", "z_T", "set_bc_temp",
           "fft_x_fwd", "fft_z_fwd", "spn", "fft_z_inv", "fft_x_inv", "phibc", "correct")
 FLAG_CHECK_FINITE = 1
+FLAG_EXACT = 4
 
 
 class Config(C.Structure):
@@ -179,4 +180,5 @@ class Context:
                 "T_int": out[4], "nonfinite": int(out[5])}
 
 
-__all__ = ["Config", "Context", "FIELDS", "FP64", "MIXED", "FLAG_CHECK_FINITE", "NseError"]
+__all__ = ["Config", "Context", "FIELDS", "FP64", "MIXED", "FLAG_CHECK_FINITE", "FLAG_EXACT",
+           "NseError"]
