@@ -308,7 +308,8 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
     return;
   }
   if (!do_spn) return;
-  // SPN mkp.f:239-254 + CTRIDIAG tridiag.f:47-56
+  // SPN mkp.f:239-254 + CTRIDIAG tridiag.f:47-56.  The right-hand side is read
+  // in batches of SPN_BATCH planes ahead of the recurrence so the loads overlap.
   const double kxz = KXZ[kx + (long)H * kz];
   double* s3 = sc + kx + sck * kz;
   const int NN = ny;
@@ -316,26 +317,45 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
   if (NN == 1) { a2 = a2 + AC1[0]; a2 = a2 + AC3[0]; }
   else a2 = a2 + AC1[0];  // AA(1,2) += AA(1,1)
   double2 b = B[0];
-  for (int I = 1; I <= NN - 1; ++I) {
-    double a3 = (I == NN) ? 0.0 : AC3[I - 1];
-    a3 = a3 / a2;
-    b = make_double2(b.x / a2, b.y / a2);
-    B[sv.sj * (I - 1)] = b;
-    s3[scj * (I - 1)] = a3;
-    double a1n = AC1[I];
-    double a2n = AC2[I] - kxz;
-    if (I + 1 == NN) a2n = a2n + AC3[NN - 1];  // AA(NY,2) += AA(NY,3)
-    double2 bn = B[sv.sj * I];
-    a2 = a2n - a1n * a3;
-    b = make_double2(bn.x - a1n * b.x, bn.y - a1n * b.y);
+  constexpr int SPN_BATCH = 8;
+  for (int I0 = 1; I0 <= NN - 1; I0 += SPN_BATCH) {
+    double2 nb[SPN_BATCH];
+#pragma unroll
+    for (int q = 0; q < SPN_BATCH; ++q)
+      if (I0 + q <= NN - 1) nb[q] = B[sv.sj * (I0 + q)];
+#pragma unroll
+    for (int q = 0; q < SPN_BATCH; ++q) {
+      int I = I0 + q;
+      if (I > NN - 1) break;
+      double a3 = AC3[I - 1] / a2;
+      b = make_double2(b.x / a2, b.y / a2);
+      B[sv.sj * (I - 1)] = b;
+      s3[scj * (I - 1)] = a3;
+      double a1n = AC1[I];
+      double a2n = AC2[I] - kxz;
+      if (I + 1 == NN) a2n = a2n + AC3[NN - 1];  // AA(NY,2) += AA(NY,3)
+      a2 = a2n - a1n * a3;
+      b = make_double2(nb[q].x - a1n * b.x, nb[q].y - a1n * b.y);
+    }
   }
   b = make_double2(b.x / a2, b.y / a2);
   B[sv.sj * (NN - 1)] = b;
-  for (int I = NN - 1; I >= 1; --I) {
-    double2 bi = B[sv.sj * (I - 1)];
-    double a3 = s3[scj * (I - 1)];
-    b = make_double2(bi.x - a3 * b.x, bi.y - a3 * b.y);
-    B[sv.sj * (I - 1)] = b;
+  for (int I0 = NN - 1; I0 >= 1; I0 -= SPN_BATCH) {
+    double2 bi[SPN_BATCH];
+    double a3v[SPN_BATCH];
+#pragma unroll
+    for (int q = 0; q < SPN_BATCH; ++q)
+      if (I0 - q >= 1) {
+        bi[q] = B[sv.sj * (I0 - q - 1)];
+        a3v[q] = s3[scj * (I0 - q - 1)];
+      }
+#pragma unroll
+    for (int q = 0; q < SPN_BATCH; ++q) {
+      int I = I0 - q;
+      if (I < 1) break;
+      b = make_double2(bi[q].x - a3v[q] * b.x, bi[q].y - a3v[q] * b.y);
+      B[sv.sj * (I - 1)] = b;
+    }
   }
 }
 
@@ -429,9 +449,9 @@ void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
 }
 
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s) {
-  dim3 grid((pp.H + 31) / 32, pp.nz);
+  dim3 grid((pp.H + 63) / 64, pp.nz);
   count_launch();
-  k_spn<<<grid, 32, 0, s>>>(pp.H, pp.ny, pp.nz, spec_internal(pp), pp.scr, pp.Hp,
+  k_spn<<<grid, 64, 0, s>>>(pp.H, pp.ny, pp.nz, spec_internal(pp), pp.scr, pp.Hp,
                             (long)pp.Hp * pp.ny, pp.AC, pp.KXZ, do_spn ? 1 : 0,
                             do_sp0b ? 1 : 0);
 }

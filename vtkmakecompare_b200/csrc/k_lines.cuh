@@ -174,6 +174,10 @@ __global__ void __launch_bounds__(32) k_lines(Dims d, double* __restrict__ f, Li
                              : (long)(l0 + lane) + (long)d.nx * (j - 1);
     const int slot = slots[lineid];
     const int L = n + 2;
+    // the recurrences run on registers in batches of LB rows: every load of
+    // a batch (shared-memory rows and table entries) is issued before the
+    // batch's dependent chain starts
+    constexpr int LB = 8;
     if (KIND <= LK_UL_T) {
       // UL elimination of implicit_uy/vy/Ty (nse_dominik.f:1549-1570) with the
       // coefficient sweep of this line from its table
@@ -183,19 +187,42 @@ __global__ void __launch_bounds__(32) k_lines(Dims d, double* __restrict__ f, Li
         Tl = b; Tdm = b + L; Trdm = b + 2 * L; Tup = b + 3 * L;
       }
       double ut = a.fb;
-#pragma unroll 4
-      for (int r = m; r >= 1; --r) {
-        double upr = EXACT ? ut / __ldg(Tdm + r) : ut * __ldg(Trdm + r);
-        double rhs = (r - 1 == 0) ? a.ft : s[r - 1];
-        s[r] = upr;
-        ut = rhs - __ldg(Tup + r - 1) * upr;
+      s[0] = a.ft;  // the boundary rhs of row 0, read like the other rows
+      for (int r0 = m; r0 >= 1; r0 -= LB) {
+        double dv[LB], uv[LB], rv[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 - q;
+          if (r >= 1) {
+            dv[q] = EXACT ? __ldg(Tdm + r) : __ldg(Trdm + r);
+            uv[q] = __ldg(Tup + r - 1);
+            rv[q] = s[r - 1];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 - q;
+          if (r >= 1) {
+            double upr = EXACT ? ut / dv[q] : ut * dv[q];
+            s[r] = upr;
+            ut = rv[q] - uv[q] * upr;
+          }
+        }
       }
       double x = EXACT ? ut / __ldg(Tdm) : ut * __ldg(Trdm);
       s[0] = x;
-#pragma unroll 4
-      for (int r = 1; r <= m; ++r) {
-        x = s[r] - __ldg(Tl + r) * x;
-        s[r] = x;
+      for (int r0 = 1; r0 <= m; r0 += LB) {
+        double lv[LB], sv[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 + q;
+          if (r <= m) { lv[q] = __ldg(Tl + r); sv[q] = s[r]; }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 + q;
+          if (r <= m) { x = sv[q] - lv[q] * x; s[r] = x; }
+        }
       }
     } else {
       // cyclic (periodic_implicit.f:67-93) on rows 0..n+1 with ft = fb = 0
@@ -209,25 +236,45 @@ __global__ void __launch_bounds__(32) k_lines(Dims d, double* __restrict__ f, Li
       }
       double x = EXACT ? 0.0 / __ldg(Tb) : 0.0 * __ldg(Trb);
       s[0] = x;
-#pragma unroll 4
-      for (int r = 1; r <= n; ++r) {
-        double t = s[r] - __ldg(Ta + r) * x;
-        x = EXACT ? t / __ldg(Tb + r) : t * __ldg(Trb + r);
-        s[r] = x;
-      }
-      {
-        double t = 0.0 - 1.0 * x;
-        x = EXACT ? t / __ldg(Tb + n + 1) : t * __ldg(Trb + n + 1);
-        s[n + 1] = x;
+      s[n + 1] = 0.0;  // rhs of row n+1 (fb)
+      // forward sweep over rows 1..n+1 (row n+1 has a = 1)
+      for (int r0 = 1; r0 <= n + 1; r0 += LB) {
+        double av[LB], bv[LB], sv[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 + q;
+          if (r <= n + 1) {
+            av[q] = (r == n + 1) ? 1.0 : __ldg(Ta + r);
+            bv[q] = EXACT ? __ldg(Tb + r) : __ldg(Trb + r);
+            sv[q] = s[r];
+          }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 + q;
+          if (r <= n + 1) {
+            double t = sv[q] - av[q] * x;
+            x = EXACT ? t / bv[q] : t * bv[q];
+            s[r] = x;
+          }
+        }
       }
       double xn1 = x;
-#pragma unroll 4
-      for (int r = n; r >= 0; --r) {
-        x = s[r] - __ldg(Tg + r + 1) * x;
-        s[r] = x;
+      for (int r0 = n; r0 >= 0; r0 -= LB) {
+        double gv[LB], sv[LB];
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 - q;
+          if (r >= 0) { gv[q] = __ldg(Tg + r + 1); sv[q] = s[r]; }
+        }
+#pragma unroll
+        for (int q = 0; q < LB; ++q) {
+          int r = r0 - q;
+          if (r >= 0) { x = sv[q] - gv[q] * x; s[r] = x; }
+        }
       }
       double fact = EXACT ? (x + beta * xn1 / gamma) / den : (x + beta * xn1 / gamma) * (1.0 / den);
-#pragma unroll 4
+#pragma unroll 8
       for (int r = 0; r <= n + 1; ++r) s[r] = s[r] - fact * __ldg(Tz + r);
     }
   }

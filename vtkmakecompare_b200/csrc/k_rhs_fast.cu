@@ -12,14 +12,69 @@
 // and its face averages vanish the immersed-boundary term is an exact zero,
 // so u_ta is not read and the implicit penalisation is the identity.
 // A CTA covers 32 x 8 cells of an (x,y) tile and marches over KCHUNK planes
-// in z so the k-1, k, k+1 planes are re-read from L1.
+// in z; the halo planes of u, v, w, T sit in a shared-memory ring that is
+// filled one plane ahead with asynchronous copies (cp.async) while the
+// current plane is computed; the ring holds five planes (k-1, k, k+1 in use,
+// k+2 and k+3 in flight) of u, v, w, T and the mask with a one-cell halo and
+// of the four AB2 histories, so every input is read from HBM about once and
+// two planes of loads are always outstanding.
 #include "common.cuh"
 
 namespace nse {
 
 #define LD(p, i) __ldg((p) + (i))
 
-constexpr int KCHUNK = 8;
+constexpr int KCHUNK = 16;           // z planes per CTA
+constexpr int TXW = 32, TYW = 8;     // interior tile of a CTA (x, y)
+constexpr int SXW = TXW + 2, SYW = TYW + 2;
+constexpr int PLANE = SXW * SYW;     // one halo plane of one field
+constexpr int TILE = TXW * TYW;      // one interior plane of one field
+// a ring slot holds plane K of: u, v, w, T, c1 (halo) and the four AB2
+// histories (interior)
+constexpr int SLOT = 5 * PLANE + 4 * TILE;
+constexpr int NSLOT = 5;             // k-1, k, k+1 in use, k+2 and k+3 in flight
+
+__device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+__device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
+template <int N>
+__device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
+
+// plane K into ring slot K mod NSLOT (one commit group, possibly empty)
+__device__ __forceinline__ void load_plane(double* sm, const Dims& d, int i0, int j0, int K,
+                                           int kmax, const double* U, const double* V,
+                                           const double* W, const double* T, const double* C1,
+                                           const double* UP, const double* VP,
+                                           const double* WP, const double* TP) {
+  if (K <= kmax) {
+    double* slot = sm + (K % NSLOT) * SLOT;
+    const int tid = threadIdx.y * TXW + threadIdx.x;
+    for (int e = tid; e < PLANE; e += TILE) {
+      int tx = e % SXW, ty = e / SXW;
+      int i = i0 - 1 + tx, j = j0 - 1 + ty;
+      if (i > d.nx + 1 || j > d.ny + 1) continue;
+      long c = d.P(i, j, K);
+      cp_async8(slot + e, U + c);
+      cp_async8(slot + PLANE + e, V + c);
+      cp_async8(slot + 2 * PLANE + e, W + c);
+      cp_async8(slot + 3 * PLANE + e, T + c);
+      if (i >= 1 && i <= d.nx && j >= 1 && j <= d.ny && K >= 1 && K <= d.nz)
+        cp_async8(slot + 4 * PLANE + e, C1 + d.C(i, j, K));
+    }
+    int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    if (i <= d.nx && j <= d.ny && K >= 1 && K <= d.nz) {
+      long c = d.P(i, j, K);
+      double* h = slot + 5 * PLANE + tid;
+      cp_async8(h, UP + c);
+      cp_async8(h + TILE, VP + c);
+      cp_async8(h + 2 * TILE, WP + c);
+      cp_async8(h + 3 * TILE, TP + c);
+    }
+  }
+  cp_async_commit();
+}
 
 __global__ void __launch_bounds__(256, 2) k_rhs_fast(
     Dims d, GridDev g, GridRcp rg, StepParams sp, const double* __restrict__ U,
@@ -29,48 +84,68 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
     double* __restrict__ W_PRE, double* __restrict__ T_PRE, const double* __restrict__ C1,
     double* __restrict__ U_A, double* __restrict__ V_A, double* __restrict__ W_A,
     double* __restrict__ U_T) {
-  const int I = 1 + blockIdx.x * 32 + threadIdx.x;
-  const int J = 1 + blockIdx.y * 8 + threadIdx.y;
-  if (I > d.nx || J > d.ny) return;
+  extern __shared__ double sm[];
+  const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
+  const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
+  const bool valid = (I <= d.nx) && (J <= d.ny);
   const int k0 = 1 + blockIdx.z * KCHUNK;
   const int k1 = min(d.nz, k0 + KCHUNK - 1);
+  const int kmax = k1 + 1;  // last plane any iteration reads
+  // prologue: planes k0-1 .. k0+2 (k0+2 stays in flight)
+  for (int q = -1; q <= 2; ++q)
+    load_plane(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
+  cp_async_wait<1>();
+  __syncthreads();
   const double DT = sp.dt;
   const double a1 = (sp.l == 1) ? 1.0 : 1.5, a2 = (sp.l == 1) ? 0.0 : -0.5;
   const double kd = DT / sp.Re * 0.5;
   const double r0 = sp.rho_cp, rr0 = 1.0 / sp.rho_cp, l0 = sp.thc;
   const double kT = 0.5 / sp.Re / sp.Sc / sp.rho_cp * DT;
-  // x and y metrics of this column
-  const double dx = LD(g.dx, I), dxp = LD(g.dx, I + 1), dxm = LD(g.dx, I - 1);
-  const double rx = LD(rg.rdx, I), rxp = LD(rg.rdx, I + 1);
-  const double rx12 = LD(rg.rdx12, I), rx12m = LD(rg.rdx12, I - 1);
-  const double dy = LD(g.dy, J), dyp = LD(g.dy, J + 1), dym = LD(g.dy, J - 1);
-  const double ry = LD(rg.rdy, J), ryp = LD(rg.rdy, J + 1);
-  const double ry12 = LD(rg.rdy12, J), ry12m = LD(rg.rdy12, J - 1);
-  const long sx = d.sx, sy = d.sy;
-  const long nxny = (long)d.nx * d.ny;
+  double dx = 0, dxp = 0, dxm = 0, rx = 0, rxp = 0, rx12 = 0, rx12m = 0;
+  double dy = 0, dyp = 0, dym = 0, ry = 0, ryp = 0, ry12 = 0, ry12m = 0;
+  if (valid) {
+    dx = LD(g.dx, I); dxp = LD(g.dx, I + 1); dxm = LD(g.dx, I - 1);
+    rx = LD(rg.rdx, I); rxp = LD(rg.rdx, I + 1);
+    rx12 = LD(rg.rdx12, I); rx12m = LD(rg.rdx12, I - 1);
+    dy = LD(g.dy, J); dyp = LD(g.dy, J + 1); dym = LD(g.dy, J - 1);
+    ry = LD(rg.rdy, J); ryp = LD(rg.rdy, J + 1);
+    ry12 = LD(rg.rdy12, J); ry12m = LD(rg.rdy12, J - 1);
+  }
+  const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;  // this cell in a halo plane
+  const int t0 = threadIdx.y * TXW + threadIdx.x;            // this cell in a tile
   for (int K = k0; K <= k1; ++K) {
-    const long c = d.P(I, J, K);
-    const double dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
-    const double rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
-    const double rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
-    // neighbourhood
-    const double uc = LD(U, c), uxp = LD(U, c + 1), uxm = LD(U, c - 1), uyp = LD(U, c + sx),
-                 uym = LD(U, c - sx), uzp = LD(U, c + sy), uzm = LD(U, c - sy),
-                 uxmyp = LD(U, c - 1 + sx), uxmzp = LD(U, c - 1 + sy);
-    const double vc = LD(V, c), vxp = LD(V, c + 1), vxm = LD(V, c - 1), vyp = LD(V, c + sx),
-                 vym = LD(V, c - sx), vzp = LD(V, c + sy), vzm = LD(V, c - sy),
-                 vxpym = LD(V, c + 1 - sx), vymzp = LD(V, c - sx + sy);
-    const double wc = LD(W, c), wxp = LD(W, c + 1), wxm = LD(W, c - 1), wyp = LD(W, c + sx),
-                 wym = LD(W, c - sx), wzp = LD(W, c + sy), wzm = LD(W, c - sy),
-                 wxpzm = LD(W, c + 1 - sy), wypzm = LD(W, c + sx - sy);
-    const double tc = LD(T, c), txp = LD(T, c + 1), txm = LD(T, c - 1), typ = LD(T, c + sx),
-                 tym = LD(T, c - sx), tzp = LD(T, c + sy), tzm = LD(T, c - sy);
-    // masks (set_immersed_boundary :1037-1080)
-    const long m = d.C(I, J, K);
-    const double cc1 = LD(C1, m);
-    const double c2 = (I < d.nx) ? (cc1 + LD(C1, m + 1)) * 0.50 : cc1;
-    const double c3 = (J < d.ny) ? (cc1 + LD(C1, m + d.nx)) * 0.50 : cc1;
-    const double c4 = (K < d.nz) ? (cc1 + LD(C1, m + nxny)) * 0.50 : cc1;
+    load_plane(sm, d, i0, j0, K + 3, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
+    if (valid) {
+      const double* pm = sm + ((K - 1) % NSLOT) * SLOT;
+      const double* pc = sm + (K % NSLOT) * SLOT;
+      const double* pp = sm + ((K + 1) % NSLOT) * SLOT;
+      const long c = d.P(I, J, K);
+      const double dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
+      const double rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
+      const double rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
+      // neighbourhood from shared memory (field f at offset f*PLANE)
+#define AT(pl, f, dxo, dyo) (pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
+      const double uc = AT(pc, 0, 0, 0), uxp = AT(pc, 0, 1, 0), uxm = AT(pc, 0, -1, 0),
+                   uyp = AT(pc, 0, 0, 1), uym = AT(pc, 0, 0, -1), uzp = AT(pp, 0, 0, 0),
+                   uzm = AT(pm, 0, 0, 0), uxmyp = AT(pc, 0, -1, 1), uxmzp = AT(pp, 0, -1, 0);
+      const double vc = AT(pc, 1, 0, 0), vxp = AT(pc, 1, 1, 0), vxm = AT(pc, 1, -1, 0),
+                   vyp = AT(pc, 1, 0, 1), vym = AT(pc, 1, 0, -1), vzp = AT(pp, 1, 0, 0),
+                   vzm = AT(pm, 1, 0, 0), vxpym = AT(pc, 1, 1, -1), vymzp = AT(pp, 1, 0, -1);
+      const double wc = AT(pc, 2, 0, 0), wxp = AT(pc, 2, 1, 0), wxm = AT(pc, 2, -1, 0),
+                   wyp = AT(pc, 2, 0, 1), wym = AT(pc, 2, 0, -1), wzp = AT(pp, 2, 0, 0),
+                   wzm = AT(pm, 2, 0, 0), wxpzm = AT(pm, 2, 1, 0), wypzm = AT(pm, 2, 0, 1);
+      const double tc = AT(pc, 3, 0, 0), txp = AT(pc, 3, 1, 0), txm = AT(pc, 3, -1, 0),
+                   typ = AT(pc, 3, 0, 1), tym = AT(pc, 3, 0, -1), tzp = AT(pp, 3, 0, 0),
+                   tzm = AT(pm, 3, 0, 0);
+      // masks (set_immersed_boundary :1037-1080) and AB2 histories
+      const double cc1 = AT(pc, 4, 0, 0);
+      const double c2 = (I < d.nx) ? (cc1 + AT(pc, 4, 1, 0)) * 0.50 : cc1;
+      const double c3 = (J < d.ny) ? (cc1 + AT(pc, 4, 0, 1)) * 0.50 : cc1;
+      const double c4 = (K < d.nz) ? (cc1 + AT(pp, 4, 0, 0)) * 0.50 : cc1;
+#undef AT
+      const double* hist = pc + 5 * PLANE + t0;
+      const double upre = hist[0], vpre = hist[TILE], wpre = hist[2 * TILE],
+                   tpre = hist[3 * TILE];
     const bool solid = (c2 != 0.0) || (c3 != 0.0) || (c4 != 0.0) || (cc1 != 0.0);
     // u
     {
@@ -84,7 +159,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
       double L = ((uxp - uc) * rxp - (uc - uxm) * rx) * rx12 +
                  ((uyp - uc) * ry12 - (uc - uym) * ry12m) * ry +
                  ((uzp - uc) * rz12 - (uc - uzm) * rz12m) * rz;
-      double ua = a1 * uv + a2 * U_PRE[c] + kd * L;
+      double ua = a1 * uv + a2 * upre + kd * L;
       U_PRE[c] = uv;
       if (solid && c2 != 0.0) {
         ua += sp.eta * c2 * LD(U_TA, c) * DT;
@@ -105,7 +180,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
       double L = ((vxp - vc) * rx12 - (vc - vxm) * rx12m) * rx +
                  ((vyp - vc) * ryp - (vc - vym) * ry) * ry12 +
                  ((vzp - vc) * rz12 - (vc - vzm) * rz12m) * rz;
-      double va = a1 * vv + a2 * V_PRE[c] + kd * L;
+      double va = a1 * vv + a2 * vpre + kd * L;
       V_PRE[c] = vv;
       if (solid && c3 != 0.0) va += sp.eta * c3 * LD(V_TA, c) * DT;
       if (J == d.ny) va = 0.0;  // set_bc(u_a,v_a,...) zeroes v_a(:,ny,:)
@@ -124,7 +199,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
       double L = ((wxp - wc) * rx12 - (wc - wxm) * rx12m) * rx +
                  ((wyp - wc) * ry12 - (wc - wym) * ry12m) * ry +
                  ((wzp - wc) * rzp - (wc - wzm) * rz) * rz12;
-      double wa = a1 * wv + a2 * W_PRE[c] + kd * L;
+      double wa = a1 * wv + a2 * wpre + kd * L;
       W_PRE[c] = wv;
       if (solid && c4 != 0.0) {
         wa += sp.eta * c4 * LD(W_TA, c) * DT;
@@ -148,7 +223,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
       double D1 = (l0 * (txp - tc) * rx12 - l0 * (tc - txm) * rx12m) * rx;
       double D2 = (l0 * (typ - tc) * ry12 - l0 * (tc - tym) * ry12m) * ry;
       double D3 = (l0 * (tzp - tc) * rz12 - l0 * (tc - tzm) * rz12m) * rz;
-      double ut = a1 * vt + a2 * T_PRE[c] + kT * (D1 + D2 + D3);
+      double ut = a1 * vt + a2 * tpre + kT * (D1 + D2 + D3);
       T_PRE[c] = vt;
       if (cc1 != 0.0) {
         double pen = sp.eta * cc1 * DT;
@@ -157,6 +232,9 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
         U_T[c] = tc + ut;
       }
     }
+    }  // valid
+    cp_async_wait<1>();
+    __syncthreads();
   }
 }
 
@@ -166,11 +244,228 @@ void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
                      double* u_pre, double* v_pre, double* w_pre, double* T_pre,
                      const double* c1, double* u_a, double* v_a, double* w_a, double* u_T,
                      cudaStream_t s) {
-  dim3 block(32, 8, 1);
-  dim3 grid((d.nx + 31) / 32, (d.ny + 7) / 8, (d.nz + KCHUNK - 1) / KCHUNK);
+  dim3 block(TXW, TYW, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
+  size_t smem = (size_t)NSLOT * SLOT * sizeof(double);
+  cudaFuncSetAttribute((const void*)k_rhs_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
   count_launch();
-  k_rhs_fast<<<grid, block, 0, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre,
+  k_rhs_fast<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre,
                                     w_pre, T_pre, c1, u_a, v_a, w_a, u_T);
+}
+
+}  // namespace nse
+
+namespace nse {
+
+// mkp.f:141-217 (gradient, correction, pressure, u_ep2, u_ta, divu) in the
+// fast form: reciprocal metrics and FMA.  One thread per cell of 0..n.
+__global__ void __launch_bounds__(256) k_correct_fast(
+    Dims d, GridRcp rg, const double* __restrict__ PHI, const double* __restrict__ ut,
+    const double* __restrict__ vt, const double* __restrict__ wt, double* __restrict__ p,
+    double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+    double* __restrict__ u_ta, double* __restrict__ v_ta, double* __restrict__ w_ta,
+    double* __restrict__ u_ep2, double* __restrict__ v_ep2, double* __restrict__ w_ep2,
+    double* __restrict__ divu, double dt) {
+  int i = blockIdx.x * blockDim.x + threadIdx.x;
+  int j = blockIdx.y * blockDim.y + threadIdx.y;
+  int k = blockIdx.z;
+  if (i > d.nx || j > d.ny || k > d.nz) return;
+  long c = d.P(i, j, k);
+  double ph = LD(PHI, c);
+  double phx = LD(PHI, c + 1), phy = LD(PHI, c + d.sx), phz = LD(PHI, c + d.sy);
+  double gx = (phx - ph) * LD(rg.rdx12, i);
+  double gy = (phy - ph) * LD(rg.rdy12, j);
+  double gz = (phz - ph) * LD(rg.rdz12, k);
+  double un = LD(ut, c) - dt * gx;
+  double vn = LD(vt, c) - dt * gy;
+  double wn = LD(wt, c) - dt * gz;
+  u[c] = un;
+  v[c] = vn;
+  w[c] = wn;
+  if (i >= 1 && j >= 1 && k >= 1) {
+    p[c] = ph;
+    double pxp = (i < d.nx) ? phx : p[c + 1];
+    double pyp = (j < d.ny) ? phy : p[c + d.sx];
+    double pzp = (k < d.nz) ? phz : p[c + d.sy];
+    double ux = u_ta[c], vx = v_ta[c], wx = w_ta[c];
+    u_ep2[c] = ux - dt * (pxp - ph) * LD(rg.rdx12, i);
+    v_ep2[c] = vx - dt * (pyp - ph) * LD(rg.rdy12, j);
+    w_ep2[c] = wx - dt * (pzp - ph) * LD(rg.rdz12, k);
+    double um = LD(ut, c - 1) - dt * ((ph - LD(PHI, c - 1)) * LD(rg.rdx12, i - 1));
+    double vm = LD(vt, c - d.sx) - dt * ((ph - LD(PHI, c - d.sx)) * LD(rg.rdy12, j - 1));
+    double wm = LD(wt, c - d.sy) - dt * ((ph - LD(PHI, c - d.sy)) * LD(rg.rdz12, k - 1));
+    divu[c] = (un - um) * LD(rg.rdx, i) + (vn - vm) * LD(rg.rdy, j) + (wn - wm) * LD(rg.rdz, k);
+  }
+  u_ta[c] = dt * gx;
+  v_ta[c] = dt * gy;
+  w_ta[c] = dt * gz;
+}
+
+void launch_correct_fast(const Dims& d, const GridRcp& rg, const double* PHI, const double* ut,
+                         const double* vt, const double* wt, double* p, double* u, double* v,
+                         double* w, double* u_ta, double* v_ta, double* w_ta, double* u_ep2,
+                         double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s) {
+  dim3 block(64, 4, 1);
+  dim3 grid((d.nx + 1 + 63) / 64, (d.ny + 1 + 3) / 4, d.nz + 1);
+  count_launch();
+  k_correct_fast<<<grid, block, 0, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta,
+                                        u_ep2, v_ep2, w_ep2, divu, dt);
+}
+
+}  // namespace nse
+
+namespace nse {
+
+// ----------------------------------------------------- pipelined correction
+// mkp.f:141-217 for interior cells (1..n in every direction), marching in z
+// like k_rhs_fast: a ring of planes of phi, u*, v*, w* (one-cell halo) and the
+// old u_ta, v_ta, w_ta (interior) filled two planes ahead by cp.async.
+constexpr int CSLOT = 4 * PLANE + 3 * TILE;
+
+__device__ __forceinline__ void load_plane_c(double* sm, const Dims& d, int i0, int j0, int K,
+                                             int kmax, const double* PHI, const double* UT,
+                                             const double* VT, const double* WT,
+                                             const double* UA, const double* VA,
+                                             const double* WA) {
+  if (K <= kmax) {
+    double* slot = sm + (K % NSLOT) * CSLOT;
+    const int tid = threadIdx.y * TXW + threadIdx.x;
+    for (int e = tid; e < PLANE; e += TILE) {
+      int tx = e % SXW, ty = e / SXW;
+      int i = i0 - 1 + tx, j = j0 - 1 + ty;
+      if (i > d.nx + 1 || j > d.ny + 1) continue;
+      long c = d.P(i, j, K);
+      cp_async8(slot + e, PHI + c);
+      cp_async8(slot + PLANE + e, UT + c);
+      cp_async8(slot + 2 * PLANE + e, VT + c);
+      cp_async8(slot + 3 * PLANE + e, WT + c);
+    }
+    int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    if (i <= d.nx && j <= d.ny && K >= 1 && K <= d.nz) {
+      long c = d.P(i, j, K);
+      double* h = slot + 4 * PLANE + tid;
+      cp_async8(h, UA + c);
+      cp_async8(h + TILE, VA + c);
+      cp_async8(h + 2 * TILE, WA + c);
+    }
+  }
+  cp_async_commit();
+}
+
+__global__ void __launch_bounds__(256, 2) k_correct_pipe(
+    Dims d, GridRcp rg, const double* __restrict__ PHI, const double* __restrict__ UT,
+    const double* __restrict__ VT, const double* __restrict__ WT, double* __restrict__ p,
+    double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
+    double* __restrict__ u_ta, double* __restrict__ v_ta, double* __restrict__ w_ta,
+    double* __restrict__ u_ep2, double* __restrict__ v_ep2, double* __restrict__ w_ep2,
+    double* __restrict__ divu, double dt) {
+  extern __shared__ double sm[];
+  const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
+  const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
+  const bool valid = (I <= d.nx) && (J <= d.ny);
+  const int k0 = 1 + blockIdx.z * KCHUNK;
+  const int k1 = min(d.nz, k0 + KCHUNK - 1);
+  const int kmax = k1 + 1;
+  for (int q = -1; q <= 2; ++q)
+    load_plane_c(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+  cp_async_wait<1>();
+  __syncthreads();
+  double rx = 0, rx12 = 0, rx12m = 0, ry = 0, ry12 = 0, ry12m = 0;
+  if (valid) {
+    rx = LD(rg.rdx, I); rx12 = LD(rg.rdx12, I); rx12m = LD(rg.rdx12, I - 1);
+    ry = LD(rg.rdy, J); ry12 = LD(rg.rdy12, J); ry12m = LD(rg.rdy12, J - 1);
+  }
+  const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;
+  const int t0 = threadIdx.y * TXW + threadIdx.x;
+  for (int K = k0; K <= k1; ++K) {
+    load_plane_c(sm, d, i0, j0, K + 3, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    if (valid) {
+      const double* pm = sm + ((K - 1) % NSLOT) * CSLOT;
+      const double* pc = sm + (K % NSLOT) * CSLOT;
+      const double* pp = sm + ((K + 1) % NSLOT) * CSLOT;
+#define AT(pl, f, dxo, dyo) (pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
+      const long c = d.P(I, J, K);
+      const double rz = LD(rg.rdz, K), rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
+      const double ph = AT(pc, 0, 0, 0), phx = AT(pc, 0, 1, 0), phy = AT(pc, 0, 0, 1),
+                   phz = AT(pp, 0, 0, 0), phxm = AT(pc, 0, -1, 0), phym = AT(pc, 0, 0, -1),
+                   phzm = AT(pm, 0, 0, 0);
+      const double gx = (phx - ph) * rx12, gy = (phy - ph) * ry12, gz = (phz - ph) * rz12;
+      const double un = AT(pc, 1, 0, 0) - dt * gx;
+      const double vn = AT(pc, 2, 0, 0) - dt * gy;
+      const double wn = AT(pc, 3, 0, 0) - dt * gz;
+      const double um = AT(pc, 1, -1, 0) - dt * ((ph - phxm) * rx12m);
+      const double vm = AT(pc, 2, 0, -1) - dt * ((ph - phym) * ry12m);
+      const double wm = AT(pm, 3, 0, 0) - dt * ((ph - phzm) * rz12m);
+#undef AT
+      const double* old = pc + 4 * PLANE + t0;
+      u[c] = un;
+      v[c] = vn;
+      w[c] = wn;
+      p[c] = ph;
+      const double pxp = (I < d.nx) ? phx : p[c + 1];
+      const double pyp = (J < d.ny) ? phy : p[c + d.sx];
+      const double pzp = (K < d.nz) ? phz : p[c + d.sy];
+      u_ep2[c] = old[0] - dt * (pxp - ph) * rx12;
+      v_ep2[c] = old[TILE] - dt * (pyp - ph) * ry12;
+      w_ep2[c] = old[2 * TILE] - dt * (pzp - ph) * rz12;
+      divu[c] = (un - um) * rx + (vn - vm) * ry + (wn - wm) * rz;
+      u_ta[c] = dt * gx;
+      v_ta[c] = dt * gy;
+      w_ta[c] = dt * gz;
+    }
+    cp_async_wait<1>();
+    __syncthreads();
+  }
+}
+
+// the same correction on the cells of 0..n with i, j or k equal to 0 (the
+// ghost faces MKP also writes)
+__global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ PHI,
+                                const double* __restrict__ ut, const double* __restrict__ vt,
+                                const double* __restrict__ wt, double* __restrict__ u,
+                                double* __restrict__ v, double* __restrict__ w,
+                                double* __restrict__ u_ta, double* __restrict__ v_ta,
+                                double* __restrict__ w_ta, double dt) {
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  long nA = (long)(ny + 1) * (nz + 1);  // i = 0
+  long nB = (long)nx * (nz + 1);        // j = 0, i >= 1
+  long nC = (long)nx * ny;              // k = 0, i,j >= 1
+  long t = (long)blockIdx.x * blockDim.x + threadIdx.x;
+  int i, j, k;
+  if (t < nA) { i = 0; j = (int)(t % (ny + 1)); k = (int)(t / (ny + 1)); }
+  else if (t < nA + nB) { long r = t - nA; j = 0; i = 1 + (int)(r % nx); k = (int)(r / nx); }
+  else if (t < nA + nB + nC) { long r = t - nA - nB; k = 0; i = 1 + (int)(r % nx); j = 1 + (int)(r / nx); }
+  else return;
+  long c = d.P(i, j, k);
+  double ph = LD(PHI, c);
+  double gx = (LD(PHI, c + 1) - ph) * LD(rg.rdx12, i);
+  double gy = (LD(PHI, c + d.sx) - ph) * LD(rg.rdy12, j);
+  double gz = (LD(PHI, c + d.sy) - ph) * LD(rg.rdz12, k);
+  u[c] = LD(ut, c) - dt * gx;
+  v[c] = LD(vt, c) - dt * gy;
+  w[c] = LD(wt, c) - dt * gz;
+  u_ta[c] = dt * gx;
+  v_ta[c] = dt * gy;
+  w_ta[c] = dt * gz;
+}
+
+void launch_correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const double* ut,
+                         const double* vt, const double* wt, double* p, double* u, double* v,
+                         double* w, double* u_ta, double* v_ta, double* w_ta, double* u_ep2,
+                         double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s) {
+  dim3 block(TXW, TYW, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
+  size_t smem = (size_t)NSLOT * CSLOT * sizeof(double);
+  cudaFuncSetAttribute((const void*)k_correct_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  count_launch();
+  k_correct_pipe<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta,
+                                           u_ep2, v_ep2, w_ep2, divu, dt);
+  long nf = (long)(d.ny + 1) * (d.nz + 1) + (long)d.nx * (d.nz + 1) + (long)d.nx * d.ny;
+  count_launch();
+  k_correct_faces<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(d, rg, PHI, ut, vt, wt, u, v, w,
+                                                               u_ta, v_ta, w_ta, dt);
 }
 
 }  // namespace nse

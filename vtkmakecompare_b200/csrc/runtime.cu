@@ -1331,9 +1331,15 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   mark(x, PH_PHIBC);
   launch_phibc(d, phi, s);
   mark(x, PH_CORRECT);
-  launch_correct(d, x->g, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V), F(x, NSE_W),
-                 F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA), F(x, NSE_U_EP2),
-                 F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU), x->cfg.dt, s);
+  if (x->cfg.flags & NSE_FLAG_EXACT)
+    launch_correct(d, x->g, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V), F(x, NSE_W),
+                   F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA), F(x, NSE_U_EP2),
+                   F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU), x->cfg.dt, s);
+  else
+    launch_correct_pipe(d, x->rg, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V),
+                        F(x, NSE_W), F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA),
+                        F(x, NSE_U_EP2), F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU),
+                        x->cfg.dt, s);
   mark(x, PH_COUNT);
 }
 
