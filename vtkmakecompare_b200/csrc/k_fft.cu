@@ -110,14 +110,14 @@ template <int R>
 __device__ __forceinline__ void stockham_stage(const double2* __restrict__ src,
                                                double2* __restrict__ dst, int N, int nb,
                                                int Ns, const double2* __restrict__ tw,
-                                               bool inv) {
+                                               bool inv, int fs) {
   int nbf = N / R;
   int total = nbf * nb;
   int tstep = N / (Ns * R);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     int f = t / nbf, j = t - f * nbf;
-    const double2* in = src + (long)f * N;
-    double2* out = dst + (long)f * N;
+    const double2* in = src + (long)f * fs;
+    double2* out = dst + (long)f * fs;
     double2 v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = in[j + r * nbf];
@@ -137,17 +137,19 @@ __device__ __forceinline__ void stockham_stage(const double2* __restrict__ src,
   }
 }
 
-// runs the full FFT; data starts in a, returns the buffer holding the result
+// runs the full FFT; data starts in a, returns the buffer holding the result;
+// FFT f occupies [f*fs, f*fs + N) (fs >= N; fs = N+1 keeps column-wise tiles
+// free of shared-memory bank conflicts)
 __device__ double2* fft_block(double2* a, double2* b, const FFTShape& sh, int nb,
-                              const double2* tw, bool inv) {
+                              const double2* tw, bool inv, int fs) {
   int Ns = 1;
   for (int s = 0; s < sh.nst; ++s) {
     int R = sh.rad[s];
     __syncthreads();
-    if (R == 4) stockham_stage<4>(a, b, sh.n, nb, Ns, tw, inv);
-    else if (R == 2) stockham_stage<2>(a, b, sh.n, nb, Ns, tw, inv);
-    else if (R == 3) stockham_stage<3>(a, b, sh.n, nb, Ns, tw, inv);
-    else stockham_stage<5>(a, b, sh.n, nb, Ns, tw, inv);
+    if (R == 4) stockham_stage<4>(a, b, sh.n, nb, Ns, tw, inv, fs);
+    else if (R == 2) stockham_stage<2>(a, b, sh.n, nb, Ns, tw, inv, fs);
+    else if (R == 3) stockham_stage<3>(a, b, sh.n, nb, Ns, tw, inv, fs);
+    else stockham_stage<5>(a, b, sh.n, nb, Ns, tw, inv, fs);
     Ns *= R;
     double2* t = a; a = b; b = t;
   }
@@ -197,7 +199,7 @@ __global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecView sv, const d
     }
     a[t] = make_double2(va, vb);
   }
-  double2* r = fft_block(a, b, sh, npair, tw, false);
+  double2* r = fft_block(a, b, sh, npair, tw, false, N);
   const int H = N / 2 + 1;
   for (int t = threadIdx.x; t < npair * H; t += blockDim.x) {
     int pr = t / H, kx = t - pr * H;
@@ -217,8 +219,9 @@ __global__ void k_fft_z(FFTShape sh, int W, int H, SpecView sv, const double2* _
                         int inv, double nrm) {
   extern __shared__ double2 smem[];
   const int N = sh.n;
+  const int FS = N + 1;
   double2* a = smem;
-  double2* b = smem + (long)W * N;
+  double2* b = smem + (long)W * FS;
   const int jj = blockIdx.y;
   const int kx0 = blockIdx.x * W;
   for (int t = threadIdx.x; t < W * N; t += blockDim.x) {
@@ -226,14 +229,14 @@ __global__ void k_fft_z(FFTShape sh, int W, int H, SpecView sv, const double2* _
     int kx = kx0 + c;
     double2 v = make_double2(0.0, 0.0);
     if (kx < H) v = sv.base[kx + sv.sj * jj + sv.sk * kz];
-    a[c * N + kz] = v;
+    a[c * FS + kz] = v;
   }
-  double2* r = fft_block(a, b, sh, W, tw, inv != 0);
+  double2* r = fft_block(a, b, sh, W, tw, inv != 0, FS);
   for (int t = threadIdx.x; t < W * N; t += blockDim.x) {
     int c = t % W, kz = t / W;
     int kx = kx0 + c;
     if (kx >= H) continue;
-    double2 v = r[c * N + kz];
+    double2 v = r[c * FS + kz];
     if (!inv) { v.x = v.x / nrm; v.y = v.y / nrm; }
     sv.base[kx + sv.sj * jj + sv.sk * kz] = v;
   }
@@ -263,7 +266,7 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecView sv, double*
     a[pr * N + kx] = make_double2(A.x - B.y, A.y + B.x);
     if (kx > 0 && 2 * kx < N) a[pr * N + (N - kx)] = make_double2(A.x + B.y, B.x - A.y);
   }
-  double2* r = fft_block(a, b, sh, npair, tw, true);
+  double2* r = fft_block(a, b, sh, npair, tw, true, N);
   for (int t = threadIdx.x; t < npair * (N + 1); t += blockDim.x) {
     int pr = t / (N + 1), i = t - pr * (N + 1);
     int ka = kk0 + 2 * pr, kb = ka + 1;
@@ -277,31 +280,35 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecView sv, double*
 }
 
 // ------------------------------------------------------ SPN / SP0B (y) --
-// thread (kx, kz); sv points at plane J = 1; scratch sc holds A(I,3)/A(I,2)
-// at [kx + scj*(J-1) + sck*kz]
+// Two threads per (kx, kz) system, on adjacent lanes: one runs the real part
+// of the right-hand side and one the imaginary part (CTRIDIAG's matrix is
+// real, tridiag.f:43-58, so both run the same coefficient recurrence and
+// write the same value of A(I,3) to the scratch).  sv points at plane J = 1;
+// scratch sc holds A(I,3)/A(I,2) at [kx + scj*(J-1) + sck*kz].
 __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, long sck,
                       const double* __restrict__ AC, const double* __restrict__ KXZ,
                       int do_spn, int do_sp0b) {
-  int kx = blockIdx.x * blockDim.x + threadIdx.x;
-  int kz = blockIdx.y;
+  const int t = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kx = t >> 1, comp = t & 1;
+  const int kz = blockIdx.y;
   if (kx >= H || kz >= nz) return;
   const double* AC1 = AC;
   const double* AC2 = AC + ny;
   const double* AC3 = AC + 2 * ny;
-  double2* B = sv.base + kx + sv.sk * kz;
+  double* B = reinterpret_cast<double*>(sv.base + kx + sv.sk * kz) + comp;
+  const long sj = 2 * sv.sj;  // doubles between planes
   if (kx == 0 && kz == 0) {
     if (!do_sp0b) return;
     // SP0B mkp.f:271-288; the ghost PHIT(0,NY+1,0) is set by the caller
-    double2 pm = make_double2(0.0, 0.0), pc = make_double2(0.0, 0.0);
-    double2 Dn = B[0];  // D(1)
-    B[0] = pc;          // PHIT(0,1,0) = 0
+    double pm = 0.0, pc = 0.0;
+    double Dn = B[0];  // D(1)
+    B[0] = pc;         // PHIT(0,1,0) = 0
     for (int J = 1; J <= ny - 1; ++J) {
-      double2 Dj = Dn;
-      Dn = B[sv.sj * J];  // D(J+1), read before it is overwritten
+      double Dj = Dn;
+      Dn = B[sj * J];  // D(J+1), read before it is overwritten
       double a1 = AC1[J - 1], a2 = AC2[J - 1], a3 = AC3[J - 1];
-      double2 pn = make_double2((Dj.x - a1 * pm.x - a2 * pc.x) / a3,
-                                (Dj.y - a1 * pm.y - a2 * pc.y) / a3);
-      B[sv.sj * J] = pn;  // PHIT(0,J+1,0)
+      double pn = (Dj - a1 * pm - a2 * pc) / a3;
+      B[sj * J] = pn;  // PHIT(0,J+1,0)
       pm = pc;
       pc = pn;
     }
@@ -316,45 +323,44 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
   double a2 = AC2[0] - kxz;
   if (NN == 1) { a2 = a2 + AC1[0]; a2 = a2 + AC3[0]; }
   else a2 = a2 + AC1[0];  // AA(1,2) += AA(1,1)
-  double2 b = B[0];
+  double b = B[0];
   constexpr int SPN_BATCH = 8;
   for (int I0 = 1; I0 <= NN - 1; I0 += SPN_BATCH) {
-    double2 nb[SPN_BATCH];
+    double nb[SPN_BATCH];
 #pragma unroll
     for (int q = 0; q < SPN_BATCH; ++q)
-      if (I0 + q <= NN - 1) nb[q] = B[sv.sj * (I0 + q)];
+      if (I0 + q <= NN - 1) nb[q] = B[sj * (I0 + q)];
 #pragma unroll
     for (int q = 0; q < SPN_BATCH; ++q) {
       int I = I0 + q;
       if (I > NN - 1) break;
       double a3 = AC3[I - 1] / a2;
-      b = make_double2(b.x / a2, b.y / a2);
-      B[sv.sj * (I - 1)] = b;
+      b = b / a2;
+      B[sj * (I - 1)] = b;
       s3[scj * (I - 1)] = a3;
       double a1n = AC1[I];
       double a2n = AC2[I] - kxz;
       if (I + 1 == NN) a2n = a2n + AC3[NN - 1];  // AA(NY,2) += AA(NY,3)
       a2 = a2n - a1n * a3;
-      b = make_double2(nb[q].x - a1n * b.x, nb[q].y - a1n * b.y);
+      b = nb[q] - a1n * b;
     }
   }
-  b = make_double2(b.x / a2, b.y / a2);
-  B[sv.sj * (NN - 1)] = b;
+  b = b / a2;
+  B[sj * (NN - 1)] = b;
   for (int I0 = NN - 1; I0 >= 1; I0 -= SPN_BATCH) {
-    double2 bi[SPN_BATCH];
-    double a3v[SPN_BATCH];
+    double bi[SPN_BATCH], a3v[SPN_BATCH];
 #pragma unroll
     for (int q = 0; q < SPN_BATCH; ++q)
       if (I0 - q >= 1) {
-        bi[q] = B[sv.sj * (I0 - q - 1)];
+        bi[q] = B[sj * (I0 - q - 1)];
         a3v[q] = s3[scj * (I0 - q - 1)];
       }
 #pragma unroll
     for (int q = 0; q < SPN_BATCH; ++q) {
       int I = I0 - q;
       if (I < 1) break;
-      b = make_double2(bi[q].x - a3v[q] * b.x, bi[q].y - a3v[q] * b.y);
-      B[sv.sj * (I - 1)] = b;
+      b = bi[q] - a3v[q] * b;
+      B[sj * (I - 1)] = b;
     }
   }
 }
@@ -439,7 +445,7 @@ void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
   if (W < 1) W = 1;
   if (W > 16) W = 16;
   dim3 grid((pp.H + W - 1) / W, pp.ny);
-  size_t sm = 2 * (size_t)W * pp.nz * sizeof(double2);
+  size_t sm = 2 * (size_t)W * (pp.nz + 1) * sizeof(double2);
   smem_optin((const void*)k_fft_z, sm);
   count_launch();
   k_fft_z<<<grid, fft_threads(W * pp.nz), sm, s>>>(sh, W, pp.H, spec_internal(pp),
@@ -449,7 +455,7 @@ void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
 }
 
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s) {
-  dim3 grid((pp.H + 63) / 64, pp.nz);
+  dim3 grid((2 * pp.H + 63) / 64, pp.nz);
   count_launch();
   k_spn<<<grid, 64, 0, s>>>(pp.H, pp.ny, pp.nz, spec_internal(pp), pp.scr, pp.Hp,
                             (long)pp.Hp * pp.ny, pp.AC, pp.KXZ, do_spn ? 1 : 0,
