@@ -165,6 +165,22 @@ void nse_set_c_stretched(int nx, int ny, int nz, double* x, double* x12, double*
                          double* dy, double* dy12, double* dz, double* dz12, double xl,
                          double yl, double zl, double y0, double gamma);
 
+/* No counterpart in the reference.  SPN (mkp.f:223) for callers that cannot
+ * allocate GPU memory: AC (ny,3), KXZ (nx/2+1, nz+1) and the complex spectrum
+ * PHIT (0:nx/2, 0:ny+1, 0:nz+1) are DEVICE pointers in the reference layouts;
+ * the solve is queued on `stream` (a cudaStream_t, NULL = legacy default
+ * stream) and the function returns without synchronising.  It allocates
+ * nothing: its scratch is a fixed array inside the library of
+ * NSE_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB, resident on every GPU that
+ * loads the library until exit), so (nx/2+1)*ny*nz must not exceed it
+ * (NSE_ERR_LIMIT otherwise).  The first call on a device looks up the array's
+ * device address; make that first call before any stream capture.  Calls
+ * share the array: calls that overlap on the GPU race and must be
+ * serialised by the caller.  Returns an nse_status. */
+#define NSE_NOALLOC_SCRATCH_DOUBLES (2L * 1024L * 1024L)
+int nse_spn_noalloc(int nx, int ny, int nz, const double* AC, const double* KXZ,
+                    double* PHIT, void* stream);
+
 /* ------------------------------------------------ tier 3: resident API ---- */
 typedef struct nse_config {
   int nx, ny, nz;

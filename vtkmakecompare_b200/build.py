@@ -26,6 +26,7 @@ SOURCES = {
     "k_lines_fast.cu": [],
     "k_rhs_fast.cu": [],
     "k_fft.cu": [],
+    "noalloc.cu": [],
 }
 
 

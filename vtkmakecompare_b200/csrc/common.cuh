@@ -207,6 +207,9 @@ void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const GridDev& g, double dt, int src_mode, cudaStream_t s);
 void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s);
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s);
+void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,
+                     long scj, long sck, const double* AC, const double* KXZ, bool do_spn,
+                     bool do_sp0b, cudaStream_t s);
 // inverse x transform into padded FP for J=1..NY with the S2P wrap fill
 void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s);
 void launch_phibc(const Dims& d, double* PHI, cudaStream_t s);

@@ -462,6 +462,21 @@ void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s
                             do_sp0b ? 1 : 0);
 }
 
+// k_spn on an arbitrary spectrum view: base points at (kx=0, J=1, kz=0),
+// complex strides sj, sk; the scratch sc is indexed kx + scj*(J-1) + sck*kz
+void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,
+                     long scj, long sck, const double* AC, const double* KXZ, bool do_spn,
+                     bool do_sp0b, cudaStream_t s) {
+  SpecView sv;
+  sv.base = reinterpret_cast<double2*>(base);
+  sv.sj = sj;
+  sv.sk = sk;
+  dim3 grid((2 * H + 63) / 64, nz);
+  count_launch();
+  k_spn<<<grid, 64, 0, s>>>(H, ny, nz, sv, sc, scj, sck, AC, KXZ, do_spn ? 1 : 0,
+                            do_sp0b ? 1 : 0);
+}
+
 void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s) {
   FFTShape sh = make_shape(pp.nx);
   int npair = 1024 / pp.nx;
