@@ -76,7 +76,10 @@ def test_context_grid_matches_oracle_grid():
 
 @pytest.mark.parametrize("exact", [False, True])
 @pytest.mark.parametrize("n,sphere,steps", [((16, 12, 8), True, 3), ((32, 24, 16), True, 10),
-                                            ((24, 16, 20), False, 10), ((40, 33, 36), True, 4)])
+                                            ((24, 16, 20), False, 10), ((40, 33, 36), True, 4),
+                                            # shapes the partitioned line solver takes
+                                            ((96, 48, 64), True, 4), ((128, 40, 96), True, 3),
+                                            ((256, 20, 24), False, 2)])
 def test_steps_match_oracle(n, sphere, steps, exact):
     g, f, c1, par = make_case(*n, sphere=sphere)
     ref = run_oracle(g, f, c1, par, steps)

@@ -24,6 +24,7 @@ SOURCES = {
     "k_levelset.cu": ["--fmad=false"],
     "k_lines_exact.cu": ["--fmad=false"],
     "k_lines_fast.cu": [],
+    "k_lines_part.cu": [],
     "k_rhs_fast.cu": [],
     "k_fft.cu": [],
     "noalloc.cu": [],

@@ -1,0 +1,611 @@
+// k_lines_part.cu -- partitioned ADI line solver of the resident step (fast
+// form).
+//
+// Every line system of the step (the UL systems of implicit_uy/vy/Ty,
+// nse_dominik.f:1505-1648,1784-1870, and the augmented cyclic systems of
+// implicit_solver/implicit_Tx, periodic_implicit.f:1-93, nse_dominik.f:
+// 1725-1781) is, after folding its boundary rows, a tridiagonal system on
+// the interior unknowns, periodic for the x and z lines:
+//   UL u, w, T:  x0 = ft - x1 and x(n+1) = fb - x(n)   (rows 0 and n+1)
+//   UL v:        x0 = ft, x(ny) = fb                     (Dirichlet)
+//   cyclic:      x0 = x(n), x(n+1) = x(1)                (the ghost rows)
+// The reference eliminates each line sequentially.  Here a line is cut into
+// P partitions of m >= 3 rows.  Within a partition every interior row is
+// written as x = g + F p + E q, where F and E are the partition's first and
+// last unknowns, g solves the interior rows with F = E = 0 and p, q are the
+// responses to unit F and E.  The first and last rows then form a reduced
+// tridiagonal system of 2P unknowns (F0, E0, F1, E1, ...), periodic when the
+// line is.  Everything that does not depend on the right-hand side -- the
+// interior factorisation, p, q, and the factorisation of the reduced system
+// -- is tabulated once per matrix: one table for all mask-free lines of a
+// kind, one per line that touches the penalisation mask (the mask is fixed
+// between level-set calls).  A solve then costs one read and one write of
+// the line plus a few FMAs per row, with the rows held in registers.
+//
+//   x lines (contiguous): one warp per line, lane k = partition k (P = 32,
+//     m = nx/32); the reduced system is reduced once more to the E unknowns
+//     and solved by parallel cyclic reduction over warp shuffles.
+//   y and z lines (strided): one CTA per 32 adjacent lines, lane = line,
+//     warp = partition; the reduced system goes through shared memory and
+//     is solved by one warp with the tabulated factorisation.
+#include <algorithm>
+
+#include "k_lines.cuh"
+
+namespace nse {
+
+namespace {
+
+// ------------------------------------------------ rows of a folded line --
+// Unknown t (0-based) of a line is reference row jr(t): t + 1, or for the
+// x kernel (which rotates the periodic unknowns so lane 0 starts at the
+// 16-byte aligned ghost position) n for t = 0 and t otherwise.
+template <int DIR, int KIND>
+struct FoldedLine {
+  Dims d;
+  GridDev g;
+  const double* c1;
+  LineArgs a;
+  bool masked;
+  int i, j, k;
+  int n, nu;  // reference interior length, number of unknowns
+  bool rot;
+
+  __device__ Row ref(int r) const {
+    if (masked) return line_row<DIR, KIND>(d, g, c1, a, i, j, k, r);
+    const double alpha = a.dt * a.eta * 0.0 + 1.0;
+    const double* D = DIR == 0 ? g.dx : (DIR == 1 ? g.dy : g.dz);
+    const double* D12 = DIR == 0 ? g.dx12 : (DIR == 1 ? g.dy12 : g.dz12);
+    if (KIND == LK_UL_U) return row_uy(a.beta, alpha, D12[r - 1], D12[r], D[r]);
+    if (KIND == LK_UL_V) return row_vy(a.beta, alpha, D[r], D[r + 1], D12[r]);
+    if (KIND == LK_CYC_VEL) return row_cyc(a.beta, alpha, D[r], D[r + 1], D12[r]);
+    return row_T(a.beta, alpha, D[r - 1], D[r], D[r + 1], D12[r - 1], D12[r], a.l0, a.l0, a.l0,
+                 a.r0);
+  }
+  __device__ int jr(int t) const { return rot ? (t == 0 ? n : t) : t + 1; }
+  // coefficients of unknown t: A x(t-1) + B x(t) + C x(t+1) (indices mod nu
+  // for periodic lines; A of the first and C of the last unknown are zero
+  // for the others)
+  __device__ void coef(int t, double& A, double& B, double& C) const {
+    Row rw = ref(jr(t));
+    A = rw.lo; B = rw.di; C = rw.up;
+    if (KIND <= LK_UL_T) {
+      if (t == 0) { if (KIND != LK_UL_V) B = B - A; A = 0.0; }
+      if (t == nu - 1) { if (KIND != LK_UL_V) B = B - C; C = 0.0; }
+    }
+  }
+};
+
+template <int DIR, int KIND>
+__device__ FoldedLine<DIR, KIND> folded_line(const Dims& d, const GridDev& g, const double* c1,
+                                             const LineArgs& a, long id, bool masked,
+                                             bool rot) {
+  FoldedLine<DIR, KIND> L;
+  L.d = d; L.g = g; L.c1 = c1; L.a = a; L.masked = masked; L.rot = rot;
+  L.i = L.j = L.k = 0;
+  if (masked) {
+    if (DIR == 1) { L.i = 1 + (int)(id % d.nx); L.k = 1 + (int)(id / d.nx); }
+    else if (DIR == 2) { L.i = 1 + (int)(id % d.nx); L.j = 1 + (int)(id / d.nx); }
+    else { L.j = 1 + (int)(id % a.jtop); L.k = 1 + (int)(id / a.jtop); }
+  }
+  L.n = DIR == 0 ? d.nx : (DIR == 1 ? d.ny : d.nz);
+  L.nu = KIND == LK_UL_V ? L.n - 1 : L.n;
+  return L;
+}
+
+// interior rows s+1..e-1 of one partition: forward multipliers W, reciprocal
+// pivots RB, super-diagonals CC and the responses P (to x(s) = 1) and Q (to
+// x(e) = 1); element t of each array is at arr[t * step]
+template <class Line>
+__device__ void partition_rows(const Line& L, int s, int e, double* W, double* RB, double* CC,
+                               double* PP, double* QQ, long step) {
+  double A, B, C, Cprev = 0.0, beta = 1.0, pp = 0.0;
+  for (int t = s + 1; t <= e - 1; ++t) {
+    L.coef(t, A, B, C);
+    double w = (t == s + 1) ? 0.0 : A / beta;
+    beta = (t == s + 1) ? B : B - w * Cprev;
+    pp = (t == s + 1) ? -A : -w * pp;  // forward sweep of the P response
+    W[t * step] = w;
+    RB[t * step] = 1.0 / beta;
+    CC[t * step] = C;
+    PP[t * step] = pp;
+    Cprev = C;
+  }
+  // back substitution of P and Q (Q's right-hand side is -C(e-1) in row e-1)
+  double pn = 0.0, qn = 0.0;
+  for (int t = e - 1; t >= s + 1; --t) {
+    double rb = RB[t * step], c = CC[t * step];
+    double pv = (PP[t * step] - c * pn) * rb;
+    double qv = ((t == e - 1 ? -c : 0.0) - c * qn) * rb;
+    PP[t * step] = pv;
+    QQ[t * step] = qv;
+    pn = pv;
+    qn = qv;
+  }
+}
+
+}  // namespace
+
+// ===================================================== y and z line tables
+// layout (nu unknowns, P partitions, R = 2P reduced unknowns):
+//   W, RB, CC, PP, QQ [nu] | CF, AE [P] | LL, RP, UU, ZZ [R] | bg, rden, fold0, foldN |
+//   MI [R x R] (inverse of the reduced system, row-major)
+__host__ __device__ size_t yz_table_stride(int nu, int P) {
+  return 5 * (size_t)nu + 2 * (size_t)P + 8 * (size_t)P + 4 + 4 * (size_t)P * P;
+}
+
+template <int DIR, int KIND>
+__global__ void k_build_yz(Dims d, GridDev g, const double* c1, LineArgs a, const int* ids,
+                           int count, int P, double* out) {
+  const int line = blockIdx.x;
+  const int lane = threadIdx.x;
+  if (line >= count) return;
+  const bool masked = ids != nullptr;
+  auto L = folded_line<DIR, KIND>(d, g, c1, a, masked ? ids[line] : 0, masked, false);
+  const int nu = L.nu, R = 2 * P;
+  double* T = out + (size_t)line * yz_table_stride(nu, P);
+  double *W = T, *RB = T + nu, *CC = T + 2 * nu, *PP = T + 3 * nu, *QQ = T + 4 * nu;
+  double *CF = T + 5 * nu, *AE = CF + P, *LL = AE + P, *RP = LL + R, *UU = RP + R, *ZZ = UU + R;
+  double* cst = ZZ + R;
+  double* MI = cst + 4;
+  const bool periodic = KIND >= LK_CYC_VEL;
+  if (lane < P) {
+    const int s = (int)((long)lane * nu / P), e = (int)((long)(lane + 1) * nu / P) - 1;
+    partition_rows(L, s, e, W, RB, CC, PP, QQ, 1);
+    double As, Bs, Cs, Ae, Be, Ce;
+    L.coef(s, As, Bs, Cs);
+    L.coef(e, Ae, Be, Ce);
+    CF[lane] = Cs;
+    AE[lane] = Ae;
+    // reduced rows: F row (couples E(k-1), F(k), E(k)), E row (F(k), E(k), F(k+1))
+    LL[2 * lane] = As;
+    RP[2 * lane] = Bs + Cs * PP[s + 1];
+    UU[2 * lane] = Cs * QQ[s + 1];
+    LL[2 * lane + 1] = Ae * PP[e - 1];
+    RP[2 * lane + 1] = Be + Ae * QQ[e - 1];
+    UU[2 * lane + 1] = Ce;
+  }
+  __syncwarp();
+  if (lane == 0) {
+    // fold constants: right-hand-side corrections of the first and last rows
+    Row r1 = L.ref(1), rn = L.ref(nu);
+    cst[2] = periodic ? 0.0 : r1.lo;
+    cst[3] = periodic ? 0.0 : rn.up;
+    // factorisation of the reduced system (in place: LL <- multipliers,
+    // RP <- reciprocal pivots); periodic: Sherman-Morrison with gamma = -b0
+    double gam = 0.0, bcorner = 0.0, acorner = 0.0;
+    if (periodic) {
+      bcorner = LL[0];      // row 0 couples y(R-1)
+      acorner = UU[R - 1];  // row R-1 couples y(0)
+      gam = -RP[0];
+      RP[0] = RP[0] - gam;
+      RP[R - 1] = RP[R - 1] - acorner * bcorner / gam;
+    }
+    double piv = RP[0];
+    LL[0] = 0.0;
+    RP[0] = 1.0 / piv;
+    for (int r = 1; r < R; ++r) {
+      double l = LL[r] / piv;
+      piv = RP[r] - l * UU[r - 1];
+      LL[r] = l;
+      RP[r] = 1.0 / piv;
+    }
+    if (periodic) {
+      // z solves the modified system for u = (gam, 0, ..., 0, acorner)
+      double zf = gam;
+      ZZ[0] = zf;
+      for (int r = 1; r < R; ++r) {
+        zf = (r == R - 1 ? acorner : 0.0) - LL[r] * zf;
+        ZZ[r] = zf;
+      }
+      double zb = ZZ[R - 1] * RP[R - 1];
+      ZZ[R - 1] = zb;
+      for (int r = R - 2; r >= 0; --r) {
+        zb = (ZZ[r] - UU[r] * zb) * RP[r];
+        ZZ[r] = zb;
+      }
+      cst[0] = bcorner / gam;
+      cst[1] = 1.0 / (1.0 + ZZ[0] + bcorner * ZZ[R - 1] / gam);
+    } else {
+      for (int r = 0; r < R; ++r) ZZ[r] = 0.0;
+      cst[0] = 0.0;
+      cst[1] = 0.0;
+    }
+  }
+  __syncwarp();
+  // column c of the inverse: the reduced solve applied to the unit vector e_c
+  if (lane < R) {
+    const int c = lane;
+    double y = (c == 0) ? 1.0 : 0.0;
+    MI[c] = y;
+    for (int r = 1; r < R; ++r) {
+      y = (r == c ? 1.0 : 0.0) - LL[r] * y;
+      MI[r * R + c] = y;
+    }
+    y = y * RP[R - 1];
+    MI[(R - 1) * R + c] = y;
+    for (int r = R - 2; r >= 0; --r) {
+      y = (MI[r * R + c] - UU[r] * y) * RP[r];
+      MI[r * R + c] = y;
+    }
+    if (periodic) {
+      const double fact = (y + cst[0] * MI[(R - 1) * R + c]) * cst[1];
+      for (int r = 0; r < R; ++r) MI[r * R + c] = MI[r * R + c] - fact * ZZ[r];
+    }
+  }
+}
+
+// ========================================================== x line tables
+// per lane k (partition k of 32): values v = 0..XV-1 at [v * 32 + k]
+enum {
+  XT_CF = 0, XT_AE, XT_MU, XT_NU, XT_K1, XT_K2 = XT_K1 + 4, XT_LAM = XT_K2 + 4, XT_KAP, XT_RDF,
+  XT_LFR, XT_UFR, XT_ROW  // then 5 values per interior row: W, RB, CC, PP, QQ
+};
+__host__ __device__ constexpr int x_table_values(int M) { return XT_ROW + 5 * (M - 2); }
+__host__ __device__ size_t x_table_stride(int M) { return 32 * (size_t)x_table_values(M); }
+
+template <int KIND>
+__global__ void k_build_x(Dims d, GridDev g, const double* c1, LineArgs a, const int* ids,
+                          int count, double* out) {
+  const int line = blockIdx.x;
+  const int k = threadIdx.x;
+  if (line >= count) return;
+  const bool masked = ids != nullptr;
+  auto L = folded_line<0, KIND>(d, g, c1, a, masked ? ids[line] : 0, masked, true);
+  const int M = L.n / 32;
+  double* T = out + (size_t)line * x_table_stride(M);
+  const int s = k * M, e = s + M - 1;
+  // interior rows: values at T[(XT_ROW + 5 (r-1) + c) * 32 + k], r = t - s;
+  // partition_rows indexes arr[t * step], so shift the bases by -s rows
+  double* rowb = T + XT_ROW * 32 + k;
+  const long step = 5 * 32;
+  double* base = rowb - (long)(s + 1) * step;
+  partition_rows(L, s, e, base, base + 32, base + 64, base + 96, base + 128, step);
+  double As, Bs, Cs, Ae, Be, Ce;
+  L.coef(s, As, Bs, Cs);
+  L.coef(e, Ae, Be, Ce);
+  const double p1 = base[(s + 1) * step + 96], q1 = base[(s + 1) * step + 128];
+  const double pm = base[(e - 1) * step + 96], qm = base[(e - 1) * step + 128];
+  // F row: LF E(k-1) + DF F(k) + UF E(k); E row: LE F(k) + DE E(k) + UE F(k+1)
+  const double LF = As, DF = Bs + Cs * p1, UF = Cs * q1;
+  const double LE = Ae * pm, DE = Be + Ae * qm, UE = Ce;
+  const unsigned FULL = 0xffffffffu;
+  const int kp = (k + 1) & 31;
+  const double LF1 = __shfl_sync(FULL, LF, kp), DF1 = __shfl_sync(FULL, DF, kp);
+  const double UF1 = __shfl_sync(FULL, UF, kp);
+  // eliminate the F unknowns: al E(k-1) + be E(k) + ga E(k+1) = rho
+  double al = -LE * LF / DF;
+  double be = DE - LE * UF / DF - UE * LF1 / DF1;
+  double ga = -UE * UF1 / DF1;
+  T[XT_CF * 32 + k] = Cs;
+  T[XT_AE * 32 + k] = Ae;
+  T[XT_MU * 32 + k] = -LE / DF;
+  T[XT_NU * 32 + k] = -UE / DF1;
+  // parallel cyclic reduction over the 32 lanes, strides 1, 2, 4, 8
+  for (int lv = 0; lv < 4; ++lv) {
+    const int sft = 1 << lv;
+    const int km = (k - sft) & 31, kq = (k + sft) & 31;
+    double alm = __shfl_sync(FULL, al, km), bem = __shfl_sync(FULL, be, km);
+    double gam = __shfl_sync(FULL, ga, km);
+    double alp = __shfl_sync(FULL, al, kq), bep = __shfl_sync(FULL, be, kq);
+    double gap = __shfl_sync(FULL, ga, kq);
+    double k1 = -al / bem, k2 = -ga / bep;
+    T[(XT_K1 + lv) * 32 + k] = k1;
+    T[(XT_K2 + lv) * 32 + k] = k2;
+    double nal = k1 * alm, nga = k2 * gap, nbe = be + k1 * gam + k2 * alp;
+    al = nal; ga = nga; be = nbe;
+  }
+  // rows k and k^16 now couple only each other
+  const int kx = k ^ 16;
+  double alx = __shfl_sync(FULL, al, kx), bex = __shfl_sync(FULL, be, kx);
+  double gax = __shfl_sync(FULL, ga, kx);
+  double a2 = al + ga;
+  double det = be * bex - a2 * (alx + gax);
+  T[XT_LAM * 32 + k] = bex / det;
+  T[XT_KAP * 32 + k] = -a2 / det;
+  T[XT_RDF * 32 + k] = 1.0 / DF;
+  T[XT_LFR * 32 + k] = -LF / DF;
+  T[XT_UFR * 32 + k] = -UF / DF;
+}
+
+// =============================================================== solvers ==
+// interior Thomas on registers: g <- solution of the interior rows with
+// zero end values; rows r = 1..m-2 of the partition, table rows at tb(r).
+// Returns g(m-2) (taken inside the unrolled chain: selecting x[m-2] after
+// the loop would make the compiler index x dynamically, in local memory).
+template <int MM, class TB>
+__device__ __forceinline__ double interior_solve(double (&x)[MM], int m, const TB& tb) {
+  double gp = x[1];
+#pragma unroll
+  for (int r = 2; r < MM - 1; ++r)
+    if (r <= m - 2) { gp = x[r] - tb.w(r) * gp; x[r] = gp; }
+  double gn = 0.0, glast = 0.0;
+#pragma unroll
+  for (int r = MM - 2; r >= 1; --r)
+    if (r <= m - 2) {
+      double v = (r == m - 2) ? x[r] * tb.rb(r) : (x[r] - tb.cc(r) * gn) * tb.rb(r);
+      if (r == m - 2) glast = v;
+      x[r] = v;
+      gn = v;
+    }
+  return glast;
+}
+
+// x lines: table of lane `lane`, values at p[v * 32 + lane] (shared memory
+// for the mask-free lines, global memory for a masked line)
+struct XTab {
+  const double* p;
+  int lane;
+  __device__ double v(int i) const { return p[i * 32 + lane]; }
+  __device__ double w(int r) const { return v(XT_ROW + 5 * (r - 1)); }
+  __device__ double rb(int r) const { return v(XT_ROW + 5 * (r - 1) + 1); }
+  __device__ double cc(int r) const { return v(XT_ROW + 5 * (r - 1) + 2); }
+  __device__ double pp(int r) const { return v(XT_ROW + 5 * (r - 1) + 3); }
+  __device__ double qq(int r) const { return v(XT_ROW + 5 * (r - 1) + 4); }
+};
+
+template <int M, bool MASKED>
+__global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, int jtop,
+                                                const double* __restrict__ tab,
+                                                const int* __restrict__ slots,
+                                                const int* __restrict__ ids, int count) {
+  constexpr int NV = x_table_values(M);
+  __shared__ double stab[MASKED ? 1 : NV * 32];
+  const int lane = threadIdx.x & 31;
+  const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
+  const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
+  const int n = d.nx;
+  const unsigned FULL = 0xffffffffu;
+  if (!MASKED) {
+    for (int t = threadIdx.x; t < NV * 32; t += blockDim.x) stab[t] = __ldg(tab + t);
+    __syncthreads();
+  }
+  const long nlines = MASKED ? count : (long)jtop * d.nz;
+  for (long l = warp; l < nlines; l += nwarps) {
+    long id;
+    XTab tb;
+    tb.lane = lane;
+    if (MASKED) {
+      id = ids[l];
+      tb.p = tab + (size_t)l * x_table_stride(M);
+    } else {
+      id = l;
+      if (slots[l] >= 0) continue;  // masked line: its own pass
+      tb.p = stab;
+    }
+    const int j = 1 + (int)(id % jtop), k = 1 + (int)(id / jtop);
+    double* line = f + d.P(0, j, k);
+    double x[M];
+    // unknowns t = lane*M + r at positions t (t = 0 stands for x(n))
+    if (M % 2 == 0) {
+      const double2* p2 = reinterpret_cast<const double2*>(line + lane * M);
+#pragma unroll
+      for (int u = 0; u < M / 2; ++u) {
+        double2 v = p2[u];
+        x[2 * u] = v.x;
+        x[2 * u + 1] = v.y;
+      }
+    } else {
+#pragma unroll
+      for (int r = 0; r < M; ++r) x[r] = line[lane * M + r];
+    }
+    if (lane == 0) x[0] = line[n];
+    // interior rows
+    interior_solve<M>(x, M, tb);
+    const double rhsF = x[0] - tb.v(XT_CF) * x[1];
+    const double rhsE = x[M - 1] - tb.v(XT_AE) * x[M - 2];
+    // reduced system on E
+    double rho = rhsE + tb.v(XT_MU) * rhsF + tb.v(XT_NU) * __shfl_sync(FULL, rhsF, (lane + 1) & 31);
+#pragma unroll
+    for (int lv = 0; lv < 4; ++lv) {
+      const int sft = 1 << lv;
+      double rm = __shfl_sync(FULL, rho, (lane - sft) & 31);
+      double rp = __shfl_sync(FULL, rho, (lane + sft) & 31);
+      rho = rho + tb.v(XT_K1 + lv) * rm + tb.v(XT_K2 + lv) * rp;
+    }
+    const double E = tb.v(XT_LAM) * rho + tb.v(XT_KAP) * __shfl_sync(FULL, rho, lane ^ 16);
+    const double Em = __shfl_sync(FULL, E, (lane - 1) & 31);
+    const double F = tb.v(XT_RDF) * rhsF + tb.v(XT_LFR) * Em + tb.v(XT_UFR) * E;
+#pragma unroll
+    for (int r = 1; r < M - 1; ++r) x[r] = x[r] + tb.pp(r) * F + tb.qq(r) * E;
+    x[0] = F;
+    x[M - 1] = E;
+    if (M % 2 == 0) {
+      double2* p2 = reinterpret_cast<double2*>(line + lane * M);
+#pragma unroll
+      for (int u = 0; u < M / 2; ++u) p2[u] = make_double2(x[2 * u], x[2 * u + 1]);
+    } else {
+#pragma unroll
+      for (int r = 0; r < M; ++r) line[lane * M + r] = x[r];
+    }
+    // position 0 received x(n), the value of the periodic ghost x(0)
+    if (lane == 0) line[n] = x[0];
+  }
+}
+
+// y / z lines: table values read through the cache (one table for all the
+// mask-free lanes, so the loads broadcast)
+struct YZTab {
+  const double* T;
+  int nu, s;
+  __device__ double w(int r) const { return __ldg(T + s + r); }
+  __device__ double rb(int r) const { return __ldg(T + nu + s + r); }
+  __device__ double cc(int r) const { return __ldg(T + 2 * nu + s + r); }
+  __device__ double pp(int r) const { return __ldg(T + 3 * nu + s + r); }
+  __device__ double qq(int r) const { return __ldg(T + 4 * nu + s + r); }
+};
+
+template <int DIR, int MM, int P>
+__global__ void __launch_bounds__(32 * P) k_yzlines(Dims d, double* __restrict__ f, int nu,
+                                                     int nother, const double* __restrict__ tab,
+                                                     const int* __restrict__ slots,
+                                                     const double* __restrict__ mtab,
+                                                     double ft, double fb, int periodic) {
+  constexpr int R = 2 * P;
+  __shared__ double red[R * 32];
+  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+  const int i = 1 + blockIdx.x * 32 + lane;
+  const int o = 1 + blockIdx.y;  // k of a y line, j of a z line
+  const bool valid = i <= d.nx && o <= nother;
+  const size_t stride = yz_table_stride(nu, P);
+  const double* T = tab;
+  if (valid) {
+    long lineid = (long)(i - 1) + (long)d.nx * (o - 1);
+    int slot = slots[lineid];
+    if (slot >= 0) T = mtab + (size_t)slot * stride;
+  }
+  const int s = (int)((long)k * nu / P), e = (int)((long)(k + 1) * nu / P) - 1;
+  const int m = e - s + 1;
+  const long es = DIR == 1 ? d.sx : d.sy;
+  double* line = f + (DIR == 1 ? d.P(i, 0, o) : d.P(i, o, 0)) + (long)(s + 1) * es;
+  double x[MM];
+  YZTab tb{T, nu, s};
+  if (valid) {
+    // right-hand-side folds of the boundary rows (zero for periodic lines)
+    const double c0 = (!periodic && k == 0) ? __ldg(T + 5 * nu + 10 * P + 2) * ft : 0.0;
+    const double cN = (!periodic && k == P - 1) ? __ldg(T + 5 * nu + 10 * P + 3) * fb : 0.0;
+    double xe = 0.0;  // the right-hand side of row m-1
+#pragma unroll
+    for (int r = 0; r < MM; ++r)
+      if (r < m) {
+        double v = line[r * es];
+        if (r == 0) v = v - c0;
+        if (r == m - 1) { v = v - cN; xe = v; }
+        x[r] = v;
+      }
+    const double xe1 = interior_solve<MM>(x, m, tb);
+    red[(2 * k) * 32 + lane] = x[0] - __ldg(T + 5 * nu + k) * x[1];
+    red[(2 * k + 1) * 32 + lane] = xe - __ldg(T + 5 * nu + P + k) * xe1;
+  }
+  __syncthreads();
+  if (!valid) return;
+  // F and E of this partition: rows 2k and 2k+1 of the reduced inverse
+  const double* MI = T + 5 * nu + 10 * P + 4;
+  double F = 0.0, E = 0.0;
+#pragma unroll
+  for (int c = 0; c < R; ++c) {
+    const double rc = red[c * 32 + lane];
+    F = F + __ldg(MI + (2 * k) * R + c) * rc;
+    E = E + __ldg(MI + (2 * k + 1) * R + c) * rc;
+  }
+#pragma unroll
+  for (int r = 1; r < MM; ++r) {
+    if (r < m - 1) x[r] = x[r] + tb.pp(r) * F + tb.qq(r) * E;
+    if (r == m - 1) x[r] = E;
+  }
+  x[0] = F;
+#pragma unroll
+  for (int r = 0; r < MM; ++r)
+    if (r < m) line[r * es] = x[r];
+}
+
+// ============================================================== launchers
+// partitions of a y/z line of nu unknowns: the fewest of 4, 8, 16 that
+// leave at most 16 rows each (rows per thread are registers)
+int yz_partitions(int nu) { return nu <= 64 ? 4 : (nu <= 128 ? 8 : 16); }
+static int yz_rows(int nu) {
+  int P = yz_partitions(nu);
+  int m = (nu + P - 1) / P;
+  return m <= 8 ? 8 : 16;
+}
+// rows per lane of the x kernel, 0 when the x kernel does not apply
+int x_rows_per_lane(int nx) {
+  if (nx % 32) return 0;
+  int M = nx / 32;
+  return (M == 3 || M == 4 || M == 5 || M == 6 || M == 8 || M == 16) ? M : 0;
+}
+// the y/z kernel needs at least 3 and at most 16 rows per partition
+static bool yz_ok(int nu) { return nu / yz_partitions(nu) >= 3 && (nu + yz_partitions(nu) - 1) / yz_partitions(nu) <= 16; }
+bool part_lines_supported(const Dims& d) {
+  return x_rows_per_lane(d.nx) > 0 && yz_ok(d.ny - 1) && yz_ok(d.ny) && yz_ok(d.nz);
+}
+size_t part_table_stride(int dir, int kind, const Dims& d) {
+  if (dir == 0) return x_table_stride(x_rows_per_lane(d.nx));
+  int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
+  return yz_table_stride(nu, yz_partitions(nu));
+}
+
+// tables of the lines `ids` (count of them), or with ids == nullptr the one
+// table of the mask-free lines
+void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, const double* c1,
+                        const LineArgs& a, const int* ids, int count, double* out,
+                        cudaStream_t s) {
+  if (count <= 0) return;
+  count_launch();
+  if (dir == 0) {
+    if (kind == LK_CYC_VEL) k_build_x<LK_CYC_VEL><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, out);
+    else k_build_x<LK_CYC_T><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, out);
+    return;
+  }
+  int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
+  int P = yz_partitions(nu);
+  if (dir == 1) {
+    if (kind == LK_UL_U) k_build_yz<1, LK_UL_U><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    else if (kind == LK_UL_V) k_build_yz<1, LK_UL_V><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    else k_build_yz<1, LK_UL_T><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+  } else {
+    if (kind == LK_CYC_VEL) k_build_yz<2, LK_CYC_VEL><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    else k_build_yz<2, LK_CYC_T><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+  }
+}
+
+template <int M>
+static void go_x(const Dims& d, double* f, int jtop, const double* tab, const int* slots,
+                 const int* ids, int nmasked, const double* mtab, cudaStream_t s) {
+  int sms = 148;
+  static int cached = 0;
+  if (!cached) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
+    if (cached <= 0) cached = 148;
+  }
+  sms = cached;
+  long nlines = (long)jtop * d.nz;
+  long blocks = std::min<long>((long)sms * 8, (nlines + 7) / 8);
+  count_launch();
+  k_xlines<M, false><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots, nullptr, 0);
+  if (nmasked > 0) {
+    long mb = std::min<long>((long)sms * 8, (nmasked + 7) / 8);
+    count_launch();
+    k_xlines<M, true><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids, nmasked);
+  }
+}
+
+void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
+                       const double* tab, const int* slots, const int* ids, int nmasked,
+                       const double* mtab, cudaStream_t s) {
+  if (dir == 0) {
+    switch (x_rows_per_lane(d.nx)) {
+      case 3: go_x<3>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 4: go_x<4>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 5: go_x<5>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 6: go_x<6>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 8: go_x<8>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      default: go_x<16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+    }
+    return;
+  }
+  int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
+  int P = yz_partitions(nu);
+  int MM = yz_rows(nu);
+  int nother = dir == 1 ? d.nz : a.jtop;
+  dim3 grid((d.nx + 31) / 32, nother);
+  int periodic = kind >= LK_CYC_VEL ? 1 : 0;
+  count_launch();
+#define NSE_YZ(DIR_, MM_, P_)                                                                    \
+  k_yzlines<DIR_, MM_, P_><<<grid, 32 * P_, 0, s>>>(d, f, nu, nother, tab, slots, mtab, a.ft, \
+                                                    a.fb, periodic)
+#define NSE_YZ_MM(DIR_, P_)               \
+  if (MM == 8) NSE_YZ(DIR_, 8, P_);       \
+  else NSE_YZ(DIR_, 16, P_);
+  if (dir == 1) {
+    if (P == 16) { NSE_YZ_MM(1, 16) } else if (P == 8) { NSE_YZ_MM(1, 8) } else { NSE_YZ_MM(1, 4) }
+  } else {
+    if (P == 16) { NSE_YZ_MM(2, 16) } else if (P == 8) { NSE_YZ_MM(2, 8) } else { NSE_YZ_MM(2, 4) }
+  }
+#undef NSE_YZ_MM
+#undef NSE_YZ
+}
+
+}  // namespace nse

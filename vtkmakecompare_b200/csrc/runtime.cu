@@ -31,6 +31,15 @@ void launch_lines_fast(int dir, int kind, const Dims& d, double* f, const LineAr
 void launch_line_tables_masked(int dir, int kind, const Dims& d, const GridDev& g,
                                const double* c1, const LineArgs& a, const int* ids, int count,
                                double* out, cudaStream_t s);
+// k_lines_part.cu
+bool part_lines_supported(const Dims& d);
+size_t part_table_stride(int dir, int kind, const Dims& d);
+void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, const double* c1,
+                        const LineArgs& a, const int* ids, int count, double* out,
+                        cudaStream_t s);
+void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
+                       const double* tab, const int* slots, const int* ids, int nmasked,
+                       const double* mtab, cudaStream_t s);
 
 // ------------------------------------------------------------------ errors --
 static thread_local int g_status = NSE_OK;
@@ -1018,9 +1027,15 @@ struct nse_ctx {
   // line ids of the masked lines and their coefficient tables
   DBuf slots[3][4], ids[3][4], mtab[3][4];
   int nmasked[3][4] = {};
+  // partitioned line solver of the fast form (k_lines_part.cu): one table
+  // per (direction, component) for the mask-free lines and one per masked line
+  bool part = false;
+  DBuf ptab[3][4], pmtab[3][4];
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
+static int line_kind(int dir, int comp);
+static LineArgs line_args(nse_ctx* x, int comp);
 
 static bool build_line_tables(nse_ctx* x) {
   const Dims& d = x->d;
@@ -1053,6 +1068,19 @@ static bool build_line_tables(nse_ctx* x) {
   }
   if (!NSE_CUDA(cudaStreamSynchronize(x->own))) return false;
   for (int t = 0; t < 7; ++t) x->tab[t].den = dens[t];
+  x->part = !(c.flags & NSE_FLAG_EXACT) && part_lines_supported(d);
+  if (x->part) {
+    for (int dir = 0; dir < 3; ++dir)
+      for (int comp = 0; comp < 4; ++comp) {
+        LineArgs a = line_args(x, comp);
+        int kind = line_kind(dir, comp);
+        if (!x->ptab[dir][comp].ensure(part_table_stride(dir, kind, d) * sizeof(double)))
+          return false;
+        launch_part_tables(dir, kind, d, x->g, nullptr, a, nullptr, 1,
+                           x->ptab[dir][comp].as<double>(), x->own);
+      }
+    if (!NSE_CUDA(cudaStreamSynchronize(x->own))) return false;
+  }
   return true;
 }
 
@@ -1126,6 +1154,13 @@ static bool refresh_line_flags(nse_ctx* x, cudaStream_t s) {
         return false;
       launch_line_tables_masked(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
                                 (int)ids.size(), x->mtab[dir][comp].as<double>(), s);
+      if (x->part) {
+        size_t ps = part_table_stride(dir, kind, d);
+        if (!x->pmtab[dir][comp].ensure(std::max<size_t>(1, ids.size()) * ps * sizeof(double)))
+          return false;
+        launch_part_tables(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
+                           (int)ids.size(), x->pmtab[dir][comp].as<double>(), s);
+      }
       // the host vectors die at the end of this iteration
       if (!NSE_CUDA(cudaStreamSynchronize(s))) return false;
     }
@@ -1242,6 +1277,8 @@ int nse_ctx_destroy(nse_ctx* x) {
       x->slots[dir][comp].release();
       x->ids[dir][comp].release();
       x->mtab[dir][comp].release();
+      x->ptab[dir][comp].release();
+      x->pmtab[dir][comp].release();
     }
   for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
   if (x->own) cudaStreamDestroy(x->own);
@@ -1410,8 +1447,13 @@ static void ctx_step(nse_ctx* x) {
     LineArgs la = line_args(x, comp);
     la.ft = ft;
     la.fb = fb;
-    lines(dir, line_kind(dir, comp), d, f, la, x->tab[tab], x->slots[dir][comp].as<int>(),
-          x->mtab[dir][comp].as<double>(), s);
+    if (x->part)
+      launch_lines_part(dir, line_kind(dir, comp), d, f, la, x->ptab[dir][comp].as<double>(),
+                        x->slots[dir][comp].as<int>(), x->ids[dir][comp].as<int>(),
+                        x->nmasked[dir][comp], x->pmtab[dir][comp].as<double>(), s);
+    else
+      lines(dir, line_kind(dir, comp), d, f, la, x->tab[tab], x->slots[dir][comp].as<int>(),
+            x->mtab[dir][comp].as<double>(), s);
   };
   mark(x, PH_YVEL);
   for (int comp = 0; comp < 3; ++comp)
