@@ -202,9 +202,12 @@ bool poisson_plan_tables(int nx, int ny, int nz, const double* dx, const double*
 // forward real 2-D FFT per y-plane.  src_mode 0: samples from a padded field
 // (P2S, sample (i,k) = FP(i,J,k)); 1: samples = divergence of u*,v*,w* / dt
 // at cell (i==0?nx:i, J, k==0?nz:k) (MKP RHS + periodic fill fused)
+// src_mode 1 forms the divergence right-hand side; with rg given it multiplies
+// by the tabulated reciprocal spacings instead of dividing (fast form)
 void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const double* ut, const double* vt, const double* wt,
-                      const GridDev& g, double dt, int src_mode, cudaStream_t s);
+                      const GridDev& g, double dt, int src_mode, cudaStream_t s,
+                      const GridRcp* rg = nullptr);
 void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s);
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s);
 void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,

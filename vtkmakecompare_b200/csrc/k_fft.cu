@@ -168,7 +168,8 @@ struct SpecView {
 // CTA: plane J (1..ny) and `npair` row pairs starting at row 2*npair*blockIdx.y
 __global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecView sv, const double* FP,
                             const double* ut, const double* vt, const double* wt, GridDev g,
-                            double dt, int src_mode, const double2* __restrict__ tw) {
+                            GridRcp rg, int use_rcp, double dt, int src_mode,
+                            const double2* __restrict__ tw) {
   extern __shared__ double2 smem[];
   const int N = sh.n;
   double2* a = smem;
@@ -191,9 +192,15 @@ __global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecView sv, const d
         if (kq >= nz) continue;
         int K = (kq == 0) ? nz : kq;
         long c = d.P(I, J, K);
-        double val = ((ut[c] - ut[c - 1]) / g.dx[I] + (vt[c] - vt[c - d.sx]) / g.dy[J] +
-                      (wt[c] - wt[c - d.sy]) / g.dz[K]) /
-                     dt;
+        double val;
+        if (use_rcp)
+          val = ((ut[c] - ut[c - 1]) * rg.rdx[I] + (vt[c] - vt[c - d.sx]) * rg.rdy[J] +
+                 (wt[c] - wt[c - d.sy]) * rg.rdz[K]) *
+                (1.0 / dt);
+        else
+          val = ((ut[c] - ut[c - 1]) / g.dx[I] + (vt[c] - vt[c - d.sx]) / g.dy[J] +
+                 (wt[c] - wt[c - d.sy]) / g.dz[K]) /
+                dt;
         if (q) vb = val; else va = val;
       }
     }
@@ -315,8 +322,10 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
     return;
   }
   if (!do_spn) return;
-  // SPN mkp.f:239-254 + CTRIDIAG tridiag.f:47-56.  The right-hand side is read
-  // in batches of SPN_BATCH planes ahead of the recurrence so the loads overlap.
+  // SPN mkp.f:239-254 + CTRIDIAG tridiag.f:47-56, with one reciprocal of the
+  // pivot per row.  The right-hand side is read in batches, double-buffered
+  // so the loads of the next batch are in flight while this one is
+  // eliminated.
   const double kxz = KXZ[kx + (long)H * kz];
   double* s3 = sc + kx + sck * kz;
   const int NN = ny;
@@ -324,43 +333,69 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
   if (NN == 1) { a2 = a2 + AC1[0]; a2 = a2 + AC3[0]; }
   else a2 = a2 + AC1[0];  // AA(1,2) += AA(1,1)
   double b = B[0];
-  constexpr int SPN_BATCH = 8;
-  for (int I0 = 1; I0 <= NN - 1; I0 += SPN_BATCH) {
-    double nb[SPN_BATCH];
+  constexpr int FB = 16;
+  auto load_f = [&](double (&v)[FB], int I0) {
 #pragma unroll
-    for (int q = 0; q < SPN_BATCH; ++q)
-      if (I0 + q <= NN - 1) nb[q] = B[sj * (I0 + q)];
+    for (int q = 0; q < FB; ++q)
+      if (I0 + q <= NN - 1) v[q] = B[sj * (I0 + q)];
+  };
+  auto elim = [&](const double (&v)[FB], int I0) {
 #pragma unroll
-    for (int q = 0; q < SPN_BATCH; ++q) {
-      int I = I0 + q;
-      if (I > NN - 1) break;
-      double a3 = AC3[I - 1] / a2;
-      b = b / a2;
-      B[sj * (I - 1)] = b;
-      s3[scj * (I - 1)] = a3;
-      double a1n = AC1[I];
-      double a2n = AC2[I] - kxz;
-      if (I + 1 == NN) a2n = a2n + AC3[NN - 1];  // AA(NY,2) += AA(NY,3)
-      a2 = a2n - a1n * a3;
-      b = nb[q] - a1n * b;
+    for (int q = 0; q < FB; ++q) {
+      const int I = I0 + q;
+      if (I <= NN - 1) {
+        const double r = 1.0 / a2;
+        const double a3 = AC3[I - 1] * r;
+        b = b * r;
+        B[sj * (I - 1)] = b;
+        s3[scj * (I - 1)] = a3;
+        const double a1n = AC1[I];
+        double a2n = AC2[I] - kxz;
+        if (I + 1 == NN) a2n = a2n + AC3[NN - 1];  // AA(NY,2) += AA(NY,3)
+        a2 = a2n - a1n * a3;
+        b = v[q] - a1n * b;
+      }
+    }
+  };
+  {
+    double va[FB], vb[FB];
+    load_f(va, 1);
+    for (int I0 = 1; I0 <= NN - 1; I0 += 2 * FB) {
+      load_f(vb, I0 + FB);
+      elim(va, I0);
+      load_f(va, I0 + 2 * FB);
+      elim(vb, I0 + FB);
     }
   }
   b = b / a2;
   B[sj * (NN - 1)] = b;
-  for (int I0 = NN - 1; I0 >= 1; I0 -= SPN_BATCH) {
-    double bi[SPN_BATCH], a3v[SPN_BATCH];
+  constexpr int BB = 8;
+  auto load_b = [&](double (&bi)[BB], double (&av)[BB], int I0) {
 #pragma unroll
-    for (int q = 0; q < SPN_BATCH; ++q)
+    for (int q = 0; q < BB; ++q)
       if (I0 - q >= 1) {
         bi[q] = B[sj * (I0 - q - 1)];
-        a3v[q] = s3[scj * (I0 - q - 1)];
+        av[q] = s3[scj * (I0 - q - 1)];
       }
+  };
+  auto back = [&](const double (&bi)[BB], const double (&av)[BB], int I0) {
 #pragma unroll
-    for (int q = 0; q < SPN_BATCH; ++q) {
-      int I = I0 - q;
-      if (I < 1) break;
-      b = bi[q] - a3v[q] * b;
-      B[sj * (I - 1)] = b;
+    for (int q = 0; q < BB; ++q) {
+      const int I = I0 - q;
+      if (I >= 1) {
+        b = bi[q] - av[q] * b;
+        B[sj * (I - 1)] = b;
+      }
+    }
+  };
+  {
+    double ba[BB], aa[BB], bb[BB], ab[BB];
+    load_b(ba, aa, NN - 1);
+    for (int I0 = NN - 1; I0 >= 1; I0 -= 2 * BB) {
+      load_b(bb, ab, I0 - BB);
+      back(ba, aa, I0);
+      load_b(ba, aa, I0 - 2 * BB);
+      back(bb, ab, I0 - BB);
     }
   }
 }
@@ -425,7 +460,10 @@ static SpecView spec_internal(const PoissonPlan& pp) {
 
 void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const double* ut, const double* vt, const double* wt,
-                      const GridDev& g, double dt, int src_mode, cudaStream_t s) {
+                      const GridDev& g, double dt, int src_mode, cudaStream_t s,
+                      const GridRcp* rg) {
+  GridRcp r{};
+  if (rg) r = *rg;
   FFTShape sh = make_shape(pp.nx);
   int npair = 1024 / pp.nx;
   if (npair < 1) npair = 1;
@@ -435,7 +473,7 @@ void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
   smem_optin((const void*)k_fft_fwd_x, sm);
   count_launch();
   k_fft_fwd_x<<<grid, fft_threads(npair * pp.nx), sm, s>>>(
-      sh, npair, d, spec_internal(pp), FP, ut, vt, wt, g, dt, src_mode,
+      sh, npair, d, spec_internal(pp), FP, ut, vt, wt, g, r, rg ? 1 : 0, dt, src_mode,
       reinterpret_cast<const double2*>(pp.twx));
 }
 

@@ -25,9 +25,10 @@
 //   x lines (contiguous): one warp per line, lane k = partition k (P = 32,
 //     m = nx/32); the reduced system is reduced once more to the E unknowns
 //     and solved by parallel cyclic reduction over warp shuffles.
-//   y and z lines (strided): one CTA per 32 adjacent lines, lane = line,
-//     warp = partition; the reduced system goes through shared memory and
-//     is solved by one warp with the tabulated factorisation.
+//   y and z lines (strided): one CTA per 16 adjacent lines, one thread per
+//     (line, partition), threads of a partition adjacent; the reduced
+//     system goes through shared memory and is applied as its tabulated
+//     inverse (two rows per partition).
 #include <algorithm>
 
 #include "k_lines.cuh"
@@ -323,7 +324,8 @@ __device__ __forceinline__ double interior_solve(double (&x)[MM], int m, const T
 #pragma unroll
   for (int r = MM - 2; r >= 1; --r)
     if (r <= m - 2) {
-      double v = (r == m - 2) ? x[r] * tb.rb(r) : (x[r] - tb.cc(r) * gn) * tb.rb(r);
+      // gn is still 0 at r = m-2, so this is x(m-2) * rb there
+      double v = (x[r] - tb.cc(r) * gn) * tb.rb(r);
       if (r == m - 2) glast = v;
       x[r] = v;
       gn = v;
@@ -344,7 +346,9 @@ struct XTab {
   __device__ double qq(int r) const { return v(XT_ROW + 5 * (r - 1) + 4); }
 };
 
-template <int M, bool MASKED>
+// NL lines per warp iteration share every table load (the table reads, not
+// the line data, dominate the L1 traffic of this kernel)
+template <int M, int NL, bool MASKED>
 __global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, int jtop,
                                                 const double* __restrict__ tab,
                                                 const int* __restrict__ slots,
@@ -361,65 +365,121 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, 
     __syncthreads();
   }
   const long nlines = MASKED ? count : (long)jtop * d.nz;
-  for (long l = warp; l < nlines; l += nwarps) {
-    long id;
+  const long ngroups = (nlines + NL - 1) / NL;
+  for (long gi = warp; gi < ngroups; gi += nwarps) {
     XTab tb;
     tb.lane = lane;
-    if (MASKED) {
-      id = ids[l];
-      tb.p = tab + (size_t)l * x_table_stride(M);
-    } else {
-      id = l;
-      if (slots[l] >= 0) continue;  // masked line: its own pass
-      tb.p = stab;
-    }
-    const int j = 1 + (int)(id % jtop), k = 1 + (int)(id / jtop);
-    double* line = f + d.P(0, j, k);
-    double x[M];
-    // unknowns t = lane*M + r at positions t (t = 0 stands for x(n))
-    if (M % 2 == 0) {
-      const double2* p2 = reinterpret_cast<const double2*>(line + lane * M);
+    tb.p = MASKED ? tab + (size_t)gi * x_table_stride(M) : stab;
+    double* line[NL];
+    bool ok[NL];
+    double x[NL][M];
 #pragma unroll
-      for (int u = 0; u < M / 2; ++u) {
-        double2 v = p2[u];
-        x[2 * u] = v.x;
-        x[2 * u + 1] = v.y;
+    for (int q = 0; q < NL; ++q) {
+      const long l = gi * NL + q;
+      long id = 0;
+      ok[q] = l < nlines;
+      if (ok[q]) {
+        if (MASKED) id = ids[l];
+        else { id = l; ok[q] = slots[l] < 0; }  // masked lines: their own pass
       }
-    } else {
+      const int j = 1 + (int)(id % jtop), k = 1 + (int)(id / jtop);
+      line[q] = f + d.P(0, j, k);
+      // unknowns t = lane*M + r at positions t (t = 0 stands for x(n))
+      if (ok[q]) {
+        if (M % 2 == 0) {
+          const double2* p2 = reinterpret_cast<const double2*>(line[q] + lane * M);
 #pragma unroll
-      for (int r = 0; r < M; ++r) x[r] = line[lane * M + r];
+          for (int u = 0; u < M / 2; ++u) {
+            double2 v = p2[u];
+            x[q][2 * u] = v.x;
+            x[q][2 * u + 1] = v.y;
+          }
+        } else {
+#pragma unroll
+          for (int r = 0; r < M; ++r) x[q][r] = line[q][lane * M + r];
+        }
+        if (lane == 0) x[q][0] = line[q][n];
+      } else {
+#pragma unroll
+        for (int r = 0; r < M; ++r) x[q][r] = 0.0;
+      }
     }
-    if (lane == 0) x[0] = line[n];
-    // interior rows
-    interior_solve<M>(x, M, tb);
-    const double rhsF = x[0] - tb.v(XT_CF) * x[1];
-    const double rhsE = x[M - 1] - tb.v(XT_AE) * x[M - 2];
-    // reduced system on E
-    double rho = rhsE + tb.v(XT_MU) * rhsF + tb.v(XT_NU) * __shfl_sync(FULL, rhsF, (lane + 1) & 31);
+    // interior rows (Thomas with the tabulated factorisation)
+    double gp[NL];
+#pragma unroll
+    for (int q = 0; q < NL; ++q) gp[q] = x[q][1];
+#pragma unroll
+    for (int r = 2; r <= M - 2; ++r) {
+      const double w = tb.w(r);
+#pragma unroll
+      for (int q = 0; q < NL; ++q) { gp[q] = x[q][r] - w * gp[q]; x[q][r] = gp[q]; }
+    }
+#pragma unroll
+    for (int r = M - 2; r >= 1; --r) {
+      const double rb = tb.rb(r), cc = tb.cc(r);
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        double v = (r == M - 2) ? x[q][r] * rb : (x[q][r] - cc * gp[q]) * rb;
+        x[q][r] = v;
+        gp[q] = v;
+      }
+    }
+    // reduced system: eliminate F, cyclic reduction over the lanes on E
+    double rhsF[NL], rho[NL];
+    {
+      const double cf = tb.v(XT_CF), ae = tb.v(XT_AE), mu = tb.v(XT_MU), nu = tb.v(XT_NU);
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        rhsF[q] = x[q][0] - cf * x[q][1];
+        const double rhsE = x[q][M - 1] - ae * x[q][M - 2];
+        rho[q] = rhsE + mu * rhsF[q] + nu * __shfl_sync(FULL, rhsF[q], (lane + 1) & 31);
+      }
+    }
 #pragma unroll
     for (int lv = 0; lv < 4; ++lv) {
       const int sft = 1 << lv;
-      double rm = __shfl_sync(FULL, rho, (lane - sft) & 31);
-      double rp = __shfl_sync(FULL, rho, (lane + sft) & 31);
-      rho = rho + tb.v(XT_K1 + lv) * rm + tb.v(XT_K2 + lv) * rp;
+      const double k1 = tb.v(XT_K1 + lv), k2 = tb.v(XT_K2 + lv);
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        const double rm = __shfl_sync(FULL, rho[q], (lane - sft) & 31);
+        const double rp = __shfl_sync(FULL, rho[q], (lane + sft) & 31);
+        rho[q] = rho[q] + k1 * rm + k2 * rp;
+      }
     }
-    const double E = tb.v(XT_LAM) * rho + tb.v(XT_KAP) * __shfl_sync(FULL, rho, lane ^ 16);
-    const double Em = __shfl_sync(FULL, E, (lane - 1) & 31);
-    const double F = tb.v(XT_RDF) * rhsF + tb.v(XT_LFR) * Em + tb.v(XT_UFR) * E;
+    {
+      const double lam = tb.v(XT_LAM), kap = tb.v(XT_KAP), rdf = tb.v(XT_RDF);
+      const double lfr = tb.v(XT_LFR), ufr = tb.v(XT_UFR);
 #pragma unroll
-    for (int r = 1; r < M - 1; ++r) x[r] = x[r] + tb.pp(r) * F + tb.qq(r) * E;
-    x[0] = F;
-    x[M - 1] = E;
-    if (M % 2 == 0) {
-      double2* p2 = reinterpret_cast<double2*>(line + lane * M);
-#pragma unroll
-      for (int u = 0; u < M / 2; ++u) p2[u] = make_double2(x[2 * u], x[2 * u + 1]);
-    } else {
-#pragma unroll
-      for (int r = 0; r < M; ++r) line[lane * M + r] = x[r];
+      for (int q = 0; q < NL; ++q) {
+        const double E = lam * rho[q] + kap * __shfl_sync(FULL, rho[q], lane ^ 16);
+        const double Em = __shfl_sync(FULL, E, (lane - 1) & 31);
+        const double F = rdf * rhsF[q] + lfr * Em + ufr * E;
+        rhsF[q] = F;
+        rho[q] = E;
+      }
     }
-    // position 0 received x(n), the value of the periodic ghost x(0)
-    if (lane == 0) line[n] = x[0];
+#pragma unroll
+    for (int r = 1; r < M - 1; ++r) {
+      const double pp = tb.pp(r), qq = tb.qq(r);
+#pragma unroll
+      for (int q = 0; q < NL; ++q) x[q][r] = x[q][r] + pp * rhsF[q] + qq * rho[q];
+    }
+#pragma unroll
+    for (int q = 0; q < NL; ++q) {
+      x[q][0] = rhsF[q];
+      x[q][M - 1] = rho[q];
+      if (!ok[q]) continue;
+      if (M % 2 == 0) {
+        double2* p2 = reinterpret_cast<double2*>(line[q] + lane * M);
+#pragma unroll
+        for (int u = 0; u < M / 2; ++u) p2[u] = make_double2(x[q][2 * u], x[q][2 * u + 1]);
+      } else {
+#pragma unroll
+        for (int r = 0; r < M; ++r) line[q][lane * M + r] = x[q][r];
+      }
+      // position 0 received x(n), the value of the periodic ghost x(0)
+      if (lane == 0) line[q][n] = x[q][0];
+    }
   }
 }
 
@@ -435,16 +495,17 @@ struct YZTab {
   __device__ double qq(int r) const { return __ldg(T + 4 * nu + s + r); }
 };
 
-template <int DIR, int MM, int P>
-__global__ void __launch_bounds__(32 * P) k_yzlines(Dims d, double* __restrict__ f, int nu,
-                                                     int nother, const double* __restrict__ tab,
-                                                     const int* __restrict__ slots,
-                                                     const double* __restrict__ mtab,
-                                                     double ft, double fb, int periodic) {
+// LPB lines per CTA (adjacent in x; 16 lines keep two CTAs resident per SM)
+template <int DIR, int MM, int P, int LPB>
+__global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, double* __restrict__ f, int nu,
+                                                      int nother, const double* __restrict__ tab,
+                                                      const int* __restrict__ slots,
+                                                      const double* __restrict__ mtab,
+                                                      double ft, double fb, int periodic) {
   constexpr int R = 2 * P;
-  __shared__ double red[R * 32];
-  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
-  const int i = 1 + blockIdx.x * 32 + lane;
+  __shared__ double red[R * LPB];
+  const int lane = threadIdx.x % LPB, k = threadIdx.x / LPB;
+  const int i = 1 + blockIdx.x * LPB + lane;
   const int o = 1 + blockIdx.y;  // k of a y line, j of a z line
   const bool valid = i <= d.nx && o <= nother;
   const size_t stride = yz_table_stride(nu, P);
@@ -464,18 +525,16 @@ __global__ void __launch_bounds__(32 * P) k_yzlines(Dims d, double* __restrict__
     // right-hand-side folds of the boundary rows (zero for periodic lines)
     const double c0 = (!periodic && k == 0) ? __ldg(T + 5 * nu + 10 * P + 2) * ft : 0.0;
     const double cN = (!periodic && k == P - 1) ? __ldg(T + 5 * nu + 10 * P + 3) * fb : 0.0;
-    double xe = 0.0;  // the right-hand side of row m-1
+    // every load is issued up front (rows past m re-read row m-1); the
+    // right-hand side of row m-1 is loaded once more on its own, so no
+    // register is selected by the run-time m
 #pragma unroll
-    for (int r = 0; r < MM; ++r)
-      if (r < m) {
-        double v = line[r * es];
-        if (r == 0) v = v - c0;
-        if (r == m - 1) { v = v - cN; xe = v; }
-        x[r] = v;
-      }
+    for (int r = 0; r < MM; ++r) x[r] = line[(long)min(r, m - 1) * es];
+    x[0] = x[0] - c0;
+    const double xe = line[(long)(m - 1) * es] - cN;
     const double xe1 = interior_solve<MM>(x, m, tb);
-    red[(2 * k) * 32 + lane] = x[0] - __ldg(T + 5 * nu + k) * x[1];
-    red[(2 * k + 1) * 32 + lane] = xe - __ldg(T + 5 * nu + P + k) * xe1;
+    red[(2 * k) * LPB + lane] = x[0] - __ldg(T + 5 * nu + k) * x[1];
+    red[(2 * k + 1) * LPB + lane] = xe - __ldg(T + 5 * nu + P + k) * xe1;
   }
   __syncthreads();
   if (!valid) return;
@@ -484,7 +543,7 @@ __global__ void __launch_bounds__(32 * P) k_yzlines(Dims d, double* __restrict__
   double F = 0.0, E = 0.0;
 #pragma unroll
   for (int c = 0; c < R; ++c) {
-    const double rc = red[c * 32 + lane];
+    const double rc = red[c * LPB + lane];
     F = F + __ldg(MI + (2 * k) * R + c) * rc;
     E = E + __ldg(MI + (2 * k + 1) * R + c) * rc;
   }
@@ -506,7 +565,7 @@ int yz_partitions(int nu) { return nu <= 64 ? 4 : (nu <= 128 ? 8 : 16); }
 static int yz_rows(int nu) {
   int P = yz_partitions(nu);
   int m = (nu + P - 1) / P;
-  return m <= 8 ? 8 : 16;
+  return m <= 8 ? 8 : (m <= 12 ? 12 : 16);
 }
 // rows per lane of the x kernel, 0 when the x kernel does not apply
 int x_rows_per_lane(int nx) {
@@ -561,14 +620,15 @@ static void go_x(const Dims& d, double* f, int jtop, const double* tab, const in
     if (cached <= 0) cached = 148;
   }
   sms = cached;
+  constexpr int NL = M <= 8 ? 4 : 2;
   long nlines = (long)jtop * d.nz;
-  long blocks = std::min<long>((long)sms * 8, (nlines + 7) / 8);
+  long blocks = std::min<long>((long)sms * 8, (nlines + 8 * NL - 1) / (8 * NL));
   count_launch();
-  k_xlines<M, false><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots, nullptr, 0);
+  k_xlines<M, NL, false><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots, nullptr, 0);
   if (nmasked > 0) {
     long mb = std::min<long>((long)sms * 8, (nmasked + 7) / 8);
     count_launch();
-    k_xlines<M, true><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids, nmasked);
+    k_xlines<M, 1, true><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids, nmasked);
   }
 }
 
@@ -590,14 +650,16 @@ void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineAr
   int P = yz_partitions(nu);
   int MM = yz_rows(nu);
   int nother = dir == 1 ? d.nz : a.jtop;
-  dim3 grid((d.nx + 31) / 32, nother);
+  constexpr int LPB = 16;
+  dim3 grid((d.nx + LPB - 1) / LPB, nother);
   int periodic = kind >= LK_CYC_VEL ? 1 : 0;
   count_launch();
-#define NSE_YZ(DIR_, MM_, P_)                                                                    \
-  k_yzlines<DIR_, MM_, P_><<<grid, 32 * P_, 0, s>>>(d, f, nu, nother, tab, slots, mtab, a.ft, \
-                                                    a.fb, periodic)
+#define NSE_YZ(DIR_, MM_, P_)                                                                \
+  k_yzlines<DIR_, MM_, P_, LPB><<<grid, LPB * P_, 0, s>>>(d, f, nu, nother, tab, slots, mtab, \
+                                                          a.ft, a.fb, periodic)
 #define NSE_YZ_MM(DIR_, P_)               \
   if (MM == 8) NSE_YZ(DIR_, 8, P_);       \
+  else if (MM == 12) NSE_YZ(DIR_, 12, P_); \
   else NSE_YZ(DIR_, 16, P_);
   if (dir == 1) {
     if (P == 16) { NSE_YZ_MM(1, 16) } else if (P == 8) { NSE_YZ_MM(1, 8) } else { NSE_YZ_MM(1, 4) }

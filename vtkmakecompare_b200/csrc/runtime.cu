@@ -1356,7 +1356,8 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   cudaStream_t s = x->stream;
   double* phi = F(x, NSE_PHI);
   mark(x, PH_FFTX_F);
-  launch_fft_fwd_x(x->pb.pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s);
+  launch_fft_fwd_x(x->pb.pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s,
+                   (x->cfg.flags & NSE_FLAG_EXACT) ? nullptr : &x->rg);
   mark(x, PH_FFTZ_F);
   launch_fft_z(x->pb.pp, false, s);
   mark(x, PH_SPN);
