@@ -197,12 +197,26 @@ typedef struct nse_config {
   int flags;
 } nse_config;
 
+/* NSE_MIXED (no counterpart in the reference): u, v, w, T, p and the Poisson
+ * solution stay FP64; the right-hand-side stencils, the line sweeps and the
+ * FFTs run on FP32 intermediates; the spectral tridiagonal recurrences, the
+ * mean mode, the divergence and the reductions are FP64, and the Poisson
+ * solve takes one FP64 residual-refinement pass.  u_ta, the AB2 histories,
+ * u_ep2 and divu are held in FP32 (upload/download convert).  Needs
+ * nx = 32*M (M in 3, 4, 5, 6, 8, 16) and 12..256 cells in y and z. */
 enum { NSE_FP64 = 0, NSE_MIXED = 1 };
 /* nse_config.flags bits */
 enum {
   NSE_FLAG_CHECK_FINITE = 1, /* nse_step checks every step for non-finite values */
-  NSE_FLAG_EXACT = 4         /* resident step rounds every operation like the reference
+  NSE_FLAG_EXACT = 4,        /* resident step rounds every operation like the reference
                                 (no FMA, true divisions); default is the fast form */
+  NSE_FLAG_REFINE2 = 8,      /* NSE_MIXED: two refinement passes instead of one */
+  NSE_FLAG_POISSON64 = 16,   /* NSE_MIXED: FP64 transforms and spectrum instead of the
+                                FP32 solve with refinement */
+  NSE_FLAG_MATH64 = 32,      /* NSE_MIXED: FP64 arithmetic in the right-hand-side stencils
+                                (their results are still stored in FP32) */
+  NSE_FLAG_LINES64 = 64      /* NSE_MIXED: FP64 arithmetic and tables in the line sweeps
+                                (FP32 storage) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

@@ -194,6 +194,8 @@ struct PoissonPlan {
   const double* KXZ;          // [nz+1][H]
   const double* twx;          // twiddles exp(-2 pi i k/nx), k<nx (complex)
   const double* twz;          // twiddles exp(-2 pi i k/nz)
+  const float* twx_f;         // the same twiddles rounded to FP32
+  const float* twz_f;
 };
 bool poisson_plan_tables(int nx, int ny, int nz, const double* dx, const double* dy,
                          const double* dz, const double* dy12, double xl, double zl,

@@ -43,94 +43,114 @@ static FFTShape make_shape(int n) {
 
 bool fft_size_ok(int n) { return n >= 2 && make_shape(n).nst > 0; }
 
-__device__ __forceinline__ double2 cmul(double2 a, double2 b) {
-  return make_double2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+// complex arithmetic on double2 / float2 (CT); CReal<CT>::T is the real type
+template <class CT> struct CReal;
+template <> struct CReal<double2> { using T = double; };
+template <> struct CReal<float2> { using T = float; };
+template <class CT>
+__device__ __forceinline__ CT mkc(typename CReal<CT>::T x, typename CReal<CT>::T y) {
+  CT r;
+  r.x = x;
+  r.y = y;
+  return r;
 }
-__device__ __forceinline__ double2 cadd(double2 a, double2 b) {
-  return make_double2(a.x + b.x, a.y + b.y);
+template <class CT>
+__device__ __forceinline__ CT cmul(CT a, CT b) {
+  return mkc<CT>(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
 }
-__device__ __forceinline__ double2 csub(double2 a, double2 b) {
-  return make_double2(a.x - b.x, a.y - b.y);
-}
+template <class CT>
+__device__ __forceinline__ CT cadd(CT a, CT b) { return mkc<CT>(a.x + b.x, a.y + b.y); }
+template <class CT>
+__device__ __forceinline__ CT csub(CT a, CT b) { return mkc<CT>(a.x - b.x, a.y - b.y); }
 // multiply by -i (forward) or +i (inverse)
-__device__ __forceinline__ double2 mul_mi(double2 a, bool inv) {
-  return inv ? make_double2(-a.y, a.x) : make_double2(a.y, -a.x);
+template <class CT>
+__device__ __forceinline__ CT mul_mi(CT a, bool inv) {
+  return inv ? mkc<CT>(-a.y, a.x) : mkc<CT>(a.y, -a.x);
 }
 
-template <int R>
-__device__ __forceinline__ void dft_small(double2* v, bool inv);
+template <int R, class CT>
+struct DftSmall;
 
-template <>
-__device__ __forceinline__ void dft_small<2>(double2* v, bool) {
-  double2 a = v[0], b = v[1];
-  v[0] = cadd(a, b);
-  v[1] = csub(a, b);
-}
-template <>
-__device__ __forceinline__ void dft_small<4>(double2* v, bool inv) {
-  double2 t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
-  double2 t2 = cadd(v[1], v[3]), t3 = mul_mi(csub(v[1], v[3]), inv);
-  v[0] = cadd(t0, t2);
-  v[2] = csub(t0, t2);
-  v[1] = cadd(t1, t3);
-  v[3] = csub(t1, t3);
-}
-template <>
-__device__ __forceinline__ void dft_small<3>(double2* v, bool inv) {
-  const double s = 0.86602540378443864676;  // sin(2 pi/3)
-  double2 t = cadd(v[1], v[2]);
-  double2 d = csub(v[1], v[2]);
-  double2 m = make_double2(v[0].x - 0.5 * t.x, v[0].y - 0.5 * t.y);
-  double2 r = mul_mi(make_double2(s * d.x, s * d.y), inv);  // -i s (v1 - v2)
-  v[0] = cadd(v[0], t);
-  v[1] = cadd(m, r);
-  v[2] = csub(m, r);
-}
-template <>
-__device__ __forceinline__ void dft_small<5>(double2* v, bool inv) {
-  const double c1 = 0.30901699437494742410, c2 = -0.80901699437494742410;
-  const double s1 = 0.95105651629515357212, s2 = 0.58778525229247312917;
-  double2 a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
-  double2 b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
-  double2 x0 = v[0];
-  double2 p1 = make_double2(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
-  double2 p2 = make_double2(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
-  double2 q1 = mul_mi(make_double2(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), inv);
-  double2 q2 = mul_mi(make_double2(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), inv);
-  v[0] = make_double2(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
-  v[1] = cadd(p1, q1);
-  v[4] = csub(p1, q1);
-  v[2] = cadd(p2, q2);
-  v[3] = csub(p2, q2);
-}
+template <class CT>
+struct DftSmall<2, CT> {
+  __device__ static void run(CT* v, bool) {
+    CT a = v[0], b = v[1];
+    v[0] = cadd(a, b);
+    v[1] = csub(a, b);
+  }
+};
+template <class CT>
+struct DftSmall<4, CT> {
+  __device__ static void run(CT* v, bool inv) {
+    CT t0 = cadd(v[0], v[2]), t1 = csub(v[0], v[2]);
+    CT t2 = cadd(v[1], v[3]), t3 = mul_mi(csub(v[1], v[3]), inv);
+    v[0] = cadd(t0, t2);
+    v[2] = csub(t0, t2);
+    v[1] = cadd(t1, t3);
+    v[3] = csub(t1, t3);
+  }
+};
+template <class CT>
+struct DftSmall<3, CT> {
+  __device__ static void run(CT* v, bool inv) {
+    using RT = typename CReal<CT>::T;
+    const RT s = (RT)0.86602540378443864676;  // sin(2 pi/3)
+    CT t = cadd(v[1], v[2]);
+    CT d = csub(v[1], v[2]);
+    CT m = mkc<CT>(v[0].x - RT(0.5) * t.x, v[0].y - RT(0.5) * t.y);
+    CT r = mul_mi(mkc<CT>(s * d.x, s * d.y), inv);  // -i s (v1 - v2)
+    v[0] = cadd(v[0], t);
+    v[1] = cadd(m, r);
+    v[2] = csub(m, r);
+  }
+};
+template <class CT>
+struct DftSmall<5, CT> {
+  __device__ static void run(CT* v, bool inv) {
+    using RT = typename CReal<CT>::T;
+    const RT c1 = (RT)0.30901699437494742410, c2 = (RT)-0.80901699437494742410;
+    const RT s1 = (RT)0.95105651629515357212, s2 = (RT)0.58778525229247312917;
+    CT a1 = cadd(v[1], v[4]), a2 = cadd(v[2], v[3]);
+    CT b1 = csub(v[1], v[4]), b2 = csub(v[2], v[3]);
+    CT x0 = v[0];
+    CT p1 = mkc<CT>(x0.x + c1 * a1.x + c2 * a2.x, x0.y + c1 * a1.y + c2 * a2.y);
+    CT p2 = mkc<CT>(x0.x + c2 * a1.x + c1 * a2.x, x0.y + c2 * a1.y + c1 * a2.y);
+    CT q1 = mul_mi(mkc<CT>(s1 * b1.x + s2 * b2.x, s1 * b1.y + s2 * b2.y), inv);
+    CT q2 = mul_mi(mkc<CT>(s2 * b1.x - s1 * b2.x, s2 * b1.y - s1 * b2.y), inv);
+    v[0] = mkc<CT>(x0.x + a1.x + a2.x, x0.y + a1.y + a2.y);
+    v[1] = cadd(p1, q1);
+    v[4] = csub(p1, q1);
+    v[2] = cadd(p2, q2);
+    v[3] = csub(p2, q2);
+  }
+};
 
-// one Stockham stage over `nb` independent FFTs of length N stored
-// contiguously (fft f at src + f*N); all threads of the block cooperate
-template <int R>
-__device__ __forceinline__ void stockham_stage(const double2* __restrict__ src,
-                                               double2* __restrict__ dst, int N, int nb,
-                                               int Ns, const double2* __restrict__ tw,
-                                               bool inv, int fs) {
+// one Stockham stage over `nb` independent FFTs of length N (fft f at
+// src + f*fs); all threads of the block cooperate
+template <int R, class CT>
+__device__ __forceinline__ void stockham_stage(const CT* __restrict__ src, CT* __restrict__ dst,
+                                               int N, int nb, int Ns,
+                                               const CT* __restrict__ tw, bool inv, int fs) {
   int nbf = N / R;
   int total = nbf * nb;
   int tstep = N / (Ns * R);
   for (int t = threadIdx.x; t < total; t += blockDim.x) {
     int f = t / nbf, j = t - f * nbf;
-    const double2* in = src + (long)f * fs;
-    double2* out = dst + (long)f * fs;
-    double2 v[R];
+    const CT* in = src + (long)f * fs;
+    CT* out = dst + (long)f * fs;
+    CT v[R];
 #pragma unroll
     for (int r = 0; r < R; ++r) v[r] = in[j + r * nbf];
     int kj = j % Ns;
     if (Ns > 1) {
 #pragma unroll
       for (int r = 1; r < R; ++r) {
-        double2 w = __ldg(tw + r * kj * tstep);
+        CT w = __ldg(tw + r * kj * tstep);
         if (inv) w.y = -w.y;
         v[r] = cmul(v[r], w);
       }
     }
-    dft_small<R>(v, inv);
+    DftSmall<R, CT>::run(v, inv);
     int idxD = (j / Ns) * Ns * R + kj;
 #pragma unroll
     for (int r = 0; r < R; ++r) out[idxD + r * Ns] = v[r];
@@ -140,8 +160,9 @@ __device__ __forceinline__ void stockham_stage(const double2* __restrict__ src,
 // runs the full FFT; data starts in a, returns the buffer holding the result;
 // FFT f occupies [f*fs, f*fs + N) (fs >= N; fs = N+1 keeps column-wise tiles
 // free of shared-memory bank conflicts)
-__device__ double2* fft_block(double2* a, double2* b, const FFTShape& sh, int nb,
-                              const double2* tw, bool inv, int fs) {
+template <class CT>
+__device__ CT* fft_block(CT* a, CT* b, const FFTShape& sh, int nb, const CT* tw, bool inv,
+                         int fs) {
   int Ns = 1;
   for (int s = 0; s < sh.nst; ++s) {
     int R = sh.rad[s];
@@ -151,7 +172,7 @@ __device__ double2* fft_block(double2* a, double2* b, const FFTShape& sh, int nb
     else if (R == 3) stockham_stage<3>(a, b, sh.n, nb, Ns, tw, inv, fs);
     else stockham_stage<5>(a, b, sh.n, nb, Ns, tw, inv, fs);
     Ns *= R;
-    double2* t = a; a = b; b = t;
+    CT* t = a; a = b; b = t;
   }
   __syncthreads();
   return a;
@@ -159,62 +180,97 @@ __device__ double2* fft_block(double2* a, double2* b, const FFTShape& sh, int nb
 
 // spectral array view: complex element (kx, J, kz) at base[kx + sj*J + sk*kz]
 // (J counted from the first stored plane)
-struct SpecView {
-  double2* base;
+template <class CT>
+struct SpecViewT {
+  CT* base;
   long sj, sk;
 };
+using SpecView = SpecViewT<double2>;
+
+// inputs of the forward x pass: src_mode 0 reads samples of FP; 1 forms the
+// divergence right-hand side of mkp.f:90-97 from ut, vt, wt; 2 forms the
+// residual of that right-hand side against the 7-point operator applied to
+// phi (the iterative-refinement step of the mixed-precision form)
+template <class S>
+struct FwdSrc {
+  const S *FP, *ut, *vt, *wt;
+  const double* phi;
+  GridDev g;
+  GridRcp rg;
+  int use_rcp;
+  double dt;
+  const double* AC;   // [3][ny]
+  double rdx2, rdz2;  // 1/dx^2, 1/dz^2 of the uniform x, z spacings
+};
+
+// FP64 divergence right-hand side at cell (I, J, K) (all three >= 1)
+template <class S>
+__device__ __forceinline__ double div_rhs(const Dims& d, const FwdSrc<S>& q, int I, int J, int K) {
+  long c = d.P(I, J, K);
+  const double du = (double)q.ut[c] - (double)q.ut[c - 1];
+  const double dv = (double)q.vt[c] - (double)q.vt[c - d.sx];
+  const double dw = (double)q.wt[c] - (double)q.wt[c - d.sy];
+  if (q.use_rcp)
+    return (du * q.rg.rdx[I] + dv * q.rg.rdy[J] + dw * q.rg.rdz[K]) * (1.0 / q.dt);
+  return (du / q.g.dx[I] + dv / q.g.dy[J] + dw / q.g.dz[K]) / q.dt;
+}
 
 // ------------------------------------------------------------- x forward --
 // CTA: plane J (1..ny) and `npair` row pairs starting at row 2*npair*blockIdx.y
-__global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecView sv, const double* FP,
-                            const double* ut, const double* vt, const double* wt, GridDev g,
-                            GridRcp rg, int use_rcp, double dt, int src_mode,
-                            const double2* __restrict__ tw) {
-  extern __shared__ double2 smem[];
+template <class CT, class S>
+__global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, FwdSrc<S> q,
+                            int src_mode, const CT* __restrict__ tw) {
+  using RT = typename CReal<CT>::T;
+  extern __shared__ __align__(16) char fsm[];
+  CT* smem = reinterpret_cast<CT*>(fsm);
   const int N = sh.n;
-  double2* a = smem;
-  double2* b = smem + (long)npair * N;
+  CT* a = smem;
+  CT* b = smem + (long)npair * N;
   const int J = 1 + blockIdx.x;
   const int kk0 = 2 * npair * blockIdx.y;
-  const int nx = d.nx, nz = d.nz;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
   for (int t = threadIdx.x; t < npair * N; t += blockDim.x) {
     int pr = t / N, i = t - pr * N;
     int ka = kk0 + 2 * pr, kb = ka + 1;
     double va = 0.0, vb = 0.0;
     if (src_mode == 0) {
-      if (ka < nz) va = FP[d.P(i, J, ka)];
-      if (kb < nz) vb = FP[d.P(i, J, kb)];
+      if (ka < nz) va = (double)q.FP[d.P(i, J, ka)];
+      if (kb < nz) vb = (double)q.FP[d.P(i, J, kb)];
     } else {
-      // divergence RHS of mkp.f:90-97 at the periodic image of sample (i,k)
+      // right-hand side at the periodic image of sample (i,k)
       int I = (i == 0) ? nx : i;
-      for (int q = 0; q < 2; ++q) {
-        int kq = q ? kb : ka;
+      for (int h = 0; h < 2; ++h) {
+        int kq = h ? kb : ka;
         if (kq >= nz) continue;
         int K = (kq == 0) ? nz : kq;
-        long c = d.P(I, J, K);
-        double val;
-        if (use_rcp)
-          val = ((ut[c] - ut[c - 1]) * rg.rdx[I] + (vt[c] - vt[c - d.sx]) * rg.rdy[J] +
-                 (wt[c] - wt[c - d.sy]) * rg.rdz[K]) *
-                (1.0 / dt);
-        else
-          val = ((ut[c] - ut[c - 1]) / g.dx[I] + (vt[c] - vt[c - d.sx]) / g.dy[J] +
-                 (wt[c] - wt[c - d.sy]) / g.dz[K]) /
-                dt;
-        if (q) vb = val; else va = val;
+        double val = div_rhs(d, q, I, J, K);
+        if (src_mode == 2) {
+          // minus the operator the spectral solve inverts (mkp.f:56-84):
+          // periodic second differences in x and z, AC rows in y with the
+          // Neumann ghosts of PHIBC
+          const double* ph = q.phi;
+          long c = d.P(I, J, K);
+          const double p0 = ph[c];
+          const double lx = (ph[c + 1] - 2.0 * p0 + ph[c - 1]) * q.rdx2;
+          const double lz = (ph[c + d.sy] - 2.0 * p0 + ph[c - d.sy]) * q.rdz2;
+          const double ly = q.AC[J - 1] * ph[c - d.sx] + q.AC[J - 1 + ny] * p0 +
+                            q.AC[J - 1 + 2 * ny] * ph[c + d.sx];
+          val = val - (lx + ly + lz);
+        }
+        if (h) vb = val; else va = val;
       }
     }
-    a[t] = make_double2(va, vb);
+    a[t] = mkc<CT>((RT)va, (RT)vb);
   }
-  double2* r = fft_block(a, b, sh, npair, tw, false, N);
+  CT* r = fft_block(a, b, sh, npair, tw, false, N);
   const int H = N / 2 + 1;
   for (int t = threadIdx.x; t < npair * H; t += blockDim.x) {
     int pr = t / H, kx = t - pr * H;
     int ka = kk0 + 2 * pr, kb = ka + 1;
-    double2 Z = r[pr * N + kx];
-    double2 Zr = r[pr * N + ((N - kx) % N)];
-    double2 A = make_double2((Z.x + Zr.x) * 0.5, (Z.y - Zr.y) * 0.5);
-    double2 B = make_double2((Z.y + Zr.y) * 0.5, (Zr.x - Z.x) * 0.5);
+    CT Z = r[pr * N + kx];
+    CT Zr = r[pr * N + ((N - kx) % N)];
+    CT A = mkc<CT>((Z.x + Zr.x) * RT(0.5), (Z.y - Zr.y) * RT(0.5));
+    CT B = mkc<CT>((Z.y + Zr.y) * RT(0.5), (Zr.x - Z.x) * RT(0.5));
     if (ka < nz) sv.base[kx + sv.sj * (J - 1) + sv.sk * ka] = A;
     if (kb < nz) sv.base[kx + sv.sj * (J - 1) + sv.sk * kb] = B;
   }
@@ -222,42 +278,50 @@ __global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecView sv, const d
 
 // -------------------------------------------------------------- z passes --
 // CTA: plane index jj (0..ny-1) and columns kx0..kx0+W-1
-__global__ void k_fft_z(FFTShape sh, int W, int H, SpecView sv, const double2* __restrict__ tw,
+template <class CT>
+__global__ void k_fft_z(FFTShape sh, int W, int H, SpecViewT<CT> sv, const CT* __restrict__ tw,
                         int inv, double nrm) {
-  extern __shared__ double2 smem[];
+  using RT = typename CReal<CT>::T;
+  extern __shared__ __align__(16) char fsm[];
+  CT* smem = reinterpret_cast<CT*>(fsm);
   const int N = sh.n;
   const int FS = N + 1;
-  double2* a = smem;
-  double2* b = smem + (long)W * FS;
+  CT* a = smem;
+  CT* b = smem + (long)W * FS;
   const int jj = blockIdx.y;
   const int kx0 = blockIdx.x * W;
   for (int t = threadIdx.x; t < W * N; t += blockDim.x) {
     int c = t % W, kz = t / W;
     int kx = kx0 + c;
-    double2 v = make_double2(0.0, 0.0);
+    CT v = mkc<CT>(RT(0), RT(0));
     if (kx < H) v = sv.base[kx + sv.sj * jj + sv.sk * kz];
     a[c * FS + kz] = v;
   }
-  double2* r = fft_block(a, b, sh, W, tw, inv != 0, FS);
+  CT* r = fft_block(a, b, sh, W, tw, inv != 0, FS);
+  const RT rn = (RT)nrm;
   for (int t = threadIdx.x; t < W * N; t += blockDim.x) {
     int c = t % W, kz = t / W;
     int kx = kx0 + c;
     if (kx >= H) continue;
-    double2 v = r[c * FS + kz];
-    if (!inv) { v.x = v.x / nrm; v.y = v.y / nrm; }
+    CT v = r[c * FS + kz];
+    if (!inv) { v.x = v.x / rn; v.y = v.y / rn; }
     sv.base[kx + sv.sj * jj + sv.sk * kz] = v;
   }
 }
 
 // ------------------------------------------------------------- x inverse --
 // c2r per row pair with the S2P wrap: FP(i,J,k) = s(i mod NX, k mod NZ) for
-// i = 0..NX, k = 0..NZ (p2s_fftw2d.f:205-216)
-__global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecView sv, double* FP,
-                            const double2* __restrict__ tw) {
-  extern __shared__ double2 smem[];
+// i = 0..NX, k = 0..NZ (p2s_fftw2d.f:205-216); with `accumulate` the
+// transform is added to FP (refinement step) instead of stored
+template <class CT>
+__global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, double* FP,
+                            const CT* __restrict__ tw, int accumulate) {
+  using RT = typename CReal<CT>::T;
+  extern __shared__ __align__(16) char fsm[];
+  CT* smem = reinterpret_cast<CT*>(fsm);
   const int N = sh.n;
-  double2* a = smem;
-  double2* b = smem + (long)npair * N;
+  CT* a = smem;
+  CT* b = smem + (long)npair * N;
   const int J = 1 + blockIdx.x;
   const int kk0 = 2 * npair * blockIdx.y;
   const int nz = d.nz;
@@ -265,24 +329,29 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecView sv, double*
   for (int t = threadIdx.x; t < npair * H; t += blockDim.x) {
     int pr = t / H, kx = t - pr * H;
     int ka = kk0 + 2 * pr, kb = ka + 1;
-    double2 A = make_double2(0.0, 0.0), B = make_double2(0.0, 0.0);
+    CT A = mkc<CT>(RT(0), RT(0)), B = mkc<CT>(RT(0), RT(0));
     if (ka < nz) A = sv.base[kx + sv.sj * (J - 1) + sv.sk * ka];
     if (kb < nz) B = sv.base[kx + sv.sj * (J - 1) + sv.sk * kb];
-    if (kx == 0 || 2 * kx == N) { A.y = 0.0; B.y = 0.0; }
+    if (kx == 0 || 2 * kx == N) { A.y = RT(0); B.y = RT(0); }
     // Z = A + iB at kx, conj(A) + i conj(B) at N - kx
-    a[pr * N + kx] = make_double2(A.x - B.y, A.y + B.x);
-    if (kx > 0 && 2 * kx < N) a[pr * N + (N - kx)] = make_double2(A.x + B.y, B.x - A.y);
+    a[pr * N + kx] = mkc<CT>(A.x - B.y, A.y + B.x);
+    if (kx > 0 && 2 * kx < N) a[pr * N + (N - kx)] = mkc<CT>(A.x + B.y, B.x - A.y);
   }
-  double2* r = fft_block(a, b, sh, npair, tw, true, N);
+  CT* r = fft_block(a, b, sh, npair, tw, true, N);
   for (int t = threadIdx.x; t < npair * (N + 1); t += blockDim.x) {
     int pr = t / (N + 1), i = t - pr * (N + 1);
     int ka = kk0 + 2 * pr, kb = ka + 1;
-    double2 z = r[pr * N + (i % N)];
+    CT z = r[pr * N + (i % N)];
     if (ka < nz) {
-      FP[d.P(i, J, ka)] = z.x;
-      if (ka == 0) FP[d.P(i, J, nz)] = z.x;
+      long c = d.P(i, J, ka);
+      double v = accumulate ? FP[c] + (double)z.x : (double)z.x;
+      FP[c] = v;
+      if (ka == 0) FP[d.P(i, J, nz)] = v;
     }
-    if (kb < nz) FP[d.P(i, J, kb)] = z.y;
+    if (kb < nz) {
+      long c = d.P(i, J, kb);
+      FP[c] = accumulate ? FP[c] + (double)z.y : (double)z.y;
+    }
   }
 }
 
@@ -290,10 +359,15 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecView sv, double*
 // Two threads per (kx, kz) system, on adjacent lanes: one runs the real part
 // of the right-hand side and one the imaginary part (CTRIDIAG's matrix is
 // real, tridiag.f:43-58, so both run the same coefficient recurrence and
-// write the same value of A(I,3) to the scratch).  sv points at plane J = 1;
-// scratch sc holds A(I,3)/A(I,2) at [kx + scj*(J-1) + sck*kz].
-__global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, long sck,
-                      const double* __restrict__ AC, const double* __restrict__ KXZ,
+// write the same value of A(I,3) to the scratch).  base points at plane
+// J = 1 (svj, svk: complex strides); scratch sc holds A(I,3)/A(I,2) at
+// [kx + scj*(J-1) + sck*kz].  RT is the storage type of the spectrum; the
+// recurrences always run in FP64 (the low wavenumbers are nearly singular
+// Neumann systems, where FP32 pivots would amplify rounding by the condition
+// number) and the scratch is FP64.
+template <class RT>
+__global__ void k_spn(int H, int ny, int nz, RT* base, long svj, long svk, double* sc, long scj,
+                      long sck, const double* __restrict__ AC, const double* __restrict__ KXZ,
                       int do_spn, int do_sp0b) {
   const int t = blockIdx.x * blockDim.x + threadIdx.x;
   const int kx = t >> 1, comp = t & 1;
@@ -302,20 +376,20 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
   const double* AC1 = AC;
   const double* AC2 = AC + ny;
   const double* AC3 = AC + 2 * ny;
-  double* B = reinterpret_cast<double*>(sv.base + kx + sv.sk * kz) + comp;
-  const long sj = 2 * sv.sj;  // doubles between planes
+  RT* B = base + 2 * (kx + svk * kz) + comp;
+  const long sj = 2 * svj;  // reals between planes
   if (kx == 0 && kz == 0) {
     if (!do_sp0b) return;
     // SP0B mkp.f:271-288; the ghost PHIT(0,NY+1,0) is set by the caller
     double pm = 0.0, pc = 0.0;
-    double Dn = B[0];  // D(1)
-    B[0] = pc;         // PHIT(0,1,0) = 0
+    double Dn = (double)B[0];  // D(1)
+    B[0] = (RT)pc;             // PHIT(0,1,0) = 0
     for (int J = 1; J <= ny - 1; ++J) {
       double Dj = Dn;
-      Dn = B[sj * J];  // D(J+1), read before it is overwritten
+      Dn = (double)B[sj * J];  // D(J+1), read before it is overwritten
       double a1 = AC1[J - 1], a2 = AC2[J - 1], a3 = AC3[J - 1];
       double pn = (Dj - a1 * pm - a2 * pc) / a3;
-      B[sj * J] = pn;  // PHIT(0,J+1,0)
+      B[sj * J] = (RT)pn;  // PHIT(0,J+1,0)
       pm = pc;
       pc = pn;
     }
@@ -332,12 +406,12 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
   double a2 = AC2[0] - kxz;
   if (NN == 1) { a2 = a2 + AC1[0]; a2 = a2 + AC3[0]; }
   else a2 = a2 + AC1[0];  // AA(1,2) += AA(1,1)
-  double b = B[0];
+  double b = (double)B[0];
   constexpr int FB = 16;
   auto load_f = [&](double (&v)[FB], int I0) {
 #pragma unroll
     for (int q = 0; q < FB; ++q)
-      if (I0 + q <= NN - 1) v[q] = B[sj * (I0 + q)];
+      if (I0 + q <= NN - 1) v[q] = (double)B[sj * (I0 + q)];
   };
   auto elim = [&](const double (&v)[FB], int I0) {
 #pragma unroll
@@ -347,7 +421,7 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
         const double r = 1.0 / a2;
         const double a3 = AC3[I - 1] * r;
         b = b * r;
-        B[sj * (I - 1)] = b;
+        B[sj * (I - 1)] = (RT)b;
         s3[scj * (I - 1)] = a3;
         const double a1n = AC1[I];
         double a2n = AC2[I] - kxz;
@@ -368,13 +442,13 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
     }
   }
   b = b / a2;
-  B[sj * (NN - 1)] = b;
+  B[sj * (NN - 1)] = (RT)b;
   constexpr int BB = 8;
   auto load_b = [&](double (&bi)[BB], double (&av)[BB], int I0) {
 #pragma unroll
     for (int q = 0; q < BB; ++q)
       if (I0 - q >= 1) {
-        bi[q] = B[sj * (I0 - q - 1)];
+        bi[q] = (double)B[sj * (I0 - q - 1)];
         av[q] = s3[scj * (I0 - q - 1)];
       }
   };
@@ -384,7 +458,7 @@ __global__ void k_spn(int H, int ny, int nz, SpecView sv, double* sc, long scj, 
       const int I = I0 - q;
       if (I >= 1) {
         b = bi[q] - av[q] * b;
-        B[sj * (I - 1)] = b;
+        B[sj * (I - 1)] = (RT)b;
       }
     }
   };
@@ -450,54 +524,84 @@ static void smem_optin(const void* kernel, size_t bytes) {
     cudaFuncSetAttribute(kernel, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-static SpecView spec_internal(const PoissonPlan& pp) {
-  SpecView sv;
-  sv.base = reinterpret_cast<double2*>(pp.spec);
+template <class CT>
+static SpecViewT<CT> spec_internal_t(const PoissonPlan& pp) {
+  SpecViewT<CT> sv;
+  sv.base = reinterpret_cast<CT*>(pp.spec);
   sv.sj = pp.Hp;
   sv.sk = (long)pp.Hp * pp.ny;
   return sv;
+}
+
+template <class CT> static const CT* twx_of(const PoissonPlan& pp);
+template <> const double2* twx_of<double2>(const PoissonPlan& pp) {
+  return reinterpret_cast<const double2*>(pp.twx);
+}
+template <> const float2* twx_of<float2>(const PoissonPlan& pp) {
+  return reinterpret_cast<const float2*>(pp.twx_f);
+}
+template <class CT> static const CT* twz_of(const PoissonPlan& pp);
+template <> const double2* twz_of<double2>(const PoissonPlan& pp) {
+  return reinterpret_cast<const double2*>(pp.twz);
+}
+template <> const float2* twz_of<float2>(const PoissonPlan& pp) {
+  return reinterpret_cast<const float2*>(pp.twz_f);
+}
+
+static int row_pairs(const PoissonPlan& pp) {
+  int npair = 1024 / pp.nx;
+  if (npair < 1) npair = 1;
+  if (npair > (pp.nz + 1) / 2) npair = (pp.nz + 1) / 2;
+  return npair;
+}
+
+template <class CT, class S>
+static void fwd_x(const PoissonPlan& pp, const Dims& d, const FwdSrc<S>& q, int src_mode,
+                  cudaStream_t s) {
+  FFTShape sh = make_shape(pp.nx);
+  int npair = row_pairs(pp);
+  dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
+  size_t sm = 2 * (size_t)npair * pp.nx * sizeof(CT);
+  smem_optin((const void*)k_fft_fwd_x<CT, S>, sm);
+  count_launch();
+  k_fft_fwd_x<CT, S><<<grid, fft_threads(npair * pp.nx), sm, s>>>(
+      sh, npair, d, spec_internal_t<CT>(pp), q, src_mode, twx_of<CT>(pp));
 }
 
 void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const double* ut, const double* vt, const double* wt,
                       const GridDev& g, double dt, int src_mode, cudaStream_t s,
                       const GridRcp* rg) {
-  GridRcp r{};
-  if (rg) r = *rg;
-  FFTShape sh = make_shape(pp.nx);
-  int npair = 1024 / pp.nx;
-  if (npair < 1) npair = 1;
-  if (npair > (pp.nz + 1) / 2) npair = (pp.nz + 1) / 2;
-  dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
-  size_t sm = 2 * (size_t)npair * pp.nx * sizeof(double2);
-  smem_optin((const void*)k_fft_fwd_x, sm);
-  count_launch();
-  k_fft_fwd_x<<<grid, fft_threads(npair * pp.nx), sm, s>>>(
-      sh, npair, d, spec_internal(pp), FP, ut, vt, wt, g, r, rg ? 1 : 0, dt, src_mode,
-      reinterpret_cast<const double2*>(pp.twx));
+  FwdSrc<double> q{};
+  q.FP = FP; q.ut = ut; q.vt = vt; q.wt = wt; q.g = g; q.dt = dt;
+  if (rg) { q.rg = *rg; q.use_rcp = 1; }
+  fwd_x<double2, double>(pp, d, q, src_mode, s);
 }
 
-void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
+template <class CT>
+static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
   FFTShape sh = make_shape(pp.nz);
   int W = 2048 / pp.nz;
   if (W < 1) W = 1;
   if (W > 16) W = 16;
   dim3 grid((pp.H + W - 1) / W, pp.ny);
-  size_t sm = 2 * (size_t)W * (pp.nz + 1) * sizeof(double2);
-  smem_optin((const void*)k_fft_z, sm);
+  size_t sm = 2 * (size_t)W * (pp.nz + 1) * sizeof(CT);
+  smem_optin((const void*)k_fft_z<CT>, sm);
   count_launch();
-  k_fft_z<<<grid, fft_threads(W * pp.nz), sm, s>>>(sh, W, pp.H, spec_internal(pp),
-                                                 reinterpret_cast<const double2*>(pp.twz),
-                                                 inverse ? 1 : 0,
-                                                 (double)pp.nx * (double)pp.nz);
+  k_fft_z<CT><<<grid, fft_threads(W * pp.nz), sm, s>>>(sh, W, pp.H, spec_internal_t<CT>(pp),
+                                                       twz_of<CT>(pp), inverse ? 1 : 0,
+                                                       (double)pp.nx * (double)pp.nz);
+}
+void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
+  fft_z<double2>(pp, inverse, s);
 }
 
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s) {
   dim3 grid((2 * pp.H + 63) / 64, pp.nz);
   count_launch();
-  k_spn<<<grid, 64, 0, s>>>(pp.H, pp.ny, pp.nz, spec_internal(pp), pp.scr, pp.Hp,
-                            (long)pp.Hp * pp.ny, pp.AC, pp.KXZ, do_spn ? 1 : 0,
-                            do_sp0b ? 1 : 0);
+  k_spn<double><<<grid, 64, 0, s>>>(pp.H, pp.ny, pp.nz, pp.spec, pp.Hp, (long)pp.Hp * pp.ny,
+                                    pp.scr, pp.Hp, (long)pp.Hp * pp.ny, pp.AC, pp.KXZ,
+                                    do_spn ? 1 : 0, do_sp0b ? 1 : 0);
 }
 
 // k_spn on an arbitrary spectrum view: base points at (kx=0, J=1, kz=0),
@@ -505,27 +609,65 @@ void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s
 void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,
                      long scj, long sck, const double* AC, const double* KXZ, bool do_spn,
                      bool do_sp0b, cudaStream_t s) {
-  SpecView sv;
-  sv.base = reinterpret_cast<double2*>(base);
-  sv.sj = sj;
-  sv.sk = sk;
   dim3 grid((2 * H + 63) / 64, nz);
   count_launch();
-  k_spn<<<grid, 64, 0, s>>>(H, ny, nz, sv, sc, scj, sck, AC, KXZ, do_spn ? 1 : 0,
-                            do_sp0b ? 1 : 0);
+  k_spn<double><<<grid, 64, 0, s>>>(H, ny, nz, base, sj, sk, sc, scj, sck, AC, KXZ,
+                                    do_spn ? 1 : 0, do_sp0b ? 1 : 0);
 }
 
-void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s) {
+template <class CT>
+static void inv_x(const PoissonPlan& pp, const Dims& d, double* FP, bool accumulate,
+                  cudaStream_t s) {
   FFTShape sh = make_shape(pp.nx);
-  int npair = 1024 / pp.nx;
-  if (npair < 1) npair = 1;
-  if (npair > (pp.nz + 1) / 2) npair = (pp.nz + 1) / 2;
+  int npair = row_pairs(pp);
   dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
-  size_t sm = 2 * (size_t)npair * pp.nx * sizeof(double2);
-  smem_optin((const void*)k_fft_inv_x, sm);
+  size_t sm = 2 * (size_t)npair * pp.nx * sizeof(CT);
+  smem_optin((const void*)k_fft_inv_x<CT>, sm);
   count_launch();
-  k_fft_inv_x<<<grid, fft_threads(npair * pp.nx), sm, s>>>(
-      sh, npair, d, spec_internal(pp), FP, reinterpret_cast<const double2*>(pp.twx));
+  k_fft_inv_x<CT><<<grid, fft_threads(npair * pp.nx), sm, s>>>(
+      sh, npair, d, spec_internal_t<CT>(pp), FP, twx_of<CT>(pp), accumulate ? 1 : 0);
+}
+void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s) {
+  inv_x<double2>(pp, d, FP, false, s);
+}
+
+// ---------------------------------------- mixed-precision Poisson solve --
+// FP32 transforms and spectrum, FP64 SPN/SP0B recurrences, and FP64 residual
+// refinement:  phi0 = S(D);  phi = phi0 + S(D - L phi0)  where S is the
+// FP32-stored spectral solve and L the discrete operator it inverts.  D is
+// formed in FP64 from the FP32 fields u*, v*, w*.  mode 1: D; mode 2: the
+// residual D - L phi (phi with PHIBC ghosts).
+void launch_fft_fwd_x_f32(const PoissonPlan& pp, const Dims& d, const GridDev& g,
+                          const GridRcp& rg, const float* ut, const float* vt, const float* wt,
+                          double dt, const double* phi, double dx, double dz, int mode,
+                          cudaStream_t s) {
+  FwdSrc<float> q{};
+  q.ut = ut; q.vt = vt; q.wt = wt; q.g = g; q.rg = rg; q.use_rcp = 1; q.dt = dt;
+  q.phi = phi; q.AC = pp.AC; q.rdx2 = 1.0 / (dx * dx); q.rdz2 = 1.0 / (dz * dz);
+  fwd_x<float2, float>(pp, d, q, mode, s);
+}
+// FP64 transform of the divergence of FP32 fields (mixed form with the FP64
+// Poisson solve)
+void launch_fft_fwd_x_src32(const PoissonPlan& pp, const Dims& d, const GridRcp& rg,
+                            const float* ut, const float* vt, const float* wt, double dt,
+                            cudaStream_t s) {
+  FwdSrc<float> q{};
+  q.ut = ut; q.vt = vt; q.wt = wt; q.rg = rg; q.use_rcp = 1; q.dt = dt;
+  fwd_x<double2, float>(pp, d, q, 1, s);
+}
+void launch_fft_z_f32(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
+  fft_z<float2>(pp, inverse, s);
+}
+void launch_spn_f32(const PoissonPlan& pp, cudaStream_t s) {
+  dim3 grid((2 * pp.H + 63) / 64, pp.nz);
+  count_launch();
+  k_spn<float><<<grid, 64, 0, s>>>(pp.H, pp.ny, pp.nz, reinterpret_cast<float*>(pp.spec), pp.Hp,
+                                   (long)pp.Hp * pp.ny, pp.scr, pp.Hp, (long)pp.Hp * pp.ny,
+                                   pp.AC, pp.KXZ, 1, 1);
+}
+void launch_fft_inv_x_f32(const PoissonPlan& pp, const Dims& d, double* phi, bool accumulate,
+                          cudaStream_t s) {
+  inv_x<float2>(pp, d, phi, accumulate, s);
 }
 
 void launch_phibc(const Dims& d, double* PHI, cudaStream_t s) {

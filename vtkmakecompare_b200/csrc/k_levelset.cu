@@ -125,8 +125,9 @@ void launch_levelset_mask(const Dims& d, const GridDev& g, const double* phi,
 // [2] sum |v| dy, [3] sum |w| dz, [4] sum T dx dy dz, [5] non-finite count of
 // u, v, w, T.  Two passes (per-block partials, then one block) so the result
 // does not depend on scheduling.
+template <class DV>
 __global__ void k_monitor_partial(Dims d, GridDev g, const double* u, const double* v,
-                                  const double* w, const double* T, const double* divu,
+                                  const double* w, const double* T, const DV* divu,
                                   double* part) {
   __shared__ double sh[6][256];
   double acc[6] = {0, 0, 0, 0, 0, 0};
@@ -139,7 +140,7 @@ __global__ void k_monitor_partial(Dims d, GridDev g, const double* u, const doub
     int k = 1 + (int)(r / d.ny);
     long c = d.P(i, j, k);
     double uu = u[c], vv = v[c], ww = w[c], tt = T[c];
-    acc[0] = fmax(acc[0], fabs(divu[c]));
+    acc[0] = fmax(acc[0], fabs((double)divu[c]));
     acc[1] += fabs(uu) * g.dx[i];
     acc[2] += fabs(vv) * g.dy[j];
     acc[3] += fabs(ww) * g.dz[k];
@@ -178,15 +179,27 @@ __global__ void k_monitor_final(const double* part, int nb, double* out) {
     for (int q = 0; q < 6; ++q) out[q] = sh[q][0];
 }
 // out6 must hold 6 + 6*592 doubles of device memory (partials follow)
-void launch_monitor(const Dims& d, const GridDev& g, const double* u, const double* v,
-                    const double* w, const double* T, const double* divu, double* out6,
+template <class DV>
+static void monitor(const Dims& d, const GridDev& g, const double* u, const double* v,
+                    const double* w, const double* T, const DV* divu, double* out6,
                     cudaStream_t s) {
   const int nb = 592;  // 4 blocks per SM on a 148-SM part
   double* part = out6 + 6;
   count_launch();
-  k_monitor_partial<<<nb, 256, 0, s>>>(d, g, u, v, w, T, divu, part);
+  k_monitor_partial<DV><<<nb, 256, 0, s>>>(d, g, u, v, w, T, divu, part);
   count_launch();
   k_monitor_final<<<1, 256, 0, s>>>(part, nb, out6);
+}
+void launch_monitor(const Dims& d, const GridDev& g, const double* u, const double* v,
+                    const double* w, const double* T, const double* divu, double* out6,
+                    cudaStream_t s) {
+  monitor<double>(d, g, u, v, w, T, divu, out6, s);
+}
+// mixed-precision form: divu stored in FP32 (the reductions stay FP64)
+void launch_monitor_f32(const Dims& d, const GridDev& g, const double* u, const double* v,
+                        const double* w, const double* T, const float* divu, double* out6,
+                        cudaStream_t s) {
+  monitor<float>(d, g, u, v, w, T, divu, out6, s);
 }
 
 }  // namespace nse

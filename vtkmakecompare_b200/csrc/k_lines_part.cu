@@ -310,22 +310,30 @@ __global__ void k_build_x(Dims d, GridDev g, const double* c1, LineArgs a, const
 }
 
 // =============================================================== solvers ==
+// The solvers are templates on the storage type S of the line data and on
+// the arithmetic and table type R (both double in the FP64 form; in the
+// mixed-precision form S is float and R float, or double with the FP64
+// tables).
+template <class T> struct Vec2T;
+template <> struct Vec2T<double> { using T = double2; };
+template <> struct Vec2T<float> { using T = float2; };
+
 // interior Thomas on registers: g <- solution of the interior rows with
 // zero end values; rows r = 1..m-2 of the partition, table rows at tb(r).
 // Returns g(m-2) (taken inside the unrolled chain: selecting x[m-2] after
 // the loop would make the compiler index x dynamically, in local memory).
-template <int MM, class TB>
-__device__ __forceinline__ double interior_solve(double (&x)[MM], int m, const TB& tb) {
-  double gp = x[1];
+template <int MM, class R, class TB>
+__device__ __forceinline__ R interior_solve(R (&x)[MM], int m, const TB& tb) {
+  R gp = x[1];
 #pragma unroll
   for (int r = 2; r < MM - 1; ++r)
     if (r <= m - 2) { gp = x[r] - tb.w(r) * gp; x[r] = gp; }
-  double gn = 0.0, glast = 0.0;
+  R gn = R(0), glast = R(0);
 #pragma unroll
   for (int r = MM - 2; r >= 1; --r)
     if (r <= m - 2) {
       // gn is still 0 at r = m-2, so this is x(m-2) * rb there
-      double v = (x[r] - tb.cc(r) * gn) * tb.rb(r);
+      R v = (x[r] - tb.cc(r) * gn) * tb.rb(r);
       if (r == m - 2) glast = v;
       x[r] = v;
       gn = v;
@@ -335,26 +343,28 @@ __device__ __forceinline__ double interior_solve(double (&x)[MM], int m, const T
 
 // x lines: table of lane `lane`, values at p[v * 32 + lane] (shared memory
 // for the mask-free lines, global memory for a masked line)
+template <class R>
 struct XTab {
-  const double* p;
+  const R* p;
   int lane;
-  __device__ double v(int i) const { return p[i * 32 + lane]; }
-  __device__ double w(int r) const { return v(XT_ROW + 5 * (r - 1)); }
-  __device__ double rb(int r) const { return v(XT_ROW + 5 * (r - 1) + 1); }
-  __device__ double cc(int r) const { return v(XT_ROW + 5 * (r - 1) + 2); }
-  __device__ double pp(int r) const { return v(XT_ROW + 5 * (r - 1) + 3); }
-  __device__ double qq(int r) const { return v(XT_ROW + 5 * (r - 1) + 4); }
+  __device__ R v(int i) const { return p[i * 32 + lane]; }
+  __device__ R w(int r) const { return v(XT_ROW + 5 * (r - 1)); }
+  __device__ R rb(int r) const { return v(XT_ROW + 5 * (r - 1) + 1); }
+  __device__ R cc(int r) const { return v(XT_ROW + 5 * (r - 1) + 2); }
+  __device__ R pp(int r) const { return v(XT_ROW + 5 * (r - 1) + 3); }
+  __device__ R qq(int r) const { return v(XT_ROW + 5 * (r - 1) + 4); }
 };
 
 // NL lines per warp iteration share every table load (the table reads, not
 // the line data, dominate the L1 traffic of this kernel)
-template <int M, int NL, bool MASKED>
-__global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, int jtop,
-                                                const double* __restrict__ tab,
+template <int M, int NL, bool MASKED, class S, class R>
+__global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int jtop,
+                                                const R* __restrict__ tab,
                                                 const int* __restrict__ slots,
                                                 const int* __restrict__ ids, int count) {
+  using V2 = typename Vec2T<S>::T;
   constexpr int NV = x_table_values(M);
-  __shared__ double stab[MASKED ? 1 : NV * 32];
+  __shared__ R stab[MASKED ? 1 : NV * 32];
   const int lane = threadIdx.x & 31;
   const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
@@ -367,12 +377,12 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, 
   const long nlines = MASKED ? count : (long)jtop * d.nz;
   const long ngroups = (nlines + NL - 1) / NL;
   for (long gi = warp; gi < ngroups; gi += nwarps) {
-    XTab tb;
+    XTab<R> tb;
     tb.lane = lane;
     tb.p = MASKED ? tab + (size_t)gi * x_table_stride(M) : stab;
-    double* line[NL];
+    S* line[NL];
     bool ok[NL];
-    double x[NL][M];
+    R x[NL][M];
 #pragma unroll
     for (int q = 0; q < NL; ++q) {
       const long l = gi * NL + q;
@@ -387,80 +397,80 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, 
       // unknowns t = lane*M + r at positions t (t = 0 stands for x(n))
       if (ok[q]) {
         if (M % 2 == 0) {
-          const double2* p2 = reinterpret_cast<const double2*>(line[q] + lane * M);
+          const V2* p2 = reinterpret_cast<const V2*>(line[q] + lane * M);
 #pragma unroll
           for (int u = 0; u < M / 2; ++u) {
-            double2 v = p2[u];
-            x[q][2 * u] = v.x;
-            x[q][2 * u + 1] = v.y;
+            V2 v = p2[u];
+            x[q][2 * u] = (R)v.x;
+            x[q][2 * u + 1] = (R)v.y;
           }
         } else {
 #pragma unroll
-          for (int r = 0; r < M; ++r) x[q][r] = line[q][lane * M + r];
+          for (int r = 0; r < M; ++r) x[q][r] = (R)line[q][lane * M + r];
         }
-        if (lane == 0) x[q][0] = line[q][n];
+        if (lane == 0) x[q][0] = (R)line[q][n];
       } else {
 #pragma unroll
-        for (int r = 0; r < M; ++r) x[q][r] = 0.0;
+        for (int r = 0; r < M; ++r) x[q][r] = R(0);
       }
     }
     // interior rows (Thomas with the tabulated factorisation)
-    double gp[NL];
+    R gp[NL];
 #pragma unroll
     for (int q = 0; q < NL; ++q) gp[q] = x[q][1];
 #pragma unroll
     for (int r = 2; r <= M - 2; ++r) {
-      const double w = tb.w(r);
+      const R w = tb.w(r);
 #pragma unroll
       for (int q = 0; q < NL; ++q) { gp[q] = x[q][r] - w * gp[q]; x[q][r] = gp[q]; }
     }
 #pragma unroll
     for (int r = M - 2; r >= 1; --r) {
-      const double rb = tb.rb(r), cc = tb.cc(r);
+      const R rb = tb.rb(r), cc = tb.cc(r);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        double v = (r == M - 2) ? x[q][r] * rb : (x[q][r] - cc * gp[q]) * rb;
+        R v = (r == M - 2) ? x[q][r] * rb : (x[q][r] - cc * gp[q]) * rb;
         x[q][r] = v;
         gp[q] = v;
       }
     }
     // reduced system: eliminate F, cyclic reduction over the lanes on E
-    double rhsF[NL], rho[NL];
+    R rhsF[NL], rho[NL];
     {
-      const double cf = tb.v(XT_CF), ae = tb.v(XT_AE), mu = tb.v(XT_MU), nu = tb.v(XT_NU);
+      const R cf = tb.v(XT_CF), ae = tb.v(XT_AE), mu = tb.v(XT_MU), nu = tb.v(XT_NU);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
         rhsF[q] = x[q][0] - cf * x[q][1];
-        const double rhsE = x[q][M - 1] - ae * x[q][M - 2];
+        const R rhsE = x[q][M - 1] - ae * x[q][M - 2];
         rho[q] = rhsE + mu * rhsF[q] + nu * __shfl_sync(FULL, rhsF[q], (lane + 1) & 31);
       }
     }
 #pragma unroll
     for (int lv = 0; lv < 4; ++lv) {
       const int sft = 1 << lv;
-      const double k1 = tb.v(XT_K1 + lv), k2 = tb.v(XT_K2 + lv);
+      const R k1 = tb.v(XT_K1 + lv), k2 = tb.v(XT_K2 + lv);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        const double rm = __shfl_sync(FULL, rho[q], (lane - sft) & 31);
-        const double rp = __shfl_sync(FULL, rho[q], (lane + sft) & 31);
+        const R rm = __shfl_sync(FULL, rho[q], (lane - sft) & 31);
+        const R rp = __shfl_sync(FULL, rho[q], (lane + sft) & 31);
         rho[q] = rho[q] + k1 * rm + k2 * rp;
       }
     }
     {
-      const double lam = tb.v(XT_LAM), kap = tb.v(XT_KAP), rdf = tb.v(XT_RDF);
-      const double lfr = tb.v(XT_LFR), ufr = tb.v(XT_UFR);
+      const R lam = tb.v(XT_LAM), kap = tb.v(XT_KAP), rdf = tb.v(XT_RDF);
+      const R lfr = tb.v(XT_LFR), ufr = tb.v(XT_UFR);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        const double E = lam * rho[q] + kap * __shfl_sync(FULL, rho[q], lane ^ 16);
-        const double Em = __shfl_sync(FULL, E, (lane - 1) & 31);
-        const double F = rdf * rhsF[q] + lfr * Em + ufr * E;
+        const R E = lam * rho[q] + kap * __shfl_sync(FULL, rho[q], lane ^ 16);
+        const R Em = __shfl_sync(FULL, E, (lane - 1) & 31);
+        const R F = rdf * rhsF[q] + lfr * Em + ufr * E;
         rhsF[q] = F;
         rho[q] = E;
       }
     }
 #pragma unroll
     for (int r = 1; r < M - 1; ++r) {
-      const double pp = tb.pp(r), qq = tb.qq(r);
+      const R pp = tb.pp(r), qq = tb.qq(r);
 #pragma unroll
       for (int q = 0; q < NL; ++q) x[q][r] = x[q][r] + pp * rhsF[q] + qq * rho[q];
     }
@@ -470,46 +480,54 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, double* __restrict__ f, 
       x[q][M - 1] = rho[q];
       if (!ok[q]) continue;
       if (M % 2 == 0) {
-        double2* p2 = reinterpret_cast<double2*>(line[q] + lane * M);
+        V2* p2 = reinterpret_cast<V2*>(line[q] + lane * M);
 #pragma unroll
-        for (int u = 0; u < M / 2; ++u) p2[u] = make_double2(x[q][2 * u], x[q][2 * u + 1]);
+        for (int u = 0; u < M / 2; ++u) {
+          V2 v;
+          v.x = (S)x[q][2 * u];
+          v.y = (S)x[q][2 * u + 1];
+          p2[u] = v;
+        }
       } else {
 #pragma unroll
-        for (int r = 0; r < M; ++r) line[q][lane * M + r] = x[q][r];
+        for (int r = 0; r < M; ++r) line[q][lane * M + r] = (S)x[q][r];
       }
       // position 0 received x(n), the value of the periodic ghost x(0)
-      if (lane == 0) line[q][n] = x[q][0];
+      if (lane == 0) line[q][n] = (S)x[q][0];
     }
   }
 }
 
 // y / z lines: table values read through the cache (one table for all the
 // mask-free lanes, so the loads broadcast)
+template <class R>
 struct YZTab {
-  const double* T;
+  const R* T;
   int nu, s;
-  __device__ double w(int r) const { return __ldg(T + s + r); }
-  __device__ double rb(int r) const { return __ldg(T + nu + s + r); }
-  __device__ double cc(int r) const { return __ldg(T + 2 * nu + s + r); }
-  __device__ double pp(int r) const { return __ldg(T + 3 * nu + s + r); }
-  __device__ double qq(int r) const { return __ldg(T + 4 * nu + s + r); }
+  __device__ R w(int r) const { return __ldg(T + s + r); }
+  __device__ R rb(int r) const { return __ldg(T + nu + s + r); }
+  __device__ R cc(int r) const { return __ldg(T + 2 * nu + s + r); }
+  __device__ R pp(int r) const { return __ldg(T + 3 * nu + s + r); }
+  __device__ R qq(int r) const { return __ldg(T + 4 * nu + s + r); }
 };
 
-// LPB lines per CTA (adjacent in x; 16 lines keep two CTAs resident per SM)
-template <int DIR, int MM, int P, int LPB>
-__global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, double* __restrict__ f, int nu,
-                                                      int nother, const double* __restrict__ tab,
+// LPB lines per CTA (adjacent in x; 16 lines keep two CTAs resident per SM).
+// The solution goes to `out` (type RO) when given, else back into f.
+template <int DIR, int MM, int P, int LPB, class S, class R, class RO>
+__global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
+                                                      RO* __restrict__ out, int nu, int nother,
+                                                      const R* __restrict__ tab,
                                                       const int* __restrict__ slots,
-                                                      const double* __restrict__ mtab,
-                                                      double ft, double fb, int periodic) {
-  constexpr int R = 2 * P;
-  __shared__ double red[R * LPB];
+                                                      const R* __restrict__ mtab, R ft, R fb,
+                                                      int periodic) {
+  constexpr int R2 = 2 * P;
+  __shared__ R red[R2 * LPB];
   const int lane = threadIdx.x % LPB, k = threadIdx.x / LPB;
   const int i = 1 + blockIdx.x * LPB + lane;
   const int o = 1 + blockIdx.y;  // k of a y line, j of a z line
   const bool valid = i <= d.nx && o <= nother;
   const size_t stride = yz_table_stride(nu, P);
-  const double* T = tab;
+  const R* T = tab;
   if (valid) {
     long lineid = (long)(i - 1) + (long)d.nx * (o - 1);
     int slot = slots[lineid];
@@ -518,34 +536,35 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, double* __restrict_
   const int s = (int)((long)k * nu / P), e = (int)((long)(k + 1) * nu / P) - 1;
   const int m = e - s + 1;
   const long es = DIR == 1 ? d.sx : d.sy;
-  double* line = f + (DIR == 1 ? d.P(i, 0, o) : d.P(i, o, 0)) + (long)(s + 1) * es;
-  double x[MM];
-  YZTab tb{T, nu, s};
+  const long off = (DIR == 1 ? d.P(i, 0, o) : d.P(i, o, 0)) + (long)(s + 1) * es;
+  const S* line = f + off;
+  R x[MM];
+  YZTab<R> tb{T, nu, s};
   if (valid) {
     // right-hand-side folds of the boundary rows (zero for periodic lines)
-    const double c0 = (!periodic && k == 0) ? __ldg(T + 5 * nu + 10 * P + 2) * ft : 0.0;
-    const double cN = (!periodic && k == P - 1) ? __ldg(T + 5 * nu + 10 * P + 3) * fb : 0.0;
+    const R c0 = (!periodic && k == 0) ? __ldg(T + 5 * nu + 10 * P + 2) * ft : R(0);
+    const R cN = (!periodic && k == P - 1) ? __ldg(T + 5 * nu + 10 * P + 3) * fb : R(0);
     // every load is issued up front (rows past m re-read row m-1); the
     // right-hand side of row m-1 is loaded once more on its own, so no
     // register is selected by the run-time m
 #pragma unroll
-    for (int r = 0; r < MM; ++r) x[r] = line[(long)min(r, m - 1) * es];
+    for (int r = 0; r < MM; ++r) x[r] = (R)line[(long)min(r, m - 1) * es];
     x[0] = x[0] - c0;
-    const double xe = line[(long)(m - 1) * es] - cN;
-    const double xe1 = interior_solve<MM>(x, m, tb);
+    const R xe = (R)line[(long)(m - 1) * es] - cN;
+    const R xe1 = interior_solve<MM>(x, m, tb);
     red[(2 * k) * LPB + lane] = x[0] - __ldg(T + 5 * nu + k) * x[1];
     red[(2 * k + 1) * LPB + lane] = xe - __ldg(T + 5 * nu + P + k) * xe1;
   }
   __syncthreads();
   if (!valid) return;
   // F and E of this partition: rows 2k and 2k+1 of the reduced inverse
-  const double* MI = T + 5 * nu + 10 * P + 4;
-  double F = 0.0, E = 0.0;
+  const R* MI = T + 5 * nu + 10 * P + 4;
+  R F = R(0), E = R(0);
 #pragma unroll
-  for (int c = 0; c < R; ++c) {
-    const double rc = red[c * LPB + lane];
-    F = F + __ldg(MI + (2 * k) * R + c) * rc;
-    E = E + __ldg(MI + (2 * k + 1) * R + c) * rc;
+  for (int c = 0; c < R2; ++c) {
+    const R rc = red[c * LPB + lane];
+    F = F + __ldg(MI + (2 * k) * R2 + c) * rc;
+    E = E + __ldg(MI + (2 * k + 1) * R2 + c) * rc;
   }
 #pragma unroll
   for (int r = 1; r < MM; ++r) {
@@ -553,9 +572,10 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, double* __restrict_
     if (r == m - 1) x[r] = E;
   }
   x[0] = F;
+  RO* dst = out ? out + off : reinterpret_cast<RO*>(f + off);
 #pragma unroll
   for (int r = 0; r < MM; ++r)
-    if (r < m) line[r * es] = x[r];
+    if (r < m) dst[r * es] = (RO)x[r];
 }
 
 // ============================================================== launchers
@@ -574,7 +594,9 @@ int x_rows_per_lane(int nx) {
   return (M == 3 || M == 4 || M == 5 || M == 6 || M == 8 || M == 16) ? M : 0;
 }
 // the y/z kernel needs at least 3 and at most 16 rows per partition
-static bool yz_ok(int nu) { return nu / yz_partitions(nu) >= 3 && (nu + yz_partitions(nu) - 1) / yz_partitions(nu) <= 16; }
+static bool yz_ok(int nu) {
+  return nu / yz_partitions(nu) >= 3 && (nu + yz_partitions(nu) - 1) / yz_partitions(nu) <= 16;
+}
 bool part_lines_supported(const Dims& d) {
   return x_rows_per_lane(d.nx) > 0 && yz_ok(d.ny - 1) && yz_ok(d.ny) && yz_ok(d.nz);
 }
@@ -608,10 +630,7 @@ void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, cons
   }
 }
 
-template <int M>
-static void go_x(const Dims& d, double* f, int jtop, const double* tab, const int* slots,
-                 const int* ids, int nmasked, const double* mtab, cudaStream_t s) {
-  int sms = 148;
+static int sm_count() {
   static int cached = 0;
   if (!cached) {
     int dev = 0;
@@ -619,22 +638,31 @@ static void go_x(const Dims& d, double* f, int jtop, const double* tab, const in
     cudaDeviceGetAttribute(&cached, cudaDevAttrMultiProcessorCount, dev);
     if (cached <= 0) cached = 148;
   }
-  sms = cached;
+  return cached;
+}
+
+template <int M, class S, class R>
+static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, const int* ids,
+                 int nmasked, const R* mtab, cudaStream_t s) {
+  const int sms = sm_count();
   constexpr int NL = M <= 8 ? 4 : 2;
   long nlines = (long)jtop * d.nz;
   long blocks = std::min<long>((long)sms * 8, (nlines + 8 * NL - 1) / (8 * NL));
   count_launch();
-  k_xlines<M, NL, false><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots, nullptr, 0);
+  k_xlines<M, NL, false, S, R><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots, nullptr,
+                                                                 0);
   if (nmasked > 0) {
     long mb = std::min<long>((long)sms * 8, (nmasked + 7) / 8);
     count_launch();
-    k_xlines<M, 1, true><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids, nmasked);
+    k_xlines<M, 1, true, S, R><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids,
+                                                            nmasked);
   }
 }
 
-void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
-                       const double* tab, const int* slots, const int* ids, int nmasked,
-                       const double* mtab, cudaStream_t s) {
+template <class S, class R, class RO>
+static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const LineArgs& a,
+                       const R* tab, const int* slots, const int* ids, int nmasked,
+                       const R* mtab, cudaStream_t s) {
   if (dir == 0) {
     switch (x_rows_per_lane(d.nx)) {
       case 3: go_x<3>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
@@ -653,12 +681,13 @@ void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineAr
   constexpr int LPB = 16;
   dim3 grid((d.nx + LPB - 1) / LPB, nother);
   int periodic = kind >= LK_CYC_VEL ? 1 : 0;
+  const R ft = (R)a.ft, fb = (R)a.fb;
   count_launch();
-#define NSE_YZ(DIR_, MM_, P_)                                                                \
-  k_yzlines<DIR_, MM_, P_, LPB><<<grid, LPB * P_, 0, s>>>(d, f, nu, nother, tab, slots, mtab, \
-                                                          a.ft, a.fb, periodic)
-#define NSE_YZ_MM(DIR_, P_)               \
-  if (MM == 8) NSE_YZ(DIR_, 8, P_);       \
+#define NSE_YZ(DIR_, MM_, P_)                                                               \
+  k_yzlines<DIR_, MM_, P_, LPB, S, R, RO><<<grid, LPB * P_, 0, s>>>(                        \
+      d, f, out, nu, nother, tab, slots, mtab, ft, fb, periodic)
+#define NSE_YZ_MM(DIR_, P_)                \
+  if (MM == 8) NSE_YZ(DIR_, 8, P_);        \
   else if (MM == 12) NSE_YZ(DIR_, 12, P_); \
   else NSE_YZ(DIR_, 16, P_);
   if (dir == 1) {
@@ -668,6 +697,48 @@ void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineAr
   }
 #undef NSE_YZ_MM
 #undef NSE_YZ
+}
+
+void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
+                       const double* tab, const int* slots, const int* ids, int nmasked,
+                       const double* mtab, cudaStream_t s) {
+  lines_part<double, double, double>(dir, kind, d, f, nullptr, a, tab, slots, ids, nmasked,
+                                     mtab, s);
+}
+
+// mixed-precision form: FP32 line data with FP32 arithmetic and tables, or
+// (tab64/mtab64 given) FP64 arithmetic and tables; a y or z solve may write
+// its result to a separate FP64 array (`out`, the temperature's last sweep)
+void launch_lines_part_f32(int dir, int kind, const Dims& d, float* f, double* out,
+                           const LineArgs& a, const float* tab, const int* slots,
+                           const int* ids, int nmasked, const float* mtab,
+                           const double* tab64, const double* mtab64, cudaStream_t s) {
+  const bool to64 = out && dir != 0;
+  if (tab64) {
+    if (to64)
+      lines_part<float, double, double>(dir, kind, d, f, out, a, tab64, slots, ids, nmasked,
+                                        mtab64, s);
+    else
+      lines_part<float, double, float>(dir, kind, d, f, nullptr, a, tab64, slots, ids, nmasked,
+                                       mtab64, s);
+  } else if (to64) {
+    lines_part<float, float, double>(dir, kind, d, f, out, a, tab, slots, ids, nmasked, mtab, s);
+  } else {
+    lines_part<float, float, float>(dir, kind, d, f, nullptr, a, tab, slots, ids, nmasked, mtab,
+                                    s);
+  }
+}
+
+// the FP64 tables rounded to FP32 for the mixed-precision form
+__global__ void k_round_table(const double* __restrict__ in, float* __restrict__ out, long n) {
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x)
+    out[t] = (float)in[t];
+}
+void launch_round_table(const double* in, float* out, long n, cudaStream_t s) {
+  if (n <= 0) return;
+  count_launch();
+  k_round_table<<<(unsigned)std::min<long>((n + 255) / 256, 4096), 256, 0, s>>>(in, out, n);
 }
 
 }  // namespace nse

@@ -30,26 +30,34 @@ constexpr int SXW = TXW + 2, SYW = TYW + 2;
 constexpr int PLANE = SXW * SYW;     // one halo plane of one field
 constexpr int TILE = TXW * TYW;      // one interior plane of one field
 // a ring slot holds plane K of: u, v, w, T, c1 (halo) and the four AB2
-// histories (interior)
-constexpr int SLOT = 5 * PLANE + 4 * TILE;
+// histories (interior); its size in bytes is slot_bytes<H>() below
 constexpr int NSLOT = 5;             // k-1, k, k+1 in use, k+2 and k+3 in flight
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
   asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(sa), "l"(gmem) : "memory");
 }
+__device__ __forceinline__ void cp_async8(float* smem, const float* gmem) {
+  unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 4;\n" ::"r"(sa), "l"(gmem) : "memory");
+}
+// bytes of one ring slot: five halo planes of FP64 fields, then four tiles of
+// the AB2 histories in their storage type H
+template <class H>
+__host__ __device__ constexpr int slot_bytes() { return 5 * PLANE * 8 + 4 * TILE * (int)sizeof(H); }
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
 // plane K into ring slot K mod NSLOT (one commit group, possibly empty)
-__device__ __forceinline__ void load_plane(double* sm, const Dims& d, int i0, int j0, int K,
+template <class H>
+__device__ __forceinline__ void load_plane(char* sm, const Dims& d, int i0, int j0, int K,
                                            int kmax, const double* U, const double* V,
                                            const double* W, const double* T, const double* C1,
-                                           const double* UP, const double* VP,
-                                           const double* WP, const double* TP) {
+                                           const H* UP, const H* VP, const H* WP,
+                                           const H* TP) {
   if (K <= kmax) {
-    double* slot = sm + (K % NSLOT) * SLOT;
+    double* slot = reinterpret_cast<double*>(sm + (K % NSLOT) * slot_bytes<H>());
     const int tid = threadIdx.y * TXW + threadIdx.x;
     for (int e = tid; e < PLANE; e += TILE) {
       int tx = e % SXW, ty = e / SXW;
@@ -66,7 +74,7 @@ __device__ __forceinline__ void load_plane(double* sm, const Dims& d, int i0, in
     int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
     if (i <= d.nx && j <= d.ny && K >= 1 && K <= d.nz) {
       long c = d.P(i, j, K);
-      double* h = slot + 5 * PLANE + tid;
+      H* h = reinterpret_cast<H*>(slot + 5 * PLANE) + tid;
       cp_async8(h, UP + c);
       cp_async8(h + TILE, VP + c);
       cp_async8(h + 2 * TILE, WP + c);
@@ -76,15 +84,19 @@ __device__ __forceinline__ void load_plane(double* sm, const Dims& d, int i0, in
   cp_async_commit();
 }
 
+// H: storage type of the histories, u_ta and the outputs (double; float in
+// the mixed-precision form); CT: arithmetic type (FP32 arithmetic rounds the
+// FP64 state as it is read from the ring)
+template <class H, class CT>
 __global__ void __launch_bounds__(256, 2) k_rhs_fast(
     Dims d, GridDev g, GridRcp rg, StepParams sp, const double* __restrict__ U,
     const double* __restrict__ V, const double* __restrict__ W, const double* __restrict__ T,
-    const double* __restrict__ U_TA, const double* __restrict__ V_TA,
-    const double* __restrict__ W_TA, double* __restrict__ U_PRE, double* __restrict__ V_PRE,
-    double* __restrict__ W_PRE, double* __restrict__ T_PRE, const double* __restrict__ C1,
-    double* __restrict__ U_A, double* __restrict__ V_A, double* __restrict__ W_A,
-    double* __restrict__ U_T) {
-  extern __shared__ double sm[];
+    const H* __restrict__ U_TA, const H* __restrict__ V_TA, const H* __restrict__ W_TA,
+    H* __restrict__ U_PRE, H* __restrict__ V_PRE, H* __restrict__ W_PRE, H* __restrict__ T_PRE,
+    const double* __restrict__ C1, H* __restrict__ U_A, H* __restrict__ V_A,
+    H* __restrict__ W_A, H* __restrict__ U_T) {
+  extern __shared__ __align__(16) char smc[];
+  char* sm = smc;
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
@@ -93,16 +105,17 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
   const int kmax = k1 + 1;  // last plane any iteration reads
   // prologue: planes k0-1 .. k0+2 (k0+2 stays in flight)
   for (int q = -1; q <= 2; ++q)
-    load_plane(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
+    load_plane<H>(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
   cp_async_wait<1>();
   __syncthreads();
-  const double DT = sp.dt;
-  const double a1 = (sp.l == 1) ? 1.0 : 1.5, a2 = (sp.l == 1) ? 0.0 : -0.5;
-  const double kd = DT / sp.Re * 0.5;
-  const double r0 = sp.rho_cp, rr0 = 1.0 / sp.rho_cp, l0 = sp.thc;
-  const double kT = 0.5 / sp.Re / sp.Sc / sp.rho_cp * DT;
-  double dx = 0, dxp = 0, dxm = 0, rx = 0, rxp = 0, rx12 = 0, rx12m = 0;
-  double dy = 0, dyp = 0, dym = 0, ry = 0, ryp = 0, ry12 = 0, ry12m = 0;
+  using R = CT;  // arithmetic type
+  const R DT = (R)sp.dt;
+  const R a1 = (sp.l == 1) ? R(1) : R(1.5), a2 = (sp.l == 1) ? R(0) : R(-0.5);
+  const R kd = (R)(sp.dt / sp.Re * 0.5);
+  const R r0 = (R)sp.rho_cp, rr0 = (R)(1.0 / sp.rho_cp), l0 = (R)sp.thc;
+  const R kT = (R)(0.5 / sp.Re / sp.Sc / sp.rho_cp * sp.dt);
+  R dx = 0, dxp = 0, dxm = 0, rx = 0, rxp = 0, rx12 = 0, rx12m = 0;
+  R dy = 0, dyp = 0, dym = 0, ry = 0, ryp = 0, ry12 = 0, ry12m = 0;
   if (valid) {
     dx = LD(g.dx, I); dxp = LD(g.dx, I + 1); dxm = LD(g.dx, I - 1);
     rx = LD(rg.rdx, I); rxp = LD(rg.rdx, I + 1);
@@ -114,120 +127,119 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
   const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;  // this cell in a halo plane
   const int t0 = threadIdx.y * TXW + threadIdx.x;            // this cell in a tile
   for (int K = k0; K <= k1; ++K) {
-    load_plane(sm, d, i0, j0, K + 3, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
+    load_plane<H>(sm, d, i0, j0, K + 3, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
     if (valid) {
-      const double* pm = sm + ((K - 1) % NSLOT) * SLOT;
-      const double* pc = sm + (K % NSLOT) * SLOT;
-      const double* pp = sm + ((K + 1) % NSLOT) * SLOT;
+      const double* pm = reinterpret_cast<const double*>(sm + ((K - 1) % NSLOT) * slot_bytes<H>());
+      const double* pc = reinterpret_cast<const double*>(sm + (K % NSLOT) * slot_bytes<H>());
+      const double* pp = reinterpret_cast<const double*>(sm + ((K + 1) % NSLOT) * slot_bytes<H>());
       const long c = d.P(I, J, K);
-      const double dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
-      const double rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
-      const double rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
+      const R dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
+      const R rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
+      const R rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
       // neighbourhood from shared memory (field f at offset f*PLANE)
-#define AT(pl, f, dxo, dyo) (pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
-      const double uc = AT(pc, 0, 0, 0), uxp = AT(pc, 0, 1, 0), uxm = AT(pc, 0, -1, 0),
+#define AT(pl, f, dxo, dyo) (R)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
+      const R uc = AT(pc, 0, 0, 0), uxp = AT(pc, 0, 1, 0), uxm = AT(pc, 0, -1, 0),
                    uyp = AT(pc, 0, 0, 1), uym = AT(pc, 0, 0, -1), uzp = AT(pp, 0, 0, 0),
                    uzm = AT(pm, 0, 0, 0), uxmyp = AT(pc, 0, -1, 1), uxmzp = AT(pp, 0, -1, 0);
-      const double vc = AT(pc, 1, 0, 0), vxp = AT(pc, 1, 1, 0), vxm = AT(pc, 1, -1, 0),
+      const R vc = AT(pc, 1, 0, 0), vxp = AT(pc, 1, 1, 0), vxm = AT(pc, 1, -1, 0),
                    vyp = AT(pc, 1, 0, 1), vym = AT(pc, 1, 0, -1), vzp = AT(pp, 1, 0, 0),
                    vzm = AT(pm, 1, 0, 0), vxpym = AT(pc, 1, 1, -1), vymzp = AT(pp, 1, 0, -1);
-      const double wc = AT(pc, 2, 0, 0), wxp = AT(pc, 2, 1, 0), wxm = AT(pc, 2, -1, 0),
+      const R wc = AT(pc, 2, 0, 0), wxp = AT(pc, 2, 1, 0), wxm = AT(pc, 2, -1, 0),
                    wyp = AT(pc, 2, 0, 1), wym = AT(pc, 2, 0, -1), wzp = AT(pp, 2, 0, 0),
                    wzm = AT(pm, 2, 0, 0), wxpzm = AT(pm, 2, 1, 0), wypzm = AT(pm, 2, 0, 1);
-      const double tc = AT(pc, 3, 0, 0), txp = AT(pc, 3, 1, 0), txm = AT(pc, 3, -1, 0),
+      const R tc = AT(pc, 3, 0, 0), txp = AT(pc, 3, 1, 0), txm = AT(pc, 3, -1, 0),
                    typ = AT(pc, 3, 0, 1), tym = AT(pc, 3, 0, -1), tzp = AT(pp, 3, 0, 0),
                    tzm = AT(pm, 3, 0, 0);
       // masks (set_immersed_boundary :1037-1080) and AB2 histories
-      const double cc1 = AT(pc, 4, 0, 0);
-      const double c2 = (I < d.nx) ? (cc1 + AT(pc, 4, 1, 0)) * 0.50 : cc1;
-      const double c3 = (J < d.ny) ? (cc1 + AT(pc, 4, 0, 1)) * 0.50 : cc1;
-      const double c4 = (K < d.nz) ? (cc1 + AT(pp, 4, 0, 0)) * 0.50 : cc1;
+      const R cc1 = AT(pc, 4, 0, 0);
+      const R c2 = (I < d.nx) ? (cc1 + AT(pc, 4, 1, 0)) * R(0.5) : cc1;
+      const R c3 = (J < d.ny) ? (cc1 + AT(pc, 4, 0, 1)) * R(0.5) : cc1;
+      const R c4 = (K < d.nz) ? (cc1 + AT(pp, 4, 0, 0)) * R(0.5) : cc1;
 #undef AT
-      const double* hist = pc + 5 * PLANE + t0;
-      const double upre = hist[0], vpre = hist[TILE], wpre = hist[2 * TILE],
-                   tpre = hist[3 * TILE];
-    const bool solid = (c2 != 0.0) || (c3 != 0.0) || (c4 != 0.0) || (cc1 != 0.0);
+      const H* hist = reinterpret_cast<const H*>(pc + 5 * PLANE) + t0;
+      const R upre = hist[0], vpre = hist[TILE], wpre = hist[2 * TILE], tpre = hist[3 * TILE];
+    const bool solid = (c2 != R(0)) || (c3 != R(0)) || (c4 != R(0)) || (cc1 != R(0));
     // u
     {
-      double s1 = uc + uxp, s2 = uc + uxm;
-      double U1 = (s1 * s1 - s2 * s2) * rx12;
-      double U2 = ((vxp * dxp + vc * dx) * (uyp + uc) - (vxpym * dxp + vym * dx) * (uc + uym)) *
+      R s1 = uc + uxp, s2 = uc + uxm;
+      R U1 = (s1 * s1 - s2 * s2) * rx12;
+      R U2 = ((vxp * dxp + vc * dx) * (uyp + uc) - (vxpym * dxp + vym * dx) * (uc + uym)) *
                   rx12 * ry;
-      double U3 = ((wxp * dxp + wc * dx) * (uzp + uc) - (wxpzm * dxp + wzm * dx) * (uc + uzm)) *
+      R U3 = ((wxp * dxp + wc * dx) * (uzp + uc) - (wxpzm * dxp + wzm * dx) * (uc + uzm)) *
                   rx12 * rz;
-      double uv = 0.25 * (-U1 - U2 - U3) * DT + sp.force * DT;
-      double L = ((uxp - uc) * rxp - (uc - uxm) * rx) * rx12 +
+      R uv = R(0.25) * (-U1 - U2 - U3) * DT + (R)sp.force * DT;
+      R L = ((uxp - uc) * rxp - (uc - uxm) * rx) * rx12 +
                  ((uyp - uc) * ry12 - (uc - uym) * ry12m) * ry +
                  ((uzp - uc) * rz12 - (uc - uzm) * rz12m) * rz;
-      double ua = a1 * uv + a2 * upre + kd * L;
+      R ua = a1 * uv + a2 * upre + kd * L;
       U_PRE[c] = uv;
-      if (solid && c2 != 0.0) {
-        ua += sp.eta * c2 * LD(U_TA, c) * DT;
-        U_A[c] = (uc + ua) / (1.0 + sp.eta * c2 * DT);
+      if (solid && c2 != R(0)) {
+        ua += (R)sp.eta * c2 * LD(U_TA, c) * DT;
+        U_A[c] = (uc + ua) / (R(1) + (R)sp.eta * c2 * DT);
       } else {
         U_A[c] = uc + ua;
       }
     }
     // v
     {
-      double V1 = ((uyp * dyp + uc * dy) * (vxp + vc) - (uxmyp * dyp + uxm * dy) * (vc + vxm)) *
+      R V1 = ((uyp * dyp + uc * dy) * (vxp + vc) - (uxmyp * dyp + uxm * dy) * (vc + vxm)) *
                   ry12 * rx;
-      double s1 = vc + vyp, s2 = vc + vym;
-      double V2 = (s1 * s1 - s2 * s2) * ry12;
-      double V3 = ((wyp * dyp + wc * dy) * (vzp + vc) - (wypzm * dyp + wzm * dy) * (vc + vzm)) *
+      R s1 = vc + vyp, s2 = vc + vym;
+      R V2 = (s1 * s1 - s2 * s2) * ry12;
+      R V3 = ((wyp * dyp + wc * dy) * (vzp + vc) - (wypzm * dyp + wzm * dy) * (vc + vzm)) *
                   ry12 * rz;
-      double vv = 0.25 * (-V1 - V2 - V3) * DT;
-      double L = ((vxp - vc) * rx12 - (vc - vxm) * rx12m) * rx +
+      R vv = R(0.25) * (-V1 - V2 - V3) * DT;
+      R L = ((vxp - vc) * rx12 - (vc - vxm) * rx12m) * rx +
                  ((vyp - vc) * ryp - (vc - vym) * ry) * ry12 +
                  ((vzp - vc) * rz12 - (vc - vzm) * rz12m) * rz;
-      double va = a1 * vv + a2 * vpre + kd * L;
+      R va = a1 * vv + a2 * vpre + kd * L;
       V_PRE[c] = vv;
-      if (solid && c3 != 0.0) va += sp.eta * c3 * LD(V_TA, c) * DT;
-      if (J == d.ny) va = 0.0;  // set_bc(u_a,v_a,...) zeroes v_a(:,ny,:)
-      if (solid && c3 != 0.0) V_A[c] = (vc + va) / (1.0 + sp.eta * c3 * DT);
+      if (solid && c3 != R(0)) va += (R)sp.eta * c3 * LD(V_TA, c) * DT;
+      if (J == d.ny) va = R(0);  // set_bc(u_a,v_a,...) zeroes v_a(:,ny,:)
+      if (solid && c3 != R(0)) V_A[c] = (vc + va) / (R(1) + (R)sp.eta * c3 * DT);
       else V_A[c] = vc + va;
     }
     // w
     {
-      double W1 = ((uzp * dzp + uc * dz) * (wxp + wc) - (uxmzp * dzp + uxm * dz) * (wc + wxm)) *
+      R W1 = ((uzp * dzp + uc * dz) * (wxp + wc) - (uxmzp * dzp + uxm * dz) * (wc + wxm)) *
                   rz12 * rx;
-      double W2 = ((vzp * dzp + vc * dz) * (wyp + wc) - (vymzp * dzp + vym * dz) * (wc + wym)) *
+      R W2 = ((vzp * dzp + vc * dz) * (wyp + wc) - (vymzp * dzp + vym * dz) * (wc + wym)) *
                   rz12 * ry;
-      double s1 = wc + wzp, s2 = wc + wzm;
-      double W3 = (s1 * s1 - s2 * s2) * rz12;
-      double wv = 0.25 * (-W1 - W2 - W3) * DT;
-      double L = ((wxp - wc) * rx12 - (wc - wxm) * rx12m) * rx +
+      R s1 = wc + wzp, s2 = wc + wzm;
+      R W3 = (s1 * s1 - s2 * s2) * rz12;
+      R wv = R(0.25) * (-W1 - W2 - W3) * DT;
+      R L = ((wxp - wc) * rx12 - (wc - wxm) * rx12m) * rx +
                  ((wyp - wc) * ry12 - (wc - wym) * ry12m) * ry +
                  ((wzp - wc) * rzp - (wc - wzm) * rz) * rz12;
-      double wa = a1 * wv + a2 * wpre + kd * L;
+      R wa = a1 * wv + a2 * wpre + kd * L;
       W_PRE[c] = wv;
-      if (solid && c4 != 0.0) {
-        wa += sp.eta * c4 * LD(W_TA, c) * DT;
-        W_A[c] = (wc + wa) / (1.0 + sp.eta * c4 * DT);
+      if (solid && c4 != R(0)) {
+        wa += (R)sp.eta * c4 * LD(W_TA, c) * DT;
+        W_A[c] = (wc + wa) / (R(1) + (R)sp.eta * c4 * DT);
       } else {
         W_A[c] = wc + wa;
       }
     }
     // T
     {
-      double UT = (-((r0 * txm * dx + r0 * tc * dxm) * uxm) * 0.5 * rx12m +
-                   ((r0 * tc * dxp + r0 * txp * dx) * uc) * 0.5 * rx12) *
+      R UT = (-((r0 * txm * dx + r0 * tc * dxm) * uxm) * R(0.5) * rx12m +
+                   ((r0 * tc * dxp + r0 * txp * dx) * uc) * R(0.5) * rx12) *
                   rx;
-      double VT = (-((r0 * tym * dy + r0 * tc * dym) * vym) * 0.5 * ry12m +
-                   ((r0 * tc * dyp + r0 * typ * dy) * vc) * 0.5 * ry12) *
+      R VT = (-((r0 * tym * dy + r0 * tc * dym) * vym) * R(0.5) * ry12m +
+                   ((r0 * tc * dyp + r0 * typ * dy) * vc) * R(0.5) * ry12) *
                   ry;
-      double WT = (-((r0 * tzm * dz + r0 * tc * dzm) * wzm) * 0.5 * rz12m +
-                   ((r0 * tc * dzp + r0 * tzp * dz) * wc) * 0.5 * rz12) *
+      R WT = (-((r0 * tzm * dz + r0 * tc * dzm) * wzm) * R(0.5) * rz12m +
+                   ((r0 * tc * dzp + r0 * tzp * dz) * wc) * R(0.5) * rz12) *
                   rz;
-      double vt = (-UT - VT - WT) * DT * rr0 + sp.source * DT;
-      double D1 = (l0 * (txp - tc) * rx12 - l0 * (tc - txm) * rx12m) * rx;
-      double D2 = (l0 * (typ - tc) * ry12 - l0 * (tc - tym) * ry12m) * ry;
-      double D3 = (l0 * (tzp - tc) * rz12 - l0 * (tc - tzm) * rz12m) * rz;
-      double ut = a1 * vt + a2 * tpre + kT * (D1 + D2 + D3);
+      R vt = (-UT - VT - WT) * DT * rr0 + (R)sp.source * DT;
+      R D1 = (l0 * (txp - tc) * rx12 - l0 * (tc - txm) * rx12m) * rx;
+      R D2 = (l0 * (typ - tc) * ry12 - l0 * (tc - tym) * ry12m) * ry;
+      R D3 = (l0 * (tzp - tc) * rz12 - l0 * (tc - tzm) * rz12m) * rz;
+      R ut = a1 * vt + a2 * tpre + kT * (D1 + D2 + D3);
       T_PRE[c] = vt;
-      if (cc1 != 0.0) {
-        double pen = sp.eta * cc1 * DT;
-        U_T[c] = (tc + ut + pen * sp.tsolid) / (1.0 + pen);
+      if (cc1 != R(0)) {
+        R pen = (R)sp.eta * cc1 * DT;
+        U_T[c] = (tc + ut + pen * (R)sp.tsolid) / (R(1) + pen);
       } else {
         U_T[c] = tc + ut;
       }
@@ -238,20 +250,44 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
   }
 }
 
+template <class H, class CT>
+static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
+                     const double* u, const double* v, const double* w, const double* T,
+                     const H* u_ta, const H* v_ta, const H* w_ta, H* u_pre, H* v_pre, H* w_pre,
+                     H* T_pre, const double* c1, H* u_a, H* v_a, H* w_a, H* u_T,
+                     cudaStream_t s) {
+  dim3 block(TXW, TYW, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
+  size_t smem = (size_t)NSLOT * slot_bytes<H>();
+  cudaFuncSetAttribute((const void*)k_rhs_fast<H, CT>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  count_launch();
+  k_rhs_fast<H, CT><<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre,
+                                              v_pre, w_pre, T_pre, c1, u_a, v_a, w_a, u_T);
+}
+
 void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                      const double* u, const double* v, const double* w, const double* T,
                      const double* u_ta, const double* v_ta, const double* w_ta,
                      double* u_pre, double* v_pre, double* w_pre, double* T_pre,
                      const double* c1, double* u_a, double* v_a, double* w_a, double* u_T,
                      cudaStream_t s) {
-  dim3 block(TXW, TYW, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
-  size_t smem = (size_t)NSLOT * SLOT * sizeof(double);
-  cudaFuncSetAttribute((const void*)k_rhs_fast, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
-  count_launch();
-  k_rhs_fast<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre,
-                                    w_pre, T_pre, c1, u_a, v_a, w_a, u_T);
+  rhs_fast<double, double>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
+                           T_pre, c1, u_a, v_a, w_a, u_T, s);
+}
+
+// FP32 storage; arithmetic in FP32, or FP64 with math64
+void launch_rhs_f32(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
+                    const double* u, const double* v, const double* w, const double* T,
+                    const float* u_ta, const float* v_ta, const float* w_ta, float* u_pre,
+                    float* v_pre, float* w_pre, float* T_pre, const double* c1, float* u_a,
+                    float* v_a, float* w_a, float* u_T, bool math64, cudaStream_t s) {
+  if (math64)
+    rhs_fast<float, double>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
+                            T_pre, c1, u_a, v_a, w_a, u_T, s);
+  else
+    rhs_fast<float, float>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
+                           T_pre, c1, u_a, v_a, w_a, u_T, s);
 }
 
 }  // namespace nse
@@ -319,32 +355,39 @@ namespace nse {
 
 // ----------------------------------------------------- pipelined correction
 // mkp.f:141-217 for interior cells (1..n in every direction), marching in z
-// like k_rhs_fast: a ring of planes of phi, u*, v*, w* (one-cell halo) and the
-// old u_ta, v_ta, w_ta (interior) filled two planes ahead by cp.async.
-constexpr int CSLOT = 4 * PLANE + 3 * TILE;
+// like k_rhs_fast: a ring of planes of phi (FP64), u*, v*, w* (one-cell halo)
+// and the old u_ta, v_ta, w_ta (interior) filled two planes ahead by
+// cp.async.  H is the storage type of u*, u_ta, u_ep2 and divu (float in the
+// mixed-precision form); the correction itself is evaluated in FP64.
+template <class H>
+__host__ __device__ constexpr int cslot_bytes() {
+  return PLANE * 8 + 3 * PLANE * (int)sizeof(H) + 3 * TILE * (int)sizeof(H);
+}
 
-__device__ __forceinline__ void load_plane_c(double* sm, const Dims& d, int i0, int j0, int K,
-                                             int kmax, const double* PHI, const double* UT,
-                                             const double* VT, const double* WT,
-                                             const double* UA, const double* VA,
-                                             const double* WA) {
+template <class H>
+__device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, int j0, int K,
+                                             int kmax, const double* PHI, const H* UT,
+                                             const H* VT, const H* WT, const H* UA,
+                                             const H* VA, const H* WA) {
   if (K <= kmax) {
-    double* slot = sm + (K % NSLOT) * CSLOT;
+    char* slot = sm + (K % NSLOT) * cslot_bytes<H>();
+    double* ph = reinterpret_cast<double*>(slot);
+    H* fl = reinterpret_cast<H*>(slot + PLANE * 8);
     const int tid = threadIdx.y * TXW + threadIdx.x;
     for (int e = tid; e < PLANE; e += TILE) {
       int tx = e % SXW, ty = e / SXW;
       int i = i0 - 1 + tx, j = j0 - 1 + ty;
       if (i > d.nx + 1 || j > d.ny + 1) continue;
       long c = d.P(i, j, K);
-      cp_async8(slot + e, PHI + c);
-      cp_async8(slot + PLANE + e, UT + c);
-      cp_async8(slot + 2 * PLANE + e, VT + c);
-      cp_async8(slot + 3 * PLANE + e, WT + c);
+      cp_async8(ph + e, PHI + c);
+      cp_async8(fl + e, UT + c);
+      cp_async8(fl + PLANE + e, VT + c);
+      cp_async8(fl + 2 * PLANE + e, WT + c);
     }
     int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
     if (i <= d.nx && j <= d.ny && K >= 1 && K <= d.nz) {
       long c = d.P(i, j, K);
-      double* h = slot + 4 * PLANE + tid;
+      H* h = fl + 3 * PLANE + tid;
       cp_async8(h, UA + c);
       cp_async8(h + TILE, VA + c);
       cp_async8(h + 2 * TILE, WA + c);
@@ -353,14 +396,15 @@ __device__ __forceinline__ void load_plane_c(double* sm, const Dims& d, int i0, 
   cp_async_commit();
 }
 
+template <class H>
 __global__ void __launch_bounds__(256, 2) k_correct_pipe(
-    Dims d, GridRcp rg, const double* __restrict__ PHI, const double* __restrict__ UT,
-    const double* __restrict__ VT, const double* __restrict__ WT, double* __restrict__ p,
+    Dims d, GridRcp rg, const double* __restrict__ PHI, const H* __restrict__ UT,
+    const H* __restrict__ VT, const H* __restrict__ WT, double* __restrict__ p,
     double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
-    double* __restrict__ u_ta, double* __restrict__ v_ta, double* __restrict__ w_ta,
-    double* __restrict__ u_ep2, double* __restrict__ v_ep2, double* __restrict__ w_ep2,
-    double* __restrict__ divu, double dt) {
-  extern __shared__ double sm[];
+    H* __restrict__ u_ta, H* __restrict__ v_ta, H* __restrict__ w_ta, H* __restrict__ u_ep2,
+    H* __restrict__ v_ep2, H* __restrict__ w_ep2, H* __restrict__ divu, double dt) {
+  extern __shared__ __align__(16) char smc[];
+  char* sm = smc;
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
@@ -368,7 +412,7 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
   const int k1 = min(d.nz, k0 + KCHUNK - 1);
   const int kmax = k1 + 1;
   for (int q = -1; q <= 2; ++q)
-    load_plane_c(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    load_plane_c<H>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
   cp_async_wait<1>();
   __syncthreads();
   double rx = 0, rx12 = 0, rx12m = 0, ry = 0, ry12 = 0, ry12m = 0;
@@ -379,26 +423,32 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
   const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;
   const int t0 = threadIdx.y * TXW + threadIdx.x;
   for (int K = k0; K <= k1; ++K) {
-    load_plane_c(sm, d, i0, j0, K + 3, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    load_plane_c<H>(sm, d, i0, j0, K + 3, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
     if (valid) {
-      const double* pm = sm + ((K - 1) % NSLOT) * CSLOT;
-      const double* pc = sm + (K % NSLOT) * CSLOT;
-      const double* pp = sm + ((K + 1) % NSLOT) * CSLOT;
-#define AT(pl, f, dxo, dyo) (pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
+      const char* sm_m = sm + ((K - 1) % NSLOT) * cslot_bytes<H>();
+      const char* sm_c = sm + (K % NSLOT) * cslot_bytes<H>();
+      const char* sm_p = sm + ((K + 1) % NSLOT) * cslot_bytes<H>();
+      const double* qm = reinterpret_cast<const double*>(sm_m);
+      const double* qc = reinterpret_cast<const double*>(sm_c);
+      const double* qp = reinterpret_cast<const double*>(sm_p);
+      const H* fm = reinterpret_cast<const H*>(sm_m + PLANE * 8);
+      const H* fc = reinterpret_cast<const H*>(sm_c + PLANE * 8);
+#define PH(pl, dxo, dyo) (pl)[e0 + (dyo) * SXW + (dxo)]
+#define FL(pl, f, dxo, dyo) (double)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
       const long c = d.P(I, J, K);
       const double rz = LD(rg.rdz, K), rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
-      const double ph = AT(pc, 0, 0, 0), phx = AT(pc, 0, 1, 0), phy = AT(pc, 0, 0, 1),
-                   phz = AT(pp, 0, 0, 0), phxm = AT(pc, 0, -1, 0), phym = AT(pc, 0, 0, -1),
-                   phzm = AT(pm, 0, 0, 0);
+      const double ph = PH(qc, 0, 0), phx = PH(qc, 1, 0), phy = PH(qc, 0, 1), phz = PH(qp, 0, 0),
+                   phxm = PH(qc, -1, 0), phym = PH(qc, 0, -1), phzm = PH(qm, 0, 0);
       const double gx = (phx - ph) * rx12, gy = (phy - ph) * ry12, gz = (phz - ph) * rz12;
-      const double un = AT(pc, 1, 0, 0) - dt * gx;
-      const double vn = AT(pc, 2, 0, 0) - dt * gy;
-      const double wn = AT(pc, 3, 0, 0) - dt * gz;
-      const double um = AT(pc, 1, -1, 0) - dt * ((ph - phxm) * rx12m);
-      const double vm = AT(pc, 2, 0, -1) - dt * ((ph - phym) * ry12m);
-      const double wm = AT(pm, 3, 0, 0) - dt * ((ph - phzm) * rz12m);
-#undef AT
-      const double* old = pc + 4 * PLANE + t0;
+      const double un = FL(fc, 0, 0, 0) - dt * gx;
+      const double vn = FL(fc, 1, 0, 0) - dt * gy;
+      const double wn = FL(fc, 2, 0, 0) - dt * gz;
+      const double um = FL(fc, 0, -1, 0) - dt * ((ph - phxm) * rx12m);
+      const double vm = FL(fc, 1, 0, -1) - dt * ((ph - phym) * ry12m);
+      const double wm = FL(fm, 2, 0, 0) - dt * ((ph - phzm) * rz12m);
+#undef PH
+#undef FL
+      const H* old = fc + 3 * PLANE + t0;
       u[c] = un;
       v[c] = vn;
       w[c] = wn;
@@ -406,13 +456,13 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
       const double pxp = (I < d.nx) ? phx : p[c + 1];
       const double pyp = (J < d.ny) ? phy : p[c + d.sx];
       const double pzp = (K < d.nz) ? phz : p[c + d.sy];
-      u_ep2[c] = old[0] - dt * (pxp - ph) * rx12;
-      v_ep2[c] = old[TILE] - dt * (pyp - ph) * ry12;
-      w_ep2[c] = old[2 * TILE] - dt * (pzp - ph) * rz12;
-      divu[c] = (un - um) * rx + (vn - vm) * ry + (wn - wm) * rz;
-      u_ta[c] = dt * gx;
-      v_ta[c] = dt * gy;
-      w_ta[c] = dt * gz;
+      u_ep2[c] = (H)((double)old[0] - dt * (pxp - ph) * rx12);
+      v_ep2[c] = (H)((double)old[TILE] - dt * (pyp - ph) * ry12);
+      w_ep2[c] = (H)((double)old[2 * TILE] - dt * (pzp - ph) * rz12);
+      divu[c] = (H)((un - um) * rx + (vn - vm) * ry + (wn - wm) * rz);
+      u_ta[c] = (H)(dt * gx);
+      v_ta[c] = (H)(dt * gy);
+      w_ta[c] = (H)(dt * gz);
     }
     cp_async_wait<1>();
     __syncthreads();
@@ -421,12 +471,13 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
 
 // the same correction on the cells of 0..n with i, j or k equal to 0 (the
 // ghost faces MKP also writes)
+template <class H>
 __global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ PHI,
-                                const double* __restrict__ ut, const double* __restrict__ vt,
-                                const double* __restrict__ wt, double* __restrict__ u,
+                                const H* __restrict__ ut, const H* __restrict__ vt,
+                                const H* __restrict__ wt, double* __restrict__ u,
                                 double* __restrict__ v, double* __restrict__ w,
-                                double* __restrict__ u_ta, double* __restrict__ v_ta,
-                                double* __restrict__ w_ta, double dt) {
+                                H* __restrict__ u_ta, H* __restrict__ v_ta,
+                                H* __restrict__ w_ta, double dt) {
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   long nA = (long)(ny + 1) * (nz + 1);  // i = 0
   long nB = (long)nx * (nz + 1);        // j = 0, i >= 1
@@ -442,30 +493,47 @@ __global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ P
   double gx = (LD(PHI, c + 1) - ph) * LD(rg.rdx12, i);
   double gy = (LD(PHI, c + d.sx) - ph) * LD(rg.rdy12, j);
   double gz = (LD(PHI, c + d.sy) - ph) * LD(rg.rdz12, k);
-  u[c] = LD(ut, c) - dt * gx;
-  v[c] = LD(vt, c) - dt * gy;
-  w[c] = LD(wt, c) - dt * gz;
-  u_ta[c] = dt * gx;
-  v_ta[c] = dt * gy;
-  w_ta[c] = dt * gz;
+  u[c] = (double)LD(ut, c) - dt * gx;
+  v[c] = (double)LD(vt, c) - dt * gy;
+  w[c] = (double)LD(wt, c) - dt * gz;
+  u_ta[c] = (H)(dt * gx);
+  v_ta[c] = (H)(dt * gy);
+  w_ta[c] = (H)(dt * gz);
+}
+
+template <class H>
+static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
+                         const H* vt, const H* wt, double* p, double* u, double* v, double* w,
+                         H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
+                         double dt, cudaStream_t s) {
+  dim3 block(TXW, TYW, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
+  size_t smem = (size_t)NSLOT * cslot_bytes<H>();
+  cudaFuncSetAttribute((const void*)k_correct_pipe<H>,
+                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  count_launch();
+  k_correct_pipe<H><<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,
+                                              w_ta, u_ep2, v_ep2, w_ep2, divu, dt);
+  long nf = (long)(d.ny + 1) * (d.nz + 1) + (long)d.nx * (d.nz + 1) + (long)d.nx * d.ny;
+  count_launch();
+  k_correct_faces<H><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(d, rg, PHI, ut, vt, wt, u, v,
+                                                                  w, u_ta, v_ta, w_ta, dt);
 }
 
 void launch_correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const double* ut,
                          const double* vt, const double* wt, double* p, double* u, double* v,
                          double* w, double* u_ta, double* v_ta, double* w_ta, double* u_ep2,
                          double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s) {
-  dim3 block(TXW, TYW, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
-  size_t smem = (size_t)NSLOT * CSLOT * sizeof(double);
-  cudaFuncSetAttribute((const void*)k_correct_pipe, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                       (int)smem);
-  count_launch();
-  k_correct_pipe<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta,
-                                           u_ep2, v_ep2, w_ep2, divu, dt);
-  long nf = (long)(d.ny + 1) * (d.nz + 1) + (long)d.nx * (d.nz + 1) + (long)d.nx * d.ny;
-  count_launch();
-  k_correct_faces<<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(d, rg, PHI, ut, vt, wt, u, v, w,
-                                                               u_ta, v_ta, w_ta, dt);
+  correct_pipe<double>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2, v_ep2,
+                       w_ep2, divu, dt, s);
+}
+
+void launch_correct_f32(const Dims& d, const GridRcp& rg, const double* PHI, const float* ut,
+                        const float* vt, const float* wt, double* p, double* u, double* v,
+                        double* w, float* u_ta, float* v_ta, float* w_ta, float* u_ep2,
+                        float* v_ep2, float* w_ep2, float* divu, double dt, cudaStream_t s) {
+  correct_pipe<float>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2, v_ep2, w_ep2,
+                      divu, dt, s);
 }
 
 }  // namespace nse

@@ -18,9 +18,12 @@ namespace nse {
 // the y rule of the field; the kernel evaluates that directly for every cell
 // of the ghost shell (and the v wall plane j=ny), reading only cells that
 // are never written, so one launch replaces the 15 sequential passes.
-__device__ __forceinline__ void bc_cell(const Dims& d, double* u, double* v, double* w,
-                                        double* p, double* T, double tbot, double ttop,
-                                        int which, int i, int j, int k) {
+// VT: storage type of u, v, w (float for the FP32 intermediates of the
+// mixed-precision form)
+template <class VT>
+__device__ __forceinline__ void bc_cell(const Dims& d, VT* u, VT* v, VT* w, double* p,
+                                        double* T, double tbot, double ttop, int which, int i,
+                                        int j, int k) {
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   int mx = (i == 0) ? nx : (i == nx + 1 ? 1 : i);
   int mz = (k == 0) ? nz : (k == nz + 1 ? 1 : k);
@@ -29,13 +32,13 @@ __device__ __forceinline__ void bc_cell(const Dims& d, double* u, double* v, dou
   long dst = d.P(i, j, k);
   long src = d.P(mx, my, mz);
   if (which & 1) {  // u: y ghosts = -interior
-    double val = u[src];
-    if (jlo || jhi) val = -1.0 * val;
+    VT val = u[src];
+    if (jlo || jhi) val = VT(-1.0) * val;
     if (dst != src) u[dst] = val;
   }
   if (which & 4) {  // w
-    double val = w[src];
-    if (jlo || jhi) val = -1.0 * val;
+    VT val = w[src];
+    if (jlo || jhi) val = VT(-1.0) * val;
     if (dst != src) w[dst] = val;
   }
   if (which & 8) {  // p: Neumann copy
@@ -49,7 +52,7 @@ __device__ __forceinline__ void bc_cell(const Dims& d, double* u, double* v, dou
   }
   if (which & 2) {  // v: v(.,0,.)=v(.,ny,.)=0; v(.,ny+1,.) only wrapped in x,z
     if (j == 0 || j == ny) {
-      v[dst] = 0.0;
+      v[dst] = VT(0.0);
     } else {
       long s2 = d.P(mx, j, mz);
       if (s2 != dst) v[dst] = v[s2];
@@ -57,8 +60,9 @@ __device__ __forceinline__ void bc_cell(const Dims& d, double* u, double* v, dou
   }
 }
 
-__global__ void k_set_bc(Dims d, double* u, double* v, double* w, double* p, double* T,
-                         double tbot, double ttop, int which) {
+template <class VT>
+__global__ void k_set_bc(Dims d, VT* u, VT* v, VT* w, double* p, double* T, double tbot,
+                         double ttop, int which) {
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   long nA = 2L * (ny + 2) * (nz + 2);  // x faces
   long nB = 3L * nx * (nz + 2);        // y faces j = 0, ny, ny+1
@@ -100,7 +104,16 @@ void launch_set_bc(const Dims& d, double* u, double* v, double* w, double* p, do
   long n = 2L * (d.ny + 2) * (d.nz + 2) + 3L * d.nx * (d.nz + 2) + 2L * d.nx * d.ny;
   int bs = 256;
   count_launch();
-  k_set_bc<<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(d, u, v, w, p, T, tbot, ttop, which);
+  k_set_bc<double><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(d, u, v, w, p, T, tbot, ttop,
+                                                                which);
+}
+void launch_set_bc_f32(const Dims& d, float* u, float* v, float* w, double* p, double* T,
+                       double tbot, double ttop, int which, cudaStream_t s) {
+  long n = 2L * (d.ny + 2) * (d.nz + 2) + 3L * d.nx * (d.nz + 2) + 2L * d.nx * d.ny;
+  int bs = 256;
+  count_launch();
+  k_set_bc<float><<<(unsigned)((n + bs - 1) / bs), bs, 0, s>>>(d, u, v, w, p, T, tbot, ttop,
+                                                               which);
 }
 
 // ------------------------------------------------------------ cell terms --

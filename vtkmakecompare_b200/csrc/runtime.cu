@@ -40,6 +40,37 @@ void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, cons
 void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineArgs& a,
                        const double* tab, const int* slots, const int* ids, int nmasked,
                        const double* mtab, cudaStream_t s);
+void launch_lines_part_f32(int dir, int kind, const Dims& d, float* f, double* out,
+                           const LineArgs& a, const float* tab, const int* slots,
+                           const int* ids, int nmasked, const float* mtab,
+                           const double* tab64, const double* mtab64, cudaStream_t s);
+void launch_round_table(const double* in, float* out, long n, cudaStream_t s);
+// mixed-precision form (FP32 intermediates)
+void launch_rhs_f32(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
+                    const double* u, const double* v, const double* w, const double* T,
+                    const float* u_ta, const float* v_ta, const float* w_ta, float* u_pre,
+                    float* v_pre, float* w_pre, float* T_pre, const double* c1, float* u_a,
+                    float* v_a, float* w_a, float* u_T, bool math64, cudaStream_t s);
+void launch_correct_f32(const Dims& d, const GridRcp& rg, const double* PHI, const float* ut,
+                        const float* vt, const float* wt, double* p, double* u, double* v,
+                        double* w, float* u_ta, float* v_ta, float* w_ta, float* u_ep2,
+                        float* v_ep2, float* w_ep2, float* divu, double dt, cudaStream_t s);
+void launch_set_bc_f32(const Dims& d, float* u, float* v, float* w, double* p, double* T,
+                       double tbot, double ttop, int which, cudaStream_t s);
+void launch_fft_fwd_x_f32(const PoissonPlan& pp, const Dims& d, const GridDev& g,
+                          const GridRcp& rg, const float* ut, const float* vt, const float* wt,
+                          double dt, const double* phi, double dx, double dz, int mode,
+                          cudaStream_t s);
+void launch_fft_fwd_x_src32(const PoissonPlan& pp, const Dims& d, const GridRcp& rg,
+                            const float* ut, const float* vt, const float* wt, double dt,
+                            cudaStream_t s);
+void launch_fft_z_f32(const PoissonPlan& pp, bool inverse, cudaStream_t s);
+void launch_spn_f32(const PoissonPlan& pp, cudaStream_t s);
+void launch_fft_inv_x_f32(const PoissonPlan& pp, const Dims& d, double* phi, bool accumulate,
+                          cudaStream_t s);
+void launch_monitor_f32(const Dims& d, const GridDev& g, const double* u, const double* v,
+                        const double* w, const double* T, const float* divu, double* out6,
+                        cudaStream_t s);
 
 // ------------------------------------------------------------------ errors --
 static thread_local int g_status = NSE_OK;
@@ -659,7 +690,7 @@ void solve_t_(double* u_T, const int* nx, const int* ny, const int* nz, const do
 // ------------------------------------------------------ Poisson staging ----
 namespace nse {
 struct PoissonBufs {
-  DBuf spec, scr, AC, KXZ, twx, twz;
+  DBuf spec, scr, AC, KXZ, twx, twz, twxf, twzf;
   PoissonPlan pp;
   bool build(int nx, int ny, int nz, const double* dx, const double* dy, const double* dz,
              const double* dy12, double xl, double zl, cudaStream_t s) {
@@ -678,7 +709,11 @@ struct PoissonBufs {
         !this->AC.ensure(AC.size() * 8) || !this->KXZ.ensure(KXZ.size() * 8) ||
         !this->twx.ensure(twx.size() * 8) || !this->twz.ensure(twz.size() * 8))
       return false;
-    if (!NSE_CUDA(cudaMemcpyAsync(this->AC.p, AC.data(), AC.size() * 8, cudaMemcpyHostToDevice, s)) ||
+    std::vector<float> twxf_h(twx.begin(), twx.end()), twzf_h(twz.begin(), twz.end());
+    if (!twxf.ensure(twxf_h.size() * 4) || !twzf.ensure(twzf_h.size() * 4)) return false;
+    if (!NSE_CUDA(cudaMemcpyAsync(twxf.p, twxf_h.data(), twxf_h.size() * 4, cudaMemcpyHostToDevice, s)) ||
+        !NSE_CUDA(cudaMemcpyAsync(twzf.p, twzf_h.data(), twzf_h.size() * 4, cudaMemcpyHostToDevice, s)) ||
+        !NSE_CUDA(cudaMemcpyAsync(this->AC.p, AC.data(), AC.size() * 8, cudaMemcpyHostToDevice, s)) ||
         !NSE_CUDA(cudaMemcpyAsync(this->KXZ.p, KXZ.data(), KXZ.size() * 8, cudaMemcpyHostToDevice, s)) ||
         !NSE_CUDA(cudaMemcpyAsync(this->twx.p, twx.data(), twx.size() * 8, cudaMemcpyHostToDevice, s)) ||
         !NSE_CUDA(cudaMemcpyAsync(this->twz.p, twz.data(), twz.size() * 8, cudaMemcpyHostToDevice, s)))
@@ -689,10 +724,12 @@ struct PoissonBufs {
     pp.spec = spec.as<double>(); pp.scr = scr.as<double>();
     pp.AC = this->AC.as<double>(); pp.KXZ = this->KXZ.as<double>();
     pp.twx = this->twx.as<double>(); pp.twz = this->twz.as<double>();
+    pp.twx_f = twxf.as<float>(); pp.twz_f = twzf.as<float>();
     return true;
   }
   void release() {
     spec.release(); scr.release(); AC.release(); KXZ.release(); twx.release(); twz.release();
+    twxf.release(); twzf.release();
   }
 };
 static PoissonBufs& legacy_poisson() {
@@ -1031,6 +1068,13 @@ struct nse_ctx {
   // per (direction, component) for the mask-free lines and one per masked line
   bool part = false;
   DBuf ptab[3][4], pmtab[3][4];
+  // mixed-precision form: FP32 intermediates (u*, v*, w*, the temperature
+  // work field, the AB2 histories, u_ta, u_ep2, divu) and FP32 line tables
+  bool mixed = false;
+  bool math64 = false;   // FP64 arithmetic in the right-hand side (FP32 storage)
+  bool lines64 = false;  // FP64 arithmetic in the line sweeps (FP32 storage)
+  int refine = 1;
+  DBuf ptab_f[3][4], pmtab_f[3][4];
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1069,6 +1113,12 @@ static bool build_line_tables(nse_ctx* x) {
   if (!NSE_CUDA(cudaStreamSynchronize(x->own))) return false;
   for (int t = 0; t < 7; ++t) x->tab[t].den = dens[t];
   x->part = !(c.flags & NSE_FLAG_EXACT) && part_lines_supported(d);
+  if (x->mixed && !x->part) {
+    set_error(NSE_ERR_ARG,
+              "nse_ctx_create: the mixed-precision form needs nx = 32*M (M in 3,4,5,6,8,16), "
+              "12 to 256 cells in y and z, and no NSE_FLAG_EXACT");
+    return false;
+  }
   if (x->part) {
     for (int dir = 0; dir < 3; ++dir)
       for (int comp = 0; comp < 4; ++comp) {
@@ -1078,6 +1128,12 @@ static bool build_line_tables(nse_ctx* x) {
           return false;
         launch_part_tables(dir, kind, d, x->g, nullptr, a, nullptr, 1,
                            x->ptab[dir][comp].as<double>(), x->own);
+        if (x->mixed) {
+          size_t n = part_table_stride(dir, kind, d);
+          if (!x->ptab_f[dir][comp].ensure(n * sizeof(float))) return false;
+          launch_round_table(x->ptab[dir][comp].as<double>(), x->ptab_f[dir][comp].as<float>(),
+                             (long)n, x->own);
+        }
       }
     if (!NSE_CUDA(cudaStreamSynchronize(x->own))) return false;
   }
@@ -1160,6 +1216,12 @@ static bool refresh_line_flags(nse_ctx* x, cudaStream_t s) {
           return false;
         launch_part_tables(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
                            (int)ids.size(), x->pmtab[dir][comp].as<double>(), s);
+        if (x->mixed) {
+          size_t n = std::max<size_t>(1, ids.size()) * ps;
+          if (!x->pmtab_f[dir][comp].ensure(n * sizeof(float))) return false;
+          launch_round_table(x->pmtab[dir][comp].as<double>(), x->pmtab_f[dir][comp].as<float>(),
+                             (long)(ids.size() * ps), s);
+        }
       }
       // the host vectors die at the end of this iteration
       if (!NSE_CUDA(cudaStreamSynchronize(s))) return false;
@@ -1171,7 +1233,7 @@ static bool refresh_line_flags(nse_ctx* x, cudaStream_t s) {
 // phases of one step, in launch order
 enum {
   PH_BC = 0, PH_RHS, PH_YVEL, PH_ZVEL, PH_XVEL, PH_YT, PH_XT, PH_ZT, PH_BC2, PH_FFTX_F,
-  PH_FFTZ_F, PH_SPN, PH_FFTZ_I, PH_FFTX_I, PH_PHIBC, PH_CORRECT, PH_COUNT
+  PH_FFTZ_F, PH_SPN, PH_FFTZ_I, PH_FFTX_I, PH_PHIBC, PH_REFINE, PH_CORRECT, PH_COUNT
 };
 
 static void mark(nse_ctx* x, int phase) {
@@ -1180,6 +1242,19 @@ static void mark(nse_ctx* x, int phase) {
 }
 
 static double* F(nse_ctx* c, int id) { return c->f[id].as<double>(); }
+static float* F32(nse_ctx* c, int id) { return c->f[id].as<float>(); }
+// fields held in FP32 by the mixed-precision form
+static bool f32_field(const nse_ctx* x, int id) {
+  if (!x->mixed) return false;
+  switch (id) {
+    case NSE_U_TA: case NSE_V_TA: case NSE_W_TA: case NSE_U_PRE: case NSE_V_PRE:
+    case NSE_W_PRE: case NSE_T_PRE: case NSE_DIVU: case NSE_U_EP2: case NSE_V_EP2:
+    case NSE_W_EP2:
+      return true;
+    default:
+      return false;
+  }
+}
 
 static int status_or(int fallback) { return g_status != NSE_OK ? g_status : fallback; }
 
@@ -1203,12 +1278,16 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
     set_error(NSE_ERR_ARG, "nse_ctx_create: dt, Re, Sc, rho_cp, thc must be positive");
     return NSE_ERR_ARG;
   }
-  if (c.precision != NSE_FP64) {
+  if (c.precision != NSE_FP64 && c.precision != NSE_MIXED) {
     set_error(NSE_ERR_ARG, "nse_ctx_create: precision %d not available", c.precision);
     return NSE_ERR_ARG;
   }
   nse_ctx* x = new nse_ctx();
   x->cfg = c;
+  x->mixed = c.precision == NSE_MIXED;
+  x->refine = (c.flags & NSE_FLAG_REFINE2) ? 2 : 1;
+  x->math64 = (c.flags & NSE_FLAG_MATH64) != 0;
+  x->lines64 = (c.flags & NSE_FLAG_LINES64) != 0;
   x->d = make_dims(c.nx, c.ny, c.nz);
   x->l = 1;
   cudaStreamCreateWithFlags(&x->own, cudaStreamNonBlocking);
@@ -1279,6 +1358,8 @@ int nse_ctx_destroy(nse_ctx* x) {
       x->mtab[dir][comp].release();
       x->ptab[dir][comp].release();
       x->pmtab[dir][comp].release();
+      x->ptab_f[dir][comp].release();
+      x->pmtab_f[dir][comp].release();
     }
   for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
   if (x->own) cudaStreamDestroy(x->own);
@@ -1299,6 +1380,13 @@ int nse_ctx_upload(nse_ctx* x, int id, const double* host) {
   }
   size_t n = (id == NSE_CELLVALUE) ? x->d.ncell : x->d.ntot;
   if (id == NSE_CELLVALUE) x->mask_dirty = true;
+  if (f32_field(x, id)) {
+    std::vector<float> h(host, host + n);
+    if (!NSE_CUDA(cudaMemcpyAsync(x->f[id].p, h.data(), n * sizeof(float),
+                                  cudaMemcpyHostToDevice, x->stream)))
+      return status_or(NSE_ERR_CUDA);
+    return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+  }
   if (!NSE_CUDA(cudaMemcpyAsync(x->f[id].p, host, n * sizeof(double), cudaMemcpyHostToDevice,
                                 x->stream)))
     return status_or(NSE_ERR_CUDA);
@@ -1311,6 +1399,15 @@ int nse_ctx_download(nse_ctx* x, int id, double* host) {
     return NSE_ERR_ARG;
   }
   size_t n = (id == NSE_CELLVALUE) ? x->d.ncell : x->d.ntot;
+  if (f32_field(x, id)) {
+    std::vector<float> h(n);
+    if (!NSE_CUDA(cudaMemcpyAsync(h.data(), x->f[id].p, n * sizeof(float),
+                                  cudaMemcpyDeviceToHost, x->stream)) ||
+        !NSE_CUDA(cudaStreamSynchronize(x->stream)))
+      return status_or(NSE_ERR_CUDA);
+    for (size_t t = 0; t < n; ++t) host[t] = (double)h[t];
+    return NSE_OK;
+  }
   if (!NSE_CUDA(cudaMemcpyAsync(host, x->f[id].p, n * sizeof(double), cudaMemcpyDeviceToHost,
                                 x->stream)))
     return status_or(NSE_ERR_CUDA);
@@ -1342,11 +1439,60 @@ int nse_start(nse_ctx* x) {
   size_t fb = x->d.ntot * sizeof(double);
   const int src[4] = {NSE_U, NSE_V, NSE_W, NSE_T};
   const int dst[4] = {NSE_U_PRE, NSE_V_PRE, NSE_W_PRE, NSE_T_PRE};
-  for (int q = 0; q < 4; ++q)
+  for (int q = 0; q < 4; ++q) {
+    if (x->mixed) {
+      launch_round_table(F(x, src[q]), F32(x, dst[q]), (long)x->d.ntot, x->stream);
+      continue;
+    }
     if (!NSE_CUDA(cudaMemcpyAsync(x->f[dst[q]].p, x->f[src[q]].p, fb, cudaMemcpyDeviceToDevice,
                                   x->stream)))
       return status_or(NSE_ERR_CUDA);
-  return NSE_OK;
+  }
+  return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+// MKP in the mixed-precision form: FP32 u*, v*, w*; FP32 spectral solve with
+// FP64 residual refinement (or, with NSE_FLAG_POISSON64, the FP64 solve of
+// the FP64 divergence); FP64 correction of the FP64 state
+static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const float* wt) {
+  const Dims& d = x->d;
+  cudaStream_t s = x->stream;
+  const PoissonPlan& pp = x->pb.pp;
+  double* phi = F(x, NSE_PHI);
+  const double dt = x->cfg.dt, dx = x->hdx[1], dz = x->hdz[1];
+  const bool p64 = (x->cfg.flags & NSE_FLAG_POISSON64) != 0;
+  mark(x, PH_FFTX_F);
+  if (p64) launch_fft_fwd_x_src32(pp, d, x->rg, ut, vt, wt, dt, s);
+  else launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, nullptr, dx, dz, 1, s);
+  mark(x, PH_FFTZ_F);
+  if (p64) launch_fft_z(pp, false, s);
+  else launch_fft_z_f32(pp, false, s);
+  mark(x, PH_SPN);
+  if (p64) launch_spn(pp, true, true, s);
+  else launch_spn_f32(pp, s);
+  mark(x, PH_FFTZ_I);
+  if (p64) launch_fft_z(pp, true, s);
+  else launch_fft_z_f32(pp, true, s);
+  mark(x, PH_FFTX_I);
+  if (p64) launch_fft_inv_x(pp, d, phi, s);
+  else launch_fft_inv_x_f32(pp, d, phi, false, s);
+  mark(x, PH_PHIBC);
+  launch_phibc(d, phi, s);
+  mark(x, PH_REFINE);
+  for (int r = 0; !p64 && r < x->refine; ++r) {
+    launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, phi, dx, dz, 2, s);
+    launch_fft_z_f32(pp, false, s);
+    launch_spn_f32(pp, s);
+    launch_fft_z_f32(pp, true, s);
+    launch_fft_inv_x_f32(pp, d, phi, true, s);
+    launch_phibc(d, phi, s);
+  }
+  mark(x, PH_CORRECT);
+  launch_correct_f32(d, x->rg, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V),
+                     F(x, NSE_W), F32(x, NSE_U_TA), F32(x, NSE_V_TA), F32(x, NSE_W_TA),
+                     F32(x, NSE_U_EP2), F32(x, NSE_V_EP2), F32(x, NSE_W_EP2), F32(x, NSE_DIVU),
+                     dt, s);
+  mark(x, PH_COUNT);
 }
 
 // MKP (mkp.f:9-220) with u_temp = (ut, vt, wt); writes u, v, w, p, u_ta,
@@ -1368,6 +1514,7 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   launch_fft_inv_x(x->pb.pp, d, phi, s);
   mark(x, PH_PHIBC);
   launch_phibc(d, phi, s);
+  mark(x, PH_REFINE);
   mark(x, PH_CORRECT);
   if (x->cfg.flags & NSE_FLAG_EXACT)
     launch_correct(d, x->g, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V), F(x, NSE_W),
@@ -1385,6 +1532,14 @@ int nse_project(nse_ctx* x) {
   if (!x) return NSE_ERR_ARG;
   size_t fb = x->d.ntot * sizeof(double);
   cudaStream_t s = x->stream;
+  if (x->mixed) {
+    const long n = (long)x->d.ntot;
+    launch_round_table(F(x, NSE_U), x->ua.as<float>(), n, s);
+    launch_round_table(F(x, NSE_V), x->va.as<float>(), n, s);
+    launch_round_table(F(x, NSE_W), x->wa.as<float>(), n, s);
+    ctx_mkp_f32(x, x->ua.as<float>(), x->va.as<float>(), x->wa.as<float>());
+    return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
+  }
   if (!NSE_CUDA(cudaMemcpyAsync(x->ua.p, x->f[NSE_U].p, fb, cudaMemcpyDeviceToDevice, s)) ||
       !NSE_CUDA(cudaMemcpyAsync(x->va.p, x->f[NSE_V].p, fb, cudaMemcpyDeviceToDevice, s)) ||
       !NSE_CUDA(cudaMemcpyAsync(x->wa.p, x->f[NSE_W].p, fb, cudaMemcpyDeviceToDevice, s)))
@@ -1407,8 +1562,68 @@ int nse_poisson(nse_ctx* x) {
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
 
+// one time step in the mixed-precision form: FP64 state u, v, w, T, p;
+// FP32 right-hand side, line sweeps and transforms
+static void ctx_step_f32(nse_ctx* x) {
+  const Dims& d = x->d;
+  const nse_config& c = x->cfg;
+  cudaStream_t s = x->stream;
+  StepParams sp;
+  sp.dt = c.dt; sp.Re = c.Re; sp.Sc = c.Sc; sp.eta = c.eta;
+  sp.force = c.body_force; sp.source = c.heat_source;
+  sp.tbot = c.t_bot; sp.ttop = c.t_top; sp.tsolid = c.t_solid;
+  sp.rho_cp = c.rho_cp; sp.thc = c.thc; sp.l = x->l;
+  double *u = F(x, NSE_U), *v = F(x, NSE_V), *w = F(x, NSE_W), *p = F(x, NSE_P);
+  double* T = F(x, NSE_T);
+  const double* c1 = F(x, NSE_CELLVALUE);
+  float *ua = x->ua.as<float>(), *va = x->va.as<float>(), *wa = x->wa.as<float>();
+  float* uT = x->uT.as<float>();
+  mark(x, PH_BC);
+  launch_set_bc(d, u, v, w, p, T, c.t_bot, c.t_top, 31, s);
+  mark(x, PH_RHS);
+  launch_rhs_f32(d, x->g, x->rg, sp, u, v, w, T, F32(x, NSE_U_TA), F32(x, NSE_V_TA),
+                 F32(x, NSE_W_TA), F32(x, NSE_U_PRE), F32(x, NSE_V_PRE), F32(x, NSE_W_PRE),
+                 F32(x, NSE_T_PRE), c1, ua, va, wa, uT, x->math64, s);
+  refresh_line_flags(x, s);
+  float* fa[3] = {ua, va, wa};
+  auto run = [&](int dir, int comp, float* f, double* out, double ft, double fb) {
+    LineArgs la = line_args(x, comp);
+    la.ft = ft;
+    la.fb = fb;
+    launch_lines_part_f32(dir, line_kind(dir, comp), d, f, out, la,
+                          x->ptab_f[dir][comp].as<float>(), x->slots[dir][comp].as<int>(),
+                          x->ids[dir][comp].as<int>(), x->nmasked[dir][comp],
+                          x->pmtab_f[dir][comp].as<float>(),
+                          x->lines64 ? x->ptab[dir][comp].as<double>() : nullptr,
+                          x->lines64 ? x->pmtab[dir][comp].as<double>() : nullptr, s);
+  };
+  mark(x, PH_YVEL);
+  for (int comp = 0; comp < 3; ++comp) run(1, comp, fa[comp], nullptr, 0.0, 0.0);
+  mark(x, PH_ZVEL);
+  for (int comp = 0; comp < 3; ++comp) run(2, comp, fa[comp], nullptr, 0.0, 0.0);
+  mark(x, PH_XVEL);
+  for (int comp = 0; comp < 3; ++comp) run(0, comp, fa[comp], nullptr, 0.0, 0.0);
+  // solve_t: y, x, z; the z sweep writes the new temperature (interior) to
+  // the FP64 state
+  mark(x, PH_YT);
+  run(1, 3, uT, nullptr, 2.0 * c.t_bot, 2.0 * c.t_top);
+  mark(x, PH_XT);
+  run(0, 3, uT, nullptr, 0.0, 0.0);
+  mark(x, PH_ZT);
+  run(2, 3, uT, T, 0.0, 0.0);
+  mark(x, PH_BC2);
+  launch_set_bc_f32(d, ua, va, wa, p, T, c.t_bot, c.t_top, 31, s);
+  ctx_mkp_f32(x, ua, va, wa);
+  if (x->prof_n < x->prof_cap) x->prof_n++;
+  x->l += 1;
+}
+
 // one time step, nse_dominik.f:290-446
 static void ctx_step(nse_ctx* x) {
+  if (x->mixed) {
+    ctx_step_f32(x);
+    return;
+  }
   const Dims& d = x->d;
   const nse_config& c = x->cfg;
   cudaStream_t s = x->stream;
@@ -1524,8 +1739,12 @@ int nse_levelset(nse_ctx* x, const double* phi0, double* phi_out, int nnn, doubl
 int nse_monitor(nse_ctx* x, double out[6]) {
   if (!x || !out) return NSE_ERR_ARG;
   double* m = x->mon.as<double>();
-  launch_monitor(x->d, x->g, F(x, NSE_U), F(x, NSE_V), F(x, NSE_W), F(x, NSE_T),
-                 F(x, NSE_DIVU), m, x->stream);
+  if (x->mixed)
+    launch_monitor_f32(x->d, x->g, F(x, NSE_U), F(x, NSE_V), F(x, NSE_W), F(x, NSE_T),
+                       F32(x, NSE_DIVU), m, x->stream);
+  else
+    launch_monitor(x->d, x->g, F(x, NSE_U), F(x, NSE_V), F(x, NSE_W), F(x, NSE_T),
+                   F(x, NSE_DIVU), m, x->stream);
   if (!NSE_CUDA(cudaMemcpyAsync(out, m, 6 * sizeof(double), cudaMemcpyDeviceToHost, x->stream)))
     return status_or(NSE_ERR_CUDA);
   return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);

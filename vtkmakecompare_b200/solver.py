@@ -15,9 +15,14 @@ FIELDS = ("u", "v", "w", "p", "T", "u_ta", "v_ta", "w_ta", "u_pre", "v_pre", "w_
 FIELD_ID = {n: i for i, n in enumerate(FIELDS)}
 FP64, MIXED = 0, 1
 PHASES = ("set_bc", "rhs", "y_vel", "z_vel", "x_vel", "y_T", "x_T", "z_T", "set_bc_temp",
-          "fft_x_fwd", "fft_z_fwd", "spn", "fft_z_inv", "fft_x_inv", "phibc", "correct")
+          "fft_x_fwd", "fft_z_fwd", "spn", "fft_z_inv", "fft_x_inv", "phibc", "refine",
+          "correct")
 FLAG_CHECK_FINITE = 1
 FLAG_EXACT = 4
+FLAG_REFINE2 = 8
+FLAG_POISSON64 = 16
+FLAG_MATH64 = 32
+FLAG_LINES64 = 64
 
 
 class Config(C.Structure):
