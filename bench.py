@@ -88,7 +88,7 @@ def algorithmic_bytes(nx, ny, nz):
 
 LAUNCHES = {"set_bc": 1, "rhs": 1, "y_vel": 3, "z_vel": 3, "x_vel": 3, "y_T": 1, "x_T": 1,
             "z_T": 1, "set_bc_temp": 1, "fft_x_fwd": 1, "fft_z_fwd": 1, "spn": 1,
-            "fft_z_inv": 1, "fft_x_inv": 1, "phibc": 2, "correct": 1}
+            "fft_z_inv": 1, "fft_x_inv": 1, "phibc": 2, "refine": 1, "correct": 1}
 
 
 class Clocks:
@@ -140,14 +140,14 @@ class Clocks:
                 "samples": len(self.samples)}
 
 
-def build_case(S, W, torch):
+def build_case(S, W, torch, precision=0, flags=0):
     """Context with the workload's initial state: level-set mask, projected field."""
     g = W.grid_arrays(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
     f = W.channel_state(g, seed=2024, t_bot=0.0, t_top=0.0)
     dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
     cfg = S.Config(NX, NY, NZ, dt, RE, PR, ETA, 2 * math.pi, 2.0, math.pi, y0=-1.0,
                    ystretch=2.0, body_force=3.0 / RE, heat_source=0.0, t_bot=0.0, t_top=0.0,
-                   t_solid=1.0)
+                   t_solid=1.0, precision=precision, flags=flags)
     ctx = S.Context(cfg)
     for k in ("u", "v", "w", "T"):
         ctx.upload(k, f[k])
@@ -159,6 +159,75 @@ def build_case(S, W, torch):
     ctx.start()
     ctx.sync()
     return g, f, cfg, ctx, ls_s
+
+
+# mixed-precision variants reported beside the FP64 line: name -> nse flags
+MIXED_VARIANTS = (("mixed", 0),                      # FP32 FFTs + 1 FP64 refinement pass
+                  ("mixed_fp64_poisson", 16),        # NSE_FLAG_POISSON64
+                  ("mixed_fp64_lines", 16 | 64))     # + NSE_FLAG_LINES64
+
+
+def run_mixed(S, W, torch, stream, args, fp64_ms):
+    """Speed of each mixed variant (same timing as the FP64 line) and its
+    accuracy against an FP64 run of the same seed after args.acc_steps steps:
+    relative L2 of u, v, w, T, of the joint velocity, and the largest
+    post-projection divergence seen after any of those steps (also split into
+    the first step, where the penalisation stops the flow inside the sphere
+    impulsively and the pressure is largest, and the rest), with the same
+    figures for the FP64 run."""
+    out = {}
+    ref = None
+
+    def divs(c, n):
+        d = []
+        for _ in range(n):
+            c.step(1)
+            d.append(c.monitor()["max_divu"])
+        return d
+
+    if args.acc_steps > 0:
+        _, _, _, ref, _ = build_case(S, W, torch)
+        rd = divs(ref, args.acc_steps)
+        refs = {k: ref.download(k) for k in ("u", "v", "w", "T")}
+        ref.close()
+        out["fp64_reference"] = {"accuracy_steps": args.acc_steps, "max_divu": max(rd),
+                                 "max_divu_step1": rd[0],
+                                 "max_divu_after_step1": max(rd[1:] or [0.0])}
+    for name, flags in MIXED_VARIANTS:
+        _, _, _, ctx, _ = build_case(S, W, torch, precision=S.MIXED, flags=flags)
+        ctx.set_stream(stream.cuda_stream)
+        with torch.cuda.stream(stream):
+            ctx.step(args.warmup)
+        torch.cuda.synchronize()
+        ctx.profile(args.steps)
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        e0.record(stream)
+        ctx.step(args.steps)
+        e1.record(stream)
+        torch.cuda.synchronize()
+        ms = e0.elapsed_time(e1)
+        phases, nprof = ctx.phase_times()
+        ctx.close()
+        rec = {"steps_per_s": round(args.steps / (ms / 1e3), 3),
+               "ms_per_step": round(ms / args.steps, 4),
+               "speedup_vs_fp64": round(fp64_ms / ms, 3),
+               "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()}}
+        if args.acc_steps > 0:
+            _, _, _, ctx, _ = build_case(S, W, torch, precision=S.MIXED, flags=flags)
+            md = divs(ctx, args.acc_steps)
+            got = {k: ctx.download(k) for k in ("u", "v", "w", "T")}
+            ctx.close()
+            rel = {k: float(np.linalg.norm(got[k] - refs[k]) / np.linalg.norm(refs[k]))
+                   for k in got}
+            num = sum(np.linalg.norm(got[k] - refs[k]) ** 2 for k in ("u", "v", "w"))
+            den = sum(np.linalg.norm(refs[k]) ** 2 for k in ("u", "v", "w"))
+            rec.update({"accuracy_steps": args.acc_steps, "max_divu": max(md),
+                        "max_divu_step1": md[0], "max_divu_after_step1": max(md[1:] or [0.0]),
+                        "rel_l2_vs_fp64": rel,
+                        "velocity_rel_l2_vs_fp64": float(math.sqrt(num / den))})
+        out[name] = rec
+    return out
 
 
 def run_ours(args, rank, world, local_rank):
@@ -265,6 +334,11 @@ def run_ours(args, rank, world, local_rank):
     e2e_ms = max_over_ranks(q0.elapsed_time(q1))
     barrier()
 
+    # ------------------------------------------------- mixed-precision form
+    mixed = None
+    if not args.no_mixed:
+        mixed = run_mixed(S, W, torch, stream, args, ms)
+
     # ---------------------------------------------------------- CPU baseline
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -304,7 +378,7 @@ def run_ours(args, rank, world, local_rank):
                     "algorithmic_bytes": BP, "gbs": round(BP / (pms / 1e3) / 1e9, 1),
                     "frac_of_hbm": round(BP / (pms / 1e3) / 1e9 / peak, 4)},
         "max_divu": mon["max_divu"],
-        "mixed_precision": None,
+        "mixed_precision": mixed,
         "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d / args.steps),
                 "d2h_bytes_per_step": int(d2h / args.steps),
@@ -402,6 +476,9 @@ def main():
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--acc-steps", type=int, default=100,
+                    help="steps of the mixed-vs-FP64 accuracy comparison")
     args = ap.parse_args()
     world = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))

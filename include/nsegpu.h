@@ -249,7 +249,8 @@ int nse_ctx_get_step(nse_ctx* ctx);
 int nse_start(nse_ctx* ctx);
 /* nsteps time steps (nse_dominik.f:290-446), asynchronous on the context stream */
 int nse_step(nse_ctx* ctx, int nsteps);
-/* MKP on the resident fields, reading u,v,w as u_temp (asynchronous) */
+/* MKP on the resident fields, reading u,v,w (with SET_BC applied to a copy,
+   as nse_dominik.f:441 does before MKP) as u_temp (asynchronous) */
 int nse_project(nse_ctx* ctx);
 /* Poisson solve P2S->SPN->SP0B->S2P->PHIBC in place on the NSE_PHI field */
 int nse_poisson(nse_ctx* ctx);

@@ -201,3 +201,24 @@ def test_full_size_step_properties():
         mon = ctx.monitor()
     assert mon["nonfinite"] == 0
     assert mon["max_divu"] < 1e-10
+
+
+def test_projection_is_divergence_free():
+    """nse_project on a noisy field (noise also on the wall values of v): the
+    boundary conditions are applied before MKP, so the projected field is
+    divergence-free everywhere, including the last plane, where the mean mode's
+    compatibility would otherwise fail (SP0B never enforces row NY)."""
+    g, f, c1, par = make_case(96, 48, 64, sphere=True)
+    for prec in (S.FP64, S.MIXED):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], precision=prec,
+                       flags=S.FLAG_POISSON64 if prec == S.MIXED else 0)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.project()
+            mon = ctx.monitor()
+            assert mon["max_divu"] < 1e-10, (prec, mon)
+

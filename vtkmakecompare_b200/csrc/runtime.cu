@@ -1532,18 +1532,26 @@ int nse_project(nse_ctx* x) {
   if (!x) return NSE_ERR_ARG;
   size_t fb = x->d.ntot * sizeof(double);
   cudaStream_t s = x->stream;
+  // the boundary conditions of u, v, w are applied first, as the time loop
+  // does before MKP (nse_dominik.f:441): walls v = 0 and periodic ghosts make
+  // the divergence compatible with the Neumann problem
+  const nse_config& c = x->cfg;
   if (x->mixed) {
     const long n = (long)x->d.ntot;
-    launch_round_table(F(x, NSE_U), x->ua.as<float>(), n, s);
-    launch_round_table(F(x, NSE_V), x->va.as<float>(), n, s);
-    launch_round_table(F(x, NSE_W), x->wa.as<float>(), n, s);
-    ctx_mkp_f32(x, x->ua.as<float>(), x->va.as<float>(), x->wa.as<float>());
+    float *ua = x->ua.as<float>(), *va = x->va.as<float>(), *wa = x->wa.as<float>();
+    launch_round_table(F(x, NSE_U), ua, n, s);
+    launch_round_table(F(x, NSE_V), va, n, s);
+    launch_round_table(F(x, NSE_W), wa, n, s);
+    launch_set_bc_f32(x->d, ua, va, wa, nullptr, nullptr, c.t_bot, c.t_top, 7, s);
+    ctx_mkp_f32(x, ua, va, wa);
     return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
   }
   if (!NSE_CUDA(cudaMemcpyAsync(x->ua.p, x->f[NSE_U].p, fb, cudaMemcpyDeviceToDevice, s)) ||
       !NSE_CUDA(cudaMemcpyAsync(x->va.p, x->f[NSE_V].p, fb, cudaMemcpyDeviceToDevice, s)) ||
       !NSE_CUDA(cudaMemcpyAsync(x->wa.p, x->f[NSE_W].p, fb, cudaMemcpyDeviceToDevice, s)))
     return status_or(NSE_ERR_CUDA);
+  launch_set_bc(x->d, x->ua.as<double>(), x->va.as<double>(), x->wa.as<double>(), nullptr,
+                nullptr, c.t_bot, c.t_top, 7, s);
   ctx_mkp(x, x->ua.as<double>(), x->va.as<double>(), x->wa.as<double>());
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
