@@ -230,6 +230,21 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
     return out
 
 
+def replica_rate(ms_local, steps, world, device="cpu"):
+    """Whole-job rate of `world` replicas that each timed `steps` steps in
+    ms_local: the slowest rank's time (all-reduce MAX over the process group;
+    one value per rank, gloo on CPU or nccl on the GPU) and world*steps
+    divided by it.  Returns (ms_max, steps_per_s)."""
+    ms_max = float(ms_local)
+    if world > 1:
+        import torch
+        import torch.distributed as dist
+        t = torch.tensor([ms_max], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        ms_max = float(t.item())
+    return ms_max, world * steps / (ms_max / 1e3)
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -273,7 +288,7 @@ def run_ours(args, rank, world, local_rank):
     launches = S.launch_count() - n0
     ms = e0.elapsed_time(e1)
     phases, nprof = ctx.phase_times()
-    ms_max = max_over_ranks(ms)
+    ms_max, steps_s = replica_rate(ms, args.steps, world, dev)
     mon = ctx.monitor()
 
     # ---------------------------------------------------------- Poisson solve
@@ -356,7 +371,6 @@ def run_ours(args, rank, world, local_rank):
     t_launch_s = per_launch[dominant] / 1e3
     achieved = algo[dominant] / t_launch_s / 1e9
     traffic = dram_traffic().get(dominant)
-    steps_s = world * args.steps / (ms_max / 1e3)
     line = {
         "metric": METRIC,
         "value": round(steps_s, 3),
