@@ -380,18 +380,41 @@ __global__ void k_spn(int H, int ny, int nz, RT* base, long svj, long svk, doubl
   const long sj = 2 * svj;  // reals between planes
   if (kx == 0 && kz == 0) {
     if (!do_sp0b) return;
-    // SP0B mkp.f:271-288; the ghost PHIT(0,NY+1,0) is set by the caller
+    // SP0B mkp.f:271-288; the ghost PHIT(0,NY+1,0) is set by the caller.
+    // Row J reads D(J) and overwrites the slot of D(J+1) after reading it;
+    // the D values are read in double-buffered batches (this single thread
+    // would otherwise wait one memory latency per row, longer than all the
+    // other systems together)
+    constexpr int SB = 16;
     double pm = 0.0, pc = 0.0;
-    double Dn = (double)B[0];  // D(1)
+    double Dj = (double)B[0];  // D(1)
     B[0] = (RT)pc;             // PHIT(0,1,0) = 0
-    for (int J = 1; J <= ny - 1; ++J) {
-      double Dj = Dn;
-      Dn = (double)B[sj * J];  // D(J+1), read before it is overwritten
-      double a1 = AC1[J - 1], a2 = AC2[J - 1], a3 = AC3[J - 1];
-      double pn = (Dj - a1 * pm - a2 * pc) / a3;
-      B[sj * J] = (RT)pn;  // PHIT(0,J+1,0)
-      pm = pc;
-      pc = pn;
+    auto load0 = [&](double (&v)[SB], int J0) {
+#pragma unroll
+      for (int q = 0; q < SB; ++q)
+        if (J0 + q <= ny - 1) v[q] = (double)B[sj * (J0 + q)];  // D(J+1)
+    };
+    auto march = [&](const double (&v)[SB], int J0) {
+#pragma unroll
+      for (int q = 0; q < SB; ++q) {
+        const int J = J0 + q;
+        if (J <= ny - 1) {
+          double a1 = AC1[J - 1], a2 = AC2[J - 1], a3 = AC3[J - 1];
+          double pn = (Dj - a1 * pm - a2 * pc) / a3;
+          B[sj * J] = (RT)pn;  // PHIT(0,J+1,0)
+          pm = pc;
+          pc = pn;
+          Dj = v[q];
+        }
+      }
+    };
+    double va[SB], vb[SB];
+    load0(va, 1);
+    for (int J0 = 1; J0 <= ny - 1; J0 += 2 * SB) {
+      load0(vb, J0 + SB);
+      march(va, J0);
+      load0(va, J0 + 2 * SB);
+      march(vb, J0 + SB);
     }
     return;
   }
