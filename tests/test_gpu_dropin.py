@@ -110,7 +110,9 @@ def test_single_line_solvers_bitexact():
 
 
 # -------------------------------------------------------------- p2s / s2p
-@pytest.mark.parametrize("n", [(8, 4, 6), (16, 5, 12), (96, 3, 160), (64, 4, 30)])
+# (256, 3, 256), (256, 2, 48), (32, 3, 256): the register-resident 256-point kernels
+@pytest.mark.parametrize("n", [(8, 4, 6), (16, 5, 12), (96, 3, 160), (64, 4, 30),
+                               (256, 3, 256), (256, 2, 48), (32, 3, 256)])
 def test_p2s_s2p(n):
     nx, ny, nz = n
     rng = np.random.default_rng(14)

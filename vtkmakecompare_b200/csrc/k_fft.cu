@@ -355,6 +355,232 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, do
   }
 }
 
+// ------------------------------------------- register FFT of length 256 --
+// N = 256 = 16 x 16: with n = 16a + b and k = c + 16e,
+//   X[c + 16e] = sum_b W256^(bc) W16^(be) [ sum_a x[16a + b] W16^(ac) ].
+// Sixteen threads run one transform: thread b holds x[16a + b] (a = 0..15),
+// does the inner 16-point DFT in registers, multiplies by W256^(bc), and the
+// values are exchanged through shared memory so that thread c holds the 16
+// partial sums of its c; the outer 16-point DFT leaves X[c + 16e] in its
+// register e.  One exchange and no block-wide barrier per transform (the
+// x kernels synchronise a warp, the z kernel its CTA).
+// W16^m = exp(-2 pi i m/16) for the products m = a1*e0 of the 4 x 4 split
+template <class CT>
+__device__ __forceinline__ CT w16(int m, bool inv) {
+  using RT = typename CReal<CT>::T;
+  const RT c1 = (RT)0.92387953251128675613, s1 = (RT)0.38268343236508977173;
+  const RT r2 = (RT)0.70710678118654752440;
+  RT x, y;
+  switch (m) {
+    case 0: x = RT(1); y = RT(0); break;
+    case 1: x = c1; y = -s1; break;
+    case 2: x = r2; y = -r2; break;
+    case 3: x = s1; y = -c1; break;
+    case 4: x = RT(0); y = RT(-1); break;
+    case 6: x = -r2; y = -r2; break;
+    default: x = -c1; y = s1; break;  // m = 9
+  }
+  return mkc<CT>(x, inv ? -y : y);
+}
+
+// in-place 16-point DFT: v[a] -> V[k], both in natural order
+template <class CT>
+__device__ __forceinline__ void dft16(CT (&v)[16], bool inv) {
+  CT t[16];  // t[a1 + 4 e0]
+#pragma unroll
+  for (int a1 = 0; a1 < 4; ++a1) {
+    CT q[4] = {v[a1], v[a1 + 4], v[a1 + 8], v[a1 + 12]};
+    DftSmall<4, CT>::run(q, inv);
+#pragma unroll
+    for (int e0 = 0; e0 < 4; ++e0)
+      t[a1 + 4 * e0] = (a1 * e0 == 0) ? q[e0] : cmul(q[e0], w16<CT>(a1 * e0, inv));
+  }
+#pragma unroll
+  for (int e0 = 0; e0 < 4; ++e0) {
+    CT q[4] = {t[4 * e0], t[4 * e0 + 1], t[4 * e0 + 2], t[4 * e0 + 3]};
+    DftSmall<4, CT>::run(q, inv);
+#pragma unroll
+    for (int e1 = 0; e1 < 4; ++e1) v[e0 + 4 * e1] = q[e1];
+  }
+}
+
+// the inner half of the transform on thread b: DFT over a, then W256^(bc)
+template <class CT>
+__device__ __forceinline__ void fft256_inner(CT (&v)[16], int b, const CT* __restrict__ tw,
+                                             bool inv) {
+  dft16(v, inv);
+#pragma unroll
+  for (int c = 1; c < 16; ++c) {
+    CT w = __ldg(tw + b * c);
+    if (inv) w.y = -w.y;
+    v[c] = cmul(v[c], w);
+  }
+}
+
+// x forward, N = 256: a half-warp transforms one row pair (two real rows
+// packed as a + ib) of plane J; 8 pairs per 128-thread CTA
+template <class CT, class S>
+__global__ void __launch_bounds__(128) k_fft256_fwd_x(Dims d, SpecViewT<CT> sv, FwdSrc<S> q,
+                                                      int src_mode, const CT* __restrict__ tw) {
+  using RT = typename CReal<CT>::T;
+  constexpr int N = 256, FS = 17;
+  __shared__ CT sbuf[8][16 * FS];
+  const int h = threadIdx.x >> 4, b = threadIdx.x & 15;
+  CT* S_ = sbuf[h];
+  const int J = 1 + blockIdx.x;
+  const int ka = 2 * (blockIdx.y * 8 + h), kb = ka + 1;
+  const int nx = d.nx, ny = d.ny, nz = d.nz;
+  CT v[16];
+#pragma unroll
+  for (int a = 0; a < 16; ++a) {
+    const int i = 16 * a + b;
+    double va = 0.0, vb = 0.0;
+    if (src_mode == 0) {
+      if (ka < nz) va = (double)q.FP[d.P(i, J, ka)];
+      if (kb < nz) vb = (double)q.FP[d.P(i, J, kb)];
+    } else {
+      const int I = (i == 0) ? nx : i;
+#pragma unroll
+      for (int hh = 0; hh < 2; ++hh) {
+        const int kq = hh ? kb : ka;
+        if (kq >= nz) continue;
+        const int K = (kq == 0) ? nz : kq;
+        double val = div_rhs(d, q, I, J, K);
+        if (src_mode == 2) {
+          const double* ph = q.phi;
+          const long c = d.P(I, J, K);
+          const double p0 = ph[c];
+          const double lx = (ph[c + 1] - 2.0 * p0 + ph[c - 1]) * q.rdx2;
+          const double lz = (ph[c + d.sy] - 2.0 * p0 + ph[c - d.sy]) * q.rdz2;
+          const double ly = q.AC[J - 1] * ph[c - d.sx] + q.AC[J - 1 + ny] * p0 +
+                            q.AC[J - 1 + 2 * ny] * ph[c + d.sx];
+          val = val - (lx + ly + lz);
+        }
+        if (hh) vb = val; else va = val;
+      }
+    }
+    v[a] = mkc<CT>((RT)va, (RT)vb);
+  }
+  fft256_inner(v, b, tw, false);
+#pragma unroll
+  for (int c = 0; c < 16; ++c) S_[b * FS + c] = v[c];
+  __syncwarp();
+#pragma unroll
+  for (int bb = 0; bb < 16; ++bb) v[bb] = S_[bb * FS + b];  // this thread is now c = b
+  __syncwarp();
+  dft16(v, false);
+  // X[b + 16e] in natural order for the Hermitian split
+#pragma unroll
+  for (int e = 0; e < 16; ++e) S_[b + 16 * e] = v[e];
+  __syncwarp();
+#pragma unroll
+  for (int qq = 0; qq <= 8; ++qq) {
+    const int kx = b + 16 * qq;
+    if (kx > N / 2) break;
+    const CT Z = S_[kx], Zr = S_[(N - kx) & (N - 1)];
+    const CT A = mkc<CT>((Z.x + Zr.x) * RT(0.5), (Z.y - Zr.y) * RT(0.5));
+    const CT B = mkc<CT>((Z.y + Zr.y) * RT(0.5), (Zr.x - Z.x) * RT(0.5));
+    if (ka < nz) sv.base[kx + sv.sj * (J - 1) + sv.sk * ka] = A;
+    if (kb < nz) sv.base[kx + sv.sj * (J - 1) + sv.sk * kb] = B;
+  }
+}
+
+// x inverse, N = 256, with the S2P wrap (and `accumulate` as k_fft_inv_x)
+template <class CT>
+__global__ void __launch_bounds__(128) k_fft256_inv_x(Dims d, SpecViewT<CT> sv, double* FP,
+                                                      const CT* __restrict__ tw, int accumulate) {
+  using RT = typename CReal<CT>::T;
+  constexpr int N = 256, FS = 17;
+  __shared__ CT sbuf[8][16 * FS];
+  const int h = threadIdx.x >> 4, b = threadIdx.x & 15;
+  CT* S_ = sbuf[h];
+  const int J = 1 + blockIdx.x;
+  const int ka = 2 * (blockIdx.y * 8 + h), kb = ka + 1;
+  const int nz = d.nz;
+#pragma unroll
+  for (int qq = 0; qq <= 8; ++qq) {
+    const int kx = b + 16 * qq;
+    if (kx > N / 2) break;
+    CT A = mkc<CT>(RT(0), RT(0)), B = mkc<CT>(RT(0), RT(0));
+    if (ka < nz) A = sv.base[kx + sv.sj * (J - 1) + sv.sk * ka];
+    if (kb < nz) B = sv.base[kx + sv.sj * (J - 1) + sv.sk * kb];
+    if (kx == 0 || 2 * kx == N) { A.y = RT(0); B.y = RT(0); }
+    // Z = A + iB at kx, conj(A) + i conj(B) at N - kx
+    S_[kx] = mkc<CT>(A.x - B.y, A.y + B.x);
+    if (kx > 0 && 2 * kx < N) S_[N - kx] = mkc<CT>(A.x + B.y, B.x - A.y);
+  }
+  __syncwarp();
+  CT v[16];
+#pragma unroll
+  for (int a = 0; a < 16; ++a) v[a] = S_[16 * a + b];
+  __syncwarp();
+  fft256_inner(v, b, tw, true);
+#pragma unroll
+  for (int c = 0; c < 16; ++c) S_[b * FS + c] = v[c];
+  __syncwarp();
+#pragma unroll
+  for (int bb = 0; bb < 16; ++bb) v[bb] = S_[bb * FS + b];
+  dft16(v, true);
+  // thread b holds z(i = b + 16e)
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    const int i = b + 16 * e;
+    const CT z = v[e];
+    if (ka < nz) {
+      const long c = d.P(i, J, ka);
+      const double val = accumulate ? FP[c] + (double)z.x : (double)z.x;
+      FP[c] = val;
+      if (i == 0) FP[d.P(N, J, ka)] = val;
+      if (ka == 0) {
+        FP[d.P(i, J, nz)] = val;
+        if (i == 0) FP[d.P(N, J, nz)] = val;
+      }
+    }
+    if (kb < nz) {
+      const long c = d.P(i, J, kb);
+      const double val = accumulate ? FP[c] + (double)z.y : (double)z.y;
+      FP[c] = val;
+      if (i == 0) FP[d.P(N, J, kb)] = val;
+    }
+  }
+}
+
+// z pass, N = 256: a CTA transforms 16 adjacent kx columns of one plane;
+// thread (col, b) holds x[16a + b] of its column (loads coalesced over col)
+template <class CT>
+__global__ void __launch_bounds__(256) k_fft256_z(int H, SpecViewT<CT> sv,
+                                                  const CT* __restrict__ tw, int inv,
+                                                  double nrm) {
+  using RT = typename CReal<CT>::T;
+  constexpr int FS = 17;
+  extern __shared__ __align__(16) char fsm[];
+  CT* S_ = reinterpret_cast<CT*>(fsm);  // [c][b][col], col stride 1, b stride 17
+  const int col = threadIdx.x & 15, b = threadIdx.x >> 4;
+  const int jj = blockIdx.y;
+  const int kx = blockIdx.x * 16 + col;
+  const bool ok = kx < H;
+  CT* base = sv.base + kx + sv.sj * jj;
+  CT v[16];
+#pragma unroll
+  for (int a = 0; a < 16; ++a) v[a] = ok ? base[sv.sk * (16 * a + b)] : mkc<CT>(RT(0), RT(0));
+  fft256_inner(v, b, tw, inv != 0);
+#pragma unroll
+  for (int c = 0; c < 16; ++c) S_[(c * 16 + b) * FS + col] = v[c];
+  __syncthreads();
+  const int c = b;  // this thread now runs the outer DFT of index c
+#pragma unroll
+  for (int bb = 0; bb < 16; ++bb) v[bb] = S_[(c * 16 + bb) * FS + col];
+  dft16(v, inv != 0);
+  if (!ok) return;
+  const RT rn = (RT)nrm;
+#pragma unroll
+  for (int e = 0; e < 16; ++e) {
+    CT w = v[e];
+    if (!inv) { w.x = w.x / rn; w.y = w.y / rn; }
+    base[sv.sk * (c + 16 * e)] = w;
+  }
+}
+
 // ------------------------------------------------------ SPN / SP0B (y) --
 // Two threads per (kx, kz) system, on adjacent lanes: one runs the real part
 // of the right-hand side and one the imaginary part (CTRIDIAG's matrix is
@@ -581,6 +807,13 @@ static int row_pairs(const PoissonPlan& pp) {
 template <class CT, class S>
 static void fwd_x(const PoissonPlan& pp, const Dims& d, const FwdSrc<S>& q, int src_mode,
                   cudaStream_t s) {
+  if (pp.nx == 256 && pp.nz % 16 == 0) {
+    dim3 grid(pp.ny, pp.nz / 16);
+    count_launch();
+    k_fft256_fwd_x<CT, S><<<grid, 128, 0, s>>>(d, spec_internal_t<CT>(pp), q, src_mode,
+                                               twx_of<CT>(pp));
+    return;
+  }
   FFTShape sh = make_shape(pp.nx);
   int npair = row_pairs(pp);
   dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
@@ -603,6 +836,15 @@ void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
 
 template <class CT>
 static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
+  if (pp.nz == 256) {
+    dim3 grid((pp.H + 15) / 16, pp.ny);
+    size_t sm = 16 * 16 * 17 * sizeof(CT);
+    smem_optin((const void*)k_fft256_z<CT>, sm);
+    count_launch();
+    k_fft256_z<CT><<<grid, 256, sm, s>>>(pp.H, spec_internal_t<CT>(pp), twz_of<CT>(pp),
+                                         inverse ? 1 : 0, (double)pp.nx * (double)pp.nz);
+    return;
+  }
   FFTShape sh = make_shape(pp.nz);
   int W = 2048 / pp.nz;
   if (W < 1) W = 1;
@@ -641,6 +883,13 @@ void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, doub
 template <class CT>
 static void inv_x(const PoissonPlan& pp, const Dims& d, double* FP, bool accumulate,
                   cudaStream_t s) {
+  if (pp.nx == 256 && pp.nz % 16 == 0) {
+    dim3 grid(pp.ny, pp.nz / 16);
+    count_launch();
+    k_fft256_inv_x<CT><<<grid, 128, 0, s>>>(d, spec_internal_t<CT>(pp), FP, twx_of<CT>(pp),
+                                            accumulate ? 1 : 0);
+    return;
+  }
   FFTShape sh = make_shape(pp.nx);
   int npair = row_pairs(pp);
   dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
