@@ -33,6 +33,14 @@
 
 #include "k_lines.cuh"
 
+// launch shapes (compile-time): x lines per warp iteration, y/z lines per CTA
+#ifndef NSE_XL_NL
+#define NSE_XL_NL 2
+#endif
+#ifndef NSE_YZ_LPB
+#define NSE_YZ_LPB 16
+#endif
+
 namespace nse {
 
 namespace {
@@ -645,7 +653,7 @@ template <int M, class S, class R>
 static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, const int* ids,
                  int nmasked, const R* mtab, cudaStream_t s) {
   const int sms = sm_count();
-  constexpr int NL = M <= 8 ? 4 : 2;
+  constexpr int NL = M <= 8 ? NSE_XL_NL : 2;
   long nlines = (long)jtop * d.nz;
   long blocks = std::min<long>((long)sms * 8, (nlines + 8 * NL - 1) / (8 * NL));
   count_launch();
@@ -678,7 +686,7 @@ static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const Li
   int P = yz_partitions(nu);
   int MM = yz_rows(nu);
   int nother = dir == 1 ? d.nz : a.jtop;
-  constexpr int LPB = 16;
+  constexpr int LPB = NSE_YZ_LPB;
   dim3 grid((d.nx + LPB - 1) / LPB, nother);
   int periodic = kind >= LK_CYC_VEL ? 1 : 0;
   const R ft = (R)a.ft, fb = (R)a.fb;

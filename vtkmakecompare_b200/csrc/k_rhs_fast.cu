@@ -24,7 +24,14 @@ namespace nse {
 
 #define LD(p, i) __ldg((p) + (i))
 
-constexpr int KCHUNK = 16;           // z planes per CTA
+#ifndef NSE_RHS_KCHUNK
+#define NSE_RHS_KCHUNK 16
+#endif
+constexpr int KCHUNK = NSE_RHS_KCHUNK;  // z planes per CTA
+#ifndef NSE_CORR_KCHUNK
+#define NSE_CORR_KCHUNK 8
+#endif
+constexpr int CKCHUNK = NSE_CORR_KCHUNK;  // z planes per CTA of the correction
 constexpr int TXW = 32, TYW = 8;     // interior tile of a CTA (x, y)
 constexpr int SXW = TXW + 2, SYW = TYW + 2;
 constexpr int PLANE = SXW * SYW;     // one halo plane of one field
@@ -408,8 +415,8 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
-  const int k0 = 1 + blockIdx.z * KCHUNK;
-  const int k1 = min(d.nz, k0 + KCHUNK - 1);
+  const int k0 = 1 + blockIdx.z * CKCHUNK;
+  const int k1 = min(d.nz, k0 + CKCHUNK - 1);
   const int kmax = k1 + 1;
   for (int q = -1; q <= 2; ++q)
     load_plane_c<H>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
@@ -507,7 +514,7 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
                          H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
                          double dt, cudaStream_t s) {
   dim3 block(TXW, TYW, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + CKCHUNK - 1) / CKCHUNK);
   size_t smem = (size_t)NSLOT * cslot_bytes<H>();
   cudaFuncSetAttribute((const void*)k_correct_pipe<H>,
                        cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
