@@ -156,6 +156,25 @@ void implicit_ty_(double* STY, const int* ny, const double* dy, const double* dy
                   const double* Re, const double* Sc, const double* dt, const double* lly,
                   const double* rry, const double* ft, const double* fb, const double* CUY,
                   const double* eta);
+/* OUTPUT (nse_dominik.f:2606): ./nseoutput2/{velocity,temperature,pressure,
+ * divergence,gridx,gridy,gridz,gridnumber,phi,cellvalue1..4}.dat, field.u,
+ * grid.u and ./temperature_check.dat, byte for byte as gfortran writes them
+ * (sequential unformatted records with 4-byte length markers) */
+void output_(const double* u, const double* v, const double* w, const double* p,
+             const double* x, const double* y, const double* z, const int* nx, const int* ny,
+             const int* nz, const double* T, const double* cellvalue, const double* u_ta,
+             const double* v_ta, const double* w_ta, const double* phi, const double* divu);
+/* OUTFIELD (nse_dominik.f:2726): ./field.u (time record first) and
+ * ./nseoutput2/grid.u */
+void outfield_(const double* x, const double* y, const double* z, const double* u,
+               const double* v, const double* w, const double* p, const int* nx,
+               const int* ny, const int* nz, const double* tid, const double* T,
+               const double* phi, const double* u_ta, const double* v_ta,
+               const double* w_ta);
+/* READFIELD (nse_dominik.f:2769): ./nseoutput2/field.u into the arrays */
+void readfield_(double* u, double* v, double* w, double* p, const int* nx, const int* ny,
+                const int* nz, double* T, double* phi, double* u_ta, double* v_ta,
+                double* w_ta);
 
 /* Extension (no counterpart in the reference): SET_C with the y faces
  * y12(j) = y0 + yl/2 (1 + tanh(gamma(2j/ny-1))/tanh(gamma)), j=0..ny, the
@@ -258,6 +277,16 @@ int nse_poisson(nse_ctx* ctx);
  * resident mask; phi_out (padded, host) may be NULL */
 int nse_levelset(nse_ctx* ctx, const double* phi0, double* phi_out, int nnn, double dtau,
                  double width);
+/* The reference's output and restart files from the resident fields (same
+ * bytes as OUTPUT / OUTFIELD / READFIELD would give for the downloaded
+ * arrays): root/nseoutput2/... and root/temperature_check.dat; field.u with
+ * the time record at `path`, grid.u at `grid_path` (NULL: not written);
+ * READFIELD's field.u (no time record) into u, v, w, p, T, the level set
+ * phi and u_ta, v_ta, w_ta.  phi is the level set of the last nse_levelset
+ * (zero before one); cellvalue 2..4 are the face masks of the current mask. */
+int nse_ctx_write_output(nse_ctx* ctx, const char* root);
+int nse_ctx_write_field(nse_ctx* ctx, const char* path, double tid, const char* grid_path);
+int nse_ctx_read_field(nse_ctx* ctx, const char* path);
 /* FP64 device reductions: out[0]=max|divu|, out[1]=sum|u|dx, out[2]=sum|v|dy,
  * out[3]=sum|w|dz, out[4]=sum T dx dy dz (all cells), out[5]=non-finite count */
 int nse_monitor(nse_ctx* ctx, double out[6]);
@@ -267,7 +296,7 @@ int nse_sync(nse_ctx* ctx);
  * summed milliseconds over the profiled steps; phases in launch order:
  * set_bc, rhs, y-lines u/v/w, z-lines u/v/w, x-lines u/v/w, T y, T x, T z,
  * set_bc(u_temp), fft x fwd, fft z fwd, spn+sp0b, fft z inv, fft x inv,
- * phibc, correction (16 phases). */
+ * phibc, refinement (mixed form), correction (17 phases). */
 int nse_ctx_profile(nse_ctx* ctx, int max_steps);
 int nse_ctx_phase_times(nse_ctx* ctx, double* ms, int nphase, int* nsteps);
 /* number of kernel launches this process has issued through the library */

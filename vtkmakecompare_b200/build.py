@@ -28,6 +28,7 @@ SOURCES = {
     "k_rhs_fast.cu": [],
     "k_fft.cu": [],
     "noalloc.cu": [],
+    "fortran_io.cu": [],
 }
 
 

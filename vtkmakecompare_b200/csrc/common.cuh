@@ -11,6 +11,8 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <string>
+
 #include "../../include/nsegpu.h"
 
 namespace nse {
@@ -84,6 +86,24 @@ bool copy_box_d2h(double* host, const double* dev, const Dims& d, int i0, int i1
                   int j1, int k0, int k1, cudaStream_t s);
 bool copy_box_h2d(double* dev, const double* host, const Dims& d, int i0, int i1, int j0,
                   int j1, int k0, int k1, cudaStream_t s);
+
+// ------------------------------------------ reference output files (host) --
+// fortran_io.cu: OUTPUT / OUTFIELD / READFIELD files of nse_dominik.f:2606-2794
+bool write_output_files(const std::string& root, int nx, int ny, int nz, const double* u,
+                        const double* v, const double* w, const double* p, const double* x,
+                        const double* y, const double* z, const double* T,
+                        const double* cellvalue, const double* u_ta, const double* v_ta,
+                        const double* w_ta, const double* phi, const double* divu);
+bool write_grid_file(const std::string& path, int nx, int ny, int nz, const double* x,
+                     const double* y, const double* z);
+bool write_field_file(const std::string& path, bool with_time, double tid, int nx, int ny,
+                      int nz, const double* u, const double* v, const double* w,
+                      const double* p, const double* T, const double* phi,
+                      const double* u_ta, const double* v_ta, const double* w_ta);
+bool read_field_file(const std::string& path, int nx, int ny, int nz, double* u, double* v,
+                     double* w, double* p, double* T, double* phi, double* u_ta, double* v_ta,
+                     double* w_ta);
+bool ensure_dir_public(const std::string& dir);
 
 // --------------------------------------------------------- kernel launchers --
 // boundary conditions (nse_dominik.f:611-753); which: bit0 u, bit1 v, bit2 w,

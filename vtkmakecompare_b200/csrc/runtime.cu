@@ -1070,6 +1070,7 @@ struct nse_ctx {
   DBuf ptab[3][4], pmtab[3][4];
   // mixed-precision form: FP32 intermediates (u*, v*, w*, the temperature
   // work field, the AB2 histories, u_ta, u_ep2, divu) and FP32 line tables
+  DBuf lsphi;  // level set of the last nse_levelset (the reference's phi)
   bool mixed = false;
   bool math64 = false;   // FP64 arithmetic in the right-hand side (FP32 storage)
   bool lines64 = false;  // FP64 arithmetic in the line sweeps (FP32 storage)
@@ -1348,7 +1349,7 @@ int nse_ctx_destroy(nse_ctx* x) {
   if (x->own) cudaStreamSynchronize(x->own);
   for (auto& b : x->f) b.release();
   for (DBuf* b : {&x->grid, &x->ua, &x->va, &x->wa, &x->uT, &x->sa, &x->sb, &x->tmp, &x->mon,
-                 &x->ltab, &x->lflags})
+                 &x->ltab, &x->lflags, &x->lsphi})
     b->release();
   x->pb.release();
   for (int dir = 0; dir < 3; ++dir)
@@ -1737,11 +1738,106 @@ int nse_levelset(nse_ctx* x, const double* phi0, double* phi_out, int nnn, doubl
   if (!run_levelset(d, x->g, x->tmp.as<double>(), F(x, NSE_PHI), x->ua.as<double>(),
                     F(x, NSE_CELLVALUE), nnn, dtau, width, s))
     return status_or(NSE_ERR_CUDA);
+  // keep the level set: NSE_PHI is the Poisson work field of the steps
+  if (!x->lsphi.ensure(d.ntot * sizeof(double)) ||
+      !NSE_CUDA(cudaMemcpyAsync(x->lsphi.p, x->f[NSE_PHI].p, d.ntot * sizeof(double),
+                                cudaMemcpyDeviceToDevice, s)))
+    return status_or(NSE_ERR_CUDA);
   if (phi_out &&
       !NSE_CUDA(cudaMemcpyAsync(phi_out, x->f[NSE_PHI].p, d.ntot * sizeof(double),
                                 cudaMemcpyDeviceToHost, s)))
     return status_or(NSE_ERR_CUDA);
   return NSE_CUDA(cudaStreamSynchronize(s)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+// ----------------------------------------------- reference output files --
+static bool download_vec(nse_ctx* x, int id, std::vector<double>& v) {
+  v.resize(id == NSE_CELLVALUE ? x->d.ncell : x->d.ntot);
+  return nse_ctx_download(x, id, v.data()) == NSE_OK;
+}
+static bool download_lsphi(nse_ctx* x, std::vector<double>& v) {
+  v.assign(x->d.ntot, 0.0);
+  if (!x->lsphi.p) return true;
+  return NSE_CUDA(cudaMemcpyAsync(v.data(), x->lsphi.p, x->d.ntot * sizeof(double),
+                                  cudaMemcpyDeviceToHost, x->stream)) &&
+         NSE_CUDA(cudaStreamSynchronize(x->stream));
+}
+
+int nse_ctx_write_output(nse_ctx* x, const char* root) {
+  if (!x || !root) return NSE_ERR_ARG;
+  const Dims& d = x->d;
+  std::vector<double> u, v, w, p, T, uta, vta, wta, divu, phi, cv;
+  bool ok = download_vec(x, NSE_U, u) && download_vec(x, NSE_V, v) &&
+            download_vec(x, NSE_W, w) && download_vec(x, NSE_P, p) &&
+            download_vec(x, NSE_T, T) && download_vec(x, NSE_U_TA, uta) &&
+            download_vec(x, NSE_V_TA, vta) && download_vec(x, NSE_W_TA, wta) &&
+            download_vec(x, NSE_DIVU, divu) && download_lsphi(x, phi);
+  if (!ok) return status_or(NSE_ERR_CUDA);
+  // cellvalue(:,:,:,1) is the mask; columns 2..4 its face averages, built
+  // on the device as set_immersed_boundary does at the first step
+  DBuf cv4;
+  const size_t nc = d.ncell;
+  ok = cv4.ensure(4 * nc * sizeof(double)) &&
+       NSE_CUDA(cudaMemcpyAsync(cv4.p, x->f[NSE_CELLVALUE].p, nc * sizeof(double),
+                                cudaMemcpyDeviceToDevice, x->stream));
+  if (ok) {
+    launch_build_face_masks(d, cv4.as<double>(), x->stream);
+    cv.resize(4 * nc);
+    ok = NSE_CUDA(cudaMemcpyAsync(cv.data(), cv4.p, 4 * nc * sizeof(double),
+                                  cudaMemcpyDeviceToHost, x->stream)) &&
+         NSE_CUDA(cudaStreamSynchronize(x->stream));
+  }
+  cv4.release();
+  if (!ok) return status_or(NSE_ERR_CUDA);
+  if (!write_output_files(root, d.nx, d.ny, d.nz, u.data(), v.data(), w.data(), p.data(),
+                          x->hx.data(), x->hy.data(), x->hz.data(), T.data(), cv.data(),
+                          uta.data(), vta.data(), wta.data(), phi.data(), divu.data()))
+    return status_or(NSE_ERR_ARG);
+  return NSE_OK;
+}
+
+int nse_ctx_write_field(nse_ctx* x, const char* path, double tid, const char* grid_path) {
+  if (!x || !path) return NSE_ERR_ARG;
+  const Dims& d = x->d;
+  std::vector<double> u, v, w, p, T, uta, vta, wta, phi;
+  bool ok = download_vec(x, NSE_U, u) && download_vec(x, NSE_V, v) &&
+            download_vec(x, NSE_W, w) && download_vec(x, NSE_P, p) &&
+            download_vec(x, NSE_T, T) && download_vec(x, NSE_U_TA, uta) &&
+            download_vec(x, NSE_V_TA, vta) && download_vec(x, NSE_W_TA, wta) &&
+            download_lsphi(x, phi);
+  if (!ok) return status_or(NSE_ERR_CUDA);
+  if (!write_field_file(path, true, tid, d.nx, d.ny, d.nz, u.data(), v.data(), w.data(),
+                        p.data(), T.data(), phi.data(), uta.data(), vta.data(), wta.data()))
+    return status_or(NSE_ERR_ARG);
+  if (grid_path && !write_grid_file(grid_path, d.nx, d.ny, d.nz, x->hx.data(), x->hy.data(),
+                                    x->hz.data())) {
+    set_error(NSE_ERR_ARG, "cannot write %s", grid_path);
+    return NSE_ERR_ARG;
+  }
+  return NSE_OK;
+}
+
+int nse_ctx_read_field(nse_ctx* x, const char* path) {
+  if (!x || !path) return NSE_ERR_ARG;
+  const Dims& d = x->d;
+  const size_t n = d.ntot;
+  std::vector<double> u(n), v(n), w(n), p(n), T(n), phi(n), uta(n), vta(n), wta(n);
+  if (!read_field_file(path, d.nx, d.ny, d.nz, u.data(), v.data(), w.data(), p.data(),
+                       T.data(), phi.data(), uta.data(), vta.data(), wta.data()))
+    return status_or(NSE_ERR_ARG);
+  const int ids[8] = {NSE_U, NSE_V, NSE_W, NSE_P, NSE_T, NSE_U_TA, NSE_V_TA, NSE_W_TA};
+  const double* src[8] = {u.data(), v.data(), w.data(), p.data(), T.data(),
+                          uta.data(), vta.data(), wta.data()};
+  for (int q = 0; q < 8; ++q) {
+    int st = nse_ctx_upload(x, ids[q], src[q]);
+    if (st != NSE_OK) return st;
+  }
+  if (!x->lsphi.ensure(n * sizeof(double)) ||
+      !NSE_CUDA(cudaMemcpyAsync(x->lsphi.p, phi.data(), n * sizeof(double),
+                                cudaMemcpyHostToDevice, x->stream)) ||
+      !NSE_CUDA(cudaStreamSynchronize(x->stream)))
+    return status_or(NSE_ERR_CUDA);
+  return NSE_OK;
 }
 
 int nse_monitor(nse_ctx* x, double out[6]) {

@@ -52,6 +52,9 @@ _SIG = {
     "implicit_vy": "aiaaddddda",           # nse_dominik.f:1583
     "implicit_tx": "aiaadddaaddda",        # nse_dominik.f:1725
     "implicit_ty": "aiaadddaaddad",        # nse_dominik.f:1784
+    "output": "aaaaaaaiiiaaaaaaa",         # nse_dominik.f:2606 (files under ./)
+    "outfield": "aaaaaaaiiidaaaaa",        # nse_dominik.f:2726
+    "readfield": "aaaaiiiaaaaa",           # nse_dominik.f:2769
 }
 
 

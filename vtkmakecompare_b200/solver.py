@@ -59,6 +59,9 @@ def _sig():
     L.nse_ctx_set_step.argtypes = [vp, C.c_int]
     L.nse_step.argtypes = [vp, C.c_int]
     L.nse_monitor.argtypes = [vp, vp]
+    L.nse_ctx_write_output.argtypes = [vp, C.c_char_p]
+    L.nse_ctx_write_field.argtypes = [vp, C.c_char_p, C.c_double, C.c_char_p]
+    L.nse_ctx_read_field.argtypes = [vp, C.c_char_p]
     L.nse_levelset.argtypes = [vp, vp, vp, C.c_int, C.c_double, C.c_double]
     L.nse_ctx_grid.argtypes = [vp] + [vp] * 12
     L.nse_ctx_profile.argtypes = [vp, C.c_int]
@@ -177,6 +180,21 @@ class Context:
         check(self.L.nse_ctx_phase_times(self.h, ms.ctypes.data, len(PHASES),
                                          C.addressof(n)))
         return dict(zip(PHASES, ms.tolist())), n.value
+
+    # the reference's output and restart files (OUTPUT / OUTFIELD / READFIELD)
+    def write_output(self, root):
+        """root/nseoutput2/*.dat, field.u, grid.u and root/temperature_check.dat"""
+        check(self.L.nse_ctx_write_output(self.h, str(root).encode()))
+
+    def write_field(self, path, tid, grid_path=None):
+        """field.u with the time record first; grid.u at grid_path if given"""
+        check(self.L.nse_ctx_write_field(self.h, str(path).encode(), float(tid),
+                                         str(grid_path).encode() if grid_path else None))
+
+    def read_field(self, path):
+        """u, v, w, p, T, the level set and u_ta, v_ta, w_ta from a field.u
+        without a time record (the one OUTPUT writes)"""
+        check(self.L.nse_ctx_read_field(self.h, str(path).encode()))
 
     def monitor(self):
         out = np.zeros(6)
