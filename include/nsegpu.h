@@ -299,6 +299,21 @@ int nse_sync(nse_ctx* ctx);
  * phibc, refinement (mixed form), correction (17 phases). */
 int nse_ctx_profile(nse_ctx* ctx, int max_steps);
 int nse_ctx_phase_times(nse_ctx* ctx, double* ms, int nphase, int* nsteps);
+/* Ensemble (no counterpart in the reference): independent cases, each a
+ * context created as usual (grids, masks and precisions may differ), stepped
+ * together.  Case i runs on stream i mod nstreams (owned by the ensemble;
+ * nse_ensemble_destroy gives each case its own stream back).  The first step
+ * of every case runs eagerly (the Euler start; it also builds the mask's
+ * line tables); later steps replay a CUDA graph captured from two steps of
+ * all cases, with an eager step for an odd remainder.  A case's mask and
+ * parameters must not change while it belongs to an ensemble, and contexts
+ * with NSE_FLAG_CHECK_FINITE are refused.  Asynchronous; nse_ensemble_sync
+ * waits for all cases. */
+typedef struct nse_ensemble nse_ensemble;
+int nse_ensemble_create(nse_ctx** cases, int n, int nstreams, nse_ensemble** out);
+int nse_ensemble_step(nse_ensemble* ens, int nsteps);
+int nse_ensemble_sync(nse_ensemble* ens);
+int nse_ensemble_destroy(nse_ensemble* ens);
 /* number of kernel launches this process has issued through the library */
 long long nse_launch_count(void);
 

@@ -46,7 +46,8 @@ VARIANTS = [(S.FLAG_REFINE2, 2e-5, 2e-5), (S.FLAG_POISSON64, 2e-5, 2e-5),
 
 
 @pytest.mark.parametrize("flags,tol,tolv", VARIANTS)
-@pytest.mark.parametrize("n,steps", [((96, 48, 64), 20), ((128, 96, 128), 10), ((256, 24, 256), 6)])
+@pytest.mark.parametrize("n,steps", [((96, 48, 64), 20), ((128, 96, 128), 10), ((256, 24, 256), 6),
+                                     ((64, 64, 64), 10)])
 def test_mixed_tracks_fp64(n, steps, flags, tol, tolv):
     g, f, c1, par = make_case(*n, sphere=True)
     with make_ctx(g, f, c1, par, S.FP64) as ref, \

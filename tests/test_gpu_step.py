@@ -79,6 +79,7 @@ def test_context_grid_matches_oracle_grid():
                                             ((24, 16, 20), False, 10), ((40, 33, 36), True, 4),
                                             # shapes the partitioned line solver takes
                                             ((96, 48, 64), True, 4), ((128, 40, 96), True, 3),
+                                            ((64, 48, 64), True, 4),  # half-warp x lines
                                             ((256, 20, 24), False, 2)])
 def test_steps_match_oracle(n, sphere, steps, exact):
     g, f, c1, par = make_case(*n, sphere=sphere)

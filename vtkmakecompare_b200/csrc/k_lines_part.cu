@@ -245,76 +245,79 @@ __global__ void k_build_yz(Dims d, GridDev g, const double* c1, LineArgs a, cons
 }
 
 // ========================================================== x line tables
-// per lane k (partition k of 32): values v = 0..XV-1 at [v * 32 + k]
+// PL partitions per line (32: one warp per line; 16: one half-warp per line),
+// values v = 0..XV-1 of partition k at [v * PL + k]
 enum {
   XT_CF = 0, XT_AE, XT_MU, XT_NU, XT_K1, XT_K2 = XT_K1 + 4, XT_LAM = XT_K2 + 4, XT_KAP, XT_RDF,
   XT_LFR, XT_UFR, XT_ROW  // then 5 values per interior row: W, RB, CC, PP, QQ
 };
 __host__ __device__ constexpr int x_table_values(int M) { return XT_ROW + 5 * (M - 2); }
-__host__ __device__ size_t x_table_stride(int M) { return 32 * (size_t)x_table_values(M); }
+__host__ __device__ size_t x_table_stride(int M, int PL) {
+  return (size_t)PL * (size_t)x_table_values(M);
+}
 
-template <int KIND>
+template <int KIND, int PL>
 __global__ void k_build_x(Dims d, GridDev g, const double* c1, LineArgs a, const int* ids,
                           int count, double* out) {
   const int line = blockIdx.x;
-  const int k = threadIdx.x;
+  const int k = threadIdx.x;  // blockDim = PL
   if (line >= count) return;
   const bool masked = ids != nullptr;
   auto L = folded_line<0, KIND>(d, g, c1, a, masked ? ids[line] : 0, masked, true);
-  const int M = L.n / 32;
-  double* T = out + (size_t)line * x_table_stride(M);
+  const int M = L.n / PL;
+  double* T = out + (size_t)line * x_table_stride(M, PL);
   const int s = k * M, e = s + M - 1;
-  // interior rows: values at T[(XT_ROW + 5 (r-1) + c) * 32 + k], r = t - s;
+  // interior rows: values at T[(XT_ROW + 5 (r-1) + c) * PL + k], r = t - s;
   // partition_rows indexes arr[t * step], so shift the bases by -s rows
-  double* rowb = T + XT_ROW * 32 + k;
-  const long step = 5 * 32;
+  double* rowb = T + XT_ROW * PL + k;
+  const long step = 5 * PL;
   double* base = rowb - (long)(s + 1) * step;
-  partition_rows(L, s, e, base, base + 32, base + 64, base + 96, base + 128, step);
+  partition_rows(L, s, e, base, base + PL, base + 2 * PL, base + 3 * PL, base + 4 * PL, step);
   double As, Bs, Cs, Ae, Be, Ce;
   L.coef(s, As, Bs, Cs);
   L.coef(e, Ae, Be, Ce);
-  const double p1 = base[(s + 1) * step + 96], q1 = base[(s + 1) * step + 128];
-  const double pm = base[(e - 1) * step + 96], qm = base[(e - 1) * step + 128];
+  const double p1 = base[(s + 1) * step + 3 * PL], q1 = base[(s + 1) * step + 4 * PL];
+  const double pm = base[(e - 1) * step + 3 * PL], qm = base[(e - 1) * step + 4 * PL];
   // F row: LF E(k-1) + DF F(k) + UF E(k); E row: LE F(k) + DE E(k) + UE F(k+1)
   const double LF = As, DF = Bs + Cs * p1, UF = Cs * q1;
   const double LE = Ae * pm, DE = Be + Ae * qm, UE = Ce;
-  const unsigned FULL = 0xffffffffu;
-  const int kp = (k + 1) & 31;
-  const double LF1 = __shfl_sync(FULL, LF, kp), DF1 = __shfl_sync(FULL, DF, kp);
-  const double UF1 = __shfl_sync(FULL, UF, kp);
+  const unsigned MASK = PL == 32 ? 0xffffffffu : 0xffffu;
+  const int kp = (k + 1) & (PL - 1);
+  const double LF1 = __shfl_sync(MASK, LF, kp, PL), DF1 = __shfl_sync(MASK, DF, kp, PL);
+  const double UF1 = __shfl_sync(MASK, UF, kp, PL);
   // eliminate the F unknowns: al E(k-1) + be E(k) + ga E(k+1) = rho
   double al = -LE * LF / DF;
   double be = DE - LE * UF / DF - UE * LF1 / DF1;
   double ga = -UE * UF1 / DF1;
-  T[XT_CF * 32 + k] = Cs;
-  T[XT_AE * 32 + k] = Ae;
-  T[XT_MU * 32 + k] = -LE / DF;
-  T[XT_NU * 32 + k] = -UE / DF1;
-  // parallel cyclic reduction over the 32 lanes, strides 1, 2, 4, 8
-  for (int lv = 0; lv < 4; ++lv) {
+  T[XT_CF * PL + k] = Cs;
+  T[XT_AE * PL + k] = Ae;
+  T[XT_MU * PL + k] = -LE / DF;
+  T[XT_NU * PL + k] = -UE / DF1;
+  // parallel cyclic reduction over the PL lanes, strides 1, 2, ..., PL/4
+  for (int lv = 0; (1 << lv) < PL / 2; ++lv) {
     const int sft = 1 << lv;
-    const int km = (k - sft) & 31, kq = (k + sft) & 31;
-    double alm = __shfl_sync(FULL, al, km), bem = __shfl_sync(FULL, be, km);
-    double gam = __shfl_sync(FULL, ga, km);
-    double alp = __shfl_sync(FULL, al, kq), bep = __shfl_sync(FULL, be, kq);
-    double gap = __shfl_sync(FULL, ga, kq);
+    const int km = (k - sft) & (PL - 1), kq = (k + sft) & (PL - 1);
+    double alm = __shfl_sync(MASK, al, km, PL), bem = __shfl_sync(MASK, be, km, PL);
+    double gam = __shfl_sync(MASK, ga, km, PL);
+    double alp = __shfl_sync(MASK, al, kq, PL), bep = __shfl_sync(MASK, be, kq, PL);
+    double gap = __shfl_sync(MASK, ga, kq, PL);
     double k1 = -al / bem, k2 = -ga / bep;
-    T[(XT_K1 + lv) * 32 + k] = k1;
-    T[(XT_K2 + lv) * 32 + k] = k2;
+    T[(XT_K1 + lv) * PL + k] = k1;
+    T[(XT_K2 + lv) * PL + k] = k2;
     double nal = k1 * alm, nga = k2 * gap, nbe = be + k1 * gam + k2 * alp;
     al = nal; ga = nga; be = nbe;
   }
-  // rows k and k^16 now couple only each other
-  const int kx = k ^ 16;
-  double alx = __shfl_sync(FULL, al, kx), bex = __shfl_sync(FULL, be, kx);
-  double gax = __shfl_sync(FULL, ga, kx);
+  // rows k and k ^ PL/2 now couple only each other
+  const int kx = k ^ (PL / 2);
+  double alx = __shfl_sync(MASK, al, kx, PL), bex = __shfl_sync(MASK, be, kx, PL);
+  double gax = __shfl_sync(MASK, ga, kx, PL);
   double a2 = al + ga;
   double det = be * bex - a2 * (alx + gax);
-  T[XT_LAM * 32 + k] = bex / det;
-  T[XT_KAP * 32 + k] = -a2 / det;
-  T[XT_RDF * 32 + k] = 1.0 / DF;
-  T[XT_LFR * 32 + k] = -LF / DF;
-  T[XT_UFR * 32 + k] = -UF / DF;
+  T[XT_LAM * PL + k] = bex / det;
+  T[XT_KAP * PL + k] = -a2 / det;
+  T[XT_RDF * PL + k] = 1.0 / DF;
+  T[XT_LFR * PL + k] = -LF / DF;
+  T[XT_UFR * PL + k] = -UF / DF;
 }
 
 // =============================================================== solvers ==
@@ -349,13 +352,13 @@ __device__ __forceinline__ R interior_solve(R (&x)[MM], int m, const TB& tb) {
   return glast;
 }
 
-// x lines: table of lane `lane`, values at p[v * 32 + lane] (shared memory
+// x lines: table of lane `lane`, values at p[v * PL + lane] (shared memory
 // for the mask-free lines, global memory for a masked line)
-template <class R>
+template <class R, int PL>
 struct XTab {
   const R* p;
   int lane;
-  __device__ R v(int i) const { return p[i * 32 + lane]; }
+  __device__ R v(int i) const { return p[i * PL + lane]; }
   __device__ R w(int r) const { return v(XT_ROW + 5 * (r - 1)); }
   __device__ R rb(int r) const { return v(XT_ROW + 5 * (r - 1) + 1); }
   __device__ R cc(int r) const { return v(XT_ROW + 5 * (r - 1) + 2); }
@@ -365,35 +368,39 @@ struct XTab {
 
 // NL lines per warp iteration share every table load (the table reads, not
 // the line data, dominate the L1 traffic of this kernel)
-template <int M, int NL, bool MASKED, class S, class R>
+// (with PL = 16 the two half-warps work on different lines)
+template <int M, int NL, bool MASKED, class S, class R, int PL>
 __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int jtop,
                                                 const R* __restrict__ tab,
                                                 const int* __restrict__ slots,
                                                 const int* __restrict__ ids, int count) {
   using V2 = typename Vec2T<S>::T;
   constexpr int NV = x_table_values(M);
-  __shared__ R stab[MASKED ? 1 : NV * 32];
-  const int lane = threadIdx.x & 31;
+  constexpr int HW = 32 / PL;  // lines per warp at a time
+  __shared__ R stab[MASKED ? 1 : NV * PL];
+  const int lane = threadIdx.x & (PL - 1), half = (threadIdx.x & 31) / PL;
   const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
   const int n = d.nx;
   const unsigned FULL = 0xffffffffu;
   if (!MASKED) {
-    for (int t = threadIdx.x; t < NV * 32; t += blockDim.x) stab[t] = __ldg(tab + t);
+    for (int t = threadIdx.x; t < NV * PL; t += blockDim.x) stab[t] = __ldg(tab + t);
     __syncthreads();
   }
   const long nlines = MASKED ? count : (long)jtop * d.nz;
-  const long ngroups = (nlines + NL - 1) / NL;
+  const long ngroups = (nlines + NL * HW - 1) / (NL * HW);
   for (long gi = warp; gi < ngroups; gi += nwarps) {
-    XTab<R> tb;
+    XTab<R, PL> tb;
     tb.lane = lane;
-    tb.p = MASKED ? tab + (size_t)gi * x_table_stride(M) : stab;
+    // (masked pass: NL = 1, table of line gi*HW + half)
+    tb.p = MASKED ? tab + (size_t)min(gi * HW + half, (long)count - 1) * x_table_stride(M, PL)
+                  : stab;
     S* line[NL];
     bool ok[NL];
     R x[NL][M];
 #pragma unroll
     for (int q = 0; q < NL; ++q) {
-      const long l = gi * NL + q;
+      const long l = (gi * NL + q) * HW + half;
       long id = 0;
       ok[q] = l < nlines;
       if (ok[q]) {
@@ -450,17 +457,17 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
       for (int q = 0; q < NL; ++q) {
         rhsF[q] = x[q][0] - cf * x[q][1];
         const R rhsE = x[q][M - 1] - ae * x[q][M - 2];
-        rho[q] = rhsE + mu * rhsF[q] + nu * __shfl_sync(FULL, rhsF[q], (lane + 1) & 31);
+        rho[q] = rhsE + mu * rhsF[q] + nu * __shfl_sync(FULL, rhsF[q], (lane + 1) & (PL - 1), PL);
       }
     }
 #pragma unroll
-    for (int lv = 0; lv < 4; ++lv) {
+    for (int lv = 0; (1 << lv) < PL / 2; ++lv) {
       const int sft = 1 << lv;
       const R k1 = tb.v(XT_K1 + lv), k2 = tb.v(XT_K2 + lv);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        const R rm = __shfl_sync(FULL, rho[q], (lane - sft) & 31);
-        const R rp = __shfl_sync(FULL, rho[q], (lane + sft) & 31);
+        const R rm = __shfl_sync(FULL, rho[q], (lane - sft) & (PL - 1), PL);
+        const R rp = __shfl_sync(FULL, rho[q], (lane + sft) & (PL - 1), PL);
         rho[q] = rho[q] + k1 * rm + k2 * rp;
       }
     }
@@ -469,8 +476,8 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
       const R lfr = tb.v(XT_LFR), ufr = tb.v(XT_UFR);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        const R E = lam * rho[q] + kap * __shfl_sync(FULL, rho[q], lane ^ 16);
-        const R Em = __shfl_sync(FULL, E, (lane - 1) & 31);
+        const R E = lam * rho[q] + kap * __shfl_sync(FULL, rho[q], lane ^ (PL / 2), PL);
+        const R Em = __shfl_sync(FULL, E, (lane - 1) & (PL - 1), PL);
         const R F = rdf * rhsF[q] + lfr * Em + ufr * E;
         rhsF[q] = F;
         rho[q] = E;
@@ -595,11 +602,24 @@ static int yz_rows(int nu) {
   int m = (nu + P - 1) / P;
   return m <= 8 ? 8 : (m <= 12 ? 12 : 16);
 }
-// rows per lane of the x kernel, 0 when the x kernel does not apply
+// partitions per line (PL) and rows per partition (M) of the x kernel;
+// M = 0 when the x kernel does not apply
+static void x_shape(int nx, int& M, int& PL) {
+  M = 0;
+  PL = 32;
+  if (nx % 32 == 0) {
+    const int m = nx / 32;
+    if (m == 3 || m == 4 || m == 5 || m == 6 || m == 8 || m == 16) { M = m; return; }
+  }
+  if (nx % 16 == 0) {
+    const int m = nx / 16;
+    if (m == 3 || m == 4 || m == 5) { M = m; PL = 16; }
+  }
+}
 int x_rows_per_lane(int nx) {
-  if (nx % 32) return 0;
-  int M = nx / 32;
-  return (M == 3 || M == 4 || M == 5 || M == 6 || M == 8 || M == 16) ? M : 0;
+  int M, PL;
+  x_shape(nx, M, PL);
+  return M;
 }
 // the y/z kernel needs at least 3 and at most 16 rows per partition
 static bool yz_ok(int nu) {
@@ -609,7 +629,11 @@ bool part_lines_supported(const Dims& d) {
   return x_rows_per_lane(d.nx) > 0 && yz_ok(d.ny - 1) && yz_ok(d.ny) && yz_ok(d.nz);
 }
 size_t part_table_stride(int dir, int kind, const Dims& d) {
-  if (dir == 0) return x_table_stride(x_rows_per_lane(d.nx));
+  if (dir == 0) {
+    int M, PL;
+    x_shape(d.nx, M, PL);
+    return x_table_stride(M, PL);
+  }
   int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
   return yz_table_stride(nu, yz_partitions(nu));
 }
@@ -622,8 +646,15 @@ void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, cons
   if (count <= 0) return;
   count_launch();
   if (dir == 0) {
-    if (kind == LK_CYC_VEL) k_build_x<LK_CYC_VEL><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, out);
-    else k_build_x<LK_CYC_T><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, out);
+    int M, PL;
+    x_shape(d.nx, M, PL);
+    if (PL == 32) {
+      if (kind == LK_CYC_VEL) k_build_x<LK_CYC_VEL, 32><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, out);
+      else k_build_x<LK_CYC_T, 32><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, out);
+    } else {
+      if (kind == LK_CYC_VEL) k_build_x<LK_CYC_VEL, 16><<<count, 16, 0, s>>>(d, g, c1, a, ids, count, out);
+      else k_build_x<LK_CYC_T, 16><<<count, 16, 0, s>>>(d, g, c1, a, ids, count, out);
+    }
     return;
   }
   int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
@@ -649,21 +680,23 @@ static int sm_count() {
   return cached;
 }
 
-template <int M, class S, class R>
+template <int M, class S, class R, int PL = 32>
 static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, const int* ids,
                  int nmasked, const R* mtab, cudaStream_t s) {
   const int sms = sm_count();
   constexpr int NL = M <= 8 ? NSE_XL_NL : 2;
+  constexpr int HW = 32 / PL;
   long nlines = (long)jtop * d.nz;
-  long blocks = std::min<long>((long)sms * 8, (nlines + 8 * NL - 1) / (8 * NL));
+  long per_blk = 8L * NL * HW;
+  long blocks = std::min<long>((long)sms * 8, (nlines + per_blk - 1) / per_blk);
   count_launch();
-  k_xlines<M, NL, false, S, R><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots, nullptr,
-                                                                 0);
+  k_xlines<M, NL, false, S, R, PL><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots,
+                                                                     nullptr, 0);
   if (nmasked > 0) {
-    long mb = std::min<long>((long)sms * 8, (nmasked + 7) / 8);
+    long mb = std::min<long>((long)sms * 8, (nmasked + 8 * HW - 1) / (8 * HW));
     count_launch();
-    k_xlines<M, 1, true, S, R><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids,
-                                                            nmasked);
+    k_xlines<M, 1, true, S, R, PL><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids,
+                                                                nmasked);
   }
 }
 
@@ -672,7 +705,15 @@ static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const Li
                        const R* tab, const int* slots, const int* ids, int nmasked,
                        const R* mtab, cudaStream_t s) {
   if (dir == 0) {
-    switch (x_rows_per_lane(d.nx)) {
+    int M, PL;
+    x_shape(d.nx, M, PL);
+    if (PL == 16) {
+      if (M == 3) go_x<3, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+      else if (M == 4) go_x<4, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+      else go_x<5, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+      return;
+    }
+    switch (M) {
       case 3: go_x<3>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
       case 4: go_x<4>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
       case 5: go_x<5>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;

@@ -1889,3 +1889,167 @@ int nse_sync(nse_ctx* x) {
 }
 
 }  // extern "C"
+
+// ---------------------------------------------------------------- ensemble --
+// Independent cases stepped together: each case runs on one of `nstreams`
+// streams so small grids overlap on the GPU, and after the first step (the
+// Euler start, which also builds the line tables of the mask) the steps are
+// replayed from a CUDA graph that holds two steps of every case (two, so the
+// FP64 form's temperature buffer swap returns to its starting pair and the
+// graph can be replayed as is).
+struct nse_ensemble {
+  std::vector<nse_ctx*> cases;
+  std::vector<cudaStream_t> saved;  // the cases' streams before the ensemble
+  std::vector<cudaStream_t> streams;
+  cudaStream_t origin = nullptr;
+  cudaEvent_t fork = nullptr;
+  std::vector<cudaEvent_t> join;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  // each case's temperature buffer when the graph was captured: the FP64
+  // form swaps it with the work buffer every step, so a replay is valid only
+  // after an even number of eager steps since the capture
+  std::vector<void*> tbuf;
+};
+
+namespace nse {
+
+// origin waits for every case stream (eager work before a replay)
+static bool ens_join_into_origin(nse_ensemble* e) {
+  for (size_t i = 0; i < e->streams.size(); ++i)
+    if (!NSE_CUDA(cudaEventRecord(e->join[i], e->streams[i])) ||
+        !NSE_CUDA(cudaStreamWaitEvent(e->origin, e->join[i], 0)))
+      return false;
+  return true;
+}
+// every case stream waits for origin (eager work after a replay)
+static bool ens_fork_from_origin(nse_ensemble* e) {
+  if (!NSE_CUDA(cudaEventRecord(e->fork, e->origin))) return false;
+  for (cudaStream_t st : e->streams)
+    if (!NSE_CUDA(cudaStreamWaitEvent(st, e->fork, 0))) return false;
+  return true;
+}
+
+static bool ens_eager_step(nse_ensemble* e) {
+  for (nse_ctx* x : e->cases) {
+    ctx_step(x);
+    if (!NSE_CUDA(cudaGetLastError())) return false;
+  }
+  return true;
+}
+
+static bool ens_capture(nse_ensemble* e) {
+  std::vector<int> l0;
+  for (nse_ctx* x : e->cases) l0.push_back(x->l);
+  e->tbuf.clear();
+  for (nse_ctx* x : e->cases) e->tbuf.push_back(x->f[NSE_T].p);
+  if (!NSE_CUDA(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeRelaxed))) return false;
+  bool ok = ens_fork_from_origin(e);
+  for (int st = 0; ok && st < 2; ++st)
+    for (nse_ctx* x : e->cases) ctx_step(x);
+  ok = ok && ens_join_into_origin(e);
+  cudaGraph_t g = nullptr;
+  cudaError_t ce = cudaStreamEndCapture(e->origin, &g);
+  for (size_t i = 0; i < e->cases.size(); ++i) e->cases[i]->l = l0[i];  // nothing ran yet
+  if (!ok || !NSE_CUDA(ce)) {
+    if (g) cudaGraphDestroy(g);
+    return false;
+  }
+  e->graph = g;
+  return NSE_CUDA(cudaGraphInstantiate(&e->exec, g, 0));
+}
+
+}  // namespace nse
+
+extern "C" {
+
+int nse_ensemble_create(nse_ctx** cases, int n, int nstreams, nse_ensemble** out) {
+  nse_clear_error();
+  if (!cases || n < 1 || !out) {
+    set_error(NSE_ERR_ARG, "nse_ensemble_create: bad arguments");
+    return NSE_ERR_ARG;
+  }
+  *out = nullptr;
+  for (int i = 0; i < n; ++i)
+    if (!cases[i] || (cases[i]->cfg.flags & NSE_FLAG_CHECK_FINITE)) {
+      set_error(NSE_ERR_ARG, "nse_ensemble_create: case %d is null or checks every step", i);
+      return NSE_ERR_ARG;
+    }
+  nse_ensemble* e = new nse_ensemble();
+  const int ns = std::max(1, std::min(nstreams, n));
+  bool ok = NSE_CUDA(cudaStreamCreateWithFlags(&e->origin, cudaStreamNonBlocking)) &&
+            NSE_CUDA(cudaEventCreateWithFlags(&e->fork, cudaEventDisableTiming));
+  e->streams.assign(ns, nullptr);
+  e->join.assign(ns, nullptr);
+  for (int i = 0; ok && i < ns; ++i)
+    ok = NSE_CUDA(cudaStreamCreateWithFlags(&e->streams[i], cudaStreamNonBlocking)) &&
+         NSE_CUDA(cudaEventCreateWithFlags(&e->join[i], cudaEventDisableTiming));
+  for (int i = 0; ok && i < n; ++i) {
+    // finish what the case has queued on its own stream first
+    ok = NSE_CUDA(cudaStreamSynchronize(cases[i]->stream));
+    e->cases.push_back(cases[i]);
+    e->saved.push_back(cases[i]->stream);
+    cases[i]->stream = e->streams[i % ns];
+  }
+  if (!ok) {
+    nse_ensemble_destroy(e);
+    return status_or(NSE_ERR_CUDA);
+  }
+  *out = e;
+  return NSE_OK;
+}
+
+int nse_ensemble_step(nse_ensemble* e, int nsteps) {
+  if (!e || nsteps < 0) return NSE_ERR_ARG;
+  bool ok = true;
+  while (ok && nsteps > 0) {
+    // eager: the first step of a case, a mask being (re)tabulated, profiled
+    // steps, a temperature buffer out of the captured parity, or one step left
+    bool eager = nsteps < 2;
+    for (nse_ctx* x : e->cases)
+      eager = eager || x->l <= 1 || x->mask_dirty || x->prof_n < x->prof_cap;
+    if (!eager && e->exec)
+      for (size_t i = 0; i < e->cases.size(); ++i)
+        eager = eager || e->cases[i]->f[NSE_T].p != e->tbuf[i];
+    if (eager) {
+      ok = ens_eager_step(e);
+      --nsteps;
+      continue;
+    }
+    if (!e->exec) ok = ens_capture(e);
+    ok = ok && ens_join_into_origin(e);
+    for (; ok && nsteps >= 2; nsteps -= 2) {
+      ok = NSE_CUDA(cudaGraphLaunch(e->exec, e->origin));
+      for (nse_ctx* x : e->cases) x->l += 2;
+    }
+    ok = ok && ens_fork_from_origin(e);
+  }
+  return ok ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_ensemble_sync(nse_ensemble* e) {
+  if (!e) return NSE_ERR_ARG;
+  bool ok = NSE_CUDA(cudaStreamSynchronize(e->origin));
+  for (cudaStream_t st : e->streams) ok = ok && NSE_CUDA(cudaStreamSynchronize(st));
+  return ok ? NSE_OK : status_or(NSE_ERR_CUDA);
+}
+
+int nse_ensemble_destroy(nse_ensemble* e) {
+  if (!e) return NSE_OK;
+  if (e->origin) cudaStreamSynchronize(e->origin);
+  for (cudaStream_t st : e->streams)
+    if (st) cudaStreamSynchronize(st);
+  for (size_t i = 0; i < e->cases.size(); ++i) e->cases[i]->stream = e->saved[i];
+  if (e->exec) cudaGraphExecDestroy(e->exec);
+  if (e->graph) cudaGraphDestroy(e->graph);
+  for (cudaEvent_t ev : e->join)
+    if (ev) cudaEventDestroy(ev);
+  if (e->fork) cudaEventDestroy(e->fork);
+  for (cudaStream_t st : e->streams)
+    if (st) cudaStreamDestroy(st);
+  if (e->origin) cudaStreamDestroy(e->origin);
+  delete e;
+  return NSE_OK;
+}
+
+}  // extern "C"

@@ -67,6 +67,10 @@ def _sig():
     L.nse_ctx_profile.argtypes = [vp, C.c_int]
     L.nse_ctx_phase_times.argtypes = [vp, vp, C.c_int, vp]
     L.nse_launch_count.restype = C.c_longlong
+    L.nse_ensemble_create.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp)]
+    L.nse_ensemble_step.argtypes = [vp, C.c_int]
+    L.nse_ensemble_sync.argtypes = [vp]
+    L.nse_ensemble_destroy.argtypes = [vp]
     return L
 
 
@@ -205,3 +209,35 @@ class Context:
 
 __all__ = ["Config", "Context", "FIELDS", "FP64", "MIXED", "FLAG_CHECK_FINITE", "FLAG_EXACT",
            "NseError"]
+
+
+class Ensemble:
+    """Independent cases (Contexts) stepped together on `nstreams` streams,
+    replaying a captured CUDA graph of two steps of all cases after the first
+    step (nse_ensemble_*)."""
+
+    def __init__(self, contexts, nstreams=8):
+        self.L = _sig()
+        self.cases = list(contexts)
+        arr = (C.c_void_p * len(self.cases))(*[c.h.value for c in self.cases])
+        h = C.c_void_p()
+        check(self.L.nse_ensemble_create(arr, len(self.cases), int(nstreams), C.byref(h)))
+        self.h = h
+
+    def step(self, n=1):
+        check(self.L.nse_ensemble_step(self.h, int(n)))
+
+    def sync(self):
+        check(self.L.nse_ensemble_sync(self.h))
+
+    def close(self):
+        if self.h:
+            self.L.nse_ensemble_destroy(self.h)
+            self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+

@@ -103,3 +103,48 @@ CONFIGS = {
                       sphere=((math.pi, 0.0, math.pi / 2), 0.25), eta=1.0e4, width=1.5,
                       t_solid=1.0, steps=200),
 }
+
+
+# ---------------------------------------------------------------- ensemble
+# grids of the ensemble workload (cases drawn uniformly among them)
+ENSEMBLE_GRIDS = ((64, 64, 64), (96, 64, 96), (128, 96, 128), (160, 128, 160))
+
+
+def box_phi0(g, center, half):
+    """phi0 = minus the signed distance to an axis-aligned cube of half-side
+    `half` (positive inside, the reference's sign), interior cells."""
+    phi0 = padded(g)
+    X = g["x"][1:-1, None, None]
+    Y = g["y"][None, 1:-1, None]
+    Z = g["z"][None, None, 1:-1]
+    q = [np.abs(X - center[0]) - half, np.abs(Y - center[1]) - half,
+         np.abs(Z - center[2]) - half]
+    q = np.broadcast_arrays(*q)
+    outside = np.sqrt(sum(np.maximum(a, 0.0) ** 2 for a in q))
+    inside = np.minimum(np.maximum(np.maximum(q[0], q[1]), q[2]), 0.0)
+    phi0[1:-1, 1:-1, 1:-1] = -(outside + inside)
+    return phi0
+
+
+def ensemble_case(seed):
+    """One case of the batched ensemble: a grid drawn among ENSEMBLE_GRIDS,
+    1-3 spheres or cubes (radius or half-side 0.1-0.3) at seeded positions in
+    the 2pi x 2 x pi channel, Re_bulk uniform in [1000, 5000], its own noise.
+    Returns (grid, fields, phi0, Re, obstacles)."""
+    rng = np.random.default_rng(seed)
+    nx, ny, nz = ENSEMBLE_GRIDS[int(rng.integers(len(ENSEMBLE_GRIDS)))]
+    g = grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = channel_state(g, seed=int(rng.integers(1 << 30)), t_bot=1.0, t_top=0.0)
+    Re = float(rng.uniform(1000.0, 5000.0))
+    obst = []
+    phi0 = None
+    for _ in range(int(rng.integers(1, 4))):
+        size = float(rng.uniform(0.1, 0.3))
+        c = (float(rng.uniform(0, 2 * math.pi)), float(rng.uniform(-1 + size + 0.1, 1 - size - 0.1)),
+             float(rng.uniform(0, math.pi)))
+        kind = "sphere" if rng.random() < 0.5 else "box"
+        p = sphere_phi0(g, c, size) if kind == "sphere" else box_phi0(g, c, size)
+        phi0 = p if phi0 is None else np.maximum(phi0, p)
+        obst.append((kind, c, size))
+    return g, f, np.asfortranarray(phi0), Re, obst
+
