@@ -245,6 +245,84 @@ def replica_rate(ms_local, steps, world, device="cpu"):
     return ms_max, world * steps / (ms_max / 1e3)
 
 
+def run_ensemble(S, W, torch, stream, args):
+    """Batched ensemble: args.ens_cases cases drawn by seed (grids among
+    64^3..160x128x160, 1-3 spheres or cubes, Re_bulk in [1000, 5000], own
+    noise), in FP64 and in the mixed form with the FP64 Poisson solve and FP64
+    line arithmetic.  Aggregate case-steps/s of args.steps steps replayed from
+    the captured graph on 8 streams, beside the same cases stepped one after
+    the other on one stream; per-case error of the mixed form against FP64
+    after args.acc_steps steps."""
+    cases = [W.ensemble_case(7000 + i) for i in range(args.ens_cases)]
+    cells = sum(g["nx"] * g["ny"] * g["nz"] for g, *_ in cases)
+
+    def build(prec, flags):
+        out = []
+        for g, f, phi0, Re, _ in cases:
+            dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+            cfg = S.Config(g["nx"], g["ny"], g["nz"], dt, Re, PR, ETA, 2 * math.pi, 2.0, math.pi,
+                           y0=-1.0, ystretch=2.0, body_force=3.0 / Re, heat_source=0.0,
+                           t_bot=1.0, t_top=0.0, t_solid=1.0, precision=prec, flags=flags)
+            c = S.Context(cfg)
+            for k in ("u", "v", "w", "T"):
+                c.upload(k, f[k])
+            c.levelset(phi0, width=WIDTH, want_phi=False)
+            c.project()
+            c.start()
+            out.append(c)
+        return out
+
+    def timed(fn):
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        torch.cuda.synchronize()
+        e0.record(stream)
+        fn()
+        e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1)
+
+    res = {"cases": args.ens_cases, "cells": cells,
+           "grids": sorted({(g["nx"], g["ny"], g["nz"]) for g, *_ in cases})}
+    finals = {}
+    for name, prec, flags in (("fp64", S.FP64, 0), ("mixed", S.MIXED, 16 | 64)):
+        ctxs = build(prec, flags)
+        for c in ctxs:
+            c.set_stream(stream.cuda_stream)
+            c.step(1)  # Euler start and the mask tables, outside the timing
+        seq_ms = timed(lambda: [c.step(args.steps) for c in ctxs])
+        with S.Ensemble(ctxs, nstreams=8) as ens:
+            ens.set_stream(stream.cuda_stream)
+            ens.step(2)
+            ens.sync()
+            ms = timed(lambda: ens.step(args.steps))
+            ens.sync()
+            if args.acc_steps > 0:
+                ens.step(args.acc_steps - 1 - args.steps - 2)
+                ens.sync()
+        finals[name] = [{k: c.download(k) for k in ("u", "v", "w", "T")} for c in ctxs]
+        divs = [c.monitor()["max_divu"] for c in ctxs]
+        for c in ctxs:
+            c.close()
+        res[name] = {"case_steps_per_s": round(args.ens_cases * args.steps / (ms / 1e3), 1),
+                     "cell_steps_per_s": round(cells * args.steps / (ms / 1e3), 1),
+                     "sequential_case_steps_per_s":
+                         round(args.ens_cases * args.steps / (seq_ms / 1e3), 1),
+                     "graph_speedup_vs_sequential": round(seq_ms / ms, 3),
+                     "max_divu_at_end": max(divs)}
+    vel, tem = [], []
+    for a, b in zip(finals["mixed"], finals["fp64"]):
+        num = sum(np.linalg.norm(a[k] - b[k]) ** 2 for k in ("u", "v", "w"))
+        den = sum(np.linalg.norm(b[k]) ** 2 for k in ("u", "v", "w"))
+        vel.append(math.sqrt(num / den))
+        tem.append(float(np.linalg.norm(a["T"] - b["T"]) / np.linalg.norm(b["T"])))
+    # steps behind the comparison: 1 + steps (sequential) + 2 + steps + the rest
+    res["mixed_vs_fp64_after_steps"] = 3 + 2 * args.steps + max(0, args.acc_steps - 3 - args.steps)
+    res["mixed_velocity_rel_l2"] = {"max": max(vel), "median": float(np.median(vel))}
+    res["mixed_T_rel_l2"] = {"max": max(tem), "median": float(np.median(tem))}
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -354,6 +432,11 @@ def run_ours(args, rank, world, local_rank):
     if not args.no_mixed:
         mixed = run_mixed(S, W, torch, stream, args, ms)
 
+    # ------------------------------------------------------- batched ensemble
+    ensemble = None
+    if args.ens_cases > 0:
+        ensemble = run_ensemble(S, W, torch, stream, args)
+
     # ---------------------------------------------------------- CPU baseline
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -393,6 +476,7 @@ def run_ours(args, rank, world, local_rank):
                     "frac_of_hbm": round(BP / (pms / 1e3) / 1e9 / peak, 4)},
         "max_divu": mon["max_divu"],
         "mixed_precision": mixed,
+        "ensemble": ensemble,
         "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d / args.steps),
                 "d2h_bytes_per_step": int(d2h / args.steps),
@@ -491,6 +575,8 @@ def main():
     ap.add_argument("--cpu-steps", type=int, default=3)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-mixed", action="store_true")
+    ap.add_argument("--ens-cases", type=int, default=32,
+                    help="cases of the batched-ensemble measurement (0 skips it)")
     ap.add_argument("--acc-steps", type=int, default=100,
                     help="steps of the mixed-vs-FP64 accuracy comparison")
     args = ap.parse_args()

@@ -312,6 +312,9 @@ int nse_ctx_phase_times(nse_ctx* ctx, double* ms, int nphase, int* nsteps);
 typedef struct nse_ensemble nse_ensemble;
 int nse_ensemble_create(nse_ctx** cases, int n, int nstreams, nse_ensemble** out);
 int nse_ensemble_step(nse_ensemble* ens, int nsteps);
+/* graph replays go to `stream` (a cudaStream_t of the caller) instead of the
+ * ensemble's own; the case streams are forked from and joined into it */
+int nse_ensemble_set_stream(nse_ensemble* ens, void* stream);
 int nse_ensemble_sync(nse_ensemble* ens);
 int nse_ensemble_destroy(nse_ensemble* ens);
 /* number of kernel launches this process has issued through the library */

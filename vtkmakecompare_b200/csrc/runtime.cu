@@ -1902,6 +1902,7 @@ struct nse_ensemble {
   std::vector<cudaStream_t> saved;  // the cases' streams before the ensemble
   std::vector<cudaStream_t> streams;
   cudaStream_t origin = nullptr;
+  bool own_origin = true;
   cudaEvent_t fork = nullptr;
   std::vector<cudaEvent_t> join;
   cudaGraph_t graph = nullptr;
@@ -2027,6 +2028,15 @@ int nse_ensemble_step(nse_ensemble* e, int nsteps) {
   return ok ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
 
+int nse_ensemble_set_stream(nse_ensemble* e, void* stream) {
+  if (!e || !stream) return NSE_ERR_ARG;
+  if (!NSE_CUDA(cudaStreamSynchronize(e->origin))) return status_or(NSE_ERR_CUDA);
+  if (e->own_origin) cudaStreamDestroy(e->origin);
+  e->own_origin = false;
+  e->origin = (cudaStream_t)stream;
+  return NSE_OK;
+}
+
 int nse_ensemble_sync(nse_ensemble* e) {
   if (!e) return NSE_ERR_ARG;
   bool ok = NSE_CUDA(cudaStreamSynchronize(e->origin));
@@ -2047,7 +2057,7 @@ int nse_ensemble_destroy(nse_ensemble* e) {
   if (e->fork) cudaEventDestroy(e->fork);
   for (cudaStream_t st : e->streams)
     if (st) cudaStreamDestroy(st);
-  if (e->origin) cudaStreamDestroy(e->origin);
+  if (e->origin && e->own_origin) cudaStreamDestroy(e->origin);
   delete e;
   return NSE_OK;
 }

@@ -69,6 +69,7 @@ def _sig():
     L.nse_launch_count.restype = C.c_longlong
     L.nse_ensemble_create.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp)]
     L.nse_ensemble_step.argtypes = [vp, C.c_int]
+    L.nse_ensemble_set_stream.argtypes = [vp, vp]
     L.nse_ensemble_sync.argtypes = [vp]
     L.nse_ensemble_destroy.argtypes = [vp]
     return L
@@ -226,6 +227,10 @@ class Ensemble:
 
     def step(self, n=1):
         check(self.L.nse_ensemble_step(self.h, int(n)))
+
+    def set_stream(self, stream):
+        """graph replays on the caller's cudaStream_t (e.g. torch's cuda_stream)"""
+        check(self.L.nse_ensemble_set_stream(self.h, stream))
 
     def sync(self):
         check(self.L.nse_ensemble_sync(self.h))
