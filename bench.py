@@ -323,6 +323,93 @@ def run_ensemble(S, W, torch, stream, args):
     return res
 
 
+def run_adjoint(S, W, torch, stream, args):
+    """Discrete adjoint at args.adj_grid^3: the sphere of the main workload at
+    the same physical size, walls at T = 1 (y = -1) and T = 0 (y = 1), sphere
+    T = 1; args.adj_steps FP64 steps from the projected noisy channel,
+    checkpointed every 20 steps in device memory; J = mean wall heat flux at
+    y = -1 over the last 100 steps.  dJ/dc1 from one adjoint sweep, checked
+    along args.adj_dirs seeded N(0,1) directions against central finite
+    differences of J with step 1e-6."""
+    n = args.adj_grid
+    g = W.grid_arrays(n, n, n, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = W.channel_state(g, seed=2025, t_bot=1.0, t_top=0.0)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    cfg = S.Config(n, n, n, dt, RE, PR, ETA, 2 * math.pi, 2.0, math.pi, y0=-1.0, ystretch=2.0,
+                   body_force=3.0 / RE, heat_source=0.0, t_bot=1.0, t_top=0.0, t_solid=1.0)
+    N = args.adj_steps
+    avg_from = max(1, N - 99)
+    res = {"grid": [n, n, n], "steps": N, "checkpoint_every": 20, "avg_from": avg_from,
+           "objective": "mean over the last 100 steps of the area-weighted wall heat flux at "
+                        "y = -1, thc (T(i,1,k) - T(i,0,k)) / dy12(0)",
+           "walls": "T = 1 at y = -1, T = 0 at y = 1, sphere T = 1", "dt": dt}
+    with S.Context(cfg) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        for k in ("u", "v", "w", "T"):
+            ctx.upload(k, f[k])
+        ctx.levelset(W.sphere_phi0(g, *SPHERE), width=WIDTH, want_phi=False)
+        ctx.project()
+        ctx.start()
+        c1 = ctx.download("cellvalue")
+        names = ("u", "v", "w", "T", "u_ta", "v_ta", "w_ta", "u_pre", "v_pre", "w_pre", "T_pre")
+        st0 = {k: ctx.download(k) for k in names}
+        l0 = ctx.step_index
+
+        def reset(c):
+            for k in names:
+                ctx.upload(k, st0[k])
+            ctx.upload("cellvalue", c)
+            ctx.step_index = l0
+
+        with S.Adjoint(ctx, N, checkpoint_every=20, avg_from=avg_from) as adj:
+            reset(c1)
+            torch.cuda.synchronize()
+            t0 = time.perf_counter()
+            J0 = adj.objective()
+            t_fwd = time.perf_counter() - t0
+            reset(c1)
+            t0 = time.perf_counter()
+            J, grad = adj.gradient()
+            t_grad = time.perf_counter() - t0
+            rng = np.random.default_rng(4242)
+            eps = 1e-6
+
+            def central(d, e):
+                reset(c1 + e * d)
+                Jp = adj.objective()
+                reset(c1 - e * d)
+                return (Jp - adj.objective()) / (2 * e)
+
+            # central differences at eps, and Richardson's combination of eps
+            # and eps/2, (4 D(eps/2) - D(eps)) / 3, which cancels the eps^2
+            # truncation term (the response to a perturbation of every cell
+            # of the mask is strongly nonlinear: the plain error scales as eps^2)
+            errs, errs_c, rows = [], [], []
+            t0 = time.perf_counter()
+            for _ in range(args.adj_dirs):
+                d = rng.standard_normal(c1.shape)
+                f1 = central(d, eps)
+                f2 = central(d, eps / 2)
+                fr = (4.0 * f2 - f1) / 3.0
+                ad = float(np.sum(grad * d))
+                errs.append(abs(fr - ad) / abs(fr))
+                errs_c.append(abs(f1 - ad) / abs(f1))
+                rows.append([fr, f1, ad])
+            t_fd = time.perf_counter() - t0
+    res.update({"J": J, "J_forward_only": J0, "forward_s": round(t_fwd, 3),
+                "gradient_s": round(t_grad, 3),
+                "gradient_over_forward": round(t_grad / t_fwd, 2),
+                "fd_directions": args.adj_dirs, "fd_step": eps,
+                "fd_rel_err": {"max": max(errs), "median": float(np.median(errs)),
+                               "kind": "Richardson-extrapolated central differences "
+                                       "(steps 1e-6 and 5e-7)"},
+                "central_fd_rel_err": {"max": max(errs_c), "median": float(np.median(errs_c)),
+                                       "kind": "central differences, step 1e-6"},
+                "fd_richardson_central_adjoint_first": rows[:4], "fd_s": round(t_fd, 2),
+                "grad_l2": float(np.linalg.norm(grad))})
+    return res
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -437,6 +524,11 @@ def run_ours(args, rank, world, local_rank):
     if args.ens_cases > 0:
         ensemble = run_ensemble(S, W, torch, stream, args)
 
+    # ------------------------------------------------------ discrete adjoint
+    adjoint = None
+    if args.adj_steps > 0:
+        adjoint = run_adjoint(S, W, torch, stream, args)
+
     # ---------------------------------------------------------- CPU baseline
     cpu = None
     if rank == 0 and not args.no_cpu:
@@ -477,6 +569,7 @@ def run_ours(args, rank, world, local_rank):
         "max_divu": mon["max_divu"],
         "mixed_precision": mixed,
         "ensemble": ensemble,
+        "adjoint": adjoint,
         "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d / args.steps),
                 "d2h_bytes_per_step": int(d2h / args.steps),
@@ -577,6 +670,10 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--ens-cases", type=int, default=32,
                     help="cases of the batched-ensemble measurement (0 skips it)")
+    ap.add_argument("--adj-steps", type=int, default=400,
+                    help="forward steps of the adjoint measurement (0 skips it)")
+    ap.add_argument("--adj-grid", type=int, default=128)
+    ap.add_argument("--adj-dirs", type=int, default=16)
     ap.add_argument("--acc-steps", type=int, default=100,
                     help="steps of the mixed-vs-FP64 accuracy comparison")
     args = ap.parse_args()

@@ -317,6 +317,61 @@ int nse_ensemble_step(nse_ensemble* ens, int nsteps);
 int nse_ensemble_set_stream(nse_ensemble* ens, void* stream);
 int nse_ensemble_sync(nse_ensemble* ens);
 int nse_ensemble_destroy(nse_ensemble* ens);
+/* Discrete adjoint (no counterpart in the reference, whose adjoint.f is a set
+ * of unconnected routines): the exact transpose of the FP64 resident step.
+ * Objective, from the context's current state over nsteps steps:
+ *   J = mean over steps avg_from..nsteps of the wall heat flux at y = y0,
+ *       sum_ik a_ik thc (T(i,1,k) - T(i,0,k)) / dy12(0), a_ik = dx_i dz_k/(xl zl),
+ *       with the wall ghost T(i,0,k) = 2 t_bot - T(i,1,k)
+ *     + sum over state fields f of <W_f, f after nsteps> (nse_adjoint_set_weight).
+ * nse_adjoint_gradient returns J and dJ/dc1 (nx*ny*nz, the layout of
+ * cellvalue's first column); the adjoint of the initial state is then read
+ * with nse_adjoint_download (padded field; u, v, w, T, u_ta, v_ta, w_ta and
+ * the AB2 histories).  The forward run is checkpointed every
+ * checkpoint_every steps in device memory and replayed per segment; the
+ * context is left at the state after nsteps.  FP64 contexts only. */
+typedef struct nse_adjoint nse_adjoint;
+typedef struct nse_adjoint_config {
+  int nsteps;
+  int checkpoint_every;
+  int avg_from;  /* first step (1-based) of the averaging window */
+} nse_adjoint_config;
+int nse_adjoint_create(nse_ctx* ctx, const nse_adjoint_config* cfg, nse_adjoint** out);
+/* weights (padded field, interior used) of a linear functional of the final
+ * state field `field` added to J; NULL removes them */
+int nse_adjoint_set_weight(nse_adjoint* adj, int field, const double* weights);
+/* forward run only: J */
+int nse_adjoint_objective(nse_adjoint* adj, double* J);
+int nse_adjoint_gradient(nse_adjoint* adj, double* J, double* grad_c1);
+int nse_adjoint_download(nse_adjoint* adj, int field, double* host);
+int nse_adjoint_destroy(nse_adjoint* adj);
+
+/* adjoint.f routines (drop-ins, same arguments): set_adj_convect adjoint.f:1,
+ * set_adj_convection_for_scalar :128, set_adj_ns_scalar :185.  They compute
+ * what the reference's routines compute (including their index slips); the
+ * reference's set_adj_NS_scalar reads its adjoint temperature T_final from an
+ * uninitialised local array, which static zero-filled storage makes zero:
+ * set_adj_ns_scalar_ uses zero, nse_adj_ns_scalar takes T_final. */
+void set_adj_convect_(double* u, double* u_v, double* v, double* v_v, double* w, double* w_v,
+                      const double* Re, const double* dt, const int* nx, const int* ny,
+                      const int* nz, const double* dx, const double* dy, const double* dz,
+                      const double* dx12, const double* dy12, const double* dz12,
+                      double* u_final, double* v_final, double* w_final);
+void set_adj_convection_for_scalar_(double* u, double* v, double* w, const double* Re,
+                                    const double* dt, const int* nx, const int* ny,
+                                    const int* nz, const double* dx, const double* dy,
+                                    const double* dz, const double* dx12, const double* dy12,
+                                    const double* dz12, double* T, double* u_vT,
+                                    double* rhoCp, double* u_final, double* v_final,
+                                    double* w_final);
+void set_adj_ns_scalar_(const double* dt, const int* nx, const int* ny, const int* nz,
+                        const double* dx12, const double* dy12, const double* dz12, double* T,
+                        double* u_s, double* v_s, double* w_s, double* u_final,
+                        double* v_final, double* w_final);
+int nse_adj_ns_scalar(const double* dt, int nx, int ny, int nz, const double* dx12,
+                      const double* dy12, const double* dz12, const double* T,
+                      const double* T_final, double* u_s, double* v_s, double* w_s);
+
 /* number of kernel launches this process has issued through the library */
 long long nse_launch_count(void);
 

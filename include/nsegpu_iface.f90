@@ -1,7 +1,9 @@
 ! nsegpu_iface.f90 -- Fortran 2003 interfaces to the resident (tier 3) API of
 ! libnsegpu.so.  The reference subroutines themselves (MKP, P2S, S2P, SPN,
 ! SP0B, PHIBC, CTRIDIAG, TRIDIAG, TRID2, implicit_solver, TDMA, cyclic,
-! set_levelset, readgrid3d and the step routines of nse_dominik.f) need no
+! set_levelset, readgrid3d, the step routines of nse_dominik.f and the
+! adjoint.f routines set_adj_convect, set_adj_convection_for_scalar,
+! set_adj_NS_scalar) need no
 ! interface: libnsegpu.so exports them under gfortran's mangled names
 ! (mkp_, p2s_, ...), so a driver that calls them links against the library
 ! instead of the reference object files.  See INTEGRATION.md.
@@ -15,6 +17,10 @@ module nsegpu
        NSE_U_TA = 5, NSE_V_TA = 6, NSE_W_TA = 7, NSE_U_PRE = 8, NSE_V_PRE = 9, &
        NSE_W_PRE = 10, NSE_T_PRE = 11, NSE_DIVU = 12, NSE_U_EP2 = 13, NSE_V_EP2 = 14, &
        NSE_W_EP2 = 15, NSE_PHI = 16, NSE_CELLVALUE = 17
+
+  type, bind(C) :: nse_adjoint_config
+     integer(c_int) :: nsteps, checkpoint_every, avg_from
+  end type nse_adjoint_config
 
   type, bind(C) :: nse_config
      integer(c_int) :: nx, ny, nz
@@ -85,6 +91,28 @@ module nsegpu
        import :: c_int, c_ptr
        type(c_ptr), value :: ctx
      end function nse_sync
+     integer(c_int) function nse_adjoint_create(ctx, cfg, adj) bind(C, name="nse_adjoint_create")
+       import :: c_int, c_ptr, nse_adjoint_config
+       type(c_ptr), value :: ctx
+       type(nse_adjoint_config), intent(in) :: cfg
+       type(c_ptr), intent(out) :: adj
+     end function nse_adjoint_create
+     integer(c_int) function nse_adjoint_gradient(adj, J, grad_c1) &
+          bind(C, name="nse_adjoint_gradient")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: adj
+       real(c_double), intent(out) :: J
+       real(c_double), intent(out) :: grad_c1(*)
+     end function nse_adjoint_gradient
+     integer(c_int) function nse_adjoint_objective(adj, J) bind(C, name="nse_adjoint_objective")
+       import :: c_int, c_ptr, c_double
+       type(c_ptr), value :: adj
+       real(c_double), intent(out) :: J
+     end function nse_adjoint_objective
+     integer(c_int) function nse_adjoint_destroy(adj) bind(C, name="nse_adjoint_destroy")
+       import :: c_int, c_ptr
+       type(c_ptr), value :: adj
+     end function nse_adjoint_destroy
      type(c_ptr) function nse_last_error() bind(C, name="nse_last_error")
        import :: c_ptr
      end function nse_last_error

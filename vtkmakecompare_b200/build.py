@@ -29,6 +29,8 @@ SOURCES = {
     "k_fft.cu": [],
     "noalloc.cu": [],
     "fortran_io.cu": [],
+    "k_adjoint.cu": ["--fmad=false"],
+    "adjoint.cu": [],
 }
 
 
@@ -49,6 +51,7 @@ def _needs(obj, deps):
 def build(verbose=False, extra=()):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "k_lines.cuh"),
+               os.path.join(CSRC, "k_adjoint.cuh"),
                os.path.join(HERE, "..", "include", "nsegpu.h")]
     jobs = []
     objs = []

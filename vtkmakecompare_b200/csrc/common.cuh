@@ -269,4 +269,21 @@ void launch_monitor(const Dims& d, const GridDev& g, const double* u, const doub
                     const double* w, const double* T, const double* divu, double* out6,
                     cudaStream_t s);
 
+// resident context internals shared with the adjoint driver (runtime.cu)
+struct CtxInfo {
+  Dims d;
+  GridDev g;
+  const nse_config* cfg;
+  cudaStream_t s;
+  const PoissonPlan* pp;
+  bool mixed;
+};
+bool ctx_info(nse_ctx* x, CtxInfo& out);
+double* ctx_field(nse_ctx* x, int id);
+int ctx_get_l(nse_ctx* x);
+void ctx_set_l(nse_ctx* x, int l);
+// one step of the context; with rec given, the line-solve passes record their
+// inputs and outputs (16 padded fields, see nse_ctx::rec)
+void ctx_step_rec(nse_ctx* x, double* const* rec);
+
 }  // namespace nse

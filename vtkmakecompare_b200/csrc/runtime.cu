@@ -13,6 +13,7 @@
 #include <vector>
 
 #include "common.cuh"
+#include "k_adjoint.cuh"
 #include "k_lines.cuh"
 
 namespace nse {
@@ -570,6 +571,94 @@ void set_diffusion_for_scalar_(const double* Re, const double* dt, const int* nx
   st.finish();
 }
 
+// ------------------------------------------------------- adjoint.f ----
+void set_adj_convect_(double* u, double* u_v, double* v, double* v_v, double* w, double* w_v,
+                      const double* Re, const double* dt, const int* nx, const int* ny,
+                      const int* nz, const double* dx, const double* dy, const double* dz,
+                      const double* dx12, const double* dy12, const double* dz12,
+                      double* u_final, double* v_final, double* w_final) {
+  (void)Re;
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_adj_convect")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  double *du = st.up(u, d.ntot), *dv = st.up(v, d.ntot), *dw = st.up(w, d.ntot);
+  double *duf = st.up(u_final, d.ntot), *dvf = st.up(v_final, d.ntot);
+  double* dwf = st.up(w_final, d.ntot);
+  double *duv = st.alloc(d.ntot), *dvv = st.alloc(d.ntot), *dwv = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_set_adj_convect(d, adj_grid(g), du, dv, dw, duf, dvf, dwf, duv, dvv, dwv, *dt, st.s);
+  down_interior(st, u_v, duv, d);
+  down_interior(st, v_v, dvv, d);
+  down_interior(st, w_v, dwv, d);
+  st.finish();
+}
+
+void set_adj_convection_for_scalar_(double* u, double* v, double* w, const double* Re,
+                                    const double* dt, const int* nx, const int* ny,
+                                    const int* nz, const double* dx, const double* dy,
+                                    const double* dz, const double* dx12, const double* dy12,
+                                    const double* dz12, double* T, double* u_vT,
+                                    double* rhoCp, double* u_final, double* v_final,
+                                    double* w_final) {
+  (void)u; (void)v; (void)w; (void)Re;
+  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_adj_convection_for_scalar")) return;
+  Dims d = make_dims(*nx, *ny, *nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx, dy, dz, dx12, dy12, dz12, g)) return;
+  double *dT = st.up(T, d.ntot), *dr = st.up(rhoCp, d.ntot);
+  double *duf = st.up(u_final, d.ntot), *dvf = st.up(v_final, d.ntot);
+  double *dwf = st.up(w_final, d.ntot), *dout = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_set_adj_cscalar(d, adj_grid(g), dT, dr, duf, dvf, dwf, dout, *dt, st.s);
+  down_interior(st, u_vT, dout, d);
+  st.finish();
+}
+
+// adjoint temperature Tf (padded) or zero when Tf is null
+static void adj_ns_scalar(const double* dt, int nx, int ny, int nz, const double* dx12,
+                          const double* dy12, const double* dz12, const double* T,
+                          const double* Tf, double* u_s, double* v_s, double* w_s) {
+  if (!ensure_device() || !dims_ok(nx, ny, nz, "set_adj_ns_scalar")) return;
+  Dims d = make_dims(nx, ny, nz);
+  Stage st;
+  GridDev g;
+  if (!stage_grid(st, d.nx, d.ny, d.nz, dx12, dy12, dz12, dx12, dy12, dz12, g)) return;
+  double* dT = st.up(T, d.ntot);
+  double* dTf = Tf ? st.up(Tf, d.ntot) : st.alloc(d.ntot);
+  if (dTf && !Tf && !NSE_CUDA(cudaMemsetAsync(dTf, 0, d.ntot * sizeof(double), st.s)))
+    st.ok = false;
+  double *dus = st.alloc(d.ntot), *dvs = st.alloc(d.ntot), *dws = st.alloc(d.ntot);
+  if (!st.ok) return;
+  launch_set_adj_ns_scalar(d, adj_grid(g), dT, dTf, dus, dvs, dws, *dt, st.s);
+  down_interior(st, u_s, dus, d);
+  down_interior(st, v_s, dvs, d);
+  down_interior(st, w_s, dws, d);
+  st.finish();
+}
+
+void set_adj_ns_scalar_(const double* dt, const int* nx, const int* ny, const int* nz,
+                        const double* dx12, const double* dy12, const double* dz12, double* T,
+                        double* u_s, double* v_s, double* w_s, double* u_final,
+                        double* v_final, double* w_final) {
+  (void)u_final; (void)v_final; (void)w_final;
+  adj_ns_scalar(dt, *nx, *ny, *nz, dx12, dy12, dz12, T, nullptr, u_s, v_s, w_s);
+}
+
+int nse_adj_ns_scalar(const double* dt, int nx, int ny, int nz, const double* dx12,
+                      const double* dy12, const double* dz12, const double* T,
+                      const double* T_final, double* u_s, double* v_s, double* w_s) {
+  nse_clear_error();
+  if (!dt || !T || !T_final || !u_s || !v_s || !w_s) {
+    set_error(NSE_ERR_ARG, "nse_adj_ns_scalar: null argument");
+    return NSE_ERR_ARG;
+  }
+  adj_ns_scalar(dt, nx, ny, nz, dx12, dy12, dz12, T, T_final, u_s, v_s, w_s);
+  return nse_last_status();
+}
+
 void set_immersed_boundary_(const double* eta, const int* nx, const int* ny, const int* nz,
                             const double* dt, double* u_l, double* v_l, double* w_l,
                             const double* dx, const double* dy, const double* dz,
@@ -1076,6 +1165,10 @@ struct nse_ctx {
   bool lines64 = false;  // FP64 arithmetic in the line sweeps (FP32 storage)
   int refine = 1;
   DBuf ptab_f[3][4], pmtab_f[3][4];
+  // when set (adjoint replays), each line-solve pass copies its input to
+  // rec[4*comp + pass] and the final line output to rec[4*comp + 3]
+  // (comp 0 u, 1 v, 2 w, 3 T; velocity passes y, z, x; temperature y, x, z)
+  double* const* rec = nullptr;
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1668,7 +1761,14 @@ static void ctx_step(nse_ctx* x) {
   const bool exact = (c.flags & NSE_FLAG_EXACT) != 0;
   auto lines = exact ? launch_lines_exact : launch_lines_fast;
   double* fa[3] = {ua, va, wa};
+  size_t fbytes = d.ntot * sizeof(double);
+  auto record = [&](int comp, int pass, const double* f) {
+    if (x->rec)
+      NSE_CUDA(cudaMemcpyAsync(x->rec[4 * comp + pass], f, fbytes, cudaMemcpyDeviceToDevice, s));
+  };
   auto run = [&](int dir, int comp, double* f, int tab, double ft, double fb) {
+    record(comp, comp == 3 ? (dir == 1 ? 0 : (dir == 0 ? 1 : 2)) : (dir == 1 ? 0 : (dir == 2 ? 1 : 2)),
+           f);
     LineArgs la = line_args(x, comp);
     la.ft = ft;
     la.fb = fb;
@@ -1694,6 +1794,8 @@ static void ctx_step(nse_ctx* x) {
   run(0, 3, uT, TB_X_T, 0.0, 0.0);
   mark(x, PH_ZT);
   run(2, 3, uT, TB_Z_T, 0.0, 0.0);
+  for (int comp = 0; comp < 3; ++comp) record(comp, 3, fa[comp]);
+  record(3, 3, uT);
   // :429-437 T = u_T (interior); the ghosts are rewritten by the next set_bc
   std::swap(x->f[NSE_T], x->uT);
   T = F(x, NSE_T);
@@ -1705,6 +1807,32 @@ static void ctx_step(nse_ctx* x) {
   if (x->prof_n < x->prof_cap) x->prof_n++;
   x->l += 1;
 }
+
+}  // extern "C"
+
+// internal hooks of the adjoint driver (adjoint.cu)
+namespace nse {
+bool ctx_info(nse_ctx* x, CtxInfo& out) {
+  if (!x) return false;
+  out.d = x->d;
+  out.g = x->g;
+  out.cfg = &x->cfg;
+  out.s = x->stream;
+  out.pp = &x->pb.pp;
+  out.mixed = x->mixed;
+  return true;
+}
+double* ctx_field(nse_ctx* x, int id) { return F(x, id); }
+int ctx_get_l(nse_ctx* x) { return x->l; }
+void ctx_set_l(nse_ctx* x, int l) { x->l = l; }
+void ctx_step_rec(nse_ctx* x, double* const* rec) {
+  x->rec = rec;
+  ctx_step(x);
+  x->rec = nullptr;
+}
+}  // namespace nse
+
+extern "C" {
 
 int nse_step(nse_ctx* x, int nsteps) {
   if (!x || nsteps < 0) return NSE_ERR_ARG;

@@ -55,6 +55,9 @@ _SIG = {
     "output": "aaaaaaaiiiaaaaaaa",         # nse_dominik.f:2606 (files under ./)
     "outfield": "aaaaaaaiiidaaaaa",        # nse_dominik.f:2726
     "readfield": "aaaaiiiaaaaa",           # nse_dominik.f:2769
+    "set_adj_convect": "aaaaaaddiiiaaaaaaaaa",                  # adjoint.f:1
+    "set_adj_convection_for_scalar": "aaaddiiiaaaaaaaaaaaa",    # adjoint.f:128
+    "set_adj_ns_scalar": "diiiaaaaaaaaaa",                      # adjoint.f:185
 }
 
 

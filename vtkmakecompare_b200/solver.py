@@ -46,6 +46,12 @@ class Config(C.Structure):
                          heat_source, t_bot, t_top, t_solid, rho_cp, thc, precision, flags)
 
 
+class AdjointConfig(C.Structure):
+    """nse_adjoint_config of include/nsegpu.h"""
+
+    _fields_ = [("nsteps", C.c_int), ("checkpoint_every", C.c_int), ("avg_from", C.c_int)]
+
+
 def _sig():
     L = lib()
     vp = C.c_void_p
@@ -72,6 +78,12 @@ def _sig():
     L.nse_ensemble_set_stream.argtypes = [vp, vp]
     L.nse_ensemble_sync.argtypes = [vp]
     L.nse_ensemble_destroy.argtypes = [vp]
+    L.nse_adjoint_create.argtypes = [vp, C.POINTER(AdjointConfig), C.POINTER(vp)]
+    L.nse_adjoint_set_weight.argtypes = [vp, C.c_int, vp]
+    L.nse_adjoint_objective.argtypes = [vp, vp]
+    L.nse_adjoint_gradient.argtypes = [vp, vp, vp]
+    L.nse_adjoint_download.argtypes = [vp, C.c_int, vp]
+    L.nse_adjoint_destroy.argtypes = [vp]
     return L
 
 
@@ -239,6 +251,88 @@ class Ensemble:
         if self.h:
             self.L.nse_ensemble_destroy(self.h)
             self.h = None
+
+    def __enter__(self):
+        return self
+
+    def __exit__(self, *a):
+        self.close()
+
+
+def adj_ns_scalar(dt, g, T, T_final):
+    """set_adj_NS_scalar (adjoint.f:185-211) with the adjoint temperature given
+    (nse_adj_ns_scalar); g: grid dict with dx12, dy12, dz12.  Returns padded
+    u_s, v_s, w_s (interior written)."""
+    L = _sig()
+    vp = C.c_void_p
+    L.nse_adj_ns_scalar.argtypes = [vp, C.c_int, C.c_int, C.c_int, vp, vp, vp, vp, vp, vp, vp, vp]
+    T = np.asfortranarray(T, dtype=np.float64)
+    Tf = np.asfortranarray(T_final, dtype=np.float64)
+    nx, ny, nz = (s - 2 for s in T.shape)
+    out = [np.zeros(T.shape, order="F") for _ in range(3)]
+    d = C.c_double(dt)
+    check(L.nse_adj_ns_scalar(C.addressof(d), nx, ny, nz, g["dx12"].ctypes.data,
+                              g["dy12"].ctypes.data, g["dz12"].ctypes.data, T.ctypes.data,
+                              Tf.ctypes.data, *[o.ctypes.data for o in out]))
+    return out
+
+
+class Adjoint:
+    """Discrete adjoint of `nsteps` FP64 steps of a Context (nse_adjoint_*).
+
+    J = mean over steps avg_from..nsteps of the wall heat flux at y = y0 plus
+    sum_f <W_f, f after nsteps> for the weights set with `set_weight`.
+    `gradient()` returns (J, dJ/dc1) with dJ/dc1 shaped (nx, ny, nz); the
+    adjoint of the initial state is then `initial_adjoint(name)`.  Both calls
+    run from the context's current state and leave it after nsteps steps."""
+
+    def __init__(self, ctx, nsteps, checkpoint_every=20, avg_from=None):
+        self.L = _sig()
+        self.ctx = ctx
+        avg_from = nsteps if avg_from is None else avg_from
+        self.cfg = AdjointConfig(int(nsteps), int(checkpoint_every), int(avg_from))
+        h = C.c_void_p()
+        check(self.L.nse_adjoint_create(ctx.h, C.byref(self.cfg), C.byref(h)))
+        self.h = h
+
+    def set_weight(self, name, weights):
+        if weights is None:
+            check(self.L.nse_adjoint_set_weight(self.h, FIELD_ID[name], None))
+            return
+        w = np.asfortranarray(weights, dtype=np.float64)
+        if w.shape != self.ctx.shape:
+            raise ValueError(f"weights of {name}: shape {w.shape}, expected {self.ctx.shape}")
+        self._keep = getattr(self, "_keep", {})
+        self._keep[name] = w
+        check(self.L.nse_adjoint_set_weight(self.h, FIELD_ID[name], w.ctypes.data))
+
+    def objective(self):
+        J = C.c_double()
+        check(self.L.nse_adjoint_objective(self.h, C.byref(J)))
+        return J.value
+
+    def gradient(self):
+        c = self.ctx.cfg
+        g = np.zeros((c.nx, c.ny, c.nz), order="F")
+        J = C.c_double()
+        check(self.L.nse_adjoint_gradient(self.h, C.byref(J), g.ctypes.data))
+        return J.value, g
+
+    def initial_adjoint(self, name):
+        out = np.zeros(self.ctx.shape, order="F")
+        check(self.L.nse_adjoint_download(self.h, FIELD_ID[name], out.ctypes.data))
+        return out
+
+    def close(self):
+        if getattr(self, "h", None):
+            self.L.nse_adjoint_destroy(self.h)
+            self.h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
 
     def __enter__(self):
         return self
