@@ -216,6 +216,7 @@ struct PoissonPlan {
   const double* twz;          // twiddles exp(-2 pi i k/nz)
   const float* twx_f;         // the same twiddles rounded to FP32
   const float* twz_f;
+  const double* spn_im;       // SPN pivot reciprocals [nz][ny][Hp] (null: none)
 };
 bool poisson_plan_tables(int nx, int ny, int nz, const double* dx, const double* dy,
                          const double* dz, const double* dy12, double xl, double zl,
@@ -226,17 +227,26 @@ bool poisson_plan_tables(int nx, int ny, int nz, const double* dx, const double*
 // at cell (i==0?nx:i, J, k==0?nz:k) (MKP RHS + periodic fill fused)
 // src_mode 1 forms the divergence right-hand side; with rg given it multiplies
 // by the tabulated reciprocal spacings instead of dividing (fast form)
+// j0, nj: window of planes J = j0+1 .. j0+nj (nj = 0: all planes)
 void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const double* ut, const double* vt, const double* wt,
                       const GridDev& g, double dt, int src_mode, cudaStream_t s,
-                      const GridRcp* rg = nullptr);
-void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s);
+                      const GridRcp* rg = nullptr, int j0 = 0, int nj = 0);
+void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 0, int nj = 0);
+
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s);
+// SPN pivot tables of the two-ended elimination (0 from spn_split: no
+// tables for this plan) and the table-driven SPN + SP0B of the fast form
+int spn_split(const PoissonPlan& pp);
+void launch_spn_tables(const PoissonPlan& pp, double* im, cudaStream_t s);
+void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s);
+void launch_spn_fast_f32(const PoissonPlan& pp, cudaStream_t s);
 void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,
                      long scj, long sck, const double* AC, const double* KXZ, bool do_spn,
                      bool do_sp0b, cudaStream_t s);
 // inverse x transform into padded FP for J=1..NY with the S2P wrap fill
-void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s);
+void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s,
+                      int j0 = 0, int nj = 0);
 void launch_phibc(const Dims& d, double* PHI, cudaStream_t s);
 // spectrum <-> reference PHIT layout (0:nx/2,0:ny+1,0:nz+1)
 void launch_spec_to_phit(const PoissonPlan& pp, double* phit, cudaStream_t s);

@@ -184,6 +184,7 @@ template <class CT>
 struct SpecViewT {
   CT* base;
   long sj, sk;
+  int j0 = 0;  // first plane (0-based) of a launch over a window of planes
 };
 using SpecView = SpecViewT<double2>;
 
@@ -226,7 +227,7 @@ __global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, Fw
   const int N = sh.n;
   CT* a = smem;
   CT* b = smem + (long)npair * N;
-  const int J = 1 + blockIdx.x;
+  const int J = 1 + sv.j0 + blockIdx.x;
   const int kk0 = 2 * npair * blockIdx.y;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   for (int t = threadIdx.x; t < npair * N; t += blockDim.x) {
@@ -288,7 +289,7 @@ __global__ void k_fft_z(FFTShape sh, int W, int H, SpecViewT<CT> sv, const CT* _
   const int FS = N + 1;
   CT* a = smem;
   CT* b = smem + (long)W * FS;
-  const int jj = blockIdx.y;
+  const int jj = sv.j0 + blockIdx.y;
   const int kx0 = blockIdx.x * W;
   for (int t = threadIdx.x; t < W * N; t += blockDim.x) {
     int c = t % W, kz = t / W;
@@ -322,7 +323,7 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, do
   const int N = sh.n;
   CT* a = smem;
   CT* b = smem + (long)npair * N;
-  const int J = 1 + blockIdx.x;
+  const int J = 1 + sv.j0 + blockIdx.x;
   const int kk0 = 2 * npair * blockIdx.y;
   const int nz = d.nz;
   const int H = N / 2 + 1;
@@ -427,7 +428,7 @@ __global__ void __launch_bounds__(128) k_fft256_fwd_x(Dims d, SpecViewT<CT> sv, 
   __shared__ CT sbuf[8][16 * FS];
   const int h = threadIdx.x >> 4, b = threadIdx.x & 15;
   CT* S_ = sbuf[h];
-  const int J = 1 + blockIdx.x;
+  const int J = 1 + sv.j0 + blockIdx.x;
   const int ka = 2 * (blockIdx.y * 8 + h), kb = ka + 1;
   const int nx = d.nx, ny = d.ny, nz = d.nz;
   CT v[16];
@@ -494,7 +495,7 @@ __global__ void __launch_bounds__(128) k_fft256_inv_x(Dims d, SpecViewT<CT> sv, 
   __shared__ CT sbuf[8][16 * FS];
   const int h = threadIdx.x >> 4, b = threadIdx.x & 15;
   CT* S_ = sbuf[h];
-  const int J = 1 + blockIdx.x;
+  const int J = 1 + sv.j0 + blockIdx.x;
   const int ka = 2 * (blockIdx.y * 8 + h), kb = ka + 1;
   const int nz = d.nz;
 #pragma unroll
@@ -556,7 +557,7 @@ __global__ void __launch_bounds__(256) k_fft256_z(int H, SpecViewT<CT> sv,
   extern __shared__ __align__(16) char fsm[];
   CT* S_ = reinterpret_cast<CT*>(fsm);  // [c][b][col], col stride 1, b stride 17
   const int col = threadIdx.x & 15, b = threadIdx.x >> 4;
-  const int jj = blockIdx.y;
+  const int jj = sv.j0 + blockIdx.y;
   const int kx = blockIdx.x * 16 + col;
   const bool ok = kx < H;
   CT* base = sv.base + kx + sv.sj * jj;
@@ -723,6 +724,168 @@ __global__ void k_spn(int H, int ny, int nz, RT* base, long svj, long svk, doubl
   }
 }
 
+// ------------------------------------- SPN: two-ended Thomas (fast form) --
+// The Neumann-folded SPN matrix of wavenumber (kx, kz) (mkp.f:239-254)
+// depends only on the grid (AC) and KXZ.  Its rows are split at m = ny/2:
+// rows 0..m-1 are eliminated downwards, x(r) = y(r) - cT(r) x(r+1), and rows
+// m..ny-1 upwards, x(r) = z(r) - cB(r) x(r-1); the two meet in a 2x2 system
+// for x(m-1), x(m).  The pivot reciprocals im(r) (top pivots above m, bottom
+// pivots from m on) are tabulated once per context, real [kz][r][kx] with
+// pitch Hp; cT(r) = AC3(r) im(r), cB(r) = AC1(r) im(r).  The mean mode keeps
+// SP0B's forward marching (mkp.f:263-290).
+__global__ void k_spn_tables(int H, int Hp, int ny, int nz, int m, const double* __restrict__ AC,
+                             const double* __restrict__ KXZ, double* im) {
+  const int kx = blockIdx.x * blockDim.x + threadIdx.x;
+  const int kz = blockIdx.y;
+  if (kx >= H) return;
+  const double* AC1 = AC;
+  const double* AC2 = AC + ny;
+  const double* AC3 = AC + 2 * ny;
+  const long sr = Hp, base = kx + (long)Hp * ny * kz;
+  if (kx == 0 && kz == 0) {
+    for (int r = 0; r < ny; ++r) im[base + sr * r] = 0.0;
+    return;
+  }
+  const double kxz = KXZ[kx + (long)H * kz];
+  auto diag = [&](int r) {
+    double b = AC2[r] - kxz;
+    if (r == 0) b = b + AC1[0];
+    if (r == ny - 1) b = b + AC3[ny - 1];
+    return b;
+  };
+  double cp = 0.0;
+  for (int r = 0; r < m; ++r) {
+    const double mm = (r == 0) ? diag(0) : diag(r) - AC1[r] * cp;
+    const double w = 1.0 / mm;
+    im[base + sr * r] = w;
+    cp = AC3[r] * w;
+  }
+  cp = 0.0;
+  for (int r = ny - 1; r >= m; --r) {
+    const double mm = (r == ny - 1) ? diag(r) : diag(r) - AC3[r] * cp;
+    const double w = 1.0 / mm;
+    im[base + sr * r] = w;
+    cp = AC1[r] * w;
+  }
+}
+
+// asynchronous global -> shared copies of 4 or 8 bytes (cp.async, waited
+// for by the issuing thread with cp.async.wait_all: no spin loop)
+template <int BYTES>
+__device__ __forceinline__ void cp_async(void* smem, const void* gmem) {
+  const unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], %2;\n" ::"r"(sa), "l"(gmem), "n"(BYTES)
+               : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() {
+  asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
+}
+
+// Four threads per (kx, kz): (re | im) x (top | bottom half), 16 systems per
+// 64-thread CTA.  Each thread first issues cp.async copies of all the rows of
+// its half (the spectrum values; the comp-0 thread of each half also the
+// pivot reciprocals) into shared memory, so every row is in flight at once,
+// then runs its recurrence from shared memory; the back substitution writes
+// the solution to global memory.  Shared memory: values [q][thread],
+// pivots [q][half].
+template <class RT>
+__global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, RT* base,
+                                                 long svj, long svk,
+                                                 const double* __restrict__ im, long tj,
+                                                 long tk, const double* __restrict__ AC) {
+  extern __shared__ __align__(16) unsigned char spn_sm[];
+  const int rmax = ny - m;  // rows of the longer (bottom) half
+  RT* vs = reinterpret_cast<RT*>(spn_sm);                                  // [rmax][64]
+  double* ws = reinterpret_cast<double*>(spn_sm + (((size_t)rmax * 64 * sizeof(RT) + 15) & ~(size_t)15));  // [rmax][32]
+  double* acs = ws + (size_t)rmax * 32;  // AC1 (ny), AC3 (ny)
+  const int lt = threadIdx.x;
+  for (int r = lt; r < ny; r += 64) {
+    acs[r] = AC[r];
+    acs[ny + r] = AC[2 * ny + r];
+  }
+  __syncthreads();
+  const int comp = lt & 1, part = (lt >> 1) & 1, hs = lt >> 1;
+  const int kx = blockIdx.x * 16 + (lt >> 2);
+  const int kz = blockIdx.y;
+  const bool mean = (kx == 0 && kz == 0);
+  const bool valid = kx < H && !mean;
+  const double* AC1 = AC;
+  const double* AC3 = AC + 2 * ny;
+  const long sj = 2 * svj;
+  RT* B = base + 2 * ((long)(kx < H ? kx : 0) + svk * kz) + comp;
+  const double* IM = im + (kx < H ? kx : 0) + tk * kz;
+  const int cnt = part ? ny - m : m;
+  auto row = [&](int q) { return part ? ny - 1 - q : q; };
+  // the mean mode's column (all ny rows) is staged in the columns of its
+  // top and bottom threads: row q at vs[q][lt] for q < rmax, else at
+  // vs[q - rmax][lt + 2]
+  auto mean_slot = [&](int q) -> RT& {
+    return q < rmax ? vs[q * 64 + lt] : vs[(q - rmax) * 64 + lt + 2];
+  };
+  if (valid) {
+    for (int q = 0; q < cnt; ++q) {
+      const int r = row(q);
+      cp_async<sizeof(RT)>(&vs[q * 64 + lt], &B[sj * r]);
+      if (comp == 0) cp_async<8>(&ws[q * 32 + hs], &IM[tj * r]);
+    }
+  } else if (mean && part == 0) {
+    for (int q = 0; q < ny; ++q) cp_async<sizeof(RT)>(&mean_slot(q), &B[sj * q]);
+  }
+  cp_async_wait_all();
+  __syncwarp();
+  if (mean && part == 0) {
+    // SP0B mkp.f:271-288 (phi(1) = 0, forward marching; see k_spn) from the
+    // staged column
+    const double* AC2 = AC + ny;
+    double pm = 0.0, pc = 0.0;
+    double Dj = (double)mean_slot(0);
+    B[0] = (RT)0.0;
+    for (int J = 1; J <= ny - 1; ++J) {
+      const double Dn = (double)mean_slot(J);
+      const double pn = (Dj - AC1[J - 1] * pm - AC2[J - 1] * pc) / AC3[J - 1];
+      B[sj * J] = (RT)pn;
+      pm = pc;
+      pc = pn;
+      Dj = Dn;
+    }
+  }
+  // elimination: top rows 0..m-1 downwards, bottom rows ny-1..m upwards;
+  // the eliminated values stay in double in place of the loaded ones when RT
+  // is double, in a register-free second pass otherwise
+  double y = 0.0;
+  double* ys = reinterpret_cast<double*>(vs);  // used only when RT is double
+  const double* cfe = acs + (part ? ny : 0);   // elimination coefficient by row
+  const double* cfb = acs + (part ? 0 : ny);   // back-substitution coefficient by row
+  if (valid) {
+#pragma unroll 4
+    for (int q = 0; q < cnt; ++q) {
+      const int r = row(q);
+      const double cf = cfe[r];
+      const double d = (double)vs[q * 64 + lt];
+      y = (q == 0 ? d : d - cf * y) * ws[q * 32 + hs];
+      if (sizeof(RT) == sizeof(double)) ys[q * 64 + lt] = y;
+      else vs[q * 64 + lt] = (RT)0;  // FP32 storage: recomputed below
+    }
+  }
+  // y(m-1) of the top thread, z(m) of the bottom thread
+  const double other = __shfl_xor_sync(0xffffffffu, y, 2);
+  if (!valid) return;
+  const double ytop = part ? other : y;
+  const double zbot = part ? y : other;
+  const double cT = AC3[m - 1] * (part ? IM[tj * (m - 1)] : ws[(m - 1) * 32 + hs]);
+  const double cB = AC1[m] * (part ? ws[(ny - 1 - m) * 32 + hs] : IM[tj * m]);
+  const double xm = (zbot - cB * ytop) / (1.0 - cB * cT);
+  double x = part ? xm : ytop - cT * xm;
+  B[sj * row(cnt - 1)] = (RT)x;
+#pragma unroll 4
+  for (int q = cnt - 2; q >= 0; --q) {
+    const int r = row(q);
+    const double cf = cfb[r] * ws[q * 32 + hs];
+    x = ys[q * 64 + lt] - cf * x;
+    B[sj * r] = (RT)x;
+  }
+}
+
 // ------------------------------------------------------------------ PHIBC --
 // mkp.f:293-320.  Phase 0 is the first loop (y ghosts (I,0|NY+1,K), I=0..NX,
 // K=1..NZ, copied from J=1|NY as they are on entry).  Phase 1 is the rest in
@@ -806,59 +969,113 @@ static int row_pairs(const PoissonPlan& pp) {
 
 template <class CT, class S>
 static void fwd_x(const PoissonPlan& pp, const Dims& d, const FwdSrc<S>& q, int src_mode,
-                  cudaStream_t s) {
+                  cudaStream_t s, int j0 = 0, int nj = 0) {
+  if (nj <= 0) { j0 = 0; nj = pp.ny; }
+  SpecViewT<CT> sv = spec_internal_t<CT>(pp);
+  sv.j0 = j0;
   if (pp.nx == 256 && pp.nz % 16 == 0) {
-    dim3 grid(pp.ny, pp.nz / 16);
+    dim3 grid(nj, pp.nz / 16);
     count_launch();
-    k_fft256_fwd_x<CT, S><<<grid, 128, 0, s>>>(d, spec_internal_t<CT>(pp), q, src_mode,
-                                               twx_of<CT>(pp));
+    k_fft256_fwd_x<CT, S><<<grid, 128, 0, s>>>(d, sv, q, src_mode, twx_of<CT>(pp));
     return;
   }
   FFTShape sh = make_shape(pp.nx);
   int npair = row_pairs(pp);
-  dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
+  dim3 grid(nj, (pp.nz + 2 * npair - 1) / (2 * npair));
   size_t sm = 2 * (size_t)npair * pp.nx * sizeof(CT);
   smem_optin((const void*)k_fft_fwd_x<CT, S>, sm);
   count_launch();
-  k_fft_fwd_x<CT, S><<<grid, fft_threads(npair * pp.nx), sm, s>>>(
-      sh, npair, d, spec_internal_t<CT>(pp), q, src_mode, twx_of<CT>(pp));
+  k_fft_fwd_x<CT, S><<<grid, fft_threads(npair * pp.nx), sm, s>>>(sh, npair, d, sv, q, src_mode,
+                                                                   twx_of<CT>(pp));
 }
 
 void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const double* ut, const double* vt, const double* wt,
                       const GridDev& g, double dt, int src_mode, cudaStream_t s,
-                      const GridRcp* rg) {
+                      const GridRcp* rg, int j0, int nj) {
   FwdSrc<double> q{};
   q.FP = FP; q.ut = ut; q.vt = vt; q.wt = wt; q.g = g; q.dt = dt;
   if (rg) { q.rg = *rg; q.use_rcp = 1; }
-  fwd_x<double2, double>(pp, d, q, src_mode, s);
+  fwd_x<double2, double>(pp, d, q, src_mode, s, j0, nj);
 }
 
 template <class CT>
-static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
+static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 0, int nj = 0) {
+  if (nj <= 0) { j0 = 0; nj = pp.ny; }
+  SpecViewT<CT> sv = spec_internal_t<CT>(pp);
+  sv.j0 = j0;
   if (pp.nz == 256) {
-    dim3 grid((pp.H + 15) / 16, pp.ny);
+    dim3 grid((pp.H + 15) / 16, nj);
     size_t sm = 16 * 16 * 17 * sizeof(CT);
     smem_optin((const void*)k_fft256_z<CT>, sm);
     count_launch();
-    k_fft256_z<CT><<<grid, 256, sm, s>>>(pp.H, spec_internal_t<CT>(pp), twz_of<CT>(pp),
-                                         inverse ? 1 : 0, (double)pp.nx * (double)pp.nz);
+    k_fft256_z<CT><<<grid, 256, sm, s>>>(pp.H, sv, twz_of<CT>(pp), inverse ? 1 : 0,
+                                         (double)pp.nx * (double)pp.nz);
     return;
   }
   FFTShape sh = make_shape(pp.nz);
   int W = 2048 / pp.nz;
   if (W < 1) W = 1;
   if (W > 16) W = 16;
-  dim3 grid((pp.H + W - 1) / W, pp.ny);
+  dim3 grid((pp.H + W - 1) / W, nj);
   size_t sm = 2 * (size_t)W * (pp.nz + 1) * sizeof(CT);
   smem_optin((const void*)k_fft_z<CT>, sm);
   count_launch();
-  k_fft_z<CT><<<grid, fft_threads(W * pp.nz), sm, s>>>(sh, W, pp.H, spec_internal_t<CT>(pp),
-                                                       twz_of<CT>(pp), inverse ? 1 : 0,
+  k_fft_z<CT><<<grid, fft_threads(W * pp.nz), sm, s>>>(sh, W, pp.H, sv, twz_of<CT>(pp),
+                                                       inverse ? 1 : 0,
                                                        (double)pp.nx * (double)pp.nz);
 }
-void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
-  fft_z<double2>(pp, inverse, s);
+void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0, int nj) {
+  fft_z<double2>(pp, inverse, s, j0, nj);
+}
+
+// split row of the two-ended SPN and its shared-memory footprint (the rows
+// of the longer half for 128 threads); 0 when the plan cannot use it
+static size_t spn_smem(int ny, int m);
+int spn_split(const PoissonPlan& pp) {
+  if (pp.ny < 4) return 0;
+  const int m = pp.ny / 2;
+  return spn_smem(pp.ny, m) <= 200 * 1024 ? m : 0;
+}
+
+void launch_spn_tables(const PoissonPlan& pp, double* im, cudaStream_t s) {
+  dim3 grid((pp.H + 63) / 64, pp.nz);
+  count_launch();
+  k_spn_tables<<<grid, 64, 0, s>>>(pp.H, pp.Hp, pp.ny, pp.nz, spn_split(pp), pp.AC, pp.KXZ, im);
+}
+
+static size_t spn_smem(int ny, int m) {
+  const size_t r = (size_t)(ny - m);
+  return ((r * 64 * sizeof(double) + 15) & ~(size_t)15) + r * 32 * sizeof(double) +
+         2 * (size_t)ny * sizeof(double);
+}
+
+template <class RT>
+static void spn_babe(const PoissonPlan& pp, RT* spec, cudaStream_t s) {
+  const int m = spn_split(pp);
+  const size_t sm = spn_smem(pp.ny, m);
+  smem_optin((const void*)k_spn_babe<RT>, sm);
+  dim3 grid((pp.H + 15) / 16, pp.nz);
+  count_launch();
+  k_spn_babe<RT><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, spec, pp.Hp, (long)pp.Hp * pp.ny,
+                                      pp.spn_im, pp.Hp, (long)pp.Hp * pp.ny, pp.AC);
+}
+
+// SPN + SP0B with the tabulated pivots (fast form); k_spn when the plan has
+// no tables
+void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s) {
+  if (!pp.spn_im) {
+    launch_spn(pp, true, true, s);
+    return;
+  }
+  spn_babe<double>(pp, pp.spec, s);
+}
+
+void launch_spn_f32(const PoissonPlan& pp, cudaStream_t s);
+void launch_spn_fast_f32(const PoissonPlan& pp, cudaStream_t s) {
+  // the FP32 spectrum keeps k_spn (FP64 recurrence); the two-ended kernel
+  // keeps its eliminated values in place of FP64 loads
+  launch_spn_f32(pp, s);
 }
 
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s) {
@@ -882,25 +1099,29 @@ void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, doub
 
 template <class CT>
 static void inv_x(const PoissonPlan& pp, const Dims& d, double* FP, bool accumulate,
-                  cudaStream_t s) {
+                  cudaStream_t s, int j0 = 0, int nj = 0) {
+  if (nj <= 0) { j0 = 0; nj = pp.ny; }
+  SpecViewT<CT> sv = spec_internal_t<CT>(pp);
+  sv.j0 = j0;
   if (pp.nx == 256 && pp.nz % 16 == 0) {
-    dim3 grid(pp.ny, pp.nz / 16);
+    dim3 grid(nj, pp.nz / 16);
     count_launch();
-    k_fft256_inv_x<CT><<<grid, 128, 0, s>>>(d, spec_internal_t<CT>(pp), FP, twx_of<CT>(pp),
-                                            accumulate ? 1 : 0);
+    k_fft256_inv_x<CT><<<grid, 128, 0, s>>>(d, sv, FP, twx_of<CT>(pp), accumulate ? 1 : 0);
     return;
   }
   FFTShape sh = make_shape(pp.nx);
   int npair = row_pairs(pp);
-  dim3 grid(pp.ny, (pp.nz + 2 * npair - 1) / (2 * npair));
+  dim3 grid(nj, (pp.nz + 2 * npair - 1) / (2 * npair));
   size_t sm = 2 * (size_t)npair * pp.nx * sizeof(CT);
   smem_optin((const void*)k_fft_inv_x<CT>, sm);
   count_launch();
-  k_fft_inv_x<CT><<<grid, fft_threads(npair * pp.nx), sm, s>>>(
-      sh, npair, d, spec_internal_t<CT>(pp), FP, twx_of<CT>(pp), accumulate ? 1 : 0);
+  k_fft_inv_x<CT><<<grid, fft_threads(npair * pp.nx), sm, s>>>(sh, npair, d, sv, FP,
+                                                               twx_of<CT>(pp),
+                                                               accumulate ? 1 : 0);
 }
-void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s) {
-  inv_x<double2>(pp, d, FP, false, s);
+void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s, int j0,
+                      int nj) {
+  inv_x<double2>(pp, d, FP, false, s, j0, nj);
 }
 
 // ---------------------------------------- mixed-precision Poisson solve --

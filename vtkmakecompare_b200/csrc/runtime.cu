@@ -779,8 +779,18 @@ void solve_t_(double* u_T, const int* nx, const int* ny, const int* nz, const do
 // ------------------------------------------------------ Poisson staging ----
 namespace nse {
 struct PoissonBufs {
-  DBuf spec, scr, AC, KXZ, twx, twz, twxf, twzf;
+  DBuf spec, scr, AC, KXZ, twx, twz, twxf, twzf, spn_im;
   PoissonPlan pp;
+  // SPN pivot table of the fast form (k_spn_babe); none when the plan's rows
+  // do not fit the kernel's shared memory
+  bool build_tables(cudaStream_t s) {
+    if (spn_split(pp) == 0) return true;
+    size_t n = (size_t)pp.Hp * pp.ny * pp.nz * sizeof(double);
+    if (!spn_im.ensure(n)) return false;
+    launch_spn_tables(pp, spn_im.as<double>(), s);
+    pp.spn_im = spn_im.as<double>();
+    return NSE_CUDA(cudaGetLastError());
+  }
   bool build(int nx, int ny, int nz, const double* dx, const double* dy, const double* dz,
              const double* dy12, double xl, double zl, cudaStream_t s) {
     if (!fft_size_ok(nx) || !fft_size_ok(nz)) {
@@ -814,11 +824,12 @@ struct PoissonBufs {
     pp.AC = this->AC.as<double>(); pp.KXZ = this->KXZ.as<double>();
     pp.twx = this->twx.as<double>(); pp.twz = this->twz.as<double>();
     pp.twx_f = twxf.as<float>(); pp.twz_f = twzf.as<float>();
+    pp.spn_im = nullptr;
     return true;
   }
   void release() {
     spec.release(); scr.release(); AC.release(); KXZ.release(); twx.release(); twz.release();
-    twxf.release(); twzf.release();
+    twxf.release(); twzf.release(); spn_im.release();
   }
 };
 static PoissonBufs& legacy_poisson() {
@@ -1428,6 +1439,7 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
   ok = ok && x->mon.ensure((6 + 6 * 592) * sizeof(double));
   ok = ok && x->pb.build(nx, ny, nz, x->hdx.data(), x->hdy.data(), x->hdz.data(),
                          x->hdy12.data(), c.xl, c.zl, x->own);
+  ok = ok && ((c.flags & NSE_FLAG_EXACT) || x->pb.build_tables(x->own));
   ok = ok && build_line_tables(x);
   if (!ok) {
     nse_ctx_destroy(x);
@@ -1562,8 +1574,8 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
   if (p64) launch_fft_z(pp, false, s);
   else launch_fft_z_f32(pp, false, s);
   mark(x, PH_SPN);
-  if (p64) launch_spn(pp, true, true, s);
-  else launch_spn_f32(pp, s);
+  if (p64) launch_spn_fast(pp, s);
+  else launch_spn_fast_f32(pp, s);
   mark(x, PH_FFTZ_I);
   if (p64) launch_fft_z(pp, true, s);
   else launch_fft_z_f32(pp, true, s);
@@ -1576,7 +1588,7 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
   for (int r = 0; !p64 && r < x->refine; ++r) {
     launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, phi, dx, dz, 2, s);
     launch_fft_z_f32(pp, false, s);
-    launch_spn_f32(pp, s);
+    launch_spn_fast_f32(pp, s);
     launch_fft_z_f32(pp, true, s);
     launch_fft_inv_x_f32(pp, d, phi, true, s);
     launch_phibc(d, phi, s);
@@ -1595,17 +1607,18 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   const Dims& d = x->d;
   cudaStream_t s = x->stream;
   double* phi = F(x, NSE_PHI);
+  const PoissonPlan& pp = x->pb.pp;
+  const GridRcp* rg = (x->cfg.flags & NSE_FLAG_EXACT) ? nullptr : &x->rg;
   mark(x, PH_FFTX_F);
-  launch_fft_fwd_x(x->pb.pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s,
-                   (x->cfg.flags & NSE_FLAG_EXACT) ? nullptr : &x->rg);
+  launch_fft_fwd_x(pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s, rg);
   mark(x, PH_FFTZ_F);
-  launch_fft_z(x->pb.pp, false, s);
+  launch_fft_z(pp, false, s);
   mark(x, PH_SPN);
-  launch_spn(x->pb.pp, true, true, s);
+  launch_spn_fast(pp, s);
   mark(x, PH_FFTZ_I);
-  launch_fft_z(x->pb.pp, true, s);
+  launch_fft_z(pp, true, s);
   mark(x, PH_FFTX_I);
-  launch_fft_inv_x(x->pb.pp, d, phi, s);
+  launch_fft_inv_x(pp, d, phi, s);
   mark(x, PH_PHIBC);
   launch_phibc(d, phi, s);
   mark(x, PH_REFINE);
@@ -1655,11 +1668,12 @@ int nse_poisson(nse_ctx* x) {
   const Dims& d = x->d;
   cudaStream_t s = x->stream;
   double* phi = F(x, NSE_PHI);
-  launch_fft_fwd_x(x->pb.pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
-  launch_fft_z(x->pb.pp, false, s);
-  launch_spn(x->pb.pp, true, true, s);
-  launch_fft_z(x->pb.pp, true, s);
-  launch_fft_inv_x(x->pb.pp, d, phi, s);
+  const PoissonPlan& pp = x->pb.pp;
+  launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+  launch_fft_z(pp, false, s);
+  launch_spn_fast(pp, s);
+  launch_fft_z(pp, true, s);
+  launch_fft_inv_x(pp, d, phi, s);
   launch_phibc(d, phi, s);
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
