@@ -8,7 +8,7 @@
 // the segment is replayed from its checkpoint with every step recording the
 // state it starts from and the inputs and outputs of its line-solve passes;
 // then its steps are reversed one by one with the transposed kernels of
-// k_adjoint.cu.  Device memory: (ceil(nsteps/ckpt) * 11 + ckpt * 23 + 38)
+// k_adjoint.cu.  Device memory: (ceil(nsteps/ckpt) * 11 + ckpt * 23 + 44)
 // padded fields.
 #include <algorithm>
 #include <vector>
@@ -26,8 +26,9 @@ const int kState[11] = {NSE_U,     NSE_V,     NSE_W,     NSE_T,     NSE_U_TA, NS
 enum { S_U = 0, S_V, S_W, S_T, S_UTA, S_VTA, S_WTA, S_UP, S_VP, S_WP, S_TP, NS };
 const int kSeg = 7;   // u, v, w, T, u_ta, v_ta, w_ta at the start of a recorded step
 const int kRec = 16;  // line-pass inputs and outputs of a recorded step
-// work fields
-enum { W_B = 0, W_O = 4, W_XS = 8, W_RB = 9, W_S1 = 10, W_S2 = 11, W_ST = 12, NW = 16 };
+// work fields (line scratch: two per component, the components' line
+// passes run concurrently on their own streams)
+enum { W_B = 0, W_O = 4, W_XS = 8, W_RB = 9, W_ST = 10, W_S = 14, NW = 22 };
 
 int state_index(int field) {
   for (int q = 0; q < NS; ++q)
@@ -49,6 +50,9 @@ struct nse_adjoint {
   bool has_w[NS] = {};
   double* barp[NS] = {};
   double* outp[4] = {};
+  // side streams of components 1..3 and the fork/join events
+  cudaStream_t side[3] = {};
+  cudaEvent_t fork = nullptr, join[3] = {};
   double* field(const DBuf& b, size_t idx) const { return b.as<double>() + idx * F; }
 };
 
@@ -70,7 +74,7 @@ bool copy_fields(nse_adjoint* a, double* dst_base, const int* ids, int n, bool t
 bool run_forward(nse_adjoint* a) {
   const CtxInfo& ci = a->ci;
   const nse_config& c = *ci.cfg;
-  const AdjGrid g = adj_grid(ci.g);
+  const AdjGrid g = adj_grid(ci.g, &ci.rg);
   const int N = a->cfg.nsteps, K = a->cfg.checkpoint_every, n0 = a->cfg.avg_from;
   const double w = 1.0 / (double)(N - n0 + 1);
   double* J = a->J.as<double>();
@@ -99,7 +103,7 @@ void adjoint_step(nse_adjoint* a, double* sg, double* const* rc, int l) {
   const CtxInfo& ci = a->ci;
   const nse_config& c = *ci.cfg;
   const Dims& D = ci.d;
-  const AdjGrid g = adj_grid(ci.g);
+  const AdjGrid g = adj_grid(ci.g, &ci.rg);
   cudaStream_t s = ci.s;
   double** bar = a->barp;
   const double* c1 = ctx_field(a->x, NSE_CELLVALUE);
@@ -119,20 +123,23 @@ void adjoint_step(nse_adjoint* a, double* sg, double* const* rc, int l) {
   launch_fft_z(*ci.pp, true, s);
   launch_fft_inv_x(*ci.pp, D, wk[W_RB], s);
   launch_adj_div(D, g, ub, wk[W_RB], c.dt, s);
-  // line passes in reverse (velocity y, z, x; temperature y, x, z forward)
-  for (int comp = 0; comp < 3; ++comp) {
-    const int dirs[3] = {1, 2, 0};
+  // line passes in reverse (velocity y, z, x; temperature y, x, z forward);
+  // the four components are independent: component 0 on the context's
+  // stream, 1..3 on side streams forked from it and joined back
+  NSE_CUDA(cudaEventRecord(a->fork, s));
+  for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(a->side[q], a->fork, 0));
+  for (int comp = 0; comp < 4; ++comp) {
+    cudaStream_t cs = comp == 0 ? s : a->side[comp - 1];
+    const int vdirs[3] = {1, 2, 0}, tdirs[3] = {1, 0, 2};
+    const int* dirs = comp == 3 ? tdirs : vdirs;
+    double* cbar = comp == 3 ? cb[0] : cb[comp + 1];
     for (int p = 2; p >= 0; --p)
-      launch_adj_line(D, g, dirs[p], comp, bar[comp], rc[4 * comp + p], rc[4 * comp + p + 1], c1,
-                      cb[comp + 1], wk[W_S1], wk[W_S2], c.Re, c.Sc, c.dt, c.eta, c.thc,
-                      c.rho_cp, s);
+      launch_adj_line(D, g, dirs[p], comp, bar[comp], rc[4 * comp + p], rc[4 * comp + p + 1],
+                      c1, cbar, wk[W_S + 2 * comp], wk[W_S + 2 * comp + 1], c.Re, c.Sc, c.dt,
+                      c.eta, c.thc, c.rho_cp, cs);
+    if (comp > 0) NSE_CUDA(cudaEventRecord(a->join[comp - 1], cs));
   }
-  {
-    const int dirs[3] = {1, 0, 2};
-    for (int p = 2; p >= 0; --p)
-      launch_adj_line(D, g, dirs[p], 3, bar[S_T], rc[12 + p], rc[12 + p + 1], c1, cb[0],
-                      wk[W_S1], wk[W_S2], c.Re, c.Sc, c.dt, c.eta, c.thc, c.rho_cp, s);
-  }
+  for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(s, a->join[q], 0));
   // penalised updates, AB2, immersed-boundary forcing
   double* A[4] = {bar[S_U], bar[S_V], bar[S_W], bar[S_T]};
   double* B[4] = {wk[W_B], wk[W_B + 1], wk[W_B + 2], wk[W_B + 3]};
@@ -148,8 +155,14 @@ void adjoint_step(nse_adjoint* a, double* sg, double* const* rc, int l) {
   launch_set_bc(D, wk[W_ST], wk[W_ST + 1], wk[W_ST + 2], nullptr, wk[W_ST + 3], c.t_bot,
                 c.t_top, 1 | 2 | 4 | 16, s);
   const double* vel[3] = {wk[W_ST], wk[W_ST + 1], wk[W_ST + 2]};
+  NSE_CUDA(cudaEventRecord(a->fork, s));
+  for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(a->side[q], a->fork, 0));
   launch_adj_explicit(D, g, vel, wk[W_ST + 3], A, B, c.dt, c.Re, c.Sc, c.rho_cp, c.thc,
-                      a->outp, s);
+                      a->outp, s, a->side);
+  for (int q = 0; q < 3; ++q) {
+    NSE_CUDA(cudaEventRecord(a->join[q], a->side[q]));
+    NSE_CUDA(cudaStreamWaitEvent(s, a->join[q], 0));
+  }
   for (int q = 0; q < 4; ++q) std::swap(bar[q], a->outp[q]);
 }
 
@@ -193,6 +206,10 @@ int nse_adjoint_create(nse_ctx* x, const nse_adjoint_config* cfg, nse_adjoint** 
             a->work.ensure(NW * fb) && a->cbar.ensure(4 * ci.d.ncell * sizeof(double)) &&
             a->J.ensure(2 * sizeof(double));
   ok = ok && NSE_CUDA(cudaMemset(a->work.p, 0, NW * fb));
+  for (int q = 0; ok && q < 3; ++q)
+    ok = NSE_CUDA(cudaStreamCreateWithFlags(&a->side[q], cudaStreamNonBlocking)) &&
+         NSE_CUDA(cudaEventCreateWithFlags(&a->join[q], cudaEventDisableTiming));
+  ok = ok && NSE_CUDA(cudaEventCreateWithFlags(&a->fork, cudaEventDisableTiming));
   if (!ok) {
     nse_adjoint_destroy(a);
     if (nse_last_status() == NSE_OK)
@@ -206,6 +223,12 @@ int nse_adjoint_create(nse_ctx* x, const nse_adjoint_config* cfg, nse_adjoint** 
 int nse_adjoint_destroy(nse_adjoint* a) {
   if (!a) return NSE_OK;
   cudaStreamSynchronize(a->ci.s);
+  for (int q = 0; q < 3; ++q) {
+    if (a->side[q]) cudaStreamSynchronize(a->side[q]);
+    if (a->side[q]) cudaStreamDestroy(a->side[q]);
+    if (a->join[q]) cudaEventDestroy(a->join[q]);
+  }
+  if (a->fork) cudaEventDestroy(a->fork);
   for (DBuf* b : {&a->ck, &a->seg, &a->rec, &a->fin, &a->bar, &a->work, &a->cbar, &a->wts, &a->J})
     b->release();
   delete a;
@@ -250,7 +273,7 @@ int nse_adjoint_gradient(nse_adjoint* a, double* J, double* grad_c1) {
   const CtxInfo& ci = a->ci;
   const nse_config& c = *ci.cfg;
   const Dims& D = ci.d;
-  const AdjGrid g = adj_grid(ci.g);
+  const AdjGrid g = adj_grid(ci.g, &ci.rg);
   cudaStream_t s = ci.s;
   const size_t fb = a->F * sizeof(double);
   const int N = a->cfg.nsteps, K = a->cfg.checkpoint_every, n0 = a->cfg.avg_from;

@@ -283,6 +283,7 @@ void launch_monitor(const Dims& d, const GridDev& g, const double* u, const doub
 struct CtxInfo {
   Dims d;
   GridDev g;
+  GridRcp rg;
   const nse_config* cfg;
   cudaStream_t s;
   const PoissonPlan* pp;

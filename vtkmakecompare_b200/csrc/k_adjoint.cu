@@ -55,6 +55,7 @@ struct XArgs {
   const double* At;      // adjoint of u_dT
   const double* Bt;      // adjoint of u_vT
   double dt, Re, Sc, R, L;
+  double cfac, dfac, qfac;  // dt/Re/2, dt/(2 Re Sc R), -dt/R
 };
 
 __device__ __forceinline__ double val(const XArgs& a, const double* f, const Pos& p) {
@@ -72,13 +73,13 @@ __device__ double sq_f(const XArgs& a, const Pos& q) {
   const double* d12 = a.g.d12[AC];
   double s = 0.0;
   if (inside(a.D, q)) {
-    const double m = qmom(a, AC, q) / d12[q.c[AC]];
+    const double m = qmom(a, AC, q) * a.g.r12[AC][q.c[AC]];
     s += 2.0 * m * ((val(a, f, q) + val(a, f, sh(q, AC, 1))) - (val(a, f, q) + val(a, f, sh(q, AC, -1))));
   }
   Pos o = sh(q, AC, -1);
-  if (inside(a.D, o)) s += 2.0 * qmom(a, AC, o) / d12[o.c[AC]] * (val(a, f, o) + val(a, f, q));
+  if (inside(a.D, o)) s += 2.0 * qmom(a, AC, o) * a.g.r12[AC][o.c[AC]] * (val(a, f, o) + val(a, f, q));
   o = sh(q, AC, 1);
-  if (inside(a.D, o)) s -= 2.0 * qmom(a, AC, o) / d12[o.c[AC]] * (val(a, f, o) + val(a, f, q));
+  if (inside(a.D, o)) s -= 2.0 * qmom(a, AC, o) * a.g.r12[AC][o.c[AC]] * (val(a, f, o) + val(a, f, q));
   return s;
 }
 
@@ -87,7 +88,7 @@ __device__ double sq_f(const XArgs& a, const Pos& q) {
 // Gp = g(o+eC) dC(o+1) + g(o) dC(o), Gm = g(o+eC-eF) dC(o+1) + g(o-eF) dC(o)
 template <int AC, int AF>
 __device__ __forceinline__ double cross_m(const XArgs& a, const Pos& o) {
-  return qmom(a, AC, o) / (a.g.d12[AC][o.c[AC]] * a.g.d[AF][o.c[AF]]);
+  return qmom(a, AC, o) * a.g.r12[AC][o.c[AC]] * a.g.r[AF][o.c[AF]];
 }
 template <int AC, int AF>
 __device__ __forceinline__ double cross_gp(const XArgs& a, const Pos& o) {
@@ -146,14 +147,14 @@ __device__ double conv_adj(const XArgs& a, const Pos& q) {
 // cp = 1/(d12(o) d(o)), cm = 1/(d12(o-1) d(o))
 __device__ __forceinline__ void lap_coef(const AdjGrid& g, int comp, int ax, int o, double& cp,
                                          double& cm) {
-  const double* d = g.d[ax];
-  const double* d12 = g.d12[ax];
+  const double* r = g.r[ax];
+  const double* r12 = g.r12[ax];
   if (ax == comp) {
-    cp = 1.0 / (d[o + 1] * d12[o]);
-    cm = 1.0 / (d[o] * d12[o]);
+    cp = r[o + 1] * r12[o];
+    cm = r[o] * r12[o];
   } else {
-    cp = 1.0 / (d12[o] * d[o]);
-    cm = 1.0 / (d12[o - 1] * d[o]);
+    cp = r12[o] * r[o];
+    cm = r12[o - 1] * r[o];
   }
 }
 
@@ -179,19 +180,16 @@ __device__ double cond_adj(const XArgs& a, const Pos& q) {
       s += cm * val(a, A, o);
     }
   }
-  return a.dt / a.Re / 2.0 * s;
+  return a.cfac * s;
 }
 
-// harmonic-mean conductance factor between cells o and o+s (uniform L)
-__device__ __forceinline__ double harm(const double* d, int o, int s, double L) {
-  return (d[o + s] + d[o]) / (d[o + s] / L + d[o] / L);
-}
+// with uniform conductivity the harmonic mean is L itself
 __device__ __forceinline__ void diffT_coef(const AdjGrid& g, int ax, int o, double L, double& cp,
                                            double& cm) {
-  const double* d = g.d[ax];
-  const double* d12 = g.d12[ax];
-  cp = harm(d, o, 1, L) / d12[o] / d[o];
-  cm = harm(d, o, -1, L) / d12[o - 1] / d[o];
+  const double* r = g.r[ax];
+  const double* r12 = g.r12[ax];
+  cp = L * r12[o] * r[o];
+  cm = L * r12[o - 1] * r[o];
 }
 
 __device__ double diffT_adj(const XArgs& a, const Pos& q) {
@@ -214,7 +212,7 @@ __device__ double diffT_adj(const XArgs& a, const Pos& q) {
       s += cm * val(a, a.At, o);
     }
   }
-  return s / 2.0 / a.Re / a.Sc / a.R * a.dt;
+  return s * a.dfac;
 }
 
 // scalar convection: per axis a, with f = vel[a], d = d_a, d12 = d12_a,
@@ -223,12 +221,12 @@ __device__ double diffT_adj(const XArgs& a, const Pos& q) {
 //   term2(o) = (R T(o) d(o+1) + R T(o+e) d(o)) f(o) m2(o),
 //   m2(o) = qT(o) / (2 d12(o) d(o)),  qT = -dt/R * adjoint of u_vT
 __device__ __forceinline__ double m1T(const XArgs& a, int ax, const Pos& o) {
-  const double qT = -a.dt / a.R * val(a, a.Bt, o);
-  return qT / (2.0 * a.g.d12[ax][o.c[ax] - 1] * a.g.d[ax][o.c[ax]]);
+  const double qT = a.qfac * val(a, a.Bt, o);
+  return 0.5 * qT * a.g.r12[ax][o.c[ax] - 1] * a.g.r[ax][o.c[ax]];
 }
 __device__ __forceinline__ double m2T(const XArgs& a, int ax, const Pos& o) {
-  const double qT = -a.dt / a.R * val(a, a.Bt, o);
-  return qT / (2.0 * a.g.d12[ax][o.c[ax]] * a.g.d[ax][o.c[ax]]);
+  const double qT = a.qfac * val(a, a.Bt, o);
+  return 0.5 * qT * a.g.r12[ax][o.c[ax]] * a.g.r[ax][o.c[ax]];
 }
 // adjoint w.r.t. vel[AX] at q
 template <int AX>
@@ -386,23 +384,18 @@ __global__ void k_adj_point(PArgs a) {
 //   ROW_T  implicit_Ty / implicit_Tx with harmonic conductances
 enum { ROW_U = 0, ROW_V = 1, ROW_T = 2 };
 
-__device__ __forceinline__ void line_row(int kind, const double* d, const double* d12, int j,
-                                         double alpha, double beta, double L, double R,
-                                         double& lo, double& di, double& up) {
-  if (kind == ROW_U) {
-    lo = -beta / alpha / d12[j - 1] / d[j];
-    di = 1.0 + beta / alpha * (1.0 / d12[j] + 1.0 / d12[j - 1]) / d[j];
-    up = -beta / alpha / d12[j] / d[j];
-  } else if (kind == ROW_V) {
-    lo = -beta / alpha / d[j] / d12[j];
-    di = 1.0 + beta / alpha * (1.0 / d[j + 1] + 1.0 / d[j]) / d12[j];
-    up = -beta / alpha / d[j + 1] / d12[j];
-  } else {
-    const double hm = harm(d, j, -1, L);
-    const double hp = harm(d, j, 1, L);
-    lo = -beta / alpha * hm / d12[j - 1] / d[j] / R;
-    di = 1.0 + beta / alpha * (hp / d12[j] / d[j] + hm / d12[j - 1] / d[j]) / R;
-    up = -beta / alpha * hp / d12[j] / d[j] / R;
+// (r, r12: reciprocal spacings; bia = beta / alpha, already divided by rhoCp
+// and multiplied by the uniform conductivity for ROW_T)
+__device__ __forceinline__ void line_row(int kind, const double* r, const double* r12, int j,
+                                         double bia, double& lo, double& di, double& up) {
+  if (kind == ROW_V) {
+    lo = -bia * r[j] * r12[j];
+    di = 1.0 + bia * (r[j + 1] + r[j]) * r12[j];
+    up = -bia * r[j + 1] * r12[j];
+  } else {  // ROW_U and ROW_T (harmonic mean of a uniform conductivity = L)
+    lo = -bia * r12[j - 1] * r[j];
+    di = 1.0 + bia * (r12[j] + r12[j - 1]) * r[j];
+    up = -bia * r12[j] * r[j];
   }
 }
 
@@ -451,7 +444,8 @@ __device__ __forceinline__ void row_coef(const LArgs& a, long t, int r, double& 
   const double cm = face_mask(a.D, a.c1, a.comp, i, j, k);
   alpha = a.dt * a.eta * cm + 1.0;
   const int jj = DIR == 0 ? i : (DIR == 1 ? j : k);
-  line_row(a.kind, a.g.d[DIR], a.g.d12[DIR], jj, alpha, a.beta, a.L, a.R, lo, di, up);
+  const double bia = cm == 0.0 ? a.beta : a.beta / alpha;
+  line_row(a.kind, a.g.r[DIR], a.g.r12[DIR], jj, bia, lo, di, up);
 }
 
 // y lines: the ghost rows x0 + x1 = ft, x_n + x_n+1 = fb folded into the first
@@ -494,7 +488,7 @@ __global__ void k_adj_line_y(LArgs a) {
     double y = a.xb[c];
     if (r < n - 1) y -= a.s1[r * nl + t] * ynext;
     a.xb[c] = y;
-    a.cbar[m] += y * a.dt * a.eta / al * (a.rin[c] - a.xout[c]);
+    a.cbar[m] += y * (al == 1.0 ? a.dt * a.eta : a.dt * a.eta / al) * (a.rin[c] - a.xout[c]);
     ynext = y;
   }
   if (a.comp == 1) a.xb[a.D.P(1 + (int)(t % a.D.nx), a.D.ny, 1 + (int)(t / a.D.nx))] = 0.0;
@@ -565,7 +559,7 @@ __global__ void k_adj_line_p(LArgs a) {
     row_coef<DIR>(a, t, r, lo, di, up, al, c, m);
     const double y = a.xb[c] - fact * a.s2[r * nl + t];
     a.xb[c] = y;
-    a.cbar[m] += y * a.dt * a.eta / al * (a.rin[c] - a.xout[c]);
+    a.cbar[m] += y * (al == 1.0 ? a.dt * a.eta : a.dt * a.eta / al) * (a.rin[c] - a.xout[c]);
   }
 }
 
@@ -586,7 +580,7 @@ struct GArgs {
 __device__ __forceinline__ double gbar(const GArgs& a, int ax, const Pos& q) {
   if (!inside(a.D, q)) return 0.0;
   const long c = at(a.D, q);
-  return a.dt * (a.tab[ax][c] - a.ub[ax][c]) / a.g.d12[ax][q.c[ax]];
+  return a.dt * (a.tab[ax][c] - a.ub[ax][c]) * a.g.r12[ax][q.c[ax]];
 }
 
 __global__ void k_adj_phibar(GArgs a) {
@@ -693,7 +687,7 @@ struct DArgs {
   AdjGrid g;
   double* ub[3];  // in: adjoint of the corrected u, v, w; out: adjoint of u*, v*, w*
   const double* rb;
-  double dt;
+  double rdt;     // 1 / dt
 };
 
 __global__ void k_adj_div(DArgs a) {
@@ -706,15 +700,15 @@ __global__ void k_adj_div(DArgs a) {
   const double r0 = a.rb[c];
   {
     const int ip = i == D.nx ? 1 : i + 1;
-    a.ub[0][c] += (r0 / a.g.d[0][i] - a.rb[D.P(ip, j, k)] / a.g.d[0][ip]) / a.dt;
+    a.ub[0][c] += (r0 * a.g.r[0][i] - a.rb[D.P(ip, j, k)] * a.g.r[0][ip]) * a.rdt;
   }
   if (j < D.ny)
-    a.ub[1][c] += (r0 / a.g.d[1][j] - a.rb[D.P(i, j + 1, k)] / a.g.d[1][j + 1]) / a.dt;
+    a.ub[1][c] += (r0 * a.g.r[1][j] - a.rb[D.P(i, j + 1, k)] * a.g.r[1][j + 1]) * a.rdt;
   else
     a.ub[1][c] = 0.0;
   {
     const int kp = k == D.nz ? 1 : k + 1;
-    a.ub[2][c] += (r0 / a.g.d[2][k] - a.rb[D.P(i, j, kp)] / a.g.d[2][kp]) / a.dt;
+    a.ub[2][c] += (r0 * a.g.r[2][k] - a.rb[D.P(i, j, kp)] * a.g.r[2][kp]) * a.rdt;
   }
 }
 
@@ -935,22 +929,26 @@ dim3 cell_grid(const Dims& D, int bx) {
 void launch_adj_explicit(const Dims& D, const AdjGrid& g, const double* const vel[3],
                          const double* T, double* const A[4], double* const B[4], double dt,
                          double Re, double Sc, double R, double L, double* const out[4],
-                         cudaStream_t s) {
+                         cudaStream_t s, const cudaStream_t* side) {
   XArgs a;
   a.D = D; a.g = g;
   for (int c = 0; c < 3; ++c) { a.vel[c] = vel[c]; a.A[c] = A[c]; a.B[c] = B[c]; }
   a.T = T; a.At = A[3]; a.Bt = B[3];
   a.dt = dt; a.Re = Re; a.Sc = Sc; a.R = R; a.L = L;
+  a.cfac = dt / Re / 2.0;
+  a.dfac = dt / (2.0 * Re * Sc * R);
+  a.qfac = -dt / R;
   const int bx = 64;
   dim3 grid = cell_grid(D, bx);
+  const cudaStream_t* ss = side ? side : nullptr;
   count_launch();
   k_adj_explicit<0><<<grid, bx, 0, s>>>(a, out[0]);
   count_launch();
-  k_adj_explicit<1><<<grid, bx, 0, s>>>(a, out[1]);
+  k_adj_explicit<1><<<grid, bx, 0, ss ? ss[0] : s>>>(a, out[1]);
   count_launch();
-  k_adj_explicit<2><<<grid, bx, 0, s>>>(a, out[2]);
+  k_adj_explicit<2><<<grid, bx, 0, ss ? ss[1] : s>>>(a, out[2]);
   count_launch();
-  k_adj_explicit<3><<<grid, bx, 0, s>>>(a, out[3]);
+  k_adj_explicit<3><<<grid, bx, 0, ss ? ss[2] : s>>>(a, out[3]);
 }
 
 void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
@@ -980,7 +978,7 @@ void launch_adj_line(const Dims& D, const AdjGrid& g, int dir, int comp, double*
   a.D = D; a.g = g; a.xb = xb; a.rin = rin; a.xout = xout; a.c1 = c1; a.cbar = cbar;
   a.s1 = s1; a.s2 = s2; a.comp = comp;
   a.dt = dt; a.eta = eta; a.L = L; a.R = R;
-  a.beta = comp == 3 ? dt / Re / Sc / 2.0 : dt / Re / 2.0;
+  a.beta = comp == 3 ? dt / Re / Sc / 2.0 * L / R : dt / Re / 2.0;
   a.jtop = comp == 1 ? D.ny - 1 : D.ny;
   if (comp == 3) a.kind = ROW_T;
   else a.kind = (dir == 1 && comp != 1) ? ROW_U : ROW_V;
@@ -1021,7 +1019,7 @@ void launch_adj_spn(const PoissonPlan& pp, cudaStream_t s) {
 void launch_adj_div(const Dims& D, const AdjGrid& g, double* const ub[3], const double* rb,
                     double dt, cudaStream_t s) {
   DArgs a;
-  a.D = D; a.g = g; a.rb = rb; a.dt = dt;
+  a.D = D; a.g = g; a.rb = rb; a.rdt = 1.0 / dt;
   for (int c = 0; c < 3; ++c) a.ub[c] = ub[c];
   count_launch();
   k_adj_div<<<cell_grid(D, 128), 128, 0, s>>>(a);

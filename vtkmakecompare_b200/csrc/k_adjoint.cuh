@@ -5,24 +5,34 @@
 
 namespace nse {
 
-// grid spacings by axis: d[0..2] = dx, dy, dz; d12[0..2] = dx12, dy12, dz12
+// grid spacings by axis: d[0..2] = dx, dy, dz; d12[0..2] = dx12, dy12, dz12;
+// r, r12 their reciprocals (the transposed kernels multiply by them; the
+// adjoint.f drop-ins divide, as the reference does, and leave them null)
 struct AdjGrid {
   const double* d[3];
   const double* d12[3];
+  const double* r[3];
+  const double* r12[3];
 };
-inline AdjGrid adj_grid(const GridDev& g) {
+inline AdjGrid adj_grid(const GridDev& g, const GridRcp* rg = nullptr) {
   AdjGrid a;
   a.d[0] = g.dx; a.d[1] = g.dy; a.d[2] = g.dz;
   a.d12[0] = g.dx12; a.d12[1] = g.dy12; a.d12[2] = g.dz12;
+  a.r[0] = rg ? rg->rdx : nullptr; a.r[1] = rg ? rg->rdy : nullptr;
+  a.r[2] = rg ? rg->rdz : nullptr;
+  a.r12[0] = rg ? rg->rdx12 : nullptr; a.r12[1] = rg ? rg->rdy12 : nullptr;
+  a.r12[2] = rg ? rg->rdz12 : nullptr;
   return a;
 }
 
 // adjoint of u, v, w, T at the start of a step from the adjoints of the
-// explicit terms (A: of u_d / u_dT, B: of u_v / u_vT); vel, T with SET_BC
+// explicit terms (A: of u_d / u_dT, B: of u_v / u_vT); vel, T with SET_BC.
+// Field 0 runs on s, fields 1..3 on side[0..2] when side is given (the
+// caller orders them)
 void launch_adj_explicit(const Dims& D, const AdjGrid& g, const double* const vel[3],
                          const double* T, double* const A[4], double* const B[4], double dt,
                          double Re, double Sc, double R, double L, double* const out[4],
-                         cudaStream_t s);
+                         cudaStream_t s, const cudaStream_t* side = nullptr);
 // penalised updates, AB2 and immersed-boundary forcing transposed
 void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
                       double* const bar_pre[4], double* const bar_ta[3],

@@ -1830,6 +1830,7 @@ bool ctx_info(nse_ctx* x, CtxInfo& out) {
   if (!x) return false;
   out.d = x->d;
   out.g = x->g;
+  out.rg = x->rg;
   out.cfg = &x->cfg;
   out.s = x->stream;
   out.pp = &x->pb.pp;
