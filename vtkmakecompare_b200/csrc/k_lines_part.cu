@@ -329,6 +329,16 @@ template <class T> struct Vec2T;
 template <> struct Vec2T<double> { using T = double2; };
 template <> struct Vec2T<float> { using T = float2; };
 
+// Products with the table entries that are close to 1 (the reciprocal pivots
+// RB, the reduced-system factors LAM and RDF and the diagonal of the reduced
+// inverse: near-identity systems, dt/Re/dx^2 ~ 1e-3).  The FP32 tables hold
+// these entries as their deviation from 1, so a * v is formed as a + a * dv:
+// a table rounded to FP32 then carries a relative error of 6e-8 of the
+// deviation, not of 1, and the solve has no systematic bias of that size
+// (which every step would repeat).  FP64 tables hold the values themselves.
+__device__ __forceinline__ double mul1(double a, double v) { return a * v; }
+__device__ __forceinline__ float mul1(float a, float dv) { return a + a * dv; }
+
 // interior Thomas on registers: g <- solution of the interior rows with
 // zero end values; rows r = 1..m-2 of the partition, table rows at tb(r).
 // Returns g(m-2) (taken inside the unrolled chain: selecting x[m-2] after
@@ -344,7 +354,7 @@ __device__ __forceinline__ R interior_solve(R (&x)[MM], int m, const TB& tb) {
   for (int r = MM - 2; r >= 1; --r)
     if (r <= m - 2) {
       // gn is still 0 at r = m-2, so this is x(m-2) * rb there
-      R v = (x[r] - tb.cc(r) * gn) * tb.rb(r);
+      R v = mul1(x[r] - tb.cc(r) * gn, tb.rb(r));
       if (r == m - 2) glast = v;
       x[r] = v;
       gn = v;
@@ -376,15 +386,19 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
                                                 const int* __restrict__ ids, int count) {
   using V2 = typename Vec2T<S>::T;
   constexpr int NV = x_table_values(M);
+  // FP32 tables (mixed form) carry the row coefficients of the increment
+  // form after the factorisation values (see line_coef_values)
+  constexpr bool INC = sizeof(R) == 4;
+  constexpr int NVC = NV + (INC ? 3 * M : 0);
   constexpr int HW = 32 / PL;  // lines per warp at a time
-  __shared__ R stab[MASKED ? 1 : NV * PL];
+  __shared__ R stab[MASKED ? 1 : NVC * PL];
   const int lane = threadIdx.x & (PL - 1), half = (threadIdx.x & 31) / PL;
   const long warp = ((long)blockIdx.x * blockDim.x + threadIdx.x) >> 5;
   const long nwarps = ((long)gridDim.x * blockDim.x) >> 5;
   const int n = d.nx;
   const unsigned FULL = 0xffffffffu;
   if (!MASKED) {
-    for (int t = threadIdx.x; t < NV * PL; t += blockDim.x) stab[t] = __ldg(tab + t);
+    for (int t = threadIdx.x; t < NVC * PL; t += blockDim.x) stab[t] = __ldg(tab + t);
     __syncthreads();
   }
   const long nlines = MASKED ? count : (long)jtop * d.nz;
@@ -393,7 +407,7 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
     XTab<R, PL> tb;
     tb.lane = lane;
     // (masked pass: NL = 1, table of line gi*HW + half)
-    tb.p = MASKED ? tab + (size_t)min(gi * HW + half, (long)count - 1) * x_table_stride(M, PL)
+    tb.p = MASKED ? tab + (size_t)min(gi * HW + half, (long)count - 1) * (size_t)(NVC * PL)
                   : stab;
     S* line[NL];
     bool ok[NL];
@@ -429,6 +443,25 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
         for (int r = 0; r < M; ++r) x[q][r] = R(0);
       }
     }
+    // increment form (FP32 tables): solve A y = r - A r and return r + y,
+    // so the FP32 rounding of the solve scales with |y| ~ |(A - I) r|
+    R xr[INC ? NL : 1][INC ? M : 1];
+    if constexpr (INC) {
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        const R left = __shfl_sync(FULL, x[q][M - 1], (lane - 1) & (PL - 1), PL);
+        const R right = __shfl_sync(FULL, x[q][0], (lane + 1) & (PL - 1), PL);
+#pragma unroll
+        for (int r = 0; r < M; ++r) xr[q][r] = x[q][r];
+#pragma unroll
+        for (int r = 0; r < M; ++r) {
+          const R xm = r == 0 ? left : xr[q][r > 0 ? r - 1 : 0];
+          const R xp = r == M - 1 ? right : xr[q][r + 1 < M ? r + 1 : M - 1];
+          x[q][r] = -(tb.v(NV + 3 * r) * xm + tb.v(NV + 3 * r + 1) * xr[q][r] +
+                      tb.v(NV + 3 * r + 2) * xp);
+        }
+      }
+    }
     // interior rows (Thomas with the tabulated factorisation)
     R gp[NL];
 #pragma unroll
@@ -444,7 +477,7 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
       const R rb = tb.rb(r), cc = tb.cc(r);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        R v = (r == M - 2) ? x[q][r] * rb : (x[q][r] - cc * gp[q]) * rb;
+        R v = (r == M - 2) ? mul1(x[q][r], rb) : mul1(x[q][r] - cc * gp[q], rb);
         x[q][r] = v;
         gp[q] = v;
       }
@@ -476,9 +509,9 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
       const R lfr = tb.v(XT_LFR), ufr = tb.v(XT_UFR);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        const R E = lam * rho[q] + kap * __shfl_sync(FULL, rho[q], lane ^ (PL / 2), PL);
+        const R E = mul1(rho[q], lam) + kap * __shfl_sync(FULL, rho[q], lane ^ (PL / 2), PL);
         const R Em = __shfl_sync(FULL, E, (lane - 1) & (PL - 1), PL);
-        const R F = rdf * rhsF[q] + lfr * Em + ufr * E;
+        const R F = mul1(rhsF[q], rdf) + lfr * Em + ufr * E;
         rhsF[q] = F;
         rho[q] = E;
       }
@@ -493,6 +526,10 @@ __global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int j
     for (int q = 0; q < NL; ++q) {
       x[q][0] = rhsF[q];
       x[q][M - 1] = rho[q];
+      if constexpr (INC) {
+#pragma unroll
+        for (int r = 0; r < M; ++r) x[q][r] = xr[q][r] + x[q][r];
+      }
       if (!ok[q]) continue;
       if (M % 2 == 0) {
         V2* p2 = reinterpret_cast<V2*>(line[q] + lane * M);
@@ -536,12 +573,15 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
                                                       const R* __restrict__ mtab, R ft, R fb,
                                                       int periodic) {
   constexpr int R2 = 2 * P;
+  // FP32 tables (mixed form): increment form, row coefficients after the
+  // factorisation values (see line_coef_values)
+  constexpr bool INC = sizeof(R) == 4;
   __shared__ R red[R2 * LPB];
   const int lane = threadIdx.x % LPB, k = threadIdx.x / LPB;
   const int i = 1 + blockIdx.x * LPB + lane;
   const int o = 1 + blockIdx.y;  // k of a y line, j of a z line
   const bool valid = i <= d.nx && o <= nother;
-  const size_t stride = yz_table_stride(nu, P);
+  const size_t stride = yz_table_stride(nu, P) + (INC ? 3 * (size_t)nu : 0);
   const R* T = tab;
   if (valid) {
     long lineid = (long)(i - 1) + (long)d.nx * (o - 1);
@@ -554,6 +594,8 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
   const long off = (DIR == 1 ? d.P(i, 0, o) : d.P(i, o, 0)) + (long)(s + 1) * es;
   const S* line = f + off;
   R x[MM];
+  R xr[INC ? MM : 1];
+  R xe = R(0), xer = R(0);
   YZTab<R> tb{T, nu, s};
   if (valid) {
     // right-hand-side folds of the boundary rows (zero for periodic lines)
@@ -565,7 +607,39 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
 #pragma unroll
     for (int r = 0; r < MM; ++r) x[r] = (R)line[(long)min(r, m - 1) * es];
     x[0] = x[0] - c0;
-    const R xe = (R)line[(long)(m - 1) * es] - cN;
+    xe = (R)line[(long)(m - 1) * es] - cN;
+  }
+  if constexpr (INC) {
+    if (valid) {
+      // right-hand side of A y = r - A r on this partition's rows s..e; the
+      // neighbouring unknowns s-1 and e+1 are read from the line (they are
+      // never folded: the folds touch unknowns 0 and nu-1 only, and every
+      // partition has at least 3 rows)
+      const R* CA = T + yz_table_stride(nu, P) + s;
+      const R* CB = CA + nu;
+      const R* CC = CB + nu;
+      R left = R(0), right = R(0);
+      if (k > 0) left = (R)line[-es];
+      else if (periodic) left = (R)line[(long)(nu - 1) * es];
+      if (k < P - 1) right = (R)line[(long)m * es];
+      else if (periodic) right = (R)line[-(long)s * es];
+#pragma unroll
+      for (int r = 0; r < MM; ++r) xr[r] = (r == m - 1) ? xe : x[r];
+      xer = xe;
+#pragma unroll
+      for (int r = 0; r < MM; ++r) {
+        if (r < m) {
+          const R xm = r == 0 ? left : xr[r > 0 ? r - 1 : 0];
+          const R xc = r == m - 1 ? xe : xr[r];
+          const R xp = r == m - 1 ? right : xr[r + 1 < MM ? r + 1 : MM - 1];
+          const R sv = -(__ldg(CA + r) * xm + __ldg(CB + r) * xc + __ldg(CC + r) * xp);
+          if (r == m - 1) xe = sv;
+          else x[r] = sv;
+        }
+      }
+    }
+  }
+  if (valid) {
     const R xe1 = interior_solve<MM>(x, m, tb);
     red[(2 * k) * LPB + lane] = x[0] - __ldg(T + 5 * nu + k) * x[1];
     red[(2 * k + 1) * LPB + lane] = xe - __ldg(T + 5 * nu + P + k) * xe1;
@@ -578,8 +652,9 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
 #pragma unroll
   for (int c = 0; c < R2; ++c) {
     const R rc = red[c * LPB + lane];
-    F = F + __ldg(MI + (2 * k) * R2 + c) * rc;
-    E = E + __ldg(MI + (2 * k + 1) * R2 + c) * rc;
+    const R mf = __ldg(MI + (2 * k) * R2 + c), me = __ldg(MI + (2 * k + 1) * R2 + c);
+    F = F + (c == 2 * k ? mul1(rc, mf) : mf * rc);
+    E = E + (c == 2 * k + 1 ? mul1(rc, me) : me * rc);
   }
 #pragma unroll
   for (int r = 1; r < MM; ++r) {
@@ -587,6 +662,10 @@ __global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
     if (r == m - 1) x[r] = E;
   }
   x[0] = F;
+  if constexpr (INC) {
+#pragma unroll
+    for (int r = 0; r < MM; ++r) x[r] = (r == m - 1 ? xer : xr[r]) + x[r];
+  }
   RO* dst = out ? out + off : reinterpret_cast<RO*>(f + off);
 #pragma unroll
   for (int r = 0; r < MM; ++r)
@@ -788,6 +867,92 @@ void launch_round_table(const double* in, float* out, long n, cudaStream_t s) {
   if (n <= 0) return;
   count_launch();
   k_round_table<<<(unsigned)std::min<long>((n + 255) / 256, 4096), 256, 0, s>>>(in, out, n);
+}
+
+// FP32 line tables of the mixed form.  Each FP32 table is the FP64 table
+// rounded, with the entries close to 1 stored as their deviation from 1 (see
+// mul1: x tables RB of every row, LAM, RDF; y/z tables RB of every unknown and
+// the reduced inverse's diagonal), followed by the row coefficients of the
+// increment form: A (to the previous unknown), B - 1, C (to the next) of
+// every unknown, FP64 values rounded once.  x tables: value NV + 3r + c of
+// lane k (unknown k*M + r) at [(NV + 3r + c) * PL + k]; y/z tables:
+// [stride64 + c*nu + t].
+size_t part_table_stride32(int dir, int kind, const Dims& d) {
+  int nu = dir == 0 ? d.nx : (dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz);
+  return part_table_stride(dir, kind, d) + 3 * (size_t)nu;
+}
+
+__global__ void k_round_line_table(const double* __restrict__ in, float* __restrict__ out,
+                                   long n, long stride64, long stride32, int PL, int nu, int P) {
+  for (long t = (long)blockIdx.x * blockDim.x + threadIdx.x; t < n;
+       t += (long)gridDim.x * blockDim.x) {
+    const long o = t % stride64, line = t / stride64;
+    bool near1;
+    if (PL > 0) {
+      const int v = (int)(o / PL);
+      near1 = v == XT_LAM || v == XT_RDF || (v >= XT_ROW && (v - XT_ROW) % 5 == 1);
+    } else {
+      const long mi = 5L * nu + 10L * P + 4, r2 = 2L * P;
+      near1 = (o >= nu && o < 2L * nu) || (o >= mi && (o - mi) / r2 == (o - mi) % r2);
+    }
+    out[line * stride32 + o] = near1 ? (float)(in[t] - 1.0) : (float)in[t];
+  }
+}
+
+template <int DIR, int KIND>
+__global__ void k_build_coef(Dims d, GridDev g, const double* c1, LineArgs a, const int* ids,
+                             int count, float* out, long stride32, long off, int PL, int M,
+                             int NV) {
+  const int line = blockIdx.x;
+  if (line >= count) return;
+  const bool masked = ids != nullptr;
+  auto L = folded_line<DIR, KIND>(d, g, c1, a, masked ? ids[line] : 0, masked, DIR == 0);
+  float* T = out + (size_t)line * stride32;
+  for (int t = threadIdx.x; t < L.nu; t += blockDim.x) {
+    double A, B, C;
+    L.coef(t, A, B, C);
+    const double v[3] = {A, B - 1.0, C};
+    for (int c = 0; c < 3; ++c) {
+      if (DIR == 0) T[(NV + 3 * (t % M) + c) * PL + t / M] = (float)v[c];
+      else T[off + (long)c * L.nu + t] = (float)v[c];
+    }
+  }
+}
+
+void launch_round_line_table(int dir, int kind, const Dims& d, const GridDev& g,
+                             const double* c1, const LineArgs& a, const int* ids,
+                             const double* in, float* out, long ntables, cudaStream_t s) {
+  if (ntables <= 0) return;
+  const long stride64 = (long)part_table_stride(dir, kind, d);
+  const long stride32 = (long)part_table_stride32(dir, kind, d);
+  int PL = 0, M = 0, nu = 0, P = 0;
+  if (dir == 0) {
+    x_shape(d.nx, M, PL);
+  } else {
+    nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
+    P = yz_partitions(nu);
+  }
+  const long n = stride64 * ntables;
+  count_launch();
+  k_round_line_table<<<(unsigned)std::min<long>((n + 255) / 256, 4096), 256, 0, s>>>(
+      in, out, n, stride64, stride32, PL, nu, P);
+  const int NV = dir == 0 ? x_table_values(M) : 0;
+  count_launch();
+#define NSE_COEF(DIR_, KIND_)                                                              \
+  k_build_coef<DIR_, KIND_><<<(unsigned)ntables, 128, 0, s>>>(d, g, c1, a, ids, (int)ntables, \
+                                                              out, stride32, stride64, PL, M, NV)
+  if (dir == 0) {
+    if (kind == LK_CYC_VEL) NSE_COEF(0, LK_CYC_VEL);
+    else NSE_COEF(0, LK_CYC_T);
+  } else if (dir == 1) {
+    if (kind == LK_UL_U) NSE_COEF(1, LK_UL_U);
+    else if (kind == LK_UL_V) NSE_COEF(1, LK_UL_V);
+    else NSE_COEF(1, LK_UL_T);
+  } else {
+    if (kind == LK_CYC_VEL) NSE_COEF(2, LK_CYC_VEL);
+    else NSE_COEF(2, LK_CYC_T);
+  }
+#undef NSE_COEF
 }
 
 }  // namespace nse

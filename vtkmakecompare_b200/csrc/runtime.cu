@@ -46,6 +46,10 @@ void launch_lines_part_f32(int dir, int kind, const Dims& d, float* f, double* o
                            const int* ids, int nmasked, const float* mtab,
                            const double* tab64, const double* mtab64, cudaStream_t s);
 void launch_round_table(const double* in, float* out, long n, cudaStream_t s);
+void launch_round_line_table(int dir, int kind, const Dims& d, const GridDev& g,
+                             const double* c1, const LineArgs& a, const int* ids,
+                             const double* in, float* out, long ntables, cudaStream_t s);
+size_t part_table_stride32(int dir, int kind, const Dims& d);
 // mixed-precision form (FP32 intermediates)
 void launch_rhs_f32(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                     const double* u, const double* v, const double* w, const double* T,
@@ -1234,10 +1238,11 @@ static bool build_line_tables(nse_ctx* x) {
         launch_part_tables(dir, kind, d, x->g, nullptr, a, nullptr, 1,
                            x->ptab[dir][comp].as<double>(), x->own);
         if (x->mixed) {
-          size_t n = part_table_stride(dir, kind, d);
+          size_t n = part_table_stride32(dir, kind, d);
           if (!x->ptab_f[dir][comp].ensure(n * sizeof(float))) return false;
-          launch_round_table(x->ptab[dir][comp].as<double>(), x->ptab_f[dir][comp].as<float>(),
-                             (long)n, x->own);
+          launch_round_line_table(dir, kind, d, x->g, nullptr, a, nullptr,
+                                  x->ptab[dir][comp].as<double>(),
+                                  x->ptab_f[dir][comp].as<float>(), 1, x->own);
         }
       }
     if (!NSE_CUDA(cudaStreamSynchronize(x->own))) return false;
@@ -1322,10 +1327,11 @@ static bool refresh_line_flags(nse_ctx* x, cudaStream_t s) {
         launch_part_tables(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
                            (int)ids.size(), x->pmtab[dir][comp].as<double>(), s);
         if (x->mixed) {
-          size_t n = std::max<size_t>(1, ids.size()) * ps;
+          size_t n = std::max<size_t>(1, ids.size()) * part_table_stride32(dir, kind, d);
           if (!x->pmtab_f[dir][comp].ensure(n * sizeof(float))) return false;
-          launch_round_table(x->pmtab[dir][comp].as<double>(), x->pmtab_f[dir][comp].as<float>(),
-                             (long)(ids.size() * ps), s);
+          launch_round_line_table(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
+                                  x->pmtab[dir][comp].as<double>(),
+                                  x->pmtab_f[dir][comp].as<float>(), (long)ids.size(), s);
         }
       }
       // the host vectors die at the end of this iteration
