@@ -8,8 +8,9 @@
 // the segment is replayed from its checkpoint with every step recording the
 // state it starts from and the inputs and outputs of its line-solve passes;
 // then its steps are reversed one by one with the transposed kernels of
-// k_adjoint.cu.  Device memory: (ceil(nsteps/ckpt) * 11 + ckpt * 23 + 44)
-// padded fields.
+// k_adjoint.cu; the transposed line solves are the step's own line solves
+// between diagonal scalings.  Device memory: (ceil(nsteps/ckpt) * 11 +
+// ckpt * 23 + 36) padded fields.
 #include <algorithm>
 #include <vector>
 
@@ -26,9 +27,8 @@ const int kState[11] = {NSE_U,     NSE_V,     NSE_W,     NSE_T,     NSE_U_TA, NS
 enum { S_U = 0, S_V, S_W, S_T, S_UTA, S_VTA, S_WTA, S_UP, S_VP, S_WP, S_TP, NS };
 const int kSeg = 7;   // u, v, w, T, u_ta, v_ta, w_ta at the start of a recorded step
 const int kRec = 16;  // line-pass inputs and outputs of a recorded step
-// work fields (line scratch: two per component, the components' line
-// passes run concurrently on their own streams)
-enum { W_B = 0, W_O = 4, W_XS = 8, W_RB = 9, W_ST = 10, W_S = 14, NW = 22 };
+// work fields
+enum { W_B = 0, W_O = 4, W_XS = 8, W_RB = 9, W_ST = 10, NW = 14 };
 
 int state_index(int field) {
   for (int q = 0; q < NS; ++q)
@@ -119,7 +119,7 @@ void adjoint_step(nse_adjoint* a, double* sg, double* const* rc, int l) {
   launch_adj_phibar(D, g, ubc, tab, c.dt, wk[W_XS], s);
   launch_fft_fwd_x(*ci.pp, D, wk[W_XS], nullptr, nullptr, nullptr, ci.g, 1.0, 0, s);
   launch_fft_z(*ci.pp, false, s);
-  launch_adj_spn(*ci.pp, s);
+  if (!launch_spn_transposed(*ci.pp, ci.rg.rdy, ci.g.dy, s)) launch_adj_spn(*ci.pp, s);
   launch_fft_z(*ci.pp, true, s);
   launch_fft_inv_x(*ci.pp, D, wk[W_RB], s);
   launch_adj_div(D, g, ub, wk[W_RB], c.dt, s);
@@ -133,10 +133,13 @@ void adjoint_step(nse_adjoint* a, double* sg, double* const* rc, int l) {
     const int vdirs[3] = {1, 2, 0}, tdirs[3] = {1, 0, 2};
     const int* dirs = comp == 3 ? tdirs : vdirs;
     double* cbar = comp == 3 ? cb[0] : cb[comp + 1];
-    for (int p = 2; p >= 0; --p)
-      launch_adj_line(D, g, dirs[p], comp, bar[comp], rc[4 * comp + p], rc[4 * comp + p + 1],
-                      c1, cbar, wk[W_S + 2 * comp], wk[W_S + 2 * comp + 1], c.Re, c.Sc, c.dt,
-                      c.eta, c.thc, c.rho_cp, cs);
+    for (int p = 2; p >= 0; --p) {
+      launch_adj_line_scale(D, g, dirs[p], comp, false, bar[comp], nullptr, nullptr, c1, nullptr,
+                            c.dt, c.eta, cs);
+      ctx_line_solve(a->x, dirs[p], comp, bar[comp], cs);
+      launch_adj_line_scale(D, g, dirs[p], comp, true, bar[comp], rc[4 * comp + p],
+                            rc[4 * comp + p + 1], c1, cbar, c.dt, c.eta, cs);
+    }
     if (comp > 0) NSE_CUDA(cudaEventRecord(a->join[comp - 1], cs));
   }
   for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(s, a->join[q], 0));

@@ -240,6 +240,8 @@ void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s
 int spn_split(const PoissonPlan& pp);
 void launch_spn_tables(const PoissonPlan& pp, double* im, cudaStream_t s);
 void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s);
+bool launch_spn_transposed(const PoissonPlan& pp, const double* rdy, const double* dy,
+                           cudaStream_t s);
 void launch_spn_fast_f32(const PoissonPlan& pp, cudaStream_t s);
 void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,
                      long scj, long sck, const double* AC, const double* KXZ, bool do_spn,
@@ -296,5 +298,7 @@ void ctx_set_l(nse_ctx* x, int l);
 // one step of the context; with rec given, the line-solve passes record their
 // inputs and outputs (16 padded fields, see nse_ctx::rec)
 void ctx_step_rec(nse_ctx* x, double* const* rec);
+// the line solve of (dir, comp) of the step on the field f (ft = fb = 0)
+void ctx_line_solve(nse_ctx* x, int dir, int comp, double* f, cudaStream_t s);
 
 }  // namespace nse

@@ -376,191 +376,47 @@ __global__ void k_adj_point(PArgs a) {
   a.A[3][c] = tb;
 }
 
-// ------------------------------------------------------ line transposes --
-// Row coefficients (lo, di, up) of the forward line systems, row j of a line
-// along `dir` (1-based grid index along the line):
-//   ROW_U  implicit_uy (u, w along y): lo = -b/a/d12(j-1)/d(j), ...
-//   ROW_V  implicit_vy (v along y) and implicit_solver (velocity along x, z)
-//   ROW_T  implicit_Ty / implicit_Tx with harmonic conductances
-enum { ROW_U = 0, ROW_V = 1, ROW_T = 2 };
-
-// (r, r12: reciprocal spacings; bia = beta / alpha, already divided by rhoCp
-// and multiplied by the uniform conductivity for ROW_T)
-__device__ __forceinline__ void line_row(int kind, const double* r, const double* r12, int j,
-                                         double bia, double& lo, double& di, double& up) {
-  if (kind == ROW_V) {
-    lo = -bia * r[j] * r12[j];
-    di = 1.0 + bia * (r[j + 1] + r[j]) * r12[j];
-    up = -bia * r[j + 1] * r12[j];
-  } else {  // ROW_U and ROW_T (harmonic mean of a uniform conductivity = L)
-    lo = -bia * r12[j - 1] * r[j];
-    di = 1.0 + bia * (r12[j] + r12[j - 1]) * r[j];
-    up = -bia * r12[j] * r[j];
-  }
-}
-
-struct LArgs {
+// ------------------------------------- line transposes by diagonal scaling --
+// Every line system of the step has rows A(j,j+-1) = -(beta/alpha_j) s(j,j+-1)/w_j
+// with s symmetric (also through the wall folds, which change diagonals
+// only, and the periodic corners, where the ghost spacing equals the
+// opposite interior one): w_j = dy (u, w, T along y), dy12 (v along y),
+// dx12 / dz12 (velocity along x / z), dx / dz (T along x / z).  So
+// A = D^-1 (D + S) with D = diag(alpha_j w_j), A^T = D A D^-1 and
+// A^-T = D A^-1 D^-1: the transposed solve is the step's own line solve
+// between two diagonal scalings.  `out` = 0: xb /= alpha w (before the
+// solve); 1: rbar = alpha w y, c_bar += rbar dt eta / alpha (r - x).
+struct SArgs {
   Dims D;
   AdjGrid g;
-  double* xb;          // in: adjoint of the pass output; out: adjoint of its input
-  const double* rin;   // forward input of the pass
-  const double* xout;  // forward output of the pass
+  double* xb;
+  const double* rin;
+  const double* xout;
   const double* c1;
-  double* cbar;        // accumulator of the mask the rows use
-  double* s1;          // scratch (n * nlines)
-  double* s2;          // scratch (periodic lines)
-  int comp;            // 0 u, 1 v, 2 w, 3 T
-  int kind;            // ROW_*
-  int n;               // rows per line
-  int jtop;            // last row index of the lines of x/z passes (ny or ny-1)
-  double beta, dt, eta, L, R;
+  double* cbar;
+  int dir, comp, out;
+  double dte;  // dt * eta
 };
 
-// line t of a pass along DIR: grid position of row r (0-based) and its mask
-template <int DIR>
-__device__ __forceinline__ void line_pos(const LArgs& a, long t, int r, int& i, int& j, int& k) {
-  if (DIR == 0) {
-    i = 1 + r;
-    j = 1 + (int)(t % a.jtop);
-    k = 1 + (int)(t / a.jtop);
-  } else if (DIR == 1) {
-    i = 1 + (int)(t % a.D.nx);
-    j = 1 + r;
-    k = 1 + (int)(t / a.D.nx);
-  } else {
-    i = 1 + (int)(t % a.D.nx);
-    j = 1 + (int)(t / a.D.nx);
-    k = 1 + r;
+__global__ void k_adj_line_scale(SArgs a) {
+  const Dims& D = a.D;
+  const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
+  const int j = 1 + blockIdx.y;
+  const int k = 1 + blockIdx.z;
+  if (i > D.nx || (a.comp == 1 && j == D.ny)) return;
+  const int idx = a.dir == 0 ? i : (a.dir == 1 ? j : k);
+  const bool wd = a.comp == 3 || (a.dir == 1 && a.comp != 1);
+  const double rw = wd ? a.g.r[a.dir][idx] : a.g.r12[a.dir][idx];  // 1 / w
+  const double cm = face_mask(D, a.c1, a.comp, i, j, k);
+  const double alpha = a.dte * cm + 1.0;
+  const long c = D.P(i, j, k);
+  if (!a.out) {
+    a.xb[c] = cm == 0.0 ? a.xb[c] * rw : a.xb[c] * rw / alpha;
+    return;
   }
-}
-
-template <int DIR>
-__device__ __forceinline__ void row_coef(const LArgs& a, long t, int r, double& lo, double& di,
-                                         double& up, double& alpha, long& c, long& m) {
-  int i, j, k;
-  line_pos<DIR>(a, t, r, i, j, k);
-  c = a.D.P(i, j, k);
-  m = a.D.C(i, j, k);
-  const double cm = face_mask(a.D, a.c1, a.comp, i, j, k);
-  alpha = a.dt * a.eta * cm + 1.0;
-  const int jj = DIR == 0 ? i : (DIR == 1 ? j : k);
-  const double bia = cm == 0.0 ? a.beta : a.beta / alpha;
-  line_row(a.kind, a.g.r[DIR], a.g.r12[DIR], jj, bia, lo, di, up);
-}
-
-// y lines: the ghost rows x0 + x1 = ft, x_n + x_n+1 = fb folded into the first
-// and last rows (u, w, T), or the Dirichlet rows of v (no fold).  Transposed
-// system: sub'(r) = up(r-1), diag(r), sup'(r) = lo(r+1).
-__global__ void k_adj_line_y(LArgs a) {
-  const long nl = (long)a.D.nx * a.D.nz;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= nl) return;
-  const int n = a.n;
-  const bool fold = a.kind != ROW_V;
-  double lo, di, up, al;
-  long c, m;
-  row_coef<1>(a, t, 0, lo, di, up, al, c, m);
-  if (fold) di -= lo;
-  double lo_n = 0.0, di_n = 0.0, up_n = 0.0, al_n = 1.0;
-  long cn = c, mn = m;
-  double up_prev = 0.0, cp_prev = 0.0, y_prev = 0.0;
-  for (int r = 0; r < n; ++r) {
-    if (r + 1 < n) {
-      row_coef<1>(a, t, r + 1, lo_n, di_n, up_n, al_n, cn, mn);
-      if (fold && r + 1 == n - 1) di_n -= up_n;
-    }
-    const double sub = r > 0 ? up_prev : 0.0;
-    const double sup = r + 1 < n ? lo_n : 0.0;
-    const double mm = di - sub * cp_prev;
-    const double cp = sup / mm;
-    const double y = (a.xb[c] - sub * y_prev) / mm;
-    a.s1[r * nl + t] = cp;
-    a.xb[c] = y;
-    cp_prev = cp;
-    y_prev = y;
-    up_prev = up;
-    lo = lo_n; di = di_n; up = up_n; c = cn;
-  }
-  // back substitution with the mask gradient of each row
-  double ynext = 0.0;
-  for (int r = n - 1; r >= 0; --r) {
-    row_coef<1>(a, t, r, lo, di, up, al, c, m);
-    double y = a.xb[c];
-    if (r < n - 1) y -= a.s1[r * nl + t] * ynext;
-    a.xb[c] = y;
-    a.cbar[m] += y * (al == 1.0 ? a.dt * a.eta : a.dt * a.eta / al) * (a.rin[c] - a.xout[c]);
-    ynext = y;
-  }
-  if (a.comp == 1) a.xb[a.D.P(1 + (int)(t % a.D.nx), a.D.ny, 1 + (int)(t / a.D.nx))] = 0.0;
-}
-
-// periodic lines (x or z): the interior system is cyclic with corners
-// P(0,n-1) = lo(0), P(n-1,0) = up(n-1); its transpose has sub'(r) = up(r-1),
-// sup'(r) = lo(r+1) (cyclic indices), solved by Sherman-Morrison with
-// gamma = -diag(0) (two Thomas sweeps sharing one elimination)
-template <int DIR>
-__global__ void k_adj_line_p(LArgs a) {
-  const long nl = DIR == 0 ? (long)a.jtop * a.D.nz : (long)a.D.nx * a.jtop;
-  const long t = blockIdx.x * (long)blockDim.x + threadIdx.x;
-  if (t >= nl) return;
-  const int n = a.n;
-  double lo0, di0, up0, al0, loL, diL, upL, alL;
-  long c0, m0, cL, mL;
-  row_coef<DIR>(a, t, 0, lo0, di0, up0, al0, c0, m0);
-  row_coef<DIR>(a, t, n - 1, loL, diL, upL, alL, cL, mL);
-  const double bc = upL;  // transposed corner (0, n-1) = P(n-1, 0)
-  const double ac = lo0;  // transposed corner (n-1, 0) = P(0, n-1)
-  const double gam = -di0;
-  double lo = lo0, di = di0, up = up0, al = al0;
-  long c = c0, m = m0;
-  double lo_n = 0.0, di_n = 0.0, up_n = 0.0, al_n = 1.0;
-  long cn = c, mn = m;
-  double up_prev = upL, cp_prev = 0.0, y_prev = 0.0, z_prev = 0.0;
-  for (int r = 0; r < n; ++r) {
-    if (r + 1 < n) row_coef<DIR>(a, t, r + 1, lo_n, di_n, up_n, al_n, cn, mn);
-    double dd = di;
-    if (r == 0) dd = di - gam;
-    if (r == n - 1) dd = dd - ac * bc / gam;
-    const double sub = r > 0 ? up_prev : 0.0;
-    const double sup = r + 1 < n ? lo_n : 0.0;
-    const double mm = dd - sub * cp_prev;
-    const double cp = sup / mm;
-    const double rz = r == 0 ? gam : (r == n - 1 ? ac : 0.0);
-    const double y = (a.xb[c] - sub * y_prev) / mm;
-    const double z = (rz - sub * z_prev) / mm;
-    a.s1[r * nl + t] = cp;
-    a.s2[r * nl + t] = z;
-    a.xb[c] = y;
-    cp_prev = cp; y_prev = y; z_prev = z;
-    up_prev = up;
-    lo = lo_n; di = di_n; up = up_n; al = al_n; c = cn; m = mn;
-  }
-  double ynext = 0.0, znext = 0.0, y0 = 0.0, z0 = 0.0, yL = 0.0, zL = 0.0;
-  for (int r = n - 1; r >= 0; --r) {
-    int i, j, k;
-    line_pos<DIR>(a, t, r, i, j, k);
-    const long cc = a.D.P(i, j, k);
-    double y = a.xb[cc];
-    double z = a.s2[r * nl + t];
-    if (r < n - 1) {
-      const double cp = a.s1[r * nl + t];
-      y -= cp * ynext;
-      z -= cp * znext;
-    }
-    a.xb[cc] = y;
-    a.s2[r * nl + t] = z;
-    if (r == n - 1) { yL = y; zL = z; }
-    if (r == 0) { y0 = y; z0 = z; }
-    ynext = y;
-    znext = z;
-  }
-  const double fact = (y0 + bc * yL / gam) / (1.0 + z0 + bc * zL / gam);
-  for (int r = 0; r < n; ++r) {
-    row_coef<DIR>(a, t, r, lo, di, up, al, c, m);
-    const double y = a.xb[c] - fact * a.s2[r * nl + t];
-    a.xb[c] = y;
-    a.cbar[m] += y * (al == 1.0 ? a.dt * a.eta : a.dt * a.eta / al) * (a.rin[c] - a.xout[c]);
-  }
+  const double rb = cm == 0.0 ? a.xb[c] / rw : alpha * a.xb[c] / rw;
+  a.xb[c] = rb;
+  a.cbar[D.C(i, j, k)] += rb * (cm == 0.0 ? a.dte : a.dte / alpha) * (a.rin[c] - a.xout[c]);
 }
 
 // -------------------------------------------------------- MKP transposes --
@@ -970,33 +826,14 @@ void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
   k_adj_point<<<cell_grid(D, 128), 128, 0, s>>>(a);
 }
 
-void launch_adj_line(const Dims& D, const AdjGrid& g, int dir, int comp, double* xb,
-                     const double* rin, const double* xout, const double* c1, double* cbar,
-                     double* s1, double* s2, double Re, double Sc, double dt, double eta,
-                     double L, double R, cudaStream_t s) {
-  LArgs a;
+void launch_adj_line_scale(const Dims& D, const AdjGrid& g, int dir, int comp, bool out,
+                           double* xb, const double* rin, const double* xout, const double* c1,
+                           double* cbar, double dt, double eta, cudaStream_t s) {
+  SArgs a;
   a.D = D; a.g = g; a.xb = xb; a.rin = rin; a.xout = xout; a.c1 = c1; a.cbar = cbar;
-  a.s1 = s1; a.s2 = s2; a.comp = comp;
-  a.dt = dt; a.eta = eta; a.L = L; a.R = R;
-  a.beta = comp == 3 ? dt / Re / Sc / 2.0 * L / R : dt / Re / 2.0;
-  a.jtop = comp == 1 ? D.ny - 1 : D.ny;
-  if (comp == 3) a.kind = ROW_T;
-  else a.kind = (dir == 1 && comp != 1) ? ROW_U : ROW_V;
-  const int bs = 128;
+  a.dir = dir; a.comp = comp; a.out = out ? 1 : 0; a.dte = dt * eta;
   count_launch();
-  if (dir == 1) {
-    a.n = comp == 1 ? D.ny - 1 : D.ny;
-    long nl = (long)D.nx * D.nz;
-    k_adj_line_y<<<(unsigned)((nl + bs - 1) / bs), bs, 0, s>>>(a);
-  } else if (dir == 0) {
-    a.n = D.nx;
-    long nl = (long)a.jtop * D.nz;
-    k_adj_line_p<0><<<(unsigned)((nl + bs - 1) / bs), bs, 0, s>>>(a);
-  } else {
-    a.n = D.nz;
-    long nl = (long)D.nx * a.jtop;
-    k_adj_line_p<2><<<(unsigned)((nl + bs - 1) / bs), bs, 0, s>>>(a);
-  }
+  k_adj_line_scale<<<cell_grid(D, 128), 128, 0, s>>>(a);
 }
 
 void launch_adj_phibar(const Dims& D, const AdjGrid& g, const double* const ub[3],

@@ -39,12 +39,12 @@ void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
                       const double* const ta[3], const double* const rin[4], const double* c1,
                       double* const cbar[4], double eta, double dt, double tsolid, int l,
                       cudaStream_t s);
-// one ADI pass transposed (dir 0 x, 1 y, 2 z; comp 0 u, 1 v, 2 w, 3 T):
-// xb <- A^-T xb, cbar += xb dt eta / alpha (rin - xout)
-void launch_adj_line(const Dims& D, const AdjGrid& g, int dir, int comp, double* xb,
-                     const double* rin, const double* xout, const double* c1, double* cbar,
-                     double* s1, double* s2, double Re, double Sc, double dt, double eta,
-                     double L, double R, cudaStream_t s);
+// diagonal scalings around the step's own line solve that make it the
+// transposed solve (A^-T = D A^-1 D^-1, D = diag(alpha w)); out = false
+// before the solve, true after (with the mask gradient of the pass)
+void launch_adj_line_scale(const Dims& D, const AdjGrid& g, int dir, int comp, bool out,
+                           double* xb, const double* rin, const double* xout, const double* c1,
+                           double* cbar, double dt, double eta, cudaStream_t s);
 // MKP transposed: phi_bar at the P2S samples, transposed SPN/SP0B on the
 // spectrum, divergence transposed
 void launch_adj_phibar(const Dims& D, const AdjGrid& g, const double* const ub[3],

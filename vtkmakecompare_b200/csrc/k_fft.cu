@@ -788,11 +788,19 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // then runs its recurrence from shared memory; the back substitution writes
 // the solution to global memory.  Shared memory: values [q][thread],
 // pivots [q][half].
+//
+// Transposed use (the discrete adjoint): the SPN matrix is diag(dy)^-1 S with
+// S symmetric (AC1(j) = 1/(dy12(j-1) dy(j)), AC3(j) = 1/(dy12(j) dy(j))), so
+// its transposed solve is the same solve between the scalings 1/dy (pre, on
+// load) and dy (post, on store); the mean mode then runs SP0B's transpose,
+// a backward marching.  pre, post: null for the forward solve.
 template <class RT>
 __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, RT* base,
                                                  long svj, long svk,
                                                  const double* __restrict__ im, long tj,
-                                                 long tk, const double* __restrict__ AC) {
+                                                 long tk, const double* __restrict__ AC,
+                                                 const double* __restrict__ pre,
+                                                 const double* __restrict__ post) {
   extern __shared__ __align__(16) unsigned char spn_sm[];
   const int rmax = ny - m;  // rows of the longer (bottom) half
   RT* vs = reinterpret_cast<RT*>(spn_sm);                                  // [rmax][64]
@@ -833,7 +841,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
   }
   cp_async_wait_all();
   __syncwarp();
-  if (mean && part == 0) {
+  if (mean && part == 0 && !pre) {
     // SP0B mkp.f:271-288 (phi(1) = 0, forward marching; see k_spn) from the
     // staged column
     const double* AC2 = AC + ny;
@@ -848,6 +856,20 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
       pc = pn;
       Dj = Dn;
     }
+  } else if (mean && part == 0) {
+    // SP0B transposed: t(J) = (phibar(J+1) - AC2(J+1) t(J+1) - AC1(J+2) t(J+2)) / AC3(J),
+    // Dbar(J) = t(J) for J = ny-1..1, Dbar(ny) = 0
+    const double* AC2 = AC + ny;
+    double t1 = 0.0, t2 = 0.0;
+    B[sj * (ny - 1)] = (RT)0.0;
+    for (int J = ny - 1; J >= 1; --J) {
+      double v = (double)mean_slot(J) - AC2[J] * t1;  // phibar(J+1) is row J
+      if (J + 1 <= ny - 1) v -= AC1[J + 1] * t2;
+      const double tj = v / AC3[J - 1];
+      B[sj * (J - 1)] = (RT)tj;
+      t2 = t1;
+      t1 = tj;
+    }
   }
   // elimination: top rows 0..m-1 downwards, bottom rows ny-1..m upwards;
   // the eliminated values stay in double in place of the loaded ones when RT
@@ -861,7 +883,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
     for (int q = 0; q < cnt; ++q) {
       const int r = row(q);
       const double cf = cfe[r];
-      const double d = (double)vs[q * 64 + lt];
+      const double d = pre ? (double)vs[q * 64 + lt] * pre[r + 1] : (double)vs[q * 64 + lt];
       y = (q == 0 ? d : d - cf * y) * ws[q * 32 + hs];
       if (sizeof(RT) == sizeof(double)) ys[q * 64 + lt] = y;
       else vs[q * 64 + lt] = (RT)0;  // FP32 storage: recomputed below
@@ -876,13 +898,13 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
   const double cB = AC1[m] * (part ? ws[(ny - 1 - m) * 32 + hs] : IM[tj * m]);
   const double xm = (zbot - cB * ytop) / (1.0 - cB * cT);
   double x = part ? xm : ytop - cT * xm;
-  B[sj * row(cnt - 1)] = (RT)x;
+  B[sj * row(cnt - 1)] = (RT)(post ? x * post[row(cnt - 1) + 1] : x);
 #pragma unroll 4
   for (int q = cnt - 2; q >= 0; --q) {
     const int r = row(q);
     const double cf = cfb[r] * ws[q * 32 + hs];
     x = ys[q * 64 + lt] - cf * x;
-    B[sj * r] = (RT)x;
+    B[sj * r] = (RT)(post ? x * post[r + 1] : x);
   }
 }
 
@@ -1058,7 +1080,25 @@ static void spn_babe(const PoissonPlan& pp, RT* spec, cudaStream_t s) {
   dim3 grid((pp.H + 15) / 16, pp.nz);
   count_launch();
   k_spn_babe<RT><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, spec, pp.Hp, (long)pp.Hp * pp.ny,
-                                      pp.spn_im, pp.Hp, (long)pp.Hp * pp.ny, pp.AC);
+                                      pp.spn_im, pp.Hp, (long)pp.Hp * pp.ny, pp.AC, nullptr,
+                                      nullptr);
+}
+
+// transposed SPN + SP0B (the discrete adjoint) on the FP64 spectrum: rdy, dy
+// are the reciprocal and plain y spacings (index 0..ny+1); false when the plan
+// has no pivot tables
+bool launch_spn_transposed(const PoissonPlan& pp, const double* rdy, const double* dy,
+                           cudaStream_t s) {
+  if (!pp.spn_im) return false;
+  const int m = spn_split(pp);
+  const size_t sm = spn_smem(pp.ny, m);
+  smem_optin((const void*)k_spn_babe<double>, sm);
+  dim3 grid((pp.H + 15) / 16, pp.nz);
+  count_launch();
+  k_spn_babe<double><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, pp.spec, pp.Hp,
+                                          (long)pp.Hp * pp.ny, pp.spn_im, pp.Hp,
+                                          (long)pp.Hp * pp.ny, pp.AC, rdy, dy);
+  return true;
 }
 
 // SPN + SP0B with the tabulated pivots (fast form); k_spn when the plan has

@@ -1851,6 +1851,27 @@ void ctx_step_rec(nse_ctx* x, double* const* rec) {
   ctx_step(x);
   x->rec = nullptr;
 }
+// the step's line solve of (dir, comp) applied to the field f with zero wall
+// values (the linear part of the pass), on stream s; FP64 contexts
+void ctx_line_solve(nse_ctx* x, int dir, int comp, double* f, cudaStream_t s) {
+  refresh_line_flags(x, s);
+  LineArgs la = line_args(x, comp);
+  la.ft = 0.0;
+  la.fb = 0.0;
+  const Dims& d = x->d;
+  if (x->part) {
+    launch_lines_part(dir, line_kind(dir, comp), d, f, la, x->ptab[dir][comp].as<double>(),
+                      x->slots[dir][comp].as<int>(), x->ids[dir][comp].as<int>(),
+                      x->nmasked[dir][comp], x->pmtab[dir][comp].as<double>(), s);
+    return;
+  }
+  static const int ytab[4] = {TB_Y_U, TB_Y_V, TB_Y_U, TB_Y_T};
+  const int tab = dir == 1 ? ytab[comp] : (dir == 2 ? (comp == 3 ? TB_Z_T : TB_Z_V)
+                                                    : (comp == 3 ? TB_X_T : TB_X_V));
+  auto lines = (x->cfg.flags & NSE_FLAG_EXACT) ? launch_lines_exact : launch_lines_fast;
+  lines(dir, line_kind(dir, comp), d, f, la, x->tab[tab], x->slots[dir][comp].as<int>(),
+        x->mtab[dir][comp].as<double>(), s);
+}
 }  // namespace nse
 
 extern "C" {

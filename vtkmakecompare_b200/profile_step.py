@@ -2,12 +2,14 @@
 
     python -m vtkmakecompare_b200.profile_step --grid 128 96 128 --steps 2 [--exact]
     python -m vtkmakecompare_b200.profile_step --poisson 5
+    python -m vtkmakecompare_b200.profile_step --grid 128 128 128 --adjoint 6
 
 Builds the penalised channel-with-sphere case of bench.py at the given size
 (level-set mask, initial projection), runs --warmup steps, then --steps
-steps (or --poisson solves) and prints the wall time.  Kernel launches
-before the measured part: the level set (2*2001+1), the projection (8) and
-the warm-up steps (23 each).
+steps (or --poisson solves, or the discrete adjoint of --adjoint steps:
+checkpoints every half, wall flux averaged over the second half) and prints
+the wall time.  Kernel launches before the measured part: the level set
+(2*2001+1), the projection (8) and the warm-up steps (23 each).
 """
 import argparse
 import math
@@ -24,6 +26,7 @@ def main():
     ap.add_argument("--warmup", type=int, default=1)
     ap.add_argument("--poisson", type=int, default=0)
     ap.add_argument("--exact", action="store_true")
+    ap.add_argument("--adjoint", type=int, default=0)
     a = ap.parse_args()
     nx, ny, nz = a.grid
     g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
@@ -47,6 +50,11 @@ def main():
             ctx.upload("phi", W.poisson_rhs(g, 7))
             for _ in range(a.poisson):
                 ctx.poisson()
+        elif a.adjoint:
+            n = a.adjoint
+            with S.Adjoint(ctx, n, checkpoint_every=max(1, n // 2), avg_from=n // 2 + 1) as adj:
+                J, _ = adj.gradient()
+            print(f"adjoint of {n} steps: J = {J:.12e}")
         else:
             ctx.step(a.steps)
         ctx.sync()
