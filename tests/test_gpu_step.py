@@ -80,7 +80,9 @@ def test_context_grid_matches_oracle_grid():
                                             # shapes the partitioned line solver takes
                                             ((96, 48, 64), True, 4), ((128, 40, 96), True, 3),
                                             ((64, 48, 64), True, 4),  # half-warp x lines
-                                            ((256, 20, 24), False, 2)])
+                                            ((256, 20, 24), False, 2),
+                                            # fused z transforms + SPN (clusters)
+                                            ((256, 32, 256), True, 2)])
 def test_steps_match_oracle(n, sphere, steps, exact):
     g, f, c1, par = make_case(*n, sphere=sphere)
     ref = run_oracle(g, f, c1, par, steps)
@@ -165,7 +167,7 @@ def laplacian(g, P):
     return X + Y + Z
 
 
-@pytest.mark.parametrize("n", [(64, 64, 64), (256, 192, 256)])
+@pytest.mark.parametrize("n", [(64, 64, 64), (256, 192, 256), (256, 24, 256), (256, 48, 256)])
 def test_poisson_manufactured(n):
     """P2S -> SPN -> SP0B -> S2P inverts the reference's 7-point operator
     (solve_p stencil nse_dominik.f:1988-1993 with PHIBC ghosts): a random phi

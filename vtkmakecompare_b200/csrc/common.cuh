@@ -242,6 +242,7 @@ void launch_spn_tables(const PoissonPlan& pp, double* im, cudaStream_t s);
 void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s);
 bool launch_spn_transposed(const PoissonPlan& pp, const double* rdy, const double* dy,
                            cudaStream_t s);
+
 void launch_spn_fast_f32(const PoissonPlan& pp, cudaStream_t s);
 void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, double* sc,
                      long scj, long sck, const double* AC, const double* KXZ, bool do_spn,
