@@ -11,13 +11,15 @@
 // scalar diffusion is the conductivity itself.  Where the penalisation mask
 // and its face averages vanish the immersed-boundary term is an exact zero,
 // so u_ta is not read and the implicit penalisation is the identity.
-// A CTA covers 32 x 8 cells of an (x,y) tile and marches over KCHUNK planes
+// A CTA covers 32 x TY cells of an (x,y) tile and marches over KCHUNK planes
 // in z; the halo planes of u, v, w, T sit in a shared-memory ring that is
-// filled one plane ahead with asynchronous copies (cp.async) while the
-// current plane is computed; the ring holds five planes (k-1, k, k+1 in use,
-// k+2 and k+3 in flight) of u, v, w, T and the mask with a one-cell halo and
-// of the four AB2 histories, so every input is read from HBM about once and
-// two planes of loads are always outstanding.
+// filled ahead with asynchronous copies (cp.async) while the current plane
+// is computed; the ring holds NS planes (k-1, k, k+1 in use, NS-3 in
+// flight) of u, v, w, T and the mask with a one-cell halo and of the four
+// AB2 histories, so every input is read from HBM about once.  The tile
+// height, ring depth and CTAs per SM are chosen per storage type (RhsShape):
+// the FP64 kernel needs ~150 registers per thread without spilling, so it
+// runs 32 x 4 tiles, three CTAs per SM.
 #include "common.cuh"
 
 namespace nse {
@@ -32,13 +34,25 @@ constexpr int KCHUNK = NSE_RHS_KCHUNK;  // z planes per CTA
 #define NSE_CORR_KCHUNK 8
 #endif
 constexpr int CKCHUNK = NSE_CORR_KCHUNK;  // z planes per CTA of the correction
-constexpr int TXW = 32, TYW = 8;     // interior tile of a CTA (x, y)
-constexpr int SXW = TXW + 2, SYW = TYW + 2;
-constexpr int PLANE = SXW * SYW;     // one halo plane of one field
-constexpr int TILE = TXW * TYW;      // one interior plane of one field
-// a ring slot holds plane K of: u, v, w, T, c1 (halo) and the four AB2
-// histories (interior); its size in bytes is slot_bytes<H>() below
-constexpr int NSLOT = 5;             // k-1, k, k+1 in use, k+2 and k+3 in flight
+constexpr int TXW = 32;              // interior tile width of a CTA (x)
+constexpr int SXW = TXW + 2;         // with the halo
+// a ring slot holds plane K of: u, v, w, T, c1 (halo, SXW x (TY+2) each) and
+// the four AB2 histories (interior, TXW x TY); its size in bytes is
+// slot_bytes<H, TY>() below
+
+// launch shapes (tile height TY, ring slots NS, CTAs per SM MINB), measured
+// at 256x192x256 on B200: FP64 32x8 tiles with two CTAs per SM spilled at
+// the 128-register cap (0.636 ms per RHS); 32x4 tiles with three CTAs per
+// SM and no spills take 0.474 ms.  FP32 storage and arithmetic fits 117
+// registers and keeps 32x8 tiles, two CTAs per SM (0.390 ms; one CTA of
+// 32x16 took 0.455 ms).
+template <class H, class CT> struct RhsShape { static constexpr int TY = 4, NS = 5, MINB = 3; };
+template <> struct RhsShape<float, float> { static constexpr int TY = 8, NS = 5, MINB = 2; };
+template <> struct RhsShape<float, double> { static constexpr int TY = 8, NS = 5, MINB = 2; };
+// the correction: FP64 32x4 tiles, four CTAs per SM (0.443 against 0.451 ms
+// for 32x8); FP32 storage 32x8 tiles, two CTAs per SM
+template <class H> struct CorrShape { static constexpr int TY = 4, NS = 5, MINB = 4; };
+template <> struct CorrShape<float> { static constexpr int TY = 8, NS = 5, MINB = 2; };
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
   unsigned sa = (unsigned)__cvta_generic_to_shared(smem);
@@ -50,21 +64,24 @@ __device__ __forceinline__ void cp_async8(float* smem, const float* gmem) {
 }
 // bytes of one ring slot: five halo planes of FP64 fields, then four tiles of
 // the AB2 histories in their storage type H
-template <class H>
-__host__ __device__ constexpr int slot_bytes() { return 5 * PLANE * 8 + 4 * TILE * (int)sizeof(H); }
+template <class H, int TY>
+__host__ __device__ constexpr int slot_bytes() {
+  return 5 * SXW * (TY + 2) * 8 + 4 * TXW * TY * (int)sizeof(H);
+}
 __device__ __forceinline__ void cp_async_commit() { asm volatile("cp.async.commit_group;\n" ::: "memory"); }
 template <int N>
 __device__ __forceinline__ void cp_async_wait() { asm volatile("cp.async.wait_group %0;\n" ::"n"(N) : "memory"); }
 
-// plane K into ring slot K mod NSLOT (one commit group, possibly empty)
-template <class H>
+// plane K into ring slot K mod NS (one commit group, possibly empty)
+template <class H, int TY, int NS>
 __device__ __forceinline__ void load_plane(char* sm, const Dims& d, int i0, int j0, int K,
                                            int kmax, const double* U, const double* V,
                                            const double* W, const double* T, const double* C1,
                                            const H* UP, const H* VP, const H* WP,
                                            const H* TP) {
   if (K <= kmax) {
-    double* slot = reinterpret_cast<double*>(sm + (K % NSLOT) * slot_bytes<H>());
+    constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+    double* slot = reinterpret_cast<double*>(sm + (K % NS) * slot_bytes<H, TY>());
     const int tid = threadIdx.y * TXW + threadIdx.x;
     for (int e = tid; e < PLANE; e += TILE) {
       int tx = e % SXW, ty = e / SXW;
@@ -94,8 +111,8 @@ __device__ __forceinline__ void load_plane(char* sm, const Dims& d, int i0, int 
 // H: storage type of the histories, u_ta and the outputs (double; float in
 // the mixed-precision form); CT: arithmetic type (FP32 arithmetic rounds the
 // FP64 state as it is read from the ring)
-template <class H, class CT>
-__global__ void __launch_bounds__(256, 2) k_rhs_fast(
+template <class H, class CT, int TY, int NS, int MINB>
+__global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     Dims d, GridDev g, GridRcp rg, StepParams sp, const double* __restrict__ U,
     const double* __restrict__ V, const double* __restrict__ W, const double* __restrict__ T,
     const H* __restrict__ U_TA, const H* __restrict__ V_TA, const H* __restrict__ W_TA,
@@ -104,16 +121,19 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
     H* __restrict__ W_A, H* __restrict__ U_T) {
   extern __shared__ __align__(16) char smc[];
   char* sm = smc;
-  const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
+  constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+  constexpr int F = NS - 3;  // planes in flight
+  const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
   const int k0 = 1 + blockIdx.z * KCHUNK;
   const int k1 = min(d.nz, k0 + KCHUNK - 1);
   const int kmax = k1 + 1;  // last plane any iteration reads
-  // prologue: planes k0-1 .. k0+2 (k0+2 stays in flight)
-  for (int q = -1; q <= 2; ++q)
-    load_plane<H>(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
-  cp_async_wait<1>();
+  // prologue: planes k0-1 .. k0+F (the last F-1 stay in flight)
+  for (int q = -1; q <= F; ++q)
+    load_plane<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE,
+                          T_PRE);
+  cp_async_wait<F - 1>();
   __syncthreads();
   using R = CT;  // arithmetic type
   const R DT = (R)sp.dt;
@@ -134,11 +154,15 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
   const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;  // this cell in a halo plane
   const int t0 = threadIdx.y * TXW + threadIdx.x;            // this cell in a tile
   for (int K = k0; K <= k1; ++K) {
-    load_plane<H>(sm, d, i0, j0, K + 3, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE, T_PRE);
+    // plane K+1+F goes into the slot of plane K-2, free since the barrier
+    // that ended the previous iteration
+    load_plane<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE,
+                          T_PRE);
     if (valid) {
-      const double* pm = reinterpret_cast<const double*>(sm + ((K - 1) % NSLOT) * slot_bytes<H>());
-      const double* pc = reinterpret_cast<const double*>(sm + (K % NSLOT) * slot_bytes<H>());
-      const double* pp = reinterpret_cast<const double*>(sm + ((K + 1) % NSLOT) * slot_bytes<H>());
+      constexpr int SB = slot_bytes<H, TY>();
+      const double* pm = reinterpret_cast<const double*>(sm + ((K - 1) % NS) * SB);
+      const double* pc = reinterpret_cast<const double*>(sm + (K % NS) * SB);
+      const double* pp = reinterpret_cast<const double*>(sm + ((K + 1) % NS) * SB);
       const long c = d.P(I, J, K);
       const R dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
       const R rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
@@ -252,7 +276,7 @@ __global__ void __launch_bounds__(256, 2) k_rhs_fast(
       }
     }
     }  // valid
-    cp_async_wait<1>();
+    cp_async_wait<F - 1>();
     __syncthreads();
   }
 }
@@ -263,14 +287,16 @@ static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
                      const H* u_ta, const H* v_ta, const H* w_ta, H* u_pre, H* v_pre, H* w_pre,
                      H* T_pre, const double* c1, H* u_a, H* v_a, H* w_a, H* u_T,
                      cudaStream_t s) {
-  dim3 block(TXW, TYW, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + KCHUNK - 1) / KCHUNK);
-  size_t smem = (size_t)NSLOT * slot_bytes<H>();
-  cudaFuncSetAttribute((const void*)k_rhs_fast<H, CT>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  using Sh = RhsShape<H, CT>;
+  constexpr int TY = Sh::TY, NS = Sh::NS;
+  dim3 block(TXW, TY, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KCHUNK - 1) / KCHUNK);
+  size_t smem = (size_t)NS * slot_bytes<H, TY>();
+  auto kern = k_rhs_fast<H, CT, TY, NS, Sh::MINB>;
+  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
-  k_rhs_fast<H, CT><<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre,
-                                              v_pre, w_pre, T_pre, c1, u_a, v_a, w_a, u_T);
+  kern<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
+                                 T_pre, c1, u_a, v_a, w_a, u_T);
 }
 
 void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
@@ -363,21 +389,23 @@ namespace nse {
 // ----------------------------------------------------- pipelined correction
 // mkp.f:141-217 for interior cells (1..n in every direction), marching in z
 // like k_rhs_fast: a ring of planes of phi (FP64), u*, v*, w* (one-cell halo)
-// and the old u_ta, v_ta, w_ta (interior) filled two planes ahead by
+// and the old u_ta, v_ta, w_ta (interior) filled NS-3 planes ahead by
 // cp.async.  H is the storage type of u*, u_ta, u_ep2 and divu (float in the
 // mixed-precision form); the correction itself is evaluated in FP64.
-template <class H>
+template <class H, int TY>
 __host__ __device__ constexpr int cslot_bytes() {
-  return PLANE * 8 + 3 * PLANE * (int)sizeof(H) + 3 * TILE * (int)sizeof(H);
+  return SXW * (TY + 2) * 8 + 3 * SXW * (TY + 2) * (int)sizeof(H) +
+         3 * TXW * TY * (int)sizeof(H);
 }
 
-template <class H>
+template <class H, int TY, int NS>
 __device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, int j0, int K,
                                              int kmax, const double* PHI, const H* UT,
                                              const H* VT, const H* WT, const H* UA,
                                              const H* VA, const H* WA) {
   if (K <= kmax) {
-    char* slot = sm + (K % NSLOT) * cslot_bytes<H>();
+    constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+    char* slot = sm + (K % NS) * cslot_bytes<H, TY>();
     double* ph = reinterpret_cast<double*>(slot);
     H* fl = reinterpret_cast<H*>(slot + PLANE * 8);
     const int tid = threadIdx.y * TXW + threadIdx.x;
@@ -403,8 +431,8 @@ __device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, in
   cp_async_commit();
 }
 
-template <class H>
-__global__ void __launch_bounds__(256, 2) k_correct_pipe(
+template <class H, int TY, int NS, int MINB>
+__global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     Dims d, GridRcp rg, const double* __restrict__ PHI, const H* __restrict__ UT,
     const H* __restrict__ VT, const H* __restrict__ WT, double* __restrict__ p,
     double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
@@ -412,15 +440,16 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
     H* __restrict__ v_ep2, H* __restrict__ w_ep2, H* __restrict__ divu, double dt) {
   extern __shared__ __align__(16) char smc[];
   char* sm = smc;
-  const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TYW;
+  constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY, F = NS - 3;
+  const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
   const int k0 = 1 + blockIdx.z * CKCHUNK;
   const int k1 = min(d.nz, k0 + CKCHUNK - 1);
   const int kmax = k1 + 1;
-  for (int q = -1; q <= 2; ++q)
-    load_plane_c<H>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
-  cp_async_wait<1>();
+  for (int q = -1; q <= F; ++q)
+    load_plane_c<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+  cp_async_wait<F - 1>();
   __syncthreads();
   double rx = 0, rx12 = 0, rx12m = 0, ry = 0, ry12 = 0, ry12m = 0;
   if (valid) {
@@ -430,11 +459,12 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
   const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;
   const int t0 = threadIdx.y * TXW + threadIdx.x;
   for (int K = k0; K <= k1; ++K) {
-    load_plane_c<H>(sm, d, i0, j0, K + 3, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    load_plane_c<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
     if (valid) {
-      const char* sm_m = sm + ((K - 1) % NSLOT) * cslot_bytes<H>();
-      const char* sm_c = sm + (K % NSLOT) * cslot_bytes<H>();
-      const char* sm_p = sm + ((K + 1) % NSLOT) * cslot_bytes<H>();
+      constexpr int SB = cslot_bytes<H, TY>();
+      const char* sm_m = sm + ((K - 1) % NS) * SB;
+      const char* sm_c = sm + (K % NS) * SB;
+      const char* sm_p = sm + ((K + 1) % NS) * SB;
       const double* qm = reinterpret_cast<const double*>(sm_m);
       const double* qc = reinterpret_cast<const double*>(sm_c);
       const double* qp = reinterpret_cast<const double*>(sm_p);
@@ -471,7 +501,7 @@ __global__ void __launch_bounds__(256, 2) k_correct_pipe(
       v_ta[c] = (H)(dt * gy);
       w_ta[c] = (H)(dt * gz);
     }
-    cp_async_wait<1>();
+    cp_async_wait<F - 1>();
     __syncthreads();
   }
 }
@@ -513,14 +543,16 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
                          const H* vt, const H* wt, double* p, double* u, double* v, double* w,
                          H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
                          double dt, cudaStream_t s) {
-  dim3 block(TXW, TYW, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TYW - 1) / TYW, (d.nz + CKCHUNK - 1) / CKCHUNK);
-  size_t smem = (size_t)NSLOT * cslot_bytes<H>();
-  cudaFuncSetAttribute((const void*)k_correct_pipe<H>,
-                       cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  using Sh = CorrShape<H>;
+  constexpr int TY = Sh::TY, NS = Sh::NS;
+  dim3 block(TXW, TY, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + CKCHUNK - 1) / CKCHUNK);
+  size_t smem = (size_t)NS * cslot_bytes<H, TY>();
+  auto kern = k_correct_pipe<H, TY, NS, Sh::MINB>;
+  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
-  k_correct_pipe<H><<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,
-                                              w_ta, u_ep2, v_ep2, w_ep2, divu, dt);
+  kern<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,
+                                 v_ep2, w_ep2, divu, dt);
   long nf = (long)(d.ny + 1) * (d.nz + 1) + (long)d.nx * (d.nz + 1) + (long)d.nx * d.ny;
   count_launch();
   k_correct_faces<H><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(d, rg, PHI, ut, vt, wt, u, v,
