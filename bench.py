@@ -77,7 +77,9 @@ def algorithmic_bytes(nx, ny, nz):
         "y_T": 8 * N * 3,
         "x_T": 8 * N * 3,
         "z_T": 8 * N * 3,
-        "fft_x_fwd": 8 * N * 3 + 16 * Hs,   # read u*,v*,w*, write half spectrum
+        # read u*,v*,w*, write half spectrum (one unit: the divergence kernel
+        # and the x transform it feeds)
+        "fft_x_fwd": 8 * N * 3 + 16 * Hs,
         "fft_z_fwd": 2 * 16 * Hs,
         "spn": 2 * 16 * Hs,
         "fft_z_inv": 2 * 16 * Hs,

@@ -133,12 +133,15 @@ void adjoint_step(nse_adjoint* a, double* sg, double* const* rc, int l) {
     const int vdirs[3] = {1, 2, 0}, tdirs[3] = {1, 0, 2};
     const int* dirs = comp == 3 ? tdirs : vdirs;
     double* cbar = comp == 3 ? cb[0] : cb[comp + 1];
+    // scale for the last pass, then each solve's output scaling also
+    // prepares the input of the pass before it (one kernel between solves)
+    launch_adj_line_scale(D, g, dirs[2], comp, false, bar[comp], nullptr, nullptr, c1, nullptr,
+                          c.dt, c.eta, cs);
     for (int p = 2; p >= 0; --p) {
-      launch_adj_line_scale(D, g, dirs[p], comp, false, bar[comp], nullptr, nullptr, c1, nullptr,
-                            c.dt, c.eta, cs);
       ctx_line_solve(a->x, dirs[p], comp, bar[comp], cs);
       launch_adj_line_scale(D, g, dirs[p], comp, true, bar[comp], rc[4 * comp + p],
-                            rc[4 * comp + p + 1], c1, cbar, c.dt, c.eta, cs);
+                            rc[4 * comp + p + 1], c1, cbar, c.dt, c.eta, cs,
+                            p > 0 ? dirs[p - 1] : -1);
     }
     if (comp > 0) NSE_CUDA(cudaEventRecord(a->join[comp - 1], cs));
   }

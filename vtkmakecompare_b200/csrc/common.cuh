@@ -233,6 +233,12 @@ void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
                       const GridDev& g, double dt, int src_mode, cudaStream_t s,
                       const GridRcp* rg = nullptr, int j0 = 0, int nj = 0);
 void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 0, int nj = 0);
+// divergence right-hand side of mkp.f:90-97 (reciprocal spacings) into the
+// P2S sample layout of `out`, for the forward x pass in src_mode 0
+void launch_div_src(const Dims& d, const GridRcp& rg, const double* ut, const double* vt,
+                    const double* wt, double dt, double* out, cudaStream_t s);
+void launch_div_src32(const Dims& d, const GridRcp& rg, const float* ut, const float* vt,
+                      const float* wt, double dt, double* out, cudaStream_t s);
 
 void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s);
 // SPN pivot tables of the two-ended elimination (0 from spn_split: no

@@ -385,7 +385,9 @@ __global__ void k_adj_point(PArgs a) {
 // A = D^-1 (D + S) with D = diag(alpha_j w_j), A^T = D A D^-1 and
 // A^-T = D A^-1 D^-1: the transposed solve is the step's own line solve
 // between two diagonal scalings.  `out` = 0: xb /= alpha w (before the
-// solve); 1: rbar = alpha w y, c_bar += rbar dt eta / alpha (r - x).
+// solve); 1: rbar = alpha w y, c_bar += rbar dt eta / alpha (r - x), and
+// when the pass has a predecessor (next >= 0, its direction) the result is
+// scaled at once for that pass's solve: xb = rbar / (alpha w_next).
 struct SArgs {
   Dims D;
   AdjGrid g;
@@ -394,9 +396,15 @@ struct SArgs {
   const double* xout;
   const double* c1;
   double* cbar;
-  int dir, comp, out;
+  int dir, comp, out, next;
   double dte;  // dt * eta
 };
+
+// 1 / w of line direction `dir` for component `comp` at index idx
+__device__ __forceinline__ double line_rw(const AdjGrid& g, int dir, int comp, int idx) {
+  const bool wd = comp == 3 || (dir == 1 && comp != 1);
+  return wd ? g.r[dir][idx] : g.r12[dir][idx];
+}
 
 __global__ void k_adj_line_scale(SArgs a) {
   const Dims& D = a.D;
@@ -404,9 +412,8 @@ __global__ void k_adj_line_scale(SArgs a) {
   const int j = 1 + blockIdx.y;
   const int k = 1 + blockIdx.z;
   if (i > D.nx || (a.comp == 1 && j == D.ny)) return;
-  const int idx = a.dir == 0 ? i : (a.dir == 1 ? j : k);
-  const bool wd = a.comp == 3 || (a.dir == 1 && a.comp != 1);
-  const double rw = wd ? a.g.r[a.dir][idx] : a.g.r12[a.dir][idx];  // 1 / w
+  const int ijk[3] = {i, j, k};
+  const double rw = line_rw(a.g, a.dir, a.comp, ijk[a.dir]);  // 1 / w
   const double cm = face_mask(D, a.c1, a.comp, i, j, k);
   const double alpha = a.dte * cm + 1.0;
   const long c = D.P(i, j, k);
@@ -415,8 +422,13 @@ __global__ void k_adj_line_scale(SArgs a) {
     return;
   }
   const double rb = cm == 0.0 ? a.xb[c] / rw : alpha * a.xb[c] / rw;
-  a.xb[c] = rb;
   a.cbar[D.C(i, j, k)] += rb * (cm == 0.0 ? a.dte : a.dte / alpha) * (a.rin[c] - a.xout[c]);
+  if (a.next < 0) {
+    a.xb[c] = rb;
+    return;
+  }
+  const double rn = line_rw(a.g, a.next, a.comp, ijk[a.next]);
+  a.xb[c] = cm == 0.0 ? rb * rn : rb * rn / alpha;
 }
 
 // -------------------------------------------------------- MKP transposes --
@@ -828,10 +840,11 @@ void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
 
 void launch_adj_line_scale(const Dims& D, const AdjGrid& g, int dir, int comp, bool out,
                            double* xb, const double* rin, const double* xout, const double* c1,
-                           double* cbar, double dt, double eta, cudaStream_t s) {
+                           double* cbar, double dt, double eta, cudaStream_t s, int next) {
   SArgs a;
   a.D = D; a.g = g; a.xb = xb; a.rin = rin; a.xout = xout; a.c1 = c1; a.cbar = cbar;
-  a.dir = dir; a.comp = comp; a.out = out ? 1 : 0; a.dte = dt * eta;
+  a.dir = dir; a.comp = comp; a.out = out ? 1 : 0; a.next = out ? next : -1;
+  a.dte = dt * eta;
   count_launch();
   k_adj_line_scale<<<cell_grid(D, 128), 128, 0, s>>>(a);
 }

@@ -44,7 +44,7 @@ void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
 // before the solve, true after (with the mask gradient of the pass)
 void launch_adj_line_scale(const Dims& D, const AdjGrid& g, int dir, int comp, bool out,
                            double* xb, const double* rin, const double* xout, const double* c1,
-                           double* cbar, double dt, double eta, cudaStream_t s);
+                           double* cbar, double dt, double eta, cudaStream_t s, int next = -1);
 // MKP transposed: phi_bar at the P2S samples, transposed SPN/SP0B on the
 // spectrum, divergence transposed
 void launch_adj_phibar(const Dims& D, const AdjGrid& g, const double* const ub[3],

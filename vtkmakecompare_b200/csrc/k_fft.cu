@@ -216,6 +216,24 @@ __device__ __forceinline__ double div_rhs(const Dims& d, const FwdSrc<S>& q, int
   return (du / q.g.dx[I] + dv / q.g.dy[J] + dw / q.g.dz[K]) / q.dt;
 }
 
+// The divergence right-hand side on its own, written in the sample layout
+// the forward x pass reads in src_mode 0: out(i, J, k) for i = 0..nx-1,
+// J = 1..ny, k = 0..nz-1, with i = 0 standing for I = nx and k = 0 for
+// K = nz (the periodic wrap of P2S, p2s_fftw2d.f:5-30).  Split from the
+// transform because the fused pass holds six loads per sample in flight
+// for two rows at once and stays latency-bound (0.180 ms at 256x192x256);
+// this streaming kernel plus the plain transform take 0.145 ms, with
+// identical values (the same expression, evaluated once per cell).
+template <class S>
+__global__ void __launch_bounds__(128) k_div_src(Dims d, FwdSrc<S> q, double* __restrict__ out) {
+  const int i = blockIdx.x * blockDim.x + threadIdx.x;
+  const int J = 1 + blockIdx.y;
+  const int k = blockIdx.z;
+  if (i >= d.nx) return;
+  const int I = (i == 0) ? d.nx : i, K = (k == 0) ? d.nz : k;
+  out[d.P(i, J, k)] = div_rhs(d, q, I, J, K);
+}
+
 // ------------------------------------------------------------- x forward --
 // CTA: plane J (1..ny) and `npair` row pairs starting at row 2*npair*blockIdx.y
 template <class CT, class S>
@@ -1021,6 +1039,24 @@ void launch_fft_fwd_x(const PoissonPlan& pp, const Dims& d, const double* FP,
   fwd_x<double2, double>(pp, d, q, src_mode, s, j0, nj);
 }
 
+template <class S>
+static void div_src(const Dims& d, const GridRcp& rg, const S* ut, const S* vt, const S* wt,
+                    double dt, double* out, cudaStream_t s) {
+  FwdSrc<S> q{};
+  q.ut = ut; q.vt = vt; q.wt = wt; q.rg = rg; q.use_rcp = 1; q.dt = dt;
+  dim3 grid((d.nx + 127) / 128, d.ny, d.nz);
+  count_launch();
+  k_div_src<S><<<grid, 128, 0, s>>>(d, q, out);
+}
+void launch_div_src(const Dims& d, const GridRcp& rg, const double* ut, const double* vt,
+                    const double* wt, double dt, double* out, cudaStream_t s) {
+  div_src<double>(d, rg, ut, vt, wt, dt, out, s);
+}
+void launch_div_src32(const Dims& d, const GridRcp& rg, const float* ut, const float* vt,
+                      const float* wt, double dt, double* out, cudaStream_t s) {
+  div_src<float>(d, rg, ut, vt, wt, dt, out, s);
+}
+
 template <class CT>
 static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 0, int nj = 0) {
   if (nj <= 0) { j0 = 0; nj = pp.ny; }
@@ -1178,15 +1214,6 @@ void launch_fft_fwd_x_f32(const PoissonPlan& pp, const Dims& d, const GridDev& g
   q.ut = ut; q.vt = vt; q.wt = wt; q.g = g; q.rg = rg; q.use_rcp = 1; q.dt = dt;
   q.phi = phi; q.AC = pp.AC; q.rdx2 = 1.0 / (dx * dx); q.rdz2 = 1.0 / (dz * dz);
   fwd_x<float2, float>(pp, d, q, mode, s);
-}
-// FP64 transform of the divergence of FP32 fields (mixed form with the FP64
-// Poisson solve)
-void launch_fft_fwd_x_src32(const PoissonPlan& pp, const Dims& d, const GridRcp& rg,
-                            const float* ut, const float* vt, const float* wt, double dt,
-                            cudaStream_t s) {
-  FwdSrc<float> q{};
-  q.ut = ut; q.vt = vt; q.wt = wt; q.rg = rg; q.use_rcp = 1; q.dt = dt;
-  fwd_x<double2, float>(pp, d, q, 1, s);
 }
 void launch_fft_z_f32(const PoissonPlan& pp, bool inverse, cudaStream_t s) {
   fft_z<float2>(pp, inverse, s);

@@ -66,9 +66,7 @@ void launch_fft_fwd_x_f32(const PoissonPlan& pp, const Dims& d, const GridDev& g
                           const GridRcp& rg, const float* ut, const float* vt, const float* wt,
                           double dt, const double* phi, double dx, double dz, int mode,
                           cudaStream_t s);
-void launch_fft_fwd_x_src32(const PoissonPlan& pp, const Dims& d, const GridRcp& rg,
-                            const float* ut, const float* vt, const float* wt, double dt,
-                            cudaStream_t s);
+
 void launch_fft_z_f32(const PoissonPlan& pp, bool inverse, cudaStream_t s);
 void launch_spn_f32(const PoissonPlan& pp, cudaStream_t s);
 void launch_fft_inv_x_f32(const PoissonPlan& pp, const Dims& d, double* phi, bool accumulate,
@@ -1574,8 +1572,12 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
   const double dt = x->cfg.dt, dx = x->hdx[1], dz = x->hdz[1];
   const bool p64 = (x->cfg.flags & NSE_FLAG_POISSON64) != 0;
   mark(x, PH_FFTX_F);
-  if (p64) launch_fft_fwd_x_src32(pp, d, x->rg, ut, vt, wt, dt, s);
-  else launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, nullptr, dx, dz, 1, s);
+  if (p64) {
+    launch_div_src32(d, x->rg, ut, vt, wt, dt, phi, s);
+    launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+  } else {
+    launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, nullptr, dx, dz, 1, s);
+  }
   mark(x, PH_FFTZ_F);
   if (p64) launch_fft_z(pp, false, s);
   else launch_fft_z_f32(pp, false, s);
@@ -1616,7 +1618,13 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   const PoissonPlan& pp = x->pb.pp;
   const GridRcp* rg = (x->cfg.flags & NSE_FLAG_EXACT) ? nullptr : &x->rg;
   mark(x, PH_FFTX_F);
-  launch_fft_fwd_x(pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s, rg);
+  if (rg) {
+    // phi is free until the inverse x pass: it holds the divergence samples
+    launch_div_src(d, *rg, ut, vt, wt, x->cfg.dt, phi, s);
+    launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+  } else {
+    launch_fft_fwd_x(pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s, rg);
+  }
   mark(x, PH_FFTZ_F);
   launch_fft_z(pp, false, s);
   mark(x, PH_SPN);

@@ -9,7 +9,7 @@ Builds the penalised channel-with-sphere case of bench.py at the given size
 steps (or --poisson solves, or the discrete adjoint of --adjoint steps:
 checkpoints every half, wall flux averaged over the second half) and prints
 the wall time.  Kernel launches before the measured part: the level set
-(2*2001+1), the projection (8) and the warm-up steps (23 each).
+(2*2001+1), the projection (8) and the warm-up steps (24 each).
 """
 import argparse
 import math
