@@ -247,16 +247,49 @@ def replica_rate(ms_local, steps, world, device="cpu"):
     return ms_max, world * steps / (ms_max / 1e3)
 
 
-def run_ensemble(S, W, torch, stream, args):
+def shard_cases(n, rank, world):
+    """Indices of the ensemble cases of this rank: the n cases are dealt
+    round-robin over the world ranks (whole cases per GPU, no exchange while
+    they run)."""
+    return list(range(rank, n, world))
+
+
+def gather_case_scalars(local, n, width, world, device="cpu"):
+    """Per-case scalars of the whole ensemble in case order.  `local` maps
+    this rank's case indices to `width` floats; every case belongs to exactly
+    one rank, so one all-reduce (SUM) of an n x width tensor in which each
+    rank fills its own rows gathers them (gloo on CPU, nccl on the GPU)."""
+    import torch
+    t = torch.zeros((n, width), dtype=torch.float64)
+    for i, vals in local.items():
+        t[i] = torch.tensor(vals, dtype=torch.float64)
+    if world > 1:
+        import torch.distributed as dist
+        t = t.to(device)
+        dist.all_reduce(t, op=dist.ReduceOp.SUM)
+    return [tuple(float(x) for x in row) for row in t.cpu()]
+
+
+def run_ensemble(S, W, torch, stream, args, rank=0, world=1, device="cpu"):
     """Batched ensemble: args.ens_cases cases drawn by seed (grids among
     64^3..160x128x160, 1-3 spheres or cubes, Re_bulk in [1000, 5000], own
     noise), in FP64 and in the mixed form with the FP64 Poisson solve and FP64
     line arithmetic.  Aggregate case-steps/s of args.steps steps replayed from
     the captured graph on 8 streams, beside the same cases stepped one after
     the other on one stream; per-case error of the mixed form against FP64
-    after args.acc_steps steps."""
-    cases = [W.ensemble_case(7000 + i) for i in range(args.ens_cases)]
-    cells = sum(g["nx"] * g["ny"] * g["nz"] for g, *_ in cases)
+    after args.acc_steps steps.  With world > 1 the cases are sharded over the
+    ranks (shard_cases), the aggregate rate uses the slowest rank's time and
+    the per-case scalars are gathered (gather_case_scalars)."""
+    import torch.distributed as dist
+    mine = shard_cases(args.ens_cases, rank, world)
+    cases = [W.ensemble_case(7000 + i) for i in mine]
+
+    def slowest(x):
+        if world == 1:
+            return x
+        t = torch.tensor([x], dtype=torch.float64, device=device)
+        dist.all_reduce(t, op=dist.ReduceOp.MAX)
+        return float(t.item())
 
     def build(prec, flags):
         out = []
@@ -278,46 +311,63 @@ def run_ensemble(S, W, torch, stream, args):
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         torch.cuda.synchronize()
+        if world > 1:
+            dist.barrier()
         e0.record(stream)
         fn()
         e1.record(stream)
         torch.cuda.synchronize()
-        return e0.elapsed_time(e1)
+        return slowest(e0.elapsed_time(e1))
 
+    shapes = gather_case_scalars({i: (g["nx"], g["ny"], g["nz"]) for i, (g, *_) in zip(mine, cases)},
+                                 args.ens_cases, 3, world, device)
+    cells = int(sum(a * b * c for a, b, c in shapes))
     res = {"cases": args.ens_cases, "cells": cells,
-           "grids": sorted({(g["nx"], g["ny"], g["nz"]) for g, *_ in cases})}
+           "grids": sorted({tuple(int(x) for x in sh) for sh in shapes})}
+    if world > 1:
+        res["ranks"] = world
+        res["sharding"] = ("whole cases dealt round-robin over the ranks; aggregate rate over "
+                           "the slowest rank's time; per-case scalars gathered by one all-reduce")
     finals = {}
+    divs = {}
     for name, prec, flags in (("fp64", S.FP64, 0), ("mixed", S.MIXED, 16 | 64)):
         ctxs = build(prec, flags)
         for c in ctxs:
             c.set_stream(stream.cuda_stream)
             c.step(1)  # Euler start and the mask tables, outside the timing
         seq_ms = timed(lambda: [c.step(args.steps) for c in ctxs])
-        with S.Ensemble(ctxs, nstreams=8) as ens:
-            ens.set_stream(stream.cuda_stream)
-            ens.step(2)
-            ens.sync()
-            ms = timed(lambda: ens.step(args.steps))
-            ens.sync()
-            if args.acc_steps > 0:
-                ens.step(args.acc_steps - 1 - args.steps - 2)
+        if ctxs:
+            with S.Ensemble(ctxs, nstreams=8) as ens:
+                ens.set_stream(stream.cuda_stream)
+                ens.step(2)
                 ens.sync()
+                ms = timed(lambda: ens.step(args.steps))
+                ens.sync()
+                if args.acc_steps > 0:
+                    ens.step(args.acc_steps - 1 - args.steps - 2)
+                    ens.sync()
+        else:
+            ms = timed(lambda: None)
         finals[name] = [{k: c.download(k) for k in ("u", "v", "w", "T")} for c in ctxs]
-        divs = [c.monitor()["max_divu"] for c in ctxs]
+        divs[name] = {i: (c.monitor()["max_divu"],) for i, c in zip(mine, ctxs)}
         for c in ctxs:
             c.close()
+        div_all = gather_case_scalars(divs[name], args.ens_cases, 1, world, device)
         res[name] = {"case_steps_per_s": round(args.ens_cases * args.steps / (ms / 1e3), 1),
                      "cell_steps_per_s": round(cells * args.steps / (ms / 1e3), 1),
                      "sequential_case_steps_per_s":
                          round(args.ens_cases * args.steps / (seq_ms / 1e3), 1),
                      "graph_speedup_vs_sequential": round(seq_ms / ms, 3),
-                     "max_divu_at_end": max(divs)}
-    vel, tem = [], []
-    for a, b in zip(finals["mixed"], finals["fp64"]):
+                     "max_divu_at_end": max(d[0] for d in div_all)}
+    errs = {}
+    for i, a, b in zip(mine, finals["mixed"], finals["fp64"]):
         num = sum(np.linalg.norm(a[k] - b[k]) ** 2 for k in ("u", "v", "w"))
         den = sum(np.linalg.norm(b[k]) ** 2 for k in ("u", "v", "w"))
-        vel.append(math.sqrt(num / den))
-        tem.append(float(np.linalg.norm(a["T"] - b["T"]) / np.linalg.norm(b["T"])))
+        errs[i] = (math.sqrt(num / den),
+                   float(np.linalg.norm(a["T"] - b["T"]) / np.linalg.norm(b["T"])))
+    allerr = gather_case_scalars(errs, args.ens_cases, 2, world, device)
+    vel = [e[0] for e in allerr]
+    tem = [e[1] for e in allerr]
     # steps behind the comparison: 1 + steps (sequential) + 2 + steps + the rest
     res["mixed_vs_fp64_after_steps"] = 3 + 2 * args.steps + max(0, args.acc_steps - 3 - args.steps)
     res["mixed_velocity_rel_l2"] = {"max": max(vel), "median": float(np.median(vel))}
@@ -524,7 +574,7 @@ def run_ours(args, rank, world, local_rank):
     # ------------------------------------------------------- batched ensemble
     ensemble = None
     if args.ens_cases > 0:
-        ensemble = run_ensemble(S, W, torch, stream, args)
+        ensemble = run_ensemble(S, W, torch, stream, args, rank, world, dev)
 
     # ------------------------------------------------------ discrete adjoint
     adjoint = None
