@@ -88,6 +88,7 @@ def algorithmic_bytes(nx, ny, nz):
     }
 
 
+LINE_PHASES = ("y_vel", "z_vel", "x_vel", "y_T", "x_T", "z_T")
 LAUNCHES = {"set_bc": 1, "rhs": 1, "y_vel": 3, "z_vel": 3, "x_vel": 3, "y_T": 1, "x_T": 1,
             "z_T": 1, "set_bc_temp": 1, "fft_x_fwd": 1, "fft_z_fwd": 1, "spn": 1,
             "fft_z_inv": 1, "fft_x_inv": 1, "phibc": 2, "refine": 1, "correct": 1}
@@ -594,7 +595,13 @@ def run_ours(args, rank, world, local_rank):
     algo = algorithmic_bytes(NX, NY, NZ)
     peak, peak_kind = peaks()
     per_launch = {k: phases[k] / max(1, nprof) / LAUNCHES[k] for k in phases}
-    dominant = max((k for k in phases if k in algo), key=lambda k: phases[k])
+    # the fast form runs the four components' line chains on concurrent
+    # streams and reports the whole block (12 line passes) under y_vel: not
+    # one kernel, so it is left out of the dominant-kernel choice
+    concurrent_lines = all(phases[k] <= 0.05 * phases["y_vel"] for k in LINE_PHASES[1:])
+    dominant = max((k for k in phases
+                    if k in algo and not (concurrent_lines and k in LINE_PHASES)),
+                   key=lambda k: phases[k])
     t_launch_s = per_launch[dominant] / 1e3
     achieved = algo[dominant] / t_launch_s / 1e9
     traffic = dram_traffic().get(dominant)
@@ -633,6 +640,9 @@ def run_ours(args, rank, world, local_rank):
                      "algorithmic_bytes_per_launch": algo[dominant],
                      "ms_per_launch": round(per_launch[dominant], 4)},
         "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()},
+        "phases_note": ("the line passes of u, v, w and T run as four concurrent chains; "
+                        "y_vel holds the whole line block" if concurrent_lines else
+                        "line passes in serial order, one phase per direction"),
         "gpu_launches": int(launches),
         "levelset_setup_s": round(ls_s, 3),
         "clocks": clk.summary(),

@@ -234,8 +234,11 @@ enum {
                                 FP32 solve with refinement */
   NSE_FLAG_MATH64 = 32,      /* NSE_MIXED: FP64 arithmetic in the right-hand-side stencils
                                 (their results are still stored in FP32) */
-  NSE_FLAG_LINES64 = 64      /* NSE_MIXED: FP64 arithmetic and tables in the line sweeps
+  NSE_FLAG_LINES64 = 64,     /* NSE_MIXED: FP64 arithmetic and tables in the line sweeps
                                 (FP32 storage) */
+  NSE_FLAG_SERIAL_LINES = 128 /* line passes of u, v, w, T one after another on the context's
+                                 stream (default: the four chains on concurrent streams);
+                                 per-phase times then split the line passes by direction */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

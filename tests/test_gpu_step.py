@@ -225,3 +225,27 @@ def test_projection_is_divergence_free():
             mon = ctx.monitor()
             assert mon["max_divu"] < 1e-10, (prec, mon)
 
+
+
+@pytest.mark.parametrize("prec,base", [(S.FP64, 0), (S.MIXED, 0), (S.MIXED, S.FLAG_POISSON64)])
+@pytest.mark.parametrize("n", [(96, 48, 64), (128, 40, 96)])
+def test_concurrent_line_chains_equal_serial(n, prec, base):
+    """The fast and mixed forms run the four components' line chains on
+    concurrent streams; every field after 4 steps is bit-identical to the
+    serial order (NSE_FLAG_SERIAL_LINES)."""
+    g, f, c1, par = make_case(*n)
+    out = []
+    for flags in (base, base | S.FLAG_SERIAL_LINES):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"], precision=prec, flags=flags)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.start()
+            ctx.step(4)
+            out.append({k: ctx.download(k) for k in STATE})
+    for k in STATE:
+        assert np.array_equal(out[0][k], out[1][k]), k

@@ -1182,6 +1182,10 @@ struct nse_ctx {
   // rec[4*comp + pass] and the final line output to rec[4*comp + 3]
   // (comp 0 u, 1 v, 2 w, 3 T; velocity passes y, z, x; temperature y, x, z)
   double* const* rec = nullptr;
+  // side streams of the line passes (FP64 fast form): v, w and T run their
+  // y/z/x chains beside u's, forked from and joined back into `stream`
+  cudaStream_t side[3] = {};
+  cudaEvent_t lfork = nullptr, ljoin[3] = {};
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1350,6 +1354,16 @@ static void mark(nse_ctx* x, int phase) {
   cudaEventRecord(x->ev[(size_t)x->prof_n * (PH_COUNT + 1) + phase], x->stream);
 }
 
+// the side streams and events of the concurrent line passes (made on first use)
+static bool ensure_side(nse_ctx* x) {
+  if (x->lfork) return true;
+  for (int q = 0; q < 3; ++q)
+    if (!NSE_CUDA(cudaStreamCreateWithFlags(&x->side[q], cudaStreamNonBlocking)) ||
+        !NSE_CUDA(cudaEventCreateWithFlags(&x->ljoin[q], cudaEventDisableTiming)))
+      return false;
+  return NSE_CUDA(cudaEventCreateWithFlags(&x->lfork, cudaEventDisableTiming));
+}
+
 static double* F(nse_ctx* c, int id) { return c->f[id].as<double>(); }
 static float* F32(nse_ctx* c, int id) { return c->f[id].as<float>(); }
 // fields held in FP32 by the mixed-precision form
@@ -1472,6 +1486,14 @@ int nse_ctx_destroy(nse_ctx* x) {
       x->pmtab_f[dir][comp].release();
     }
   for (cudaEvent_t e : x->ev) cudaEventDestroy(e);
+  for (int q = 0; q < 3; ++q) {
+    if (x->side[q]) {
+      cudaStreamSynchronize(x->side[q]);
+      cudaStreamDestroy(x->side[q]);
+    }
+    if (x->ljoin[q]) cudaEventDestroy(x->ljoin[q]);
+  }
+  if (x->lfork) cudaEventDestroy(x->lfork);
   if (x->own) cudaStreamDestroy(x->own);
   delete x;
   return NSE_OK;
@@ -1716,7 +1738,8 @@ static void ctx_step_f32(nse_ctx* x) {
                  F32(x, NSE_T_PRE), c1, ua, va, wa, uT, x->math64, s);
   refresh_line_flags(x, s);
   float* fa[3] = {ua, va, wa};
-  auto run = [&](int dir, int comp, float* f, double* out, double ft, double fb) {
+  auto run_on = [&](cudaStream_t st, int dir, int comp, float* f, double* out, double ft,
+                    double fb) {
     LineArgs la = line_args(x, comp);
     la.ft = ft;
     la.fb = fb;
@@ -1725,22 +1748,46 @@ static void ctx_step_f32(nse_ctx* x) {
                           x->ids[dir][comp].as<int>(), x->nmasked[dir][comp],
                           x->pmtab_f[dir][comp].as<float>(),
                           x->lines64 ? x->ptab[dir][comp].as<double>() : nullptr,
-                          x->lines64 ? x->pmtab[dir][comp].as<double>() : nullptr, s);
+                          x->lines64 ? x->pmtab[dir][comp].as<double>() : nullptr, st);
   };
-  mark(x, PH_YVEL);
-  for (int comp = 0; comp < 3; ++comp) run(1, comp, fa[comp], nullptr, 0.0, 0.0);
-  mark(x, PH_ZVEL);
-  for (int comp = 0; comp < 3; ++comp) run(2, comp, fa[comp], nullptr, 0.0, 0.0);
-  mark(x, PH_XVEL);
-  for (int comp = 0; comp < 3; ++comp) run(0, comp, fa[comp], nullptr, 0.0, 0.0);
-  // solve_t: y, x, z; the z sweep writes the new temperature (interior) to
-  // the FP64 state
-  mark(x, PH_YT);
-  run(1, 3, uT, nullptr, 2.0 * c.t_bot, 2.0 * c.t_top);
-  mark(x, PH_XT);
-  run(0, 3, uT, nullptr, 0.0, 0.0);
-  mark(x, PH_ZT);
-  run(2, 3, uT, T, 0.0, 0.0);
+  auto run = [&](int dir, int comp, float* f, double* out, double ft, double fb) {
+    run_on(s, dir, comp, f, out, ft, fb);
+  };
+  // the four components' chains on concurrent streams, as in the FP64 form
+  if (!(c.flags & NSE_FLAG_SERIAL_LINES) && ensure_side(x)) {
+    mark(x, PH_YVEL);
+    NSE_CUDA(cudaEventRecord(x->lfork, s));
+    for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(x->side[q], x->lfork, 0));
+    cudaStream_t cs[4] = {s, x->side[0], x->side[1], x->side[2]};
+    for (int comp = 0; comp < 3; ++comp) {
+      run_on(cs[comp], 1, comp, fa[comp], nullptr, 0.0, 0.0);
+      run_on(cs[comp], 2, comp, fa[comp], nullptr, 0.0, 0.0);
+      run_on(cs[comp], 0, comp, fa[comp], nullptr, 0.0, 0.0);
+    }
+    run_on(cs[3], 1, 3, uT, nullptr, 2.0 * c.t_bot, 2.0 * c.t_top);
+    run_on(cs[3], 0, 3, uT, nullptr, 0.0, 0.0);
+    run_on(cs[3], 2, 3, uT, T, 0.0, 0.0);
+    for (int q = 0; q < 3; ++q) {
+      NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
+      NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
+    }
+    for (int ph = PH_ZVEL; ph <= PH_ZT; ++ph) mark(x, ph);
+  } else {
+    mark(x, PH_YVEL);
+    for (int comp = 0; comp < 3; ++comp) run(1, comp, fa[comp], nullptr, 0.0, 0.0);
+    mark(x, PH_ZVEL);
+    for (int comp = 0; comp < 3; ++comp) run(2, comp, fa[comp], nullptr, 0.0, 0.0);
+    mark(x, PH_XVEL);
+    for (int comp = 0; comp < 3; ++comp) run(0, comp, fa[comp], nullptr, 0.0, 0.0);
+    // solve_t: y, x, z; the z sweep writes the new temperature (interior) to
+    // the FP64 state
+    mark(x, PH_YT);
+    run(1, 3, uT, nullptr, 2.0 * c.t_bot, 2.0 * c.t_top);
+    mark(x, PH_XT);
+    run(0, 3, uT, nullptr, 0.0, 0.0);
+    mark(x, PH_ZT);
+    run(2, 3, uT, T, 0.0, 0.0);
+  }
   mark(x, PH_BC2);
   launch_set_bc_f32(d, ua, va, wa, p, T, c.t_bot, c.t_top, 31, s);
   ctx_mkp_f32(x, ua, va, wa);
@@ -1794,7 +1841,8 @@ static void ctx_step(nse_ctx* x) {
     if (x->rec)
       NSE_CUDA(cudaMemcpyAsync(x->rec[4 * comp + pass], f, fbytes, cudaMemcpyDeviceToDevice, s));
   };
-  auto run = [&](int dir, int comp, double* f, int tab, double ft, double fb) {
+  auto run_on = [&](cudaStream_t st, int dir, int comp, double* f, int tab, double ft,
+                    double fb) {
     record(comp, comp == 3 ? (dir == 1 ? 0 : (dir == 0 ? 1 : 2)) : (dir == 1 ? 0 : (dir == 2 ? 1 : 2)),
            f);
     LineArgs la = line_args(x, comp);
@@ -1803,11 +1851,46 @@ static void ctx_step(nse_ctx* x) {
     if (x->part)
       launch_lines_part(dir, line_kind(dir, comp), d, f, la, x->ptab[dir][comp].as<double>(),
                         x->slots[dir][comp].as<int>(), x->ids[dir][comp].as<int>(),
-                        x->nmasked[dir][comp], x->pmtab[dir][comp].as<double>(), s);
+                        x->nmasked[dir][comp], x->pmtab[dir][comp].as<double>(), st);
     else
       lines(dir, line_kind(dir, comp), d, f, la, x->tab[tab], x->slots[dir][comp].as<int>(),
-            x->mtab[dir][comp].as<double>(), s);
+            x->mtab[dir][comp].as<double>(), st);
   };
+  auto run = [&](int dir, int comp, double* f, int tab, double ft, double fb) {
+    run_on(s, dir, comp, f, tab, ft, fb);
+  };
+  // The four components' chains are independent (each pass reads and writes
+  // its own field with read-only tables): u on the context's stream, v, w
+  // and T on side streams.  The line phases are then one block: its time
+  // is reported under y_vel.  Adjoint recording and NSE_FLAG_SERIAL_LINES
+  // keep the serial order.
+  if (x->part && !exact && !x->rec && !(c.flags & NSE_FLAG_SERIAL_LINES) && ensure_side(x)) {
+    mark(x, PH_YVEL);
+    NSE_CUDA(cudaEventRecord(x->lfork, s));
+    for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(x->side[q], x->lfork, 0));
+    cudaStream_t cs[4] = {s, x->side[0], x->side[1], x->side[2]};
+    for (int comp = 0; comp < 3; ++comp) {
+      run_on(cs[comp], 1, comp, fa[comp], comp == 1 ? TB_Y_V : TB_Y_U, 0.0, 0.0);
+      run_on(cs[comp], 2, comp, fa[comp], TB_Z_V, 0.0, 0.0);
+      run_on(cs[comp], 0, comp, fa[comp], TB_X_V, 0.0, 0.0);
+    }
+    run_on(cs[3], 1, 3, uT, TB_Y_T, 2.0 * c.t_bot, 2.0 * c.t_top);
+    run_on(cs[3], 0, 3, uT, TB_X_T, 0.0, 0.0);
+    run_on(cs[3], 2, 3, uT, TB_Z_T, 0.0, 0.0);
+    for (int q = 0; q < 3; ++q) {
+      NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
+      NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
+    }
+    for (int ph = PH_ZVEL; ph <= PH_ZT; ++ph) mark(x, ph);
+    std::swap(x->f[NSE_T], x->uT);
+    T = F(x, NSE_T);
+    mark(x, PH_BC2);
+    launch_set_bc(d, ua, va, wa, p, T, c.t_bot, c.t_top, 31, s);
+    ctx_mkp(x, ua, va, wa);
+    if (x->prof_n < x->prof_cap) x->prof_n++;
+    x->l += 1;
+    return;
+  }
   mark(x, PH_YVEL);
   for (int comp = 0; comp < 3; ++comp)
     run(1, comp, fa[comp], comp == 1 ? TB_Y_V : TB_Y_U, 0.0, 0.0);
