@@ -202,7 +202,6 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
         with torch.cuda.stream(stream):
             ctx.step(args.warmup)
         torch.cuda.synchronize()
-        ctx.profile(args.steps)
         e0 = torch.cuda.Event(enable_timing=True)
         e1 = torch.cuda.Event(enable_timing=True)
         e0.record(stream)
@@ -210,6 +209,12 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
         e1.record(stream)
         torch.cuda.synchronize()
         ms = e0.elapsed_time(e1)
+        # per-phase times from as many further steps with the phase events on
+        # (the events themselves cost a few microseconds each, so they stay
+        # out of the timed steps)
+        ctx.profile(args.steps)
+        ctx.step(args.steps)
+        torch.cuda.synchronize()
         phases, nprof = ctx.phase_times()
         ctx.close()
         rec = {"steps_per_s": round(args.steps / (ms / 1e3), 3),
@@ -491,7 +496,6 @@ def run_ours(args, rank, world, local_rank):
         ctx.step(args.warmup)
     torch.cuda.synchronize()
     barrier()
-    ctx.profile(args.steps)
     n0 = S.launch_count()
     e0 = torch.cuda.Event(enable_timing=True)
     e1 = torch.cuda.Event(enable_timing=True)
@@ -505,9 +509,15 @@ def run_ours(args, rank, world, local_rank):
         barrier()
     launches = S.launch_count() - n0
     ms = e0.elapsed_time(e1)
-    phases, nprof = ctx.phase_times()
     ms_max, steps_s = replica_rate(ms, args.steps, world, dev)
     mon = ctx.monitor()
+    # per-phase times (roofline, phases_ms_per_step) from K further steps with
+    # the phase events on, outside the timed region
+    ctx.profile(args.steps)
+    with torch.cuda.stream(stream):
+        ctx.step(args.steps)
+    torch.cuda.synchronize()
+    phases, nprof = ctx.phase_times()
 
     # ---------------------------------------------------------- Poisson solve
     ctx.upload("phi", W.poisson_rhs(g, 7))

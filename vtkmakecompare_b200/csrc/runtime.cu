@@ -1767,11 +1767,18 @@ static void ctx_step_f32(nse_ctx* x) {
     run_on(cs[3], 1, 3, uT, nullptr, 2.0 * c.t_bot, 2.0 * c.t_top);
     run_on(cs[3], 0, 3, uT, nullptr, 0.0, 0.0);
     run_on(cs[3], 2, 3, uT, T, 0.0, 0.0);
-    for (int q = 0; q < 3; ++q) {
-      NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
-      NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
-    }
+    // the temperature chain sets T's ghosts itself and rejoins after MKP
+    launch_set_bc_f32(d, nullptr, nullptr, nullptr, nullptr, T, c.t_bot, c.t_top, 16, cs[3]);
+    for (int q = 0; q < 3; ++q) NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
+    for (int q = 0; q < 2; ++q) NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
     for (int ph = PH_ZVEL; ph <= PH_ZT; ++ph) mark(x, ph);
+    mark(x, PH_BC2);
+    launch_set_bc_f32(d, ua, va, wa, p, T, c.t_bot, c.t_top, 1 | 2 | 4 | 8, s);
+    ctx_mkp_f32(x, ua, va, wa);
+    NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[2], 0));
+    if (x->prof_n < x->prof_cap) x->prof_n++;
+    x->l += 1;
+    return;
   } else {
     mark(x, PH_YVEL);
     for (int comp = 0; comp < 3; ++comp) run(1, comp, fa[comp], nullptr, 0.0, 0.0);
@@ -1877,16 +1884,19 @@ static void ctx_step(nse_ctx* x) {
     run_on(cs[3], 1, 3, uT, TB_Y_T, 2.0 * c.t_bot, 2.0 * c.t_top);
     run_on(cs[3], 0, 3, uT, TB_X_T, 0.0, 0.0);
     run_on(cs[3], 2, 3, uT, TB_Z_T, 0.0, 0.0);
-    for (int q = 0; q < 3; ++q) {
-      NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
-      NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
-    }
-    for (int ph = PH_ZVEL; ph <= PH_ZT; ++ph) mark(x, ph);
     std::swap(x->f[NSE_T], x->uT);
     T = F(x, NSE_T);
+    // MKP needs u*, v*, w* only: the temperature chain also sets T's ghosts
+    // (the T part of set_bc, which reads interior cells only) and rejoins
+    // at the end of the step, so it overlaps the projection
+    launch_set_bc(d, nullptr, nullptr, nullptr, nullptr, T, c.t_bot, c.t_top, 16, cs[3]);
+    for (int q = 0; q < 3; ++q) NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
+    for (int q = 0; q < 2; ++q) NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
+    for (int ph = PH_ZVEL; ph <= PH_ZT; ++ph) mark(x, ph);
     mark(x, PH_BC2);
-    launch_set_bc(d, ua, va, wa, p, T, c.t_bot, c.t_top, 31, s);
+    launch_set_bc(d, ua, va, wa, p, T, c.t_bot, c.t_top, 1 | 2 | 4 | 8, s);
     ctx_mkp(x, ua, va, wa);
+    NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[2], 0));
     if (x->prof_n < x->prof_cap) x->prof_n++;
     x->l += 1;
     return;
