@@ -652,7 +652,9 @@ def run_ours(args, rank, world, local_rank):
         "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()},
         "phases_note": ("the line passes of u, v, w and T run as four concurrent chains; "
                         "y_vel holds the whole line block" if concurrent_lines else
-                        "line passes in serial order, one phase per direction"),
+                        "from K further steps with the phase events on, which run every "
+                        "pass on one stream in order; the timed steps run the four line "
+                        "chains and the two halves of the transforms concurrently"),
         "gpu_launches": int(launches),
         "levelset_setup_s": round(ls_s, 3),
         "clocks": clk.summary(),

@@ -236,9 +236,10 @@ enum {
                                 (their results are still stored in FP32) */
   NSE_FLAG_LINES64 = 64,     /* NSE_MIXED: FP64 arithmetic and tables in the line sweeps
                                 (FP32 storage) */
-  NSE_FLAG_SERIAL_LINES = 128 /* line passes of u, v, w, T one after another on the context's
-                                 stream (default: the four chains on concurrent streams);
-                                 per-phase times then split the line passes by direction */
+  NSE_FLAG_ONE_STREAM = 128  /* everything on the context's stream, in the reference's
+                                order (default: the line passes of u, v, w, T as four
+                                concurrent chains and the FFT passes of the Poisson solve in
+                                two halves of the planes on two streams; same results) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

@@ -232,10 +232,10 @@ def test_projection_is_divergence_free():
 def test_concurrent_line_chains_equal_serial(n, prec, base):
     """The fast and mixed forms run the four components' line chains on
     concurrent streams; every field after 4 steps is bit-identical to the
-    serial order (NSE_FLAG_SERIAL_LINES)."""
+    order on one stream (NSE_FLAG_ONE_STREAM)."""
     g, f, c1, par = make_case(*n)
     out = []
-    for flags in (base, base | S.FLAG_SERIAL_LINES):
+    for flags in (base, base | S.FLAG_ONE_STREAM):
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                        g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
                        body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],

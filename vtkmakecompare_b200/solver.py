@@ -23,7 +23,7 @@ FLAG_REFINE2 = 8
 FLAG_POISSON64 = 16
 FLAG_MATH64 = 32
 FLAG_LINES64 = 64
-FLAG_SERIAL_LINES = 128
+FLAG_ONE_STREAM = 128
 
 
 class Config(C.Structure):
@@ -221,7 +221,7 @@ class Context:
                 "T_int": out[4], "nonfinite": int(out[5])}
 
 
-__all__ = ["Config", "Context", "FIELDS", "FP64", "MIXED", "FLAG_CHECK_FINITE", "FLAG_EXACT", "FLAG_SERIAL_LINES",
+__all__ = ["Config", "Context", "FIELDS", "FP64", "MIXED", "FLAG_CHECK_FINITE", "FLAG_EXACT", "FLAG_ONE_STREAM",
            "NseError"]
 
 
