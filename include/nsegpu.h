@@ -300,7 +300,9 @@ int nse_sync(nse_ctx* ctx);
  * summed milliseconds over the profiled steps; phases in launch order:
  * set_bc, rhs, y-lines u/v/w, z-lines u/v/w, x-lines u/v/w, T y, T x, T z,
  * set_bc(u_temp), fft x fwd, fft z fwd, spn+sp0b, fft z inv, fft x inv,
- * phibc, refinement (mixed form), correction (17 phases). */
+ * phibc, refinement (mixed form), correction (17 phases).  Profiled steps
+ * run every pass in order on the context's stream (no side streams), so each
+ * phase is timed on its own. */
 int nse_ctx_profile(nse_ctx* ctx, int max_steps);
 int nse_ctx_phase_times(nse_ctx* ctx, double* ms, int nphase, int* nsteps);
 /* Ensemble (no counterpart in the reference): independent cases, each a

@@ -188,7 +188,8 @@ class Context:
         return out
 
     def profile(self, max_steps):
-        """Record CUDA events around every phase of the next max_steps steps."""
+        """Record CUDA events around every phase of the next max_steps steps
+        (those steps run every pass in order on the context's stream)."""
         check(self.L.nse_ctx_profile(self.h, int(max_steps)))
 
     def phase_times(self):
