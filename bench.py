@@ -654,7 +654,7 @@ def run_ours(args, rank, world, local_rank):
                         "y_vel holds the whole line block" if concurrent_lines else
                         "from K further steps with the phase events on, which run every "
                         "pass on one stream in order; the timed steps run the four line "
-                        "chains and the two halves of the transforms concurrently"),
+                        "chains concurrently"),
         "gpu_launches": int(launches),
         "levelset_setup_s": round(ls_s, 3),
         "clocks": clk.summary(),

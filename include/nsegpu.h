@@ -238,8 +238,7 @@ enum {
                                 (FP32 storage) */
   NSE_FLAG_ONE_STREAM = 128  /* everything on the context's stream, in the reference's
                                 order (default: the line passes of u, v, w, T as four
-                                concurrent chains and the FFT passes of the Poisson solve in
-                                two halves of the planes on two streams; same results) */
+                                concurrent chains on side streams; same results) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

@@ -250,19 +250,3 @@ def test_concurrent_line_chains_equal_serial(n, prec, base):
     for k in STATE:
         assert np.array_equal(out[0][k], out[1][k]), k
 
-
-def test_poisson_halves_equal_one_stream():
-    """nse_poisson runs its x and z passes as two halves of the planes on two
-    streams; the solution is bit-identical to the one-stream order."""
-    n = (128, 40, 96)
-    g, f, c1, par = make_case(*n, sphere=False)
-    rhs = W.poisson_rhs(g, 5)
-    out = []
-    for flags in (0, S.FLAG_ONE_STREAM):
-        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
-                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0, flags=flags)
-        with S.Context(cfg) as ctx:
-            ctx.upload("phi", rhs)
-            ctx.poisson()
-            out.append(ctx.download("phi"))
-    assert np.array_equal(out[0], out[1])

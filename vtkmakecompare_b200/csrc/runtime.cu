@@ -1186,7 +1186,6 @@ struct nse_ctx {
   // y/z/x chains beside u's, forked from and joined back into `stream`
   cudaStream_t side[3] = {};
   cudaEvent_t lfork = nullptr, ljoin[3] = {};
-  cudaEvent_t pfork = nullptr, pjoin = nullptr;  // halves of the Poisson transforms
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1362,42 +1361,16 @@ static bool ensure_side(nse_ctx* x) {
     if (!NSE_CUDA(cudaStreamCreateWithFlags(&x->side[q], cudaStreamNonBlocking)) ||
         !NSE_CUDA(cudaEventCreateWithFlags(&x->ljoin[q], cudaEventDisableTiming)))
       return false;
-  return NSE_CUDA(cudaEventCreateWithFlags(&x->pfork, cudaEventDisableTiming)) &&
-         NSE_CUDA(cudaEventCreateWithFlags(&x->pjoin, cudaEventDisableTiming)) &&
-         NSE_CUDA(cudaEventCreateWithFlags(&x->lfork, cudaEventDisableTiming));
+  return NSE_CUDA(cudaEventCreateWithFlags(&x->lfork, cudaEventDisableTiming));
 }
 
-// the concurrent forms (line chains on side streams, transform halves):
-// not with NSE_FLAG_ONE_STREAM, and not in profiled steps, whose phases are
+// the concurrent form (line chains on side streams): not with
+// NSE_FLAG_ONE_STREAM, and not in profiled steps, whose phases are
 // timed one after another on the context's stream
 static bool concurrent(nse_ctx* x) {
   return !(x->cfg.flags & NSE_FLAG_ONE_STREAM) && x->prof_n >= x->prof_cap && ensure_side(x);
 }
 
-// FP64 x and z passes of the Poisson solve: the passes of a window of planes
-// J depend on nothing outside it, so the two halves of the planes run on
-// the context's stream and side stream 0 and one half's z pass overlaps the
-// other half's x pass (inverse: z then x)
-static void poisson_halves(nse_ctx* x, double* phi, bool inverse, cudaStream_t s) {
-  const PoissonPlan& pp = x->pb.pp;
-  const int h = pp.ny / 2;
-  NSE_CUDA(cudaEventRecord(x->pfork, s));
-  NSE_CUDA(cudaStreamWaitEvent(x->side[0], x->pfork, 0));
-  for (int q = 0; q < 2; ++q) {
-    cudaStream_t st = q == 0 ? s : x->side[0];
-    const int j0 = q == 0 ? 0 : h, nj = q == 0 ? h : pp.ny - h;
-    if (!inverse) {
-      launch_fft_fwd_x(pp, x->d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, st, nullptr,
-                       j0, nj);
-      launch_fft_z(pp, false, st, j0, nj);
-    } else {
-      launch_fft_z(pp, true, st, j0, nj);
-      launch_fft_inv_x(pp, x->d, phi, st, j0, nj);
-    }
-  }
-  NSE_CUDA(cudaEventRecord(x->pjoin, x->side[0]));
-  NSE_CUDA(cudaStreamWaitEvent(s, x->pjoin, 0));
-}
 
 static double* F(nse_ctx* c, int id) { return c->f[id].as<double>(); }
 static float* F32(nse_ctx* c, int id) { return c->f[id].as<float>(); }
@@ -1529,8 +1502,6 @@ int nse_ctx_destroy(nse_ctx* x) {
     if (x->ljoin[q]) cudaEventDestroy(x->ljoin[q]);
   }
   if (x->lfork) cudaEventDestroy(x->lfork);
-  if (x->pfork) cudaEventDestroy(x->pfork);
-  if (x->pjoin) cudaEventDestroy(x->pjoin);
   if (x->own) cudaStreamDestroy(x->own);
   delete x;
   return NSE_OK;
@@ -1631,27 +1602,24 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
   const double dt = x->cfg.dt, dx = x->hdx[1], dz = x->hdz[1];
   const bool p64 = (x->cfg.flags & NSE_FLAG_POISSON64) != 0;
   mark(x, PH_FFTX_F);
-  const bool halves = p64 && pp.ny >= 2 && concurrent(x);
   if (p64) {
     launch_div_src32(d, x->rg, ut, vt, wt, dt, phi, s);
-    if (halves) poisson_halves(x, phi, false, s);
-    else launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+    launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
   } else {
     launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, nullptr, dx, dz, 1, s);
   }
   mark(x, PH_FFTZ_F);
-  if (p64 && !halves) launch_fft_z(pp, false, s);
-  else if (!p64) launch_fft_z_f32(pp, false, s);
+  if (p64) launch_fft_z(pp, false, s);
+  else launch_fft_z_f32(pp, false, s);
   mark(x, PH_SPN);
   if (p64) launch_spn_fast(pp, s);
   else launch_spn_fast_f32(pp, s);
   mark(x, PH_FFTZ_I);
-  if (halves) poisson_halves(x, phi, true, s);
-  else if (p64) launch_fft_z(pp, true, s);
+  if (p64) launch_fft_z(pp, true, s);
   else launch_fft_z_f32(pp, true, s);
   mark(x, PH_FFTX_I);
-  if (p64 && !halves) launch_fft_inv_x(pp, d, phi, s);
-  else if (!p64) launch_fft_inv_x_f32(pp, d, phi, false, s);
+  if (p64) launch_fft_inv_x(pp, d, phi, s);
+  else launch_fft_inv_x_f32(pp, d, phi, false, s);
   mark(x, PH_PHIBC);
   launch_phibc(d, phi, s);
   mark(x, PH_REFINE);
@@ -1680,28 +1648,21 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   const PoissonPlan& pp = x->pb.pp;
   const GridRcp* rg = (x->cfg.flags & NSE_FLAG_EXACT) ? nullptr : &x->rg;
   mark(x, PH_FFTX_F);
-  const bool halves = rg && pp.ny >= 2 && concurrent(x);
   if (rg) {
     // phi is free until the inverse x pass: it holds the divergence samples
     launch_div_src(d, *rg, ut, vt, wt, x->cfg.dt, phi, s);
-    if (!halves) launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+    launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
   } else {
     launch_fft_fwd_x(pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s, rg);
   }
-  if (halves) poisson_halves(x, phi, false, s);
   mark(x, PH_FFTZ_F);
-  if (!halves) launch_fft_z(pp, false, s);
+  launch_fft_z(pp, false, s);
   mark(x, PH_SPN);
   launch_spn_fast(pp, s);
   mark(x, PH_FFTZ_I);
-  if (halves) {
-    poisson_halves(x, phi, true, s);
-  } else {
-    launch_fft_z(pp, true, s);
-    mark(x, PH_FFTX_I);
-    launch_fft_inv_x(pp, d, phi, s);
-  }
-  if (halves) mark(x, PH_FFTX_I);
+  launch_fft_z(pp, true, s);
+  mark(x, PH_FFTX_I);
+  launch_fft_inv_x(pp, d, phi, s);
   mark(x, PH_PHIBC);
   launch_phibc(d, phi, s);
   mark(x, PH_REFINE);
@@ -1752,17 +1713,11 @@ int nse_poisson(nse_ctx* x) {
   cudaStream_t s = x->stream;
   double* phi = F(x, NSE_PHI);
   const PoissonPlan& pp = x->pb.pp;
-  if (pp.ny >= 2 && concurrent(x)) {
-    poisson_halves(x, phi, false, s);
-    launch_spn_fast(pp, s);
-    poisson_halves(x, phi, true, s);
-  } else {
-    launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
-    launch_fft_z(pp, false, s);
-    launch_spn_fast(pp, s);
-    launch_fft_z(pp, true, s);
-    launch_fft_inv_x(pp, d, phi, s);
-  }
+  launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+  launch_fft_z(pp, false, s);
+  launch_spn_fast(pp, s);
+  launch_fft_z(pp, true, s);
+  launch_fft_inv_x(pp, d, phi, s);
   launch_phibc(d, phi, s);
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
