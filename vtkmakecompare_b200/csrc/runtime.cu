@@ -1852,14 +1852,17 @@ static void ctx_step(nse_ctx* x) {
   auto lines = exact ? launch_lines_exact : launch_lines_fast;
   double* fa[3] = {ua, va, wa};
   size_t fbytes = d.ntot * sizeof(double);
-  auto record = [&](int comp, int pass, const double* f) {
+  // (on the stream of the component's chain, so each copy sees its pass's input)
+  auto record_on = [&](cudaStream_t st, int comp, int pass, const double* f) {
     if (x->rec)
-      NSE_CUDA(cudaMemcpyAsync(x->rec[4 * comp + pass], f, fbytes, cudaMemcpyDeviceToDevice, s));
+      NSE_CUDA(cudaMemcpyAsync(x->rec[4 * comp + pass], f, fbytes, cudaMemcpyDeviceToDevice, st));
   };
+  auto record = [&](int comp, int pass, const double* f) { record_on(s, comp, pass, f); };
   auto run_on = [&](cudaStream_t st, int dir, int comp, double* f, int tab, double ft,
                     double fb) {
-    record(comp, comp == 3 ? (dir == 1 ? 0 : (dir == 0 ? 1 : 2)) : (dir == 1 ? 0 : (dir == 2 ? 1 : 2)),
-           f);
+    record_on(st, comp,
+              comp == 3 ? (dir == 1 ? 0 : (dir == 0 ? 1 : 2)) : (dir == 1 ? 0 : (dir == 2 ? 1 : 2)),
+              f);
     LineArgs la = line_args(x, comp);
     la.ft = ft;
     la.fb = fb;
@@ -1876,9 +1879,10 @@ static void ctx_step(nse_ctx* x) {
   };
   // The four components' chains are independent (each pass reads and writes
   // its own field with read-only tables): u on the context's stream, v, w
-  // and T on side streams.  Adjoint recording, profiled steps (each phase
-  // timed on its own) and NSE_FLAG_ONE_STREAM keep the serial order.
-  if (x->part && !exact && !x->rec && concurrent(x)) {
+  // and T on side streams (an adjoint replay's recording copies go on the
+  // same chains).  Profiled steps (each phase timed on its own) and
+  // NSE_FLAG_ONE_STREAM keep the serial order.
+  if (x->part && !exact && concurrent(x)) {
     mark(x, PH_YVEL);
     NSE_CUDA(cudaEventRecord(x->lfork, s));
     for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(x->side[q], x->lfork, 0));
@@ -1891,6 +1895,7 @@ static void ctx_step(nse_ctx* x) {
     run_on(cs[3], 1, 3, uT, TB_Y_T, 2.0 * c.t_bot, 2.0 * c.t_top);
     run_on(cs[3], 0, 3, uT, TB_X_T, 0.0, 0.0);
     run_on(cs[3], 2, 3, uT, TB_Z_T, 0.0, 0.0);
+    for (int comp = 0; comp < 4; ++comp) record_on(cs[comp], comp, 3, comp < 3 ? fa[comp] : uT);
     std::swap(x->f[NSE_T], x->uT);
     T = F(x, NSE_T);
     // MKP needs u*, v*, w* only: the temperature chain also sets T's ghosts
