@@ -420,6 +420,10 @@ def run_adjoint(S, W, torch, stream, args):
             ctx.step_index = l0
 
         with S.Adjoint(ctx, N, checkpoint_every=20, avg_from=avg_from) as adj:
+            # one untimed forward run first (first-use costs: kernel loading,
+            # the context's side streams), then the timed one
+            reset(c1)
+            adj.objective()
             reset(c1)
             torch.cuda.synchronize()
             t0 = time.perf_counter()
