@@ -40,6 +40,20 @@
 #ifndef NSE_YZ_LPB
 #define NSE_YZ_LPB 16
 #endif
+// Register caps of the line kernels, as CTAs that must fit on an SM.  Left
+// to itself the compiler gives the FP64 y/z kernel 60-80 registers (3-4
+// CTAs of 256 threads) and the x kernel 76 (3 CTAs).  Measured at
+// 256x192x256: a cap of 64 registers (1024 threads per SM) takes the FP64 y
+// lines 0.247 -> 0.222 ms, the FP32 z lines 0.169 -> 0.149 and the x lines
+// 0.194 -> 0.188 (FP32 0.144 -> 0.126) per step; the FP64 kernel with 16 rows
+// per thread spills at 64 (z lines 0.219 -> 0.239) and keeps 768 threads, and
+// the x kernel with 16 rows per lane (nx = 512) keeps 128 registers.
+template <int NT, int MM, class R>
+struct YZMinB {
+  static constexpr int value = ((sizeof(R) == 8 && MM > 12) ? 768 : 1024) / NT > 0
+                                   ? ((sizeof(R) == 8 && MM > 12) ? 768 : 1024) / NT
+                                   : 1;
+};
 
 namespace nse {
 
@@ -380,7 +394,7 @@ struct XTab {
 // the line data, dominate the L1 traffic of this kernel)
 // (with PL = 16 the two half-warps work on different lines)
 template <int M, int NL, bool MASKED, class S, class R, int PL>
-__global__ void __launch_bounds__(256) k_xlines(Dims d, S* __restrict__ f, int jtop,
+__global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __restrict__ f, int jtop,
                                                 const R* __restrict__ tab,
                                                 const int* __restrict__ slots,
                                                 const int* __restrict__ ids, int count) {
@@ -566,7 +580,7 @@ struct YZTab {
 // LPB lines per CTA (adjacent in x; 16 lines keep two CTAs resident per SM).
 // The solution goes to `out` (type RO) when given, else back into f.
 template <int DIR, int MM, int P, int LPB, class S, class R, class RO>
-__global__ void __launch_bounds__(LPB * P) k_yzlines(Dims d, S* __restrict__ f,
+__global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yzlines(Dims d, S* __restrict__ f,
                                                       RO* __restrict__ out, int nu, int nother,
                                                       const R* __restrict__ tab,
                                                       const int* __restrict__ slots,
