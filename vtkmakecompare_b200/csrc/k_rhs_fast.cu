@@ -51,7 +51,7 @@ template <> struct RhsShape<float, float> { static constexpr int TY = 8, NS = 5,
 template <> struct RhsShape<float, double> { static constexpr int TY = 8, NS = 5, MINB = 2; };
 // the correction: FP64 32x4 tiles, four CTAs per SM (0.443 against 0.451 ms
 // for 32x8); FP32 storage 32x8 tiles, two CTAs per SM
-template <class H> struct CorrShape { static constexpr int TY = 4, NS = 5, MINB = 5; };
+template <class H> struct CorrShape { static constexpr int TY = 4, NS = 5, MINB = 4; };
 template <> struct CorrShape<float> { static constexpr int TY = 8, NS = 5, MINB = 2; };
 
 __device__ __forceinline__ void cp_async8(double* smem, const double* gmem) {
@@ -392,23 +392,11 @@ namespace nse {
 // and the old u_ta, v_ta, w_ta (interior) filled NS-3 planes ahead by
 // cp.async.  H is the storage type of u*, u_ta, u_ep2 and divu (float in the
 // mixed-precision form); the correction itself is evaluated in FP64.
-// A ring slot of the correction holds plane K of: phi with a one-cell halo
-// (SXW x (TY+2), FP64); u* for the tile's rows with the x halo (SXW x TY;
-// the kernel reads u*(i-1)); v* for the tile's columns with the row below
-// (TXW x (TY+1); v*(j-1)); w* on the tile (w*(k-1) comes from the previous
-// slot); the old u_ta, v_ta, w_ta on the tile.  Only what the correction
-// reads: 16 % less shared memory than full halo planes of u*, v*, w*.
 template <class H, int TY>
-struct CSlot {
-  static constexpr int PH = SXW * (TY + 2);   // phi (double)
-  static constexpr int UP = SXW * TY;         // u*
-  static constexpr int VP = TXW * (TY + 1);   // v*
-  static constexpr int TILE = TXW * TY;       // w*, u_ta, v_ta, w_ta
-  static constexpr int U0 = 0, V0 = UP, W0 = UP + VP, A0 = UP + VP + TILE;
-  static constexpr int bytes = PH * 8 + (UP + VP + 4 * TILE) * (int)sizeof(H);
-};
-template <class H, int TY>
-__host__ __device__ constexpr int cslot_bytes() { return CSlot<H, TY>::bytes; }
+__host__ __device__ constexpr int cslot_bytes() {
+  return SXW * (TY + 2) * 8 + 3 * SXW * (TY + 2) * (int)sizeof(H) +
+         3 * TXW * TY * (int)sizeof(H);
+}
 
 template <class H, int TY, int NS>
 __device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, int j0, int K,
@@ -416,32 +404,28 @@ __device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, in
                                              const H* VT, const H* WT, const H* UA,
                                              const H* VA, const H* WA) {
   if (K <= kmax) {
-    using L = CSlot<H, TY>;
-    char* slot = sm + (K % NS) * L::bytes;
+    constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+    char* slot = sm + (K % NS) * cslot_bytes<H, TY>();
     double* ph = reinterpret_cast<double*>(slot);
-    H* fl = reinterpret_cast<H*>(slot + L::PH * 8);
+    H* fl = reinterpret_cast<H*>(slot + PLANE * 8);
     const int tid = threadIdx.y * TXW + threadIdx.x;
-    for (int e = tid; e < L::PH; e += L::TILE) {
-      const int tx = e % SXW, ty = e / SXW;
-      const int i = i0 - 1 + tx, j = j0 - 1 + ty;
+    for (int e = tid; e < PLANE; e += TILE) {
+      int tx = e % SXW, ty = e / SXW;
+      int i = i0 - 1 + tx, j = j0 - 1 + ty;
       if (i > d.nx + 1 || j > d.ny + 1) continue;
-      const long c = d.P(i, j, K);
+      long c = d.P(i, j, K);
       cp_async8(ph + e, PHI + c);
-      // u*: rows j0..j0+TY-1, columns i0-1..i0+32
-      if (ty >= 1 && ty <= TY) cp_async8(fl + L::U0 + (ty - 1) * SXW + tx, UT + c);
-      // v*: rows j0-1..j0+TY-1, columns i0..i0+31
-      if (tx >= 1 && tx <= TXW && ty <= TY) cp_async8(fl + L::V0 + ty * TXW + (tx - 1), VT + c);
+      cp_async8(fl + e, UT + c);
+      cp_async8(fl + PLANE + e, VT + c);
+      cp_async8(fl + 2 * PLANE + e, WT + c);
     }
-    const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
-    if (i <= d.nx && j <= d.ny) {
-      const long c = d.P(i, j, K);
-      cp_async8(fl + L::W0 + tid, WT + c);
-      if (K >= 1 && K <= d.nz) {
-        H* h = fl + L::A0 + tid;
-        cp_async8(h, UA + c);
-        cp_async8(h + L::TILE, VA + c);
-        cp_async8(h + 2 * L::TILE, WA + c);
-      }
+    int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+    if (i <= d.nx && j <= d.ny && K >= 1 && K <= d.nz) {
+      long c = d.P(i, j, K);
+      H* h = fl + 3 * PLANE + tid;
+      cp_async8(h, UA + c);
+      cp_async8(h + TILE, VA + c);
+      cp_async8(h + 2 * TILE, WA + c);
     }
   }
   cp_async_commit();
@@ -456,8 +440,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     H* __restrict__ v_ep2, H* __restrict__ w_ep2, H* __restrict__ divu, double dt) {
   extern __shared__ __align__(16) char smc[];
   char* sm = smc;
-  using L = CSlot<H, TY>;
-  constexpr int F = NS - 3;
+  constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY, F = NS - 3;
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
@@ -485,25 +468,24 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
       const double* qm = reinterpret_cast<const double*>(sm_m);
       const double* qc = reinterpret_cast<const double*>(sm_c);
       const double* qp = reinterpret_cast<const double*>(sm_p);
-      const H* fm = reinterpret_cast<const H*>(sm_m + L::PH * 8);
-      const H* fc = reinterpret_cast<const H*>(sm_c + L::PH * 8);
+      const H* fm = reinterpret_cast<const H*>(sm_m + PLANE * 8);
+      const H* fc = reinterpret_cast<const H*>(sm_c + PLANE * 8);
 #define PH(pl, dxo, dyo) (pl)[e0 + (dyo) * SXW + (dxo)]
+#define FL(pl, f, dxo, dyo) (double)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
       const long c = d.P(I, J, K);
       const double rz = LD(rg.rdz, K), rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
       const double ph = PH(qc, 0, 0), phx = PH(qc, 1, 0), phy = PH(qc, 0, 1), phz = PH(qp, 0, 0),
                    phxm = PH(qc, -1, 0), phym = PH(qc, 0, -1), phzm = PH(qm, 0, 0);
-#undef PH
-      // u* at (i, i-1), v* at (j, j-1), w* at (k, k-1)
-      const int eu = L::U0 + threadIdx.y * SXW + threadIdx.x + 1;
-      const int ev = L::V0 + (threadIdx.y + 1) * TXW + threadIdx.x;
       const double gx = (phx - ph) * rx12, gy = (phy - ph) * ry12, gz = (phz - ph) * rz12;
-      const double un = (double)fc[eu] - dt * gx;
-      const double vn = (double)fc[ev] - dt * gy;
-      const double wn = (double)fc[L::W0 + t0] - dt * gz;
-      const double um = (double)fc[eu - 1] - dt * ((ph - phxm) * rx12m);
-      const double vm = (double)fc[ev - TXW] - dt * ((ph - phym) * ry12m);
-      const double wm = (double)fm[L::W0 + t0] - dt * ((ph - phzm) * rz12m);
-      const H* old = fc + L::A0 + t0;
+      const double un = FL(fc, 0, 0, 0) - dt * gx;
+      const double vn = FL(fc, 1, 0, 0) - dt * gy;
+      const double wn = FL(fc, 2, 0, 0) - dt * gz;
+      const double um = FL(fc, 0, -1, 0) - dt * ((ph - phxm) * rx12m);
+      const double vm = FL(fc, 1, 0, -1) - dt * ((ph - phym) * ry12m);
+      const double wm = FL(fm, 2, 0, 0) - dt * ((ph - phzm) * rz12m);
+#undef PH
+#undef FL
+      const H* old = fc + 3 * PLANE + t0;
       u[c] = un;
       v[c] = vn;
       w[c] = wn;
@@ -512,8 +494,8 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
       const double pyp = (J < d.ny) ? phy : p[c + d.sx];
       const double pzp = (K < d.nz) ? phz : p[c + d.sy];
       u_ep2[c] = (H)((double)old[0] - dt * (pxp - ph) * rx12);
-      v_ep2[c] = (H)((double)old[L::TILE] - dt * (pyp - ph) * ry12);
-      w_ep2[c] = (H)((double)old[2 * L::TILE] - dt * (pzp - ph) * rz12);
+      v_ep2[c] = (H)((double)old[TILE] - dt * (pyp - ph) * ry12);
+      w_ep2[c] = (H)((double)old[2 * TILE] - dt * (pzp - ph) * rz12);
       divu[c] = (H)((un - um) * rx + (vn - vm) * ry + (wn - wm) * rz);
       u_ta[c] = (H)(dt * gx);
       v_ta[c] = (H)(dt * gy);
