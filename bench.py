@@ -34,6 +34,7 @@ UNIT = "steps/s"
 NX, NY, NZ = 256, 192, 256
 RE, PR, ETA, WIDTH = 3000.0, 0.71, 1.0e4, 1.5
 SPHERE = ((math.pi, 0.0, math.pi / 2), 0.25)
+DATA = "synthetic (seeded channel flow + sphere mask; no dataset)"
 WORKLOAD = ("sphere256: channel 2pi x 2 x pi, y walls at -1,1 (tanh stretch 2), "
             "256x192x256 cells, sphere R=0.25 at (pi,0,pi/2) by volume penalisation "
             "(eta=1e4, smoothed Heaviside 1.5 dx), heat transfer (sphere T=1, walls T=0), "
@@ -143,25 +144,56 @@ class Clocks:
                 "samples": len(self.samples)}
 
 
-def build_case(S, W, torch, precision=0, flags=0):
-    """Context with the workload's initial state: level-set mask, projected field."""
-    g = W.grid_arrays(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+def workload_inputs(g, W):
+    """Seeded initial fields, CFL time step and the sphere mask of the
+    workload on the grid g (numpy only; the GPU arm and the CPU reference arm
+    take the same inputs).  The mask is the smoothed Heaviside of
+    set_levelset.f:157-170 applied to the exact signed distance of the
+    sphere."""
     f = W.channel_state(g, seed=2024, t_bot=0.0, t_top=0.0)
     dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    c1 = W.smoothed_mask(g, W.sphere_phi0(g, *SPHERE), WIDTH)
+    return f, dt, c1
+
+
+def config_dict(dt):
+    """The `config` of the JSON line, identical in both arms."""
+    return {"workload": WORKLOAD, "grid": [NX, NY, NZ], "precision": "fp64 plain",
+            "mask": "smoothed Heaviside (1.5 dx) of the exact sphere signed distance, "
+                    "same array in both arms",
+            "initial_state": "seeded noise, then one projection (set_bc + MKP)",
+            "l2": "inputs larger than L2 (16 resident FP64 fields of 103 MB)",
+            "dt": float("%.12g" % dt)}
+
+
+def build_case(S, W, torch, precision=0, flags=0, levelset=True):
+    """Context with the workload's initial state: the sphere mask, the
+    projected field.  With `levelset` the level-set setup (2001 reinitialisation
+    sweeps + mask on the GPU, set_levelset.f) is run and timed first; the
+    mask the steps use is then replaced by the workload's mask, so that the
+    GPU and the CPU reference step from the same array."""
+    g = W.grid_arrays(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f, dt, c1 = workload_inputs(g, W)
     cfg = S.Config(NX, NY, NZ, dt, RE, PR, ETA, 2 * math.pi, 2.0, math.pi, y0=-1.0,
                    ystretch=2.0, body_force=3.0 / RE, heat_source=0.0, t_bot=0.0, t_top=0.0,
                    t_solid=1.0, precision=precision, flags=flags)
     ctx = S.Context(cfg)
     for k in ("u", "v", "w", "T"):
         ctx.upload(k, f[k])
-    phi0 = W.sphere_phi0(g, *SPHERE)
-    t0 = time.perf_counter()
-    ctx.levelset(phi0, width=WIDTH, want_phi=False)
-    ls_s = time.perf_counter() - t0
+    ls = None
+    if levelset:
+        phi0 = W.sphere_phi0(g, *SPHERE)
+        torch.cuda.synchronize()
+        t0 = time.perf_counter()
+        ctx.levelset(phi0, width=WIDTH, want_phi=False)
+        ls = {"seconds": round(time.perf_counter() - t0, 3)}
+        ls["mask_max_abs_diff_vs_exact_sdf_mask"] = float(
+            np.abs(ctx.download("cellvalue") - c1).max())
+    ctx.upload("cellvalue", c1)
     ctx.project()
     ctx.start()
     ctx.sync()
-    return g, f, cfg, ctx, ls_s
+    return g, f, cfg, ctx, ls
 
 
 # mixed-precision variants reported beside the FP64 line: name -> nse flags
@@ -189,7 +221,7 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
         return d
 
     if args.acc_steps > 0:
-        _, _, _, ref, _ = build_case(S, W, torch)
+        _, _, _, ref, _ = build_case(S, W, torch, levelset=False)
         rd = divs(ref, args.acc_steps)
         refs = {k: ref.download(k) for k in ("u", "v", "w", "T")}
         ref.close()
@@ -197,7 +229,8 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
                                  "max_divu_step1": rd[0],
                                  "max_divu_after_step1": max(rd[1:] or [0.0])}
     for name, flags in MIXED_VARIANTS:
-        _, _, _, ctx, _ = build_case(S, W, torch, precision=S.MIXED, flags=flags)
+        _, _, _, ctx, _ = build_case(S, W, torch, precision=S.MIXED, flags=flags,
+                                        levelset=False)
         ctx.set_stream(stream.cuda_stream)
         with torch.cuda.stream(stream):
             ctx.step(args.warmup)
@@ -222,7 +255,8 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
                "speedup_vs_fp64": round(fp64_ms / ms, 3),
                "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()}}
         if args.acc_steps > 0:
-            _, _, _, ctx, _ = build_case(S, W, torch, precision=S.MIXED, flags=flags)
+            _, _, _, ctx, _ = build_case(S, W, torch, precision=S.MIXED, flags=flags,
+                                        levelset=False)
             md = divs(ctx, args.acc_steps)
             got = {k: ctx.download(k) for k in ("u", "v", "w", "T")}
             ctx.close()
@@ -472,6 +506,25 @@ def run_adjoint(S, W, torch, stream, args):
     return res
 
 
+def summary(line):
+    """The headline figures of the line in a few keys (printed last, so a
+    truncated log tail still shows them)."""
+    out = {"fp64_steps_per_s": line["value"], "e2e_steps_per_s": line["e2e"]["value"],
+           "poisson_ms": line["poisson"]["ms_per_solve"],
+           "poisson_frac_of_hbm": line["poisson"]["frac_of_hbm"]}
+    mp = line.get("mixed_precision") or {}
+    for name, rec in mp.items():
+        if name == "fp64_reference":
+            continue
+        out[name] = {"speedup_vs_fp64": rec.get("speedup_vs_fp64"),
+                     "max_divu": rec.get("max_divu"),
+                     "velocity_rel_l2_vs_fp64": rec.get("velocity_rel_l2_vs_fp64")}
+    if line.get("parity"):
+        out["parity_max_rel_l2"] = line["parity"]["max_rel_l2"]
+        out["parity_pass"] = line["parity"]["pass"]
+    return out
+
+
 def run_ours(args, rank, world, local_rank):
     import torch
     import torch.distributed as dist
@@ -480,7 +533,7 @@ def run_ours(args, rank, world, local_rank):
 
     torch.cuda.set_device(local_rank)
     dev = torch.device("cuda", local_rank)
-    g, f0, cfg, ctx, ls_s = build_case(S, W, torch)
+    g, f0, cfg, ctx, ls = build_case(S, W, torch)
     stream = torch.cuda.Stream(device=dev)
     ctx.set_stream(stream.cuda_stream)
 
@@ -596,10 +649,10 @@ def run_ours(args, rank, world, local_rank):
     if args.adj_steps > 0:
         adjoint = run_adjoint(S, W, torch, stream, args)
 
-    # ---------------------------------------------------------- CPU baseline
-    cpu = None
-    if rank == 0 and not args.no_cpu:
-        cpu = cpu_baseline(g, f0, c1, cfg, nsteps=args.cpu_steps)
+    # ---------------------------------- parity against the CPU oracle + CPU baseline
+    parity, cpu = None, None
+    if rank == 0 and args.parity_steps > 0:
+        parity, cpu = run_parity(S, W, torch, args.parity_steps)
 
     if rank != 0:
         ctx.close()
@@ -619,6 +672,9 @@ def run_ours(args, rank, world, local_rank):
     t_launch_s = per_launch[dominant] / 1e3
     achieved = algo[dominant] / t_launch_s / 1e9
     traffic = dram_traffic().get(dominant)
+    poisson = {"solves_per_s": round(world * 1e3 / pms, 2), "ms_per_solve": round(pms, 4),
+               "algorithmic_bytes": BP, "gbs": round(BP / (pms / 1e3) / 1e9, 1),
+               "frac_of_hbm": round(BP / (pms / 1e3) / 1e9 / peak, 4)}
     line = {
         "metric": METRIC,
         "value": round(steps_s, 3),
@@ -631,18 +687,23 @@ def run_ours(args, rank, world, local_rank):
         "scaling": "weak",
         "vs_baseline": None,
         "dtype": "f64",
-        "data": "synthetic (seeded channel flow + sphere level set; no dataset)",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "precision": "fp64 plain",
-                   "parallelism": f"replicas x{world}",
-                   "l2": "inputs larger than L2 (16 resident FP64 fields of 103 MB)",
-                   "dt": cfg.dt},
-        "poisson": {"solves_per_s": round(world * 1e3 / pms, 2), "ms_per_solve": round(pms, 4),
-                    "algorithmic_bytes": BP, "gbs": round(BP / (pms / 1e3) / 1e9, 1),
-                    "frac_of_hbm": round(BP / (pms / 1e3) / 1e9 / peak, 4)},
-        "max_divu": mon["max_divu"],
-        "mixed_precision": mixed,
+        "data": DATA,
+        "config": config_dict(cfg.dt),
+        "parallelism": f"replicas x{world}",
+        "gpu_launches": int(launches),
+        "levelset_setup": ls,
         "ensemble": ensemble,
         "adjoint": adjoint,
+        "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()},
+        "phases_note": ("the line passes of u, v, w and T run as four concurrent chains; "
+                        "y_vel holds the whole line block" if concurrent_lines else
+                        "from K further steps with the phase events on, which run every "
+                        "pass on one stream in order; the timed steps run the four line "
+                        "chains concurrently"),
+        "mixed_precision": mixed,
+        "max_divu": mon["max_divu"],
+        "poisson": poisson,
+        "parity": parity,
         "e2e": {"value": round(world * args.steps / (e2e_ms / 1e3), 3), "unit": UNIT,
                 "h2d_bytes_per_step": int(h2d / args.steps),
                 "d2h_bytes_per_step": int(d2h / args.steps),
@@ -653,17 +714,10 @@ def run_ours(args, rank, world, local_rank):
                      "traffic": traffic, "peak_source": peak_kind,
                      "algorithmic_bytes_per_launch": algo[dominant],
                      "ms_per_launch": round(per_launch[dominant], 4)},
-        "phases_ms_per_step": {k: round(v / max(1, nprof), 4) for k, v in phases.items()},
-        "phases_note": ("the line passes of u, v, w and T run as four concurrent chains; "
-                        "y_vel holds the whole line block" if concurrent_lines else
-                        "from K further steps with the phase events on, which run every "
-                        "pass on one stream in order; the timed steps run the four line "
-                        "chains concurrently"),
-        "gpu_launches": int(launches),
-        "levelset_setup_s": round(ls_s, 3),
-        "clocks": clk.summary(),
         "cpu_baseline": cpu,
+        "clocks": clk.summary(),
     }
+    line["summary"] = summary(line)
     ctx.close()
     return line
 
@@ -675,46 +729,81 @@ class _OGrid:
         self.__dict__.update(g)
 
 
-def cpu_baseline(g, f0, c1, cfg, nsteps=3):
-    """The oracle (C++ restatement of the reference, faithful mode with the
-    per-line dense matrix zeroing) on all host cores: `nsteps` full steps."""
-    from oracle import oracle as O
-    O.set_faithful(True)
-    s = O.Solver(_OGrid(g), cfg.dt, cfg.Re, cfg.Sc, cfg.eta, force=cfg.body_force,
-                 source=cfg.heat_source, tbot=cfg.t_bot, ttop=cfg.t_top, tsolid=cfg.t_solid)
-    for k in ("u", "v", "w", "T"):
-        s.f[k][...] = f0[k]
-    s.cellvalue[..., 0] = c1
-    s.start()
-    s.step(1)  # warm (first-touch of the 45 work arrays)
-    t0 = time.perf_counter()
-    s.step(nsteps)
-    el = time.perf_counter() - t0
-    return {"value": round(nsteps / el, 4), "unit": UNIT, "cores": O.num_threads(),
-            "kind": "port",
-            "sample": f"{nsteps} full FP64 time steps of the 256x192x256 workload "
-                      f"({el:.1f} s) after one warm step; oracle faithful mode"}
-
-
-def run_reference(args, rank, world):
-    if rank != 0:
-        return None
-    from oracle import oracle as O
-    from vtkmakecompare_b200 import workload as W
-    g = W.grid_arrays(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
-    f = W.channel_state(g, seed=2024, t_bot=0.0, t_top=0.0)
-    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
-    phi = W.sphere_phi0(g, *SPHERE)[1:-1, 1:-1, 1:-1]
-    h = WIDTH * g["dx"][1:-1, None, None]
-    c1 = np.where(phi >= h, 1.0, np.where(phi <= -h, 0.0,
-                                          (np.sin(3.1415926535 * phi / 2 / h) + 1) / 2))
-    O.set_faithful(True)
-    s = O.Solver(_OGrid(g), dt, RE, PR, ETA, force=3.0 / RE, source=0.0, tbot=0.0,
-                 ttop=0.0, tsolid=1.0)
+def oracle_case(O, g, f, dt, c1):
+    """The CPU restatement of the reference time loop on the workload's
+    inputs: same fields, mask and dt, the initial projection (set_bc + MKP),
+    the AB2 history copy (nse_dominik.f:246-257)."""
+    s = O.Solver(g, dt, RE, PR, ETA, force=3.0 / RE, source=0.0, tbot=0.0, ttop=0.0,
+                 tsolid=1.0)
     for k in ("u", "v", "w", "T"):
         s.f[k][...] = f[k]
     s.cellvalue[..., 0] = c1
+    s.project()
     s.start()
+    return s
+
+
+PARITY_FIELDS = ("u", "v", "w", "p", "T", "u_ta", "v_ta", "w_ta", "u_pre", "v_pre", "w_pre",
+                 "T_pre")
+
+
+def run_parity(S, W, torch, nsteps):
+    """The GPU FP64 step (default fast form, a fresh context) against the CPU
+    oracle on identical inputs: both project the same seeded field with the
+    same mask, take one warm step and then `nsteps` timed steps.  Relative L2
+    of every state field after 1 + nsteps steps (bound 1e-10) and the largest
+    post-projection divergence of both.  The oracle's timed steps (faithful
+    mode: the reference's per-line dense matrix zeroing, all host threads)
+    are the CPU baseline."""
+    from oracle import oracle as O
+    g, f, cfg, ctx, _ = build_case(S, W, torch, levelset=False)
+    c1 = ctx.download("cellvalue")
+    ctx.step(1 + nsteps)
+    mon = ctx.monitor()
+    got = {k: ctx.download(k) for k in PARITY_FIELDS}
+    gdiv = np.abs(ctx.download("divu")).max()
+    ctx.close()
+    O.set_faithful(True)
+    s = oracle_case(O, _OGrid(g), f, cfg.dt, c1)
+    s.step(1)  # warm (first touch of the work arrays) and the Euler start
+    t0 = time.perf_counter()
+    s.step(nsteps)
+    el = time.perf_counter() - t0
+    rel = {k: float(np.linalg.norm(got[k] - s.f[k]) / np.linalg.norm(s.f[k]))
+           for k in PARITY_FIELDS}
+    odiv = float(np.abs(s.f["divu"]).max())
+    umax = float(np.abs(s.f["u"]).max())
+    dx = float(g["dx"][1])
+    parity = {"steps": 1 + nsteps, "grid": [NX, NY, NZ], "form": "fp64 fast (default)",
+              "rel_l2_vs_oracle": rel, "max_rel_l2": max(rel.values()), "bound": 1e-10,
+              "max_divu_gpu": float(mon["max_divu"]), "max_abs_divu_field_gpu": float(gdiv),
+              "max_divu_oracle": odiv, "divu_bound": 1e-12 * max(1.0, umax / dx),
+              "pass": bool(max(rel.values()) <= 1e-10 and
+                           mon["max_divu"] <= 1e-12 * max(1.0, umax / dx))}
+    cpu = {"value": round(nsteps / el, 4), "unit": UNIT, "cores": O.num_threads(),
+           "kind": "port",
+           "sample": f"{nsteps} full FP64 time steps of the 256x192x256 workload ({el:.1f} s) "
+                     "after the projection and one warm step; oracle faithful mode, the same "
+                     "run the parity block compares against"}
+    return parity, cpu
+
+
+def run_reference(args, rank, world):
+    """The CPU reference arm: the oracle (C++/OpenMP restatement of the
+    reference Fortran, faithful mode) on all host threads, on the same
+    inputs as the GPU arm (grid from the oracle's own SET_C restatement,
+    the same seeded fields, dt and mask), each step a full time step."""
+    if rank != 0:
+        return None
+    from oracle import oracle as O
+    from vtkmakecompare_b200 import workload as W  # numpy input generators only
+    og = O.Grid(NX, NY, NZ, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    g = {k: getattr(og, k) for k in ("x", "x12", "y", "y12", "z", "z12", "dx", "dx12", "dy",
+                                     "dy12", "dz", "dz12")}
+    g.update(nx=NX, ny=NY, nz=NZ, xl=og.xl, yl=og.yl, zl=og.zl)
+    f, dt, c1 = workload_inputs(g, W)
+    O.set_faithful(True)
+    s = oracle_case(O, og, f, dt, c1)
     s.step(max(1, args.warmup))
     t0 = time.perf_counter()
     s.step(args.steps)
@@ -724,8 +813,8 @@ def run_reference(args, rank, world):
         "metric": METRIC, "value": round(v, 4), "unit": UNIT, "n_gpus": world,
         "steps": args.steps, "warmup": args.warmup, "ms_per_step": round(1e3 * el / args.steps, 1),
         "higher_is_better": True, "scaling": "weak", "vs_baseline": None, "dtype": "f64",
-        "data": "synthetic (seeded channel flow + sphere mask)",
-        "config": {"workload": WORKLOAD, "grid": [NX, NY, NZ], "precision": "fp64 plain"},
+        "data": DATA,
+        "config": config_dict(dt),
         "impl": "reference",
         "cpu_baseline": {"value": round(v, 4), "unit": UNIT, "cores": O.num_threads(),
                          "kind": "port",
@@ -743,8 +832,9 @@ def main():
     ap.add_argument("--steps", type=int, default=20)
     ap.add_argument("--warmup", type=int, default=3)
     ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
-    ap.add_argument("--cpu-steps", type=int, default=3)
-    ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--parity-steps", type=int, default=10,
+                    help="timed steps of the GPU-vs-oracle parity run at the bench size "
+                         "(its oracle timing is the CPU baseline; 0 skips both)")
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--ens-cases", type=int, default=32,
                     help="cases of the batched-ensemble measurement (0 skips it)")

@@ -156,6 +156,42 @@ void implicit_ty_(double* STY, const int* ny, const double* dy, const double* dy
                   const double* Re, const double* Sc, const double* dt, const double* lly,
                   const double* rry, const double* ft, const double* fb, const double* CUY,
                   const double* eta);
+/* line drivers of the reference's OpenMP loops, nse_dominik.f:2893 parallel_uy,
+ * :2912 parallel_z, :2931 parallel_x, :2950 parallel_vy, :2969 parallel_Tx,
+ * :2995 parallel_Ty, :3021 parallel_Tz: one line of the padded field (line
+ * indices 1-based, mask column n of cellvalue), solved by the single-line
+ * solver above; each writes the entries its reference routine writes
+ * (u_a(i,0:ny+1,k); v_a(i,0:ny,k); u_a(i,j,0:nz+1); u_a(0:nx+1,j,k); u_T on
+ * the interior of the line).  The end entries of the rhoCp/thc line locals,
+ * which the reference leaves unset, are the fields' ghost cells. */
+void parallel_uy_(const int* i, const int* k, double* u_a, const double* cellvalue,
+                  const int* nx, const int* ny, const int* nz, const double* dy,
+                  const double* dy12, const double* Re, const double* dt, const double* eta,
+                  const int* n);
+void parallel_vy_(const int* i, const int* k, double* v_a, const double* cellvalue,
+                  const int* nx, const int* ny, const int* nz, const double* dy,
+                  const double* dy12, const double* Re, const double* dt, const double* eta,
+                  const int* n);
+void parallel_z_(const int* i, const int* j, double* u_a, const double* cellvalue,
+                 const int* nx, const int* ny, const int* nz, const double* dz,
+                 const double* dz12, const double* Re, const double* dt, const double* eta,
+                 const int* n);
+void parallel_x_(const int* j, const int* k, double* u_a, const double* cellvalue,
+                 const int* nx, const int* ny, const int* nz, const double* dx,
+                 const double* dx12, const double* Re, const double* dt, const double* eta,
+                 const int* n);
+void parallel_tx_(const int* k, const int* j, const int* nx, const int* ny, const int* nz,
+                  const double* rhoCp, const double* thc, double* u_T,
+                  const double* cellvalue, const double* dx, const double* dx12,
+                  const double* Re, const double* Sc, const double* dt, const double* eta);
+void parallel_ty_(const int* i, const int* k, const int* nx, const int* ny, const int* nz,
+                  const double* rhoCp, const double* thc, double* u_T,
+                  const double* cellvalue, const double* dy, const double* dy12,
+                  const double* Re, const double* Sc, const double* dt, const double* eta);
+void parallel_tz_(const int* i, const int* j, const int* nx, const int* ny, const int* nz,
+                  const double* rhoCp, const double* thc, double* u_T,
+                  const double* cellvalue, const double* dz, const double* dz12,
+                  const double* Re, const double* Sc, const double* dt, const double* eta);
 /* OUTPUT (nse_dominik.f:2606): ./nseoutput2/{velocity,temperature,pressure,
  * divergence,gridx,gridy,gridz,gridnumber,phi,cellvalue1..4}.dat, field.u,
  * grid.u and ./temperature_check.dat, byte for byte as gfortran writes them
@@ -191,11 +227,14 @@ void nse_set_c_stretched(int nx, int ny, int nz, double* x, double* x12, double*
  * stream) and the function returns without synchronising.  It allocates
  * nothing: its scratch is a fixed array inside the library of
  * NSE_NOALLOC_SCRATCH_DOUBLES doubles (16 MiB, resident on every GPU that
- * loads the library until exit), so (nx/2+1)*ny*nz must not exceed it
- * (NSE_ERR_LIMIT otherwise).  The first call on a device looks up the array's
- * device address; make that first call before any stream capture.  Calls
- * share the array: calls that overlap on the GPU race and must be
- * serialised by the caller.  Returns an nse_status. */
+ * loads the library until exit), so (nx/2+1)*ny*nz must not exceed it, nor
+ * nz 65535 (NSE_ERR_LIMIT otherwise).  The first call on a device looks up
+ * the array's device address and keeps it for the life of the process; make
+ * that first call before any stream capture, and do not call this entry
+ * point on a device after cudaDeviceReset.  Calls share the array: calls
+ * that overlap on the GPU race and must be serialised by the caller.  A CUDA
+ * error pending from the caller's earlier work is reported (NSE_ERR_CUDA)
+ * and left in place.  Returns an nse_status. */
 #define NSE_NOALLOC_SCRATCH_DOUBLES (2L * 1024L * 1024L)
 int nse_spn_noalloc(int nx, int ny, int nz, const double* AC, const double* KXZ,
                     double* PHIT, void* stream);
@@ -376,6 +415,14 @@ void set_adj_ns_scalar_(const double* dt, const int* nx, const int* ny, const in
 int nse_adj_ns_scalar(const double* dt, int nx, int ny, int nz, const double* dx12,
                       const double* dy12, const double* dz12, const double* T,
                       const double* T_final, double* u_s, double* v_s, double* w_s);
+
+/* Device memory the library holds at once (all its allocations: contexts,
+ * ensembles, adjoints and the staging buffers of the legacy entry points),
+ * capped at `bytes` (0 = no cap, the default).  An allocation beyond the cap
+ * fails like an out-of-memory one: NSE_ERR_NOMEM, and a context being
+ * created is released.  No counterpart in the reference. */
+void nse_set_alloc_limit(long long bytes);
+long long nse_alloc_bytes(void);
 
 /* number of kernel launches this process has issued through the library */
 long long nse_launch_count(void);

@@ -1,12 +1,14 @@
 ! nsegpu_iface.f90 -- Fortran 2003 interfaces to the resident (tier 3) API of
 ! libnsegpu.so.  The reference subroutines themselves (MKP, P2S, S2P, SPN,
 ! SP0B, PHIBC, CTRIDIAG, TRIDIAG, TRID2, implicit_solver, TDMA, cyclic,
-! set_levelset, readgrid3d, the step routines of nse_dominik.f and the
-! adjoint.f routines set_adj_convect, set_adj_convection_for_scalar,
-! set_adj_NS_scalar) need no
-! interface: libnsegpu.so exports them under gfortran's mangled names
-! (mkp_, p2s_, ...), so a driver that calls them links against the library
-! instead of the reference object files.  See INTEGRATION.md.
+! set_levelset, readgrid3d, the step routines of nse_dominik.f with their
+! parallel_* line drivers, and the adjoint.f routines set_adj_convect,
+! set_adj_convection_for_scalar, set_adj_NS_scalar) need no interface:
+! libnsegpu.so exports them under gfortran's mangled names (mkp_, p2s_, ...),
+! so a driver that calls them links against the library instead of the
+! reference object files (link line: -L<dir of libnsegpu.so> -lnsegpu, with
+! the reference's mkp.f, p2s_fftw2d.f, tridiag.f, periodic_implicit.f and
+! set_levelset.f left out of the link).
 module nsegpu
   use iso_c_binding
   implicit none
@@ -116,5 +118,9 @@ module nsegpu
      type(c_ptr) function nse_last_error() bind(C, name="nse_last_error")
        import :: c_ptr
      end function nse_last_error
+     subroutine nse_set_alloc_limit(bytes) bind(C, name="nse_set_alloc_limit")
+       import :: c_long_long
+       integer(c_long_long), value :: bytes
+     end subroutine nse_set_alloc_limit
   end interface
 end module nsegpu

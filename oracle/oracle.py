@@ -212,6 +212,22 @@ class Solver:
                            source=source, tbot=tbot, ttop=ttop, tsolid=tsolid)
         self.l = 1
 
+    def project(self):
+        """Initial projection of the benchmark workloads (the seeded field is
+        "then projected divergence-free"): SET_BC (nse_dominik.f:611-753) on
+        copies of u, v, w, then MKP (mkp.f:9-220) with those copies as
+        u_temp, v_temp, w_temp.  MKP writes u, v, w, p, u_ta, u_ep2 and divu;
+        p's ghosts are left as they are (the time loop's first SET_BC sets
+        them)."""
+        g = self.g
+        f = self.f
+        tmp = {k: f[k].copy(order="F") for k in ("u", "v", "w", "p", "T")}
+        set_bc(tmp["u"], tmp["v"], tmp["w"], tmp["p"], tmp["T"], self.params["tbot"],
+               self.params["ttop"])
+        mkp(g, f["p"], tmp["u"], tmp["v"], tmp["w"], self.params["dt"], f["u_ta"], f["v_ta"],
+            f["w_ta"], f["u_ep2"], f["v_ep2"], f["w_ep2"], f["divu"], f["u"], f["v"], f["w"],
+            phi_work=f["phi_work"], Re=self.params["Re"])
+
     def start(self):
         """Copy the state into the AB2 history, as nse_dominik.f:246-257 does."""
         for a, b in (("u", "u_pre"), ("v", "v_pre"), ("w", "w_pre"), ("T", "T_pre")):

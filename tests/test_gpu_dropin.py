@@ -309,3 +309,79 @@ def test_step_routines_bitexact(n):
     G.solve_t(b, nx, ny, nz, g["dx"], g["dy"], g["dz"], g["dx12"], g["dy12"], g["dz12"], Re, Sc,
               dt, rcp, thc, cv, eta)
     assert bit_equal(a, b)
+
+
+# --------------------------------------------------- parallel_* line drivers
+def test_parallel_line_drivers_bitexact():
+    """parallel_uy/vy/z/x/Tx/Ty/Tz (nse_dominik.f:2893-3045): each call equals
+    the reference's gather, single-line solve (oracle) and scatter on its
+    line, bit for bit, and leaves every other entry of the field untouched."""
+    rng = np.random.default_rng(29)
+    nx, ny, nz = 12, 10, 8
+    g, go = grid(nx, ny, nz)
+    Re, Sc, dt, eta = 300.0, 0.71, 0.01, 1.0e4
+    cv = mask(rng, nx, ny, nz)
+    f0 = rand_field(rng, nx, ny, nz)
+    rho = np.asfortranarray(0.5 + rng.random(f0.shape))
+    thc = np.asfortranarray(0.5 + rng.random(f0.shape))
+    d = {"x": (g["dx"], g["dx12"]), "y": (g["dy"], g["dy12"]), "z": (g["dz"], g["dz12"])}
+
+    def vel(name, axis, a, b, ncol, solver, lo, hi_out):
+        """gather along `axis` at the other two indices (a, b), 1-based"""
+        n = {"x": nx, "y": ny, "z": nz}[axis]
+        idx = lambda q: {"x": (q, a, b), "y": (a, q, b), "z": (a, b, q)}[axis]
+        cidx = lambda q: {"x": (q - 1, a - 1, b - 1), "y": (a - 1, q - 1, b - 1),
+                          "z": (a - 1, b - 1, q - 1)}[axis]
+        S = np.zeros(n + 2)
+        C = np.zeros(n)
+        for q in range(1, hi_in[name] + 1):
+            S[q] = f0[idx(q)]
+            C[q - 1] = cv[cidx(q) + (ncol - 1,)]
+        solver(S, n, *d[axis], Re, dt, 0.0, 0.0, eta, C)
+        ref = f0.copy(order="F")
+        for q in range(lo, hi_out + 1):
+            ref[idx(q)] = S[q]
+        got = f0.copy(order="F")
+        getattr(G, name)(a, b, got, cv, nx, ny, nz, *d[axis], Re, dt, eta, ncol)
+        assert bit_equal(got, ref), name
+
+    hi_in = {"parallel_uy": ny, "parallel_vy": ny - 1, "parallel_z": nz, "parallel_x": nx}
+    for (a, b) in ((1, 1), (nx // 2, nz), (nx, 3)):
+        vel("parallel_uy", "y", a, b, 2, O.implicit_uy, 0, ny + 1)
+        vel("parallel_vy", "y", a, b, 3, O.implicit_vy, 0, ny)
+    for (a, b) in ((1, 1), (nx, ny // 2)):
+        vel("parallel_z", "z", a, b, 4, O.implicit_solver, 0, nz + 1)
+    for (a, b) in ((1, 1), (ny, nz)):
+        vel("parallel_x", "x", a, b, 2, O.implicit_solver, 0, nx + 1)
+
+    def temp(name, axis, a, b, solver):
+        n = {"x": nx, "y": ny, "z": nz}[axis]
+        idx = lambda q: {"x": (q, a, b), "y": (a, q, b), "z": (a, b, q)}[axis]
+        S = np.zeros(n + 2)
+        R = np.zeros(n + 2)
+        L = np.zeros(n + 2)
+        C = np.zeros(n + 2)
+        for q in range(0, n + 2):
+            R[q] = rho[idx(q)]
+            L[q] = thc[idx(q)]
+            if 1 <= q <= n:
+                S[q] = f0[idx(q)]
+                i, j, k = idx(q)
+                C[q] = cv[i - 1, j - 1, k - 1, 0]
+        if axis == "y":
+            solver(S, n, *d[axis], Re, Sc, dt, L, R, 0.0, 0.0, C, eta)
+        else:
+            solver(S, n, *d[axis], Re, Sc, dt, L, R, 0.0, 0.0, eta, C)
+        ref = f0.copy(order="F")
+        for q in range(1, n + 1):
+            ref[idx(q)] = S[q]
+        got = f0.copy(order="F")
+        # parallel_Tx takes (k, j), parallel_Ty (i, k), parallel_Tz (i, j)
+        first, second = (b, a) if axis == "x" else (a, b)
+        getattr(G, name)(first, second, nx, ny, nz, rho, thc, got, cv, *d[axis], Re, Sc, dt,
+                         eta)
+        assert bit_equal(got, ref), name
+
+    temp("parallel_tx", "x", 2, 3, O.implicit_tx)
+    temp("parallel_ty", "y", nx, 1, O.implicit_ty)
+    temp("parallel_tz", "z", 4, ny, O.implicit_tx)

@@ -1,0 +1,163 @@
+"""Parity of the resident GPU step with the CPU oracle on the benchmark
+workloads themselves, from identical seeded inputs:
+
+* the 64^3 plain channel (2pi x 2 x pi, tanh stretching 2, Re 3000, Pr 0.71,
+  noise 0.05 on u, v, w, T linear from 1 to 0, no obstacle, CFL 0.5) after
+  its initial projection and 10 steps;
+* the seeded N(0,1) Poisson right-hand side with its dy-weighted mean
+  removed, through the resident solve and through the tier-1 drop-ins
+  (p2s_ -> spn_ -> sp0b_ -> s2p_ -> phibc_), against the oracle's
+  P2S/SPN/SP0B/S2P/PHIBC (mkp.f:223-320, p2s_fftw2d.f);
+* the ensemble grids 96x64x96 and 160x128x160 (x lines through the
+  partitioned solver with 3 and 5 rows per lane) with obstacles;
+* the 256x192x256 sphere workload of the benchmark for 3 steps.
+
+Bounds (north star): state after N steps within 1e-10 relative L2,
+Poisson solution within 1e-12 relative L2, post-projection divergence
+at most 1e-12 (scaled by max|u|/dx, the size of one difference quotient).
+"""
+import math
+
+import numpy as np
+import pytest
+
+from oracle import oracle as O
+from tests._helpers import oracle_grid, rel_l2
+from vtkmakecompare_b200 import legacy as G
+from vtkmakecompare_b200 import solver as S
+from vtkmakecompare_b200 import workload as W
+
+pytestmark = pytest.mark.gpu
+
+STATE = ("u", "v", "w", "p", "T", "u_ta", "v_ta", "w_ta", "u_pre", "v_pre", "w_pre", "T_pre",
+         "u_ep2", "v_ep2", "w_ep2")
+
+
+def channel(nx, ny, nz, seed, t_bot, t_top):
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = W.channel_state(g, seed=seed, t_bot=t_bot, t_top=t_top)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    return g, f, dt
+
+
+def run_pair(g, f, dt, c1, Re, Pr, t_bot, t_top, t_solid, nsteps):
+    """Both sides: upload/copy the same fields and mask, project, copy into the
+    AB2 history, step nsteps times.  Returns (gpu fields, gpu monitor, oracle)."""
+    kw = dict(force=3.0 / Re, source=0.0, tbot=t_bot, ttop=t_top, tsolid=t_solid)
+    s = O.Solver(oracle_grid(g), dt, Re, Pr, 1.0e4, **kw)
+    for k in ("u", "v", "w", "T"):
+        s.f[k][...] = f[k]
+    s.cellvalue[..., 0] = c1
+    s.project()
+    s.start()
+    s.step(nsteps)
+    cfg = S.Config(g["nx"], g["ny"], g["nz"], dt, Re, Pr, 1.0e4, g["xl"], g["yl"], g["zl"],
+                   y0=-1.0, ystretch=2.0, body_force=3.0 / Re, heat_source=0.0, t_bot=t_bot,
+                   t_top=t_top, t_solid=t_solid)
+    with S.Context(cfg) as ctx:
+        for k in ("u", "v", "w", "T"):
+            ctx.upload(k, f[k])
+        ctx.upload("cellvalue", c1)
+        ctx.project()
+        ctx.start()
+        ctx.step(nsteps)
+        got = {k: ctx.download(k) for k in STATE + ("divu",)}
+        mon = ctx.monitor()
+    return got, mon, s
+
+
+def check_state(got, mon, s, g, bound=1e-10):
+    scale = max(1.0, np.abs(s.f["u"]).max() / g["dx"][1])
+    errs = {k: rel_l2(got[k], s.f[k]) for k in STATE}
+    bad = {k: e for k, e in errs.items() if not e <= bound}
+    assert not bad, bad
+    assert mon["nonfinite"] == 0
+    assert mon["max_divu"] <= 1e-12 * scale, mon
+    assert np.abs(s.f["divu"]).max() <= 1e-12 * scale
+    assert np.abs(got["divu"] - s.f["divu"]).max() <= 1e-12 * scale
+    return errs
+
+
+def test_channel64_plain_10_steps():
+    """64^3 plain channel, no obstacle (mask 0), T = 1 at y = -1 and 0 at
+    y = 1: projection and 10 FP64 steps against the oracle."""
+    n = 64
+    g, f, dt = channel(n, n, n, seed=11, t_bot=1.0, t_top=0.0)
+    c1 = np.zeros((n, n, n), order="F")
+    got, mon, s = run_pair(g, f, dt, c1, 3000.0, 0.71, 1.0, 0.0, 0.0, 10)
+    check_state(got, mon, s, g)
+
+
+def oracle_poisson(g, rhs):
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    og = oracle_grid(g)
+    AC, KXZ = O.mkp_coeffs(og)
+    PT = O.p2s(rhs, nx, ny, nz)
+    O.spn(nx, ny, nz, AC, KXZ, PT)
+    O.sp0b(nx, ny, nz, AC, PT)
+    phi = O.s2p(PT, nx, ny, nz)
+    O.phibc(nx, ny, nz, phi)
+    return phi, AC, KXZ
+
+
+@pytest.mark.parametrize("n", [(64, 64, 64), (256, 192, 256)])
+def test_seeded_poisson_rhs(n):
+    """The seeded N(0,1) right-hand side with its dy-weighted mean removed
+    (W.poisson_rhs): the resident solve and the tier-1 drop-in chain against
+    the oracle's P2S -> SPN -> SP0B -> S2P -> PHIBC to 1e-12 relative L2."""
+    nx, ny, nz = n
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    rhs = W.poisson_rhs(g, seed=7)
+    ref, AC, KXZ = oracle_poisson(g, rhs)
+    I = (slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1))
+    cfg = S.Config(nx, ny, nz, 1.0, 1.0, 1.0, 0.0, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                   ystretch=2.0)
+    with S.Context(cfg) as ctx:
+        ctx.upload("phi", rhs)
+        ctx.poisson()
+        sol = ctx.download("phi")
+    assert rel_l2(sol[I], ref[I]) < 1e-12
+    if nx > 64:
+        return
+    # the same chain through the reference's own subroutine names
+    PT = np.zeros((nx // 2 + 1, ny + 2, nz + 2), dtype=np.complex128, order="F")
+    G.p2s(rhs.copy(order="F"), PT, nx, ny, nz)
+    G.spn(nx, ny, nz, AC, KXZ, PT)
+    G.sp0b(nx, ny, nz, AC, PT)
+    phi = W.padded(g)
+    G.s2p(PT, phi, nx, ny, nz)
+    G.phibc(nx, ny, nz, phi)
+    assert rel_l2(phi[I], ref[I]) < 1e-12
+
+
+@pytest.mark.parametrize("seed", [7000, 7001, 7002, 7005])
+def test_ensemble_cases_match_oracle(seed):
+    """Cases of the batched-ensemble workload (grids 64^3 .. 160x128x160,
+    1-3 spheres or cubes, own Re and noise, T = 1 at y = -1 and 0 at y = 1,
+    obstacles at T = 1) stepped alone: projection and 4 FP64 steps against
+    the oracle."""
+    g, f, phi0, Re, _ = W.ensemble_case(seed)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    c1 = W.smoothed_mask(g, phi0, 1.5)
+    got, mon, s = run_pair(g, f, dt, c1, Re, 0.71, 1.0, 0.0, 1.0, 4)
+    check_state(got, mon, s, g)
+
+
+@pytest.mark.parametrize("n", [(96, 64, 96), (160, 128, 160)])
+def test_ensemble_grids_with_sphere(n):
+    """The two ensemble grids whose x lines take the partitioned solver with
+    3 and 5 rows per lane, with the benchmark sphere, 5 FP64 steps."""
+    g, f, dt = channel(*n, seed=21, t_bot=1.0, t_top=0.0)
+    c1 = W.smoothed_mask(g, W.sphere_phi0(g, (math.pi, 0.0, math.pi / 2), 0.25), 1.5)
+    got, mon, s = run_pair(g, f, dt, c1, 3000.0, 0.71, 1.0, 0.0, 1.0, 5)
+    check_state(got, mon, s, g)
+
+
+def test_benchmark_workload_3_steps():
+    """The 256x192x256 benchmark workload (sphere R = 0.25 at (pi, 0, pi/2),
+    walls T = 0, sphere T = 1): projection and 3 FP64 steps against the
+    oracle."""
+    g, f, dt = channel(256, 192, 256, seed=2024, t_bot=0.0, t_top=0.0)
+    c1 = W.smoothed_mask(g, W.sphere_phi0(g, (math.pi, 0.0, math.pi / 2), 0.25), 1.5)
+    got, mon, s = run_pair(g, f, dt, c1, 3000.0, 0.71, 0.0, 0.0, 1.0, 3)
+    check_state(got, mon, s, g)

@@ -4,9 +4,11 @@ Fortran data region, or their time loop must not hit cudaMalloc, which
 stalls the whole device).  The caller passes device pointers; the solve's
 scratch is a fixed array inside the library.
 
-Checked through the C-ABI against the host-array entry point spn_ on two
-calls in a row (the fixed scratch keeps the previous call's contents), and
-a size beyond the fixed scratch must be refused with NSE_ERR_LIMIT.
+Checked through the C-ABI against the host-array entry point spn_ and the
+CPU oracle's SPN (mkp.f:223-260) on two calls in a row (the fixed scratch
+keeps the previous call's contents), including an odd size; a size beyond
+the fixed scratch, or beyond the launch grid's limit in z, must be refused
+with NSE_ERR_LIMIT.
 """
 import ctypes
 import math
@@ -38,9 +40,10 @@ def to_device(torch, a):
     return torch.from_numpy(flat.copy()).to("cuda:0")
 
 
-def test_noalloc_spn_matches_spn_on_two_calls():
+@pytest.mark.parametrize("n", [(32, 24, 20), (6, 5, 3)])
+def test_noalloc_spn_matches_spn_on_two_calls(n):
     import torch
-    nx, ny, nz = 32, 24, 20
+    nx, ny, nz = n
     g = O.Grid(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
     AC, KXZ = O.mkp_coeffs(g)
     dAC, dK = to_device(torch, AC), to_device(torch, KXZ)
@@ -52,12 +55,15 @@ def test_noalloc_spn_matches_spn_on_two_calls():
                                1j * rng.standard_normal((H, ny + 2, nz + 2)))
         ref = PT.copy(order="F")
         G.spn(nx, ny, nz, AC, KXZ, ref)
+        cpu = PT.copy(order="F")
+        O.spn(nx, ny, nz, AC, KXZ, cpu)
         d = to_device(torch, PT)
         st = entry()(nx, ny, nz, dAC.data_ptr(), dK.data_ptr(), d.data_ptr(), stream)
         assert st == NSE_OK, lib().nse_last_error()
         torch.cuda.synchronize()
         got = d.cpu().numpy().view(np.complex128).reshape(PT.shape, order="F")
         assert rel_l2(got, ref) < 1e-13
+        assert rel_l2(got, cpu) < 1e-13
         # entries SPN does not write are untouched
         assert np.array_equal(got[:, 0, :], PT[:, 0, :])
         assert np.array_equal(got[:, ny + 1, :], PT[:, ny + 1, :])
@@ -69,6 +75,10 @@ def test_noalloc_spn_refuses_sizes_beyond_its_scratch():
     buf = torch.zeros(16, dtype=torch.float64, device="cuda:0")
     p = buf.data_ptr()
     st = entry()(512, 256, 512, p, p, p, torch.cuda.current_stream().cuda_stream)
+    assert st == NSE_ERR_LIMIT
+    lib().nse_clear_error()
+    # fits the scratch (2 * 1 * 70000 values) but not the launch grid in z
+    st = entry()(2, 1, 70000, p, p, p, torch.cuda.current_stream().cuda_stream)
     assert st == NSE_ERR_LIMIT
     lib().nse_clear_error()
     assert torch.all(buf == 0)

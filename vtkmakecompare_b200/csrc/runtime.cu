@@ -95,20 +95,35 @@ bool cuda_ok(cudaError_t e, const char* what) {
   return false;
 }
 
+// device bytes the library holds (every allocation goes through DBuf) and
+// the cap set by nse_set_alloc_limit (0: none)
+static std::atomic<long long> g_alloc_bytes{0};
+static std::atomic<long long> g_alloc_limit{0};
+
 bool DBuf::ensure(size_t n) {
   if (n <= bytes && p) return true;
   release();
   if (n == 0) n = 16;
+  const long long lim = g_alloc_limit.load();
+  if (lim > 0 && g_alloc_bytes.load() + (long long)n > lim) {
+    set_error(NSE_ERR_NOMEM, "device allocation of %zu bytes refused: the library holds %lld "
+              "bytes and its limit is %lld (nse_set_alloc_limit)", n, g_alloc_bytes.load(), lim);
+    return false;
+  }
   if (!NSE_CUDA(cudaMalloc(&p, n))) {
     p = nullptr;
     bytes = 0;
     return false;
   }
   bytes = n;
+  g_alloc_bytes.fetch_add((long long)n);
   return true;
 }
 void DBuf::release() {
-  if (p) cudaFree(p);
+  if (p) {
+    cudaFree(p);
+    g_alloc_bytes.fetch_sub((long long)bytes);
+  }
   p = nullptr;
   bytes = 0;
 }
@@ -226,6 +241,8 @@ using namespace nse;
 extern "C" {
 
 const char* nse_last_error(void) { return g_msg; }
+void nse_set_alloc_limit(long long bytes) { g_alloc_limit.store(bytes > 0 ? bytes : 0); }
+long long nse_alloc_bytes(void) { return g_alloc_bytes.load(); }
 long long nse_launch_count(void) { return g_launches.load(); }
 int nse_last_status(void) { return g_status; }
 void nse_clear_error(void) {
@@ -411,6 +428,193 @@ void implicit_tx_(double* STX, const int* nx, const double* dx, const double* dx
   st.finish();
 }
 
+// ------------------------------------- parallel_* line drivers (tier 2) ----
+// nse_dominik.f:2893-3045: the reference's OpenMP loops in solve_u_temp and
+// solve_t call one of these per line; each gathers the line of a padded
+// field and its mask column into locals, calls the single-line solver and
+// scatters the result.  Here the gather and scatter are host loops around
+// the GPU single-line solvers above (one launch per call); solve_u_temp_,
+// solve_t_ and the resident step solve all lines of a field in one launch,
+// so these exist for a driver that calls them directly.
+static long pad_at(int nx, int ny, int i, int j, int k) {
+  return i + (long)(nx + 2) * (j + (long)(ny + 2) * k);
+}
+static long cell_at(int nx, int ny, int nz, int i, int j, int k, int n) {
+  return (i - 1) + (long)nx * ((j - 1) + (long)ny * ((k - 1) + (long)nz * (n - 1)));
+}
+// a line index pair inside 1..na x 1..nb and a mask column 1..4
+static bool line_ok(const char* who, int a, int na, int b, int nb, int n) {
+  if (a < 1 || a > na || b < 1 || b > nb || n < 1 || n > 4) {
+    set_error(NSE_ERR_ARG, "%s: line (%d, %d) or mask column %d out of range", who, a, b, n);
+    return false;
+  }
+  return true;
+}
+
+// parallel_uy(i,k,u_a,cellvalue,nx,ny,nz,dy,dy12,Re,dt,eta,n) :2893;
+// writes u_a(i,0:ny+1,k)
+void parallel_uy_(const int* i, const int* k, double* u_a, const double* cellvalue,
+                  const int* nx, const int* ny, const int* nz, const double* dy,
+                  const double* dy12, const double* Re, const double* dt, const double* eta,
+                  const int* n) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_uy") || !line_ok("parallel_uy", *i, NX, *k, NZ, *n))
+    return;
+  std::vector<double> S(NY + 2, 0.0), C(NY, 0.0);
+  for (int j = 1; j <= NY; ++j) {
+    S[j] = u_a[pad_at(NX, NY, *i, j, *k)];
+    C[j - 1] = cellvalue[cell_at(NX, NY, NZ, *i, j, *k, *n)];
+  }
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_uy_(S.data(), ny, dy, dy12, Re, dt, &ft, &fb, eta, C.data());
+  if (g_status != NSE_OK) return;
+  for (int j = 0; j <= NY + 1; ++j) u_a[pad_at(NX, NY, *i, j, *k)] = S[j];
+}
+
+// parallel_vy(i,k,v_a,...) :2950; gathers j = 1..ny-1, writes v_a(i,0:ny,k)
+void parallel_vy_(const int* i, const int* k, double* v_a, const double* cellvalue,
+                  const int* nx, const int* ny, const int* nz, const double* dy,
+                  const double* dy12, const double* Re, const double* dt, const double* eta,
+                  const int* n) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_vy") || !line_ok("parallel_vy", *i, NX, *k, NZ, *n))
+    return;
+  std::vector<double> S(NY + 2, 0.0), C(NY, 0.0);
+  for (int j = 1; j <= NY - 1; ++j) {
+    S[j] = v_a[pad_at(NX, NY, *i, j, *k)];
+    C[j - 1] = cellvalue[cell_at(NX, NY, NZ, *i, j, *k, *n)];
+  }
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_vy_(S.data(), ny, dy, dy12, Re, dt, &ft, &fb, eta, C.data());
+  if (g_status != NSE_OK) return;
+  for (int j = 0; j <= NY; ++j) v_a[pad_at(NX, NY, *i, j, *k)] = S[j];
+}
+
+// parallel_z(i,j,u_a,cellvalue,nx,ny,nz,dz,dz12,Re,dt,eta,n) :2912;
+// writes u_a(i,j,0:nz+1)
+void parallel_z_(const int* i, const int* j, double* u_a, const double* cellvalue,
+                 const int* nx, const int* ny, const int* nz, const double* dz,
+                 const double* dz12, const double* Re, const double* dt, const double* eta,
+                 const int* n) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_z") || !line_ok("parallel_z", *i, NX, *j, NY, *n))
+    return;
+  std::vector<double> S(NZ + 2, 0.0), C(NZ, 0.0);
+  for (int k = 1; k <= NZ; ++k) {
+    S[k] = u_a[pad_at(NX, NY, *i, *j, k)];
+    C[k - 1] = cellvalue[cell_at(NX, NY, NZ, *i, *j, k, *n)];
+  }
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_solver_(S.data(), nz, dz, dz12, Re, dt, &ft, &fb, eta, C.data());
+  if (g_status != NSE_OK) return;
+  for (int k = 0; k <= NZ + 1; ++k) u_a[pad_at(NX, NY, *i, *j, k)] = S[k];
+}
+
+// parallel_x(j,k,u_a,cellvalue,nx,ny,nz,dx,dx12,Re,dt,eta,n) :2931;
+// writes u_a(0:nx+1,j,k)
+void parallel_x_(const int* j, const int* k, double* u_a, const double* cellvalue,
+                 const int* nx, const int* ny, const int* nz, const double* dx,
+                 const double* dx12, const double* Re, const double* dt, const double* eta,
+                 const int* n) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_x") || !line_ok("parallel_x", *j, NY, *k, NZ, *n))
+    return;
+  std::vector<double> S(NX + 2, 0.0), C(NX, 0.0);
+  for (int i = 1; i <= NX; ++i) {
+    S[i] = u_a[pad_at(NX, NY, i, *j, *k)];
+    C[i - 1] = cellvalue[cell_at(NX, NY, NZ, i, *j, *k, *n)];
+  }
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_solver_(S.data(), nx, dx, dx12, Re, dt, &ft, &fb, eta, C.data());
+  if (g_status != NSE_OK) return;
+  for (int i = 0; i <= NX + 1; ++i) u_a[pad_at(NX, NY, i, *j, *k)] = S[i];
+}
+
+// gather of a temperature line along `dir` (0 x, 1 y, 2 z) through cell
+// (a, b) of the other two directions: STX/rrx/llx/CUX of parallel_Tx/Ty/Tz.
+// The reference leaves the end entries of its rr/ll locals unset while
+// implicit_Tx/Ty read them (nse_dominik.f:2979-2984); they are taken here
+// from the rhoCp and thc ghost cells of the line.
+static int t_line(int dir, int a, int b, int NX, int NY, int NZ, const double* rhoCp,
+                  const double* thc, const double* u_T, const double* cellvalue,
+                  std::vector<double>& S, std::vector<double>& R, std::vector<double>& Lc,
+                  std::vector<double>& C) {
+  const int n = dir == 0 ? NX : (dir == 1 ? NY : NZ);
+  S.assign(n + 2, 0.0); R.assign(n + 2, 0.0); Lc.assign(n + 2, 0.0); C.assign(n + 2, 0.0);
+  for (int q = 0; q <= n + 1; ++q) {
+    const int i = dir == 0 ? q : a, j = dir == 1 ? q : (dir == 0 ? a : b),
+              k = dir == 2 ? q : b;
+    const long c = pad_at(NX, NY, i, j, k);
+    R[q] = rhoCp[c];
+    Lc[q] = thc[c];
+    if (q >= 1 && q <= n) {
+      S[q] = u_T[c];
+      C[q] = cellvalue[cell_at(NX, NY, NZ, i, j, k, 1)];
+    }
+  }
+  return n;
+}
+
+// parallel_Tx(k,j,nx,ny,nz,rhoCp,thc,u_T,cellvalue,dx,dx12,Re,Sc,dt,eta) :2969;
+// writes u_T(1:nx,j,k)
+void parallel_tx_(const int* k, const int* j, const int* nx, const int* ny, const int* nz,
+                  const double* rhoCp, const double* thc, double* u_T,
+                  const double* cellvalue, const double* dx, const double* dx12,
+                  const double* Re, const double* Sc, const double* dt, const double* eta) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_tx") || !line_ok("parallel_tx", *j, NY, *k, NZ, 1))
+    return;
+  std::vector<double> S, R, Lc, C;
+  t_line(0, *j, *k, NX, NY, NZ, rhoCp, thc, u_T, cellvalue, S, R, Lc, C);
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_tx_(S.data(), nx, dx, dx12, Re, Sc, dt, Lc.data(), R.data(), &ft, &fb, eta,
+               C.data());
+  if (g_status != NSE_OK) return;
+  for (int i = 1; i <= NX; ++i) u_T[pad_at(NX, NY, i, *j, *k)] = S[i];
+}
+
+// parallel_Ty(i,k,...,dy,dy12,Re,Sc,dt,eta) :2995; writes u_T(i,1:ny,k)
+void parallel_ty_(const int* i, const int* k, const int* nx, const int* ny, const int* nz,
+                  const double* rhoCp, const double* thc, double* u_T,
+                  const double* cellvalue, const double* dy, const double* dy12,
+                  const double* Re, const double* Sc, const double* dt, const double* eta) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_ty") || !line_ok("parallel_ty", *i, NX, *k, NZ, 1))
+    return;
+  std::vector<double> S, R, Lc, C;
+  t_line(1, *i, *k, NX, NY, NZ, rhoCp, thc, u_T, cellvalue, S, R, Lc, C);
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_ty_(S.data(), ny, dy, dy12, Re, Sc, dt, Lc.data(), R.data(), &ft, &fb, C.data(),
+               eta);
+  if (g_status != NSE_OK) return;
+  for (int j = 1; j <= NY; ++j) u_T[pad_at(NX, NY, *i, j, *k)] = S[j];
+}
+
+// parallel_Tz(i,j,...,dz,dz12,Re,Sc,dt,eta) :3021 (through implicit_Tx, as
+// the reference does at :3039); writes u_T(i,j,1:nz)
+void parallel_tz_(const int* i, const int* j, const int* nx, const int* ny, const int* nz,
+                  const double* rhoCp, const double* thc, double* u_T,
+                  const double* cellvalue, const double* dz, const double* dz12,
+                  const double* Re, const double* Sc, const double* dt, const double* eta) {
+  const int NX = *nx, NY = *ny, NZ = *nz;
+  if (!dims_ok(NX, NY, NZ, "parallel_tz") || !line_ok("parallel_tz", *i, NX, *j, NY, 1))
+    return;
+  std::vector<double> S, R, Lc, C;
+  t_line(2, *i, *j, NX, NY, NZ, rhoCp, thc, u_T, cellvalue, S, R, Lc, C);
+  const double ft = 0.0, fb = 0.0;
+  nse_clear_error();
+  implicit_tx_(S.data(), nz, dz, dz12, Re, Sc, dt, Lc.data(), R.data(), &ft, &fb, eta,
+               C.data());
+  if (g_status != NSE_OK) return;
+  for (int k = 1; k <= NZ; ++k) u_T[pad_at(NX, NY, *i, *j, k)] = S[k];
+}
+
 // ------------------------------------------------------------- SET_C ------
 // grid setup (nse_dominik.f:553-607); O(n) host arithmetic, not a GPU path
 static void set_c_dir(int n, double L, double* X, double* X12, double* D, double* D12) {
@@ -481,7 +685,7 @@ extern "C" {
 // ----------------------------------------------------- tier-2 stencils ----
 void set_bc_(double* u, double* v, double* w, double* p, const int* nx, const int* ny,
              const int* nz, double* T) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_bc")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_bc") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   double *du = st.up(u, d.ntot), *dv = st.up(v, d.ntot), *dw = st.up(w, d.ntot);
@@ -503,7 +707,7 @@ void set_convect_(double* u, double* u_v, double* v, double* v_v, double* w, dou
                   const double* dt, const int* nx, const int* ny, const int* nz,
                   const double* dx, const double* dy, const double* dz, const double* dx12,
                   const double* dy12, const double* dz12) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_convect")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_convect") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -523,7 +727,7 @@ void set_convection_for_scalar_(double* u, double* v, double* w, const double* d
                                 const double* dx, const double* dy, const double* dz,
                                 const double* dx12, const double* dy12, const double* dz12,
                                 double* T, double* u_vT, double* rhoCp) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_convection_for_scalar")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_convection_for_scalar") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -540,7 +744,7 @@ void set_conduction_(double* u, double* u_d, double* v, double* v_d, double* w, 
                      const double* Re, const double* dt, const int* nx, const int* ny,
                      const int* nz, const double* dx, const double* dy, const double* dz,
                      const double* dx12, const double* dy12, const double* dz12) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_conduction")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_conduction") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -560,7 +764,7 @@ void set_diffusion_for_scalar_(const double* Re, const double* dt, const int* nx
                                const double* dy, const double* dz, const double* dx12,
                                const double* dy12, const double* dz12, double* T,
                                double* u_dT, const double* Sc, double* thc, double* rhoCp) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_diffusion_for_scalar")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_diffusion_for_scalar") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -580,7 +784,7 @@ void set_adj_convect_(double* u, double* u_v, double* v, double* v_v, double* w,
                       const double* dx12, const double* dy12, const double* dz12,
                       double* u_final, double* v_final, double* w_final) {
   (void)Re;
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_adj_convect")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_adj_convect") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -605,7 +809,7 @@ void set_adj_convection_for_scalar_(double* u, double* v, double* w, const doubl
                                     double* rhoCp, double* u_final, double* v_final,
                                     double* w_final) {
   (void)u; (void)v; (void)w; (void)Re;
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_adj_convection_for_scalar")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_adj_convection_for_scalar") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -623,7 +827,7 @@ void set_adj_convection_for_scalar_(double* u, double* v, double* w, const doubl
 static void adj_ns_scalar(const double* dt, int nx, int ny, int nz, const double* dx12,
                           const double* dy12, const double* dz12, const double* T,
                           const double* Tf, double* u_s, double* v_s, double* w_s) {
-  if (!ensure_device() || !dims_ok(nx, ny, nz, "set_adj_ns_scalar")) return;
+  if (!dims_ok(nx, ny, nz, "set_adj_ns_scalar") || !ensure_device()) return;
   Dims d = make_dims(nx, ny, nz);
   Stage st;
   GridDev g;
@@ -667,7 +871,7 @@ void set_immersed_boundary_(const double* eta, const int* nx, const int* ny, con
                             double* T_l, double* cellvalue, double* u_ta, double* v_ta,
                             double* w_ta, const int* l, double* cons_cell) {
   (void)dx; (void)dy; (void)dz;
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_immersed_boundary")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_immersed_boundary") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   double* dcv = st.up(cellvalue, 4 * (size_t)d.ncell);
@@ -692,7 +896,7 @@ void set_explicit_(double* u_v, double* u_pre, double* u_d, double* u_a, double*
                    double* v_pre, double* v_d, double* v_a, double* w_v, double* w_pre,
                    double* w_d, double* w_a, double* u_l, double* v_l, double* w_l,
                    const int* nx, const int* ny, const int* nz, const int* l) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_explicit")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_explicit") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   size_t n = d.ntot;
@@ -712,7 +916,7 @@ void set_explicit_(double* u_v, double* u_pre, double* u_d, double* u_a, double*
 void set_explicit_for_tempreture_(double* u_vT, double* u_dT, double* u_T, double* T_pre,
                                   double* T_l, const int* nx, const int* ny, const int* nz,
                                   const int* l) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_explicit_for_tempreture")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_explicit_for_tempreture") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   size_t n = d.ntot;
@@ -730,7 +934,7 @@ void solve_u_temp_(double* u_a, double* v_a, double* w_a, const int* nx, const i
                    const double* dx12, const double* dy12, const double* dz12,
                    const double* Re, const double* dt, const double* eta,
                    double* cellvalue, double* u, double* v, double* w) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "solve_u_temp")) return;
+  if (!dims_ok(*nx, *ny, *nz, "solve_u_temp") || !ensure_device()) return;
   if (*ny < 2) { set_error(NSE_ERR_ARG, "solve_u_temp: ny=%d < 2", *ny); return; }
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
@@ -759,7 +963,7 @@ void solve_t_(double* u_T, const int* nx, const int* ny, const int* nz, const do
               const double* dy, const double* dz, const double* dx12, const double* dy12,
               const double* dz12, const double* Re, const double* Sc, const double* dt,
               double* rhoCp, double* thc, double* cellvalue, const double* eta) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "solve_t")) return;
+  if (!dims_ok(*nx, *ny, *nz, "solve_t") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -867,7 +1071,7 @@ extern "C" {
 
 // ------------------------------------------------------------ p2s / s2p ----
 void p2s_(double* FP, double* FPT, const int* NX, const int* NY, const int* NZ) {
-  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "p2s")) return;
+  if (!dims_ok(*NX, *NY, *NZ, "p2s") || !ensure_device()) return;
   int nx = *NX, ny = *NY, nz = *NZ;
   Dims d = make_dims(nx, ny, nz);
   Stage st;
@@ -892,7 +1096,7 @@ void p2s_(double* FP, double* FPT, const int* NX, const int* NY, const int* NZ) 
 }
 
 void s2p_(double* FPT, double* FP, const int* NX, const int* NY, const int* NZ) {
-  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "s2p")) return;
+  if (!dims_ok(*NX, *NY, *NZ, "s2p") || !ensure_device()) return;
   int nx = *NX, ny = *NY, nz = *NZ;
   Dims d = make_dims(nx, ny, nz);
   Stage st;
@@ -916,7 +1120,7 @@ void s2p_(double* FPT, double* FP, const int* NX, const int* NY, const int* NZ) 
 // --------------------------------------------------- SPN / SP0B / PHIBC ----
 void spn_(const int* NX, const int* NY, const int* NZ, const double* AC, const double* KXZ,
           double* PHIT) {
-  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "spn")) return;
+  if (!dims_ok(*NX, *NY, *NZ, "spn") || !ensure_device()) return;
   int nx = *NX, ny = *NY, nz = *NZ;
   Stage st;
   int H = nx / 2 + 1;
@@ -941,7 +1145,7 @@ void spn_(const int* NX, const int* NY, const int* NZ, const double* AC, const d
 }
 
 void sp0b_(const int* NX, const int* NY, const int* NZ, const double* AC, double* PHIT) {
-  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "sp0b")) return;
+  if (!dims_ok(*NX, *NY, *NZ, "sp0b") || !ensure_device()) return;
   int nx = *NX, ny = *NY;
   Stage st;
   int H = nx / 2 + 1;
@@ -960,7 +1164,7 @@ void sp0b_(const int* NX, const int* NY, const int* NZ, const double* AC, double
 }
 
 void phibc_(const int* NX, const int* NY, const int* NZ, double* PHI) {
-  if (!ensure_device() || !dims_ok(*NX, *NY, *NZ, "phibc")) return;
+  if (!dims_ok(*NX, *NY, *NZ, "phibc") || !ensure_device()) return;
   Dims d = make_dims(*NX, *NY, *NZ);
   Stage st;
   double* dphi = st.up(PHI, d.ntot);
@@ -978,7 +1182,7 @@ void mkp_(double* p, double* u_temp, double* v_temp, double* w_temp, const doubl
           double* w_ta, double* u_ep2, double* v_ep2, double* w_ep2, double* divu,
           double* u, double* v, double* w, const double* xl, const double* zl) {
   (void)Re; (void)ompnthreads;
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "mkp")) return;
+  if (!dims_ok(*nx, *ny, *nz, "mkp") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   PoissonBufs& pb = legacy_poisson();
@@ -1083,7 +1287,7 @@ void set_levelset_(const int* nx, const int* ny, const int* nz, const double* dx
                    const double* dx12, const double* dy12, const double* dz12,
                    const double* phi0, double* phi, const double* x, const double* y,
                    const double* z, double* cellvalue) {
-  if (!ensure_device() || !dims_ok(*nx, *ny, *nz, "set_levelset")) return;
+  if (!dims_ok(*nx, *ny, *nz, "set_levelset") || !ensure_device()) return;
   Dims d = make_dims(*nx, *ny, *nz);
   Stage st;
   GridDev g;
@@ -1395,7 +1599,6 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
   nse_clear_error();
   if (!cfg || !out) { set_error(NSE_ERR_ARG, "nse_ctx_create: null argument"); return NSE_ERR_ARG; }
   *out = nullptr;
-  if (!ensure_device()) return NSE_ERR_CUDA;
   const nse_config& c = *cfg;
   if (c.nx < 2 || c.ny < 3 || c.nz < 2) {
     set_error(NSE_ERR_ARG, "nse_ctx_create: need nx>=2, ny>=3, nz>=2 (got %d %d %d)", c.nx, c.ny, c.nz);
@@ -1413,6 +1616,9 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
     set_error(NSE_ERR_ARG, "nse_ctx_create: precision %d not available", c.precision);
     return NSE_ERR_ARG;
   }
+  // arguments are checked first, so a bad call reports NSE_ERR_ARG with or
+  // without a usable GPU
+  if (!ensure_device()) return NSE_ERR_CUDA;
   nse_ctx* x = new nse_ctx();
   x->cfg = c;
   x->mixed = c.precision == NSE_MIXED;

@@ -52,6 +52,13 @@ _SIG = {
     "implicit_vy": "aiaaddddda",           # nse_dominik.f:1583
     "implicit_tx": "aiaadddaaddda",        # nse_dominik.f:1725
     "implicit_ty": "aiaadddaaddad",        # nse_dominik.f:1784
+    "parallel_uy": "iiaaiiiaadddi",        # nse_dominik.f:2893
+    "parallel_z": "iiaaiiiaadddi",         # nse_dominik.f:2912
+    "parallel_x": "iiaaiiiaadddi",         # nse_dominik.f:2931
+    "parallel_vy": "iiaaiiiaadddi",        # nse_dominik.f:2950
+    "parallel_tx": "iiiiiaaaaaadddd",      # nse_dominik.f:2969
+    "parallel_ty": "iiiiiaaaaaadddd",      # nse_dominik.f:2995
+    "parallel_tz": "iiiiiaaaaaadddd",      # nse_dominik.f:3021
     "output": "aaaaaaaiiiaaaaaaa",         # nse_dominik.f:2606 (files under ./)
     "outfield": "aaaaaaaiiidaaaaa",        # nse_dominik.f:2726
     "readfield": "aaaaiiiaaaaa",           # nse_dominik.f:2769

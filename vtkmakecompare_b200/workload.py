@@ -54,6 +54,19 @@ def sphere_phi0(g, center, radius):
     return phi0
 
 
+def smoothed_mask(g, phi0, width):
+    """Cell mask c1 of set_levelset.f:157-170 applied directly to a level set
+    phi0 (padded, interior used) that is already a signed distance, without
+    the reinitialisation sweeps: 1 where phi >= w*dx_i, 0 where phi <= -w*dx_i,
+    (sin(pi phi / (2 w dx_i)) + 1)/2 between, with the reference's
+    pi = 3.1415926535 (set_levelset.f:7).  numpy only (no library call), so
+    the GPU run and the CPU reference run start from the same mask."""
+    phi = phi0[1:-1, 1:-1, 1:-1]
+    h = width * g["dx"][1:-1, None, None]
+    c = (np.sin(3.1415926535 * phi / 2.0 / h) + 1.0) / 2.0
+    return np.asfortranarray(np.where(phi >= h, 1.0, np.where(phi <= -h, 0.0, c)))
+
+
 def channel_state(g, seed, noise=0.05, t_bot=1.0, t_top=0.0, bulk=True):
     """u = 1.5(1 - y^2) + N(0, noise^2), v, w ~ N(0, noise^2) on interior cells
     (y measured so that the walls are at -1, 1), T linear from t_bot to t_top."""
