@@ -197,9 +197,10 @@ def build_case(S, W, torch, precision=0, flags=0, levelset=True):
 
 
 # mixed-precision variants reported beside the FP64 line: name -> nse flags
-MIXED_VARIANTS = (("mixed", 0),                      # FP32 FFTs + 1 FP64 refinement pass
-                  ("mixed_fp64_poisson", 16),        # NSE_FLAG_POISSON64
-                  ("mixed_fp64_lines", 16 | 64))     # + NSE_FLAG_LINES64
+MIXED_VARIANTS = (("mixed", 0),                      # default: FP64 Poisson solve
+                  ("mixed_fp64_lines", 64),          # + NSE_FLAG_LINES64
+                  ("mixed_fp32_poisson", 512))       # NSE_FLAG_POISSON32: FP32 FFTs + 1
+                                                     # FP64 refinement pass
 
 
 def run_mixed(S, W, torch, stream, args, fp64_ms):
@@ -370,7 +371,7 @@ def run_ensemble(S, W, torch, stream, args, rank=0, world=1, device="cpu"):
                            "the slowest rank's time; per-case scalars gathered by one all-reduce")
     finals = {}
     divs = {}
-    for name, prec, flags in (("fp64", S.FP64, 0), ("mixed", S.MIXED, 16 | 64)):
+    for name, prec, flags in (("fp64", S.FP64, 0), ("mixed", S.MIXED, 64)):
         ctxs = build(prec, flags)
         for c in ctxs:
             c.set_stream(stream.cuda_stream)

@@ -256,28 +256,36 @@ typedef struct nse_config {
 } nse_config;
 
 /* NSE_MIXED (no counterpart in the reference): u, v, w, T, p and the Poisson
- * solution stay FP64; the right-hand-side stencils, the line sweeps and the
- * FFTs run on FP32 intermediates; the spectral tridiagonal recurrences, the
- * mean mode, the divergence and the reductions are FP64, and the Poisson
- * solve takes one FP64 residual-refinement pass.  u_ta, the AB2 histories,
- * u_ep2 and divu are held in FP32 (upload/download convert).  Needs
- * nx = 32*M (M in 3, 4, 5, 6, 8, 16) and 12..256 cells in y and z. */
+ * solution stay FP64; the right-hand-side stencils and the line sweeps run
+ * on FP32 intermediates; the divergence of the FP32 provisional velocity,
+ * the Poisson solve (transforms, spectral recurrences, mean mode), the
+ * correction and the reductions are FP64.  With NSE_FLAG_POISSON32 the
+ * Poisson transforms and spectrum are FP32 instead (FP64 recurrences) with
+ * one FP64 residual-refinement pass (two with NSE_FLAG_REFINE2).  u_ta, the
+ * AB2 histories, u_ep2 and divu are held in FP32 (upload/download convert).
+ * Needs nx = 32*M (M in 3, 4, 5, 6, 8, 16) and 12..512 cells in y and z. */
 enum { NSE_FP64 = 0, NSE_MIXED = 1 };
 /* nse_config.flags bits */
 enum {
   NSE_FLAG_CHECK_FINITE = 1, /* nse_step checks every step for non-finite values */
   NSE_FLAG_EXACT = 4,        /* resident step rounds every operation like the reference
                                 (no FMA, true divisions); default is the fast form */
-  NSE_FLAG_REFINE2 = 8,      /* NSE_MIXED: two refinement passes instead of one */
-  NSE_FLAG_POISSON64 = 16,   /* NSE_MIXED: FP64 transforms and spectrum instead of the
-                                FP32 solve with refinement */
+  NSE_FLAG_REFINE2 = 8,      /* NSE_MIXED + NSE_FLAG_POISSON32: two refinement passes
+                                instead of one */
+  NSE_FLAG_POISSON64 = 16,   /* NSE_MIXED: FP64 Poisson solve (the default; kept so
+                                callers that set it keep working) */
   NSE_FLAG_MATH64 = 32,      /* NSE_MIXED: FP64 arithmetic in the right-hand-side stencils
                                 (their results are still stored in FP32) */
   NSE_FLAG_LINES64 = 64,     /* NSE_MIXED: FP64 arithmetic and tables in the line sweeps
                                 (FP32 storage) */
-  NSE_FLAG_ONE_STREAM = 128  /* everything on the context's stream, in the reference's
+  NSE_FLAG_ONE_STREAM = 128, /* everything on the context's stream, in the reference's
                                 order (default: the line passes of u, v, w, T as four
                                 concurrent chains on side streams; same results) */
+  NSE_FLAG_POISSON5 = 256,   /* FP64 Poisson solve as five launches (x and z transforms
+                                separate) instead of three (each plane's 2-D transform
+                                in one cluster launch; NX = NZ = 256, ny = 16 m) */
+  NSE_FLAG_POISSON32 = 512   /* NSE_MIXED: FP32 Poisson transforms and spectrum with FP64
+                                residual refinement instead of the FP64 solve */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

@@ -216,7 +216,7 @@ def test_projection_is_divergence_free():
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                        g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
                        body_force=par["force"], heat_source=par["source"], precision=prec,
-                       flags=S.FLAG_POISSON64 if prec == S.MIXED else 0)
+                       flags=0)
         with S.Context(cfg) as ctx:
             for k in ("u", "v", "w", "T"):
                 ctx.upload(k, f[k])
@@ -227,7 +227,7 @@ def test_projection_is_divergence_free():
 
 
 
-@pytest.mark.parametrize("prec,base", [(S.FP64, 0), (S.MIXED, 0), (S.MIXED, S.FLAG_POISSON64)])
+@pytest.mark.parametrize("prec,base", [(S.FP64, 0), (S.MIXED, 0), (S.MIXED, S.FLAG_POISSON32)])
 @pytest.mark.parametrize("n", [(96, 48, 64), (128, 40, 96)])
 def test_concurrent_line_chains_equal_serial(n, prec, base):
     """The fast and mixed forms run the four components' line chains on

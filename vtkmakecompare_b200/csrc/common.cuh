@@ -257,6 +257,14 @@ void launch_spn_view(int H, int ny, int nz, double* base, long sj, long sk, doub
 void launch_fft_inv_x(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s,
                       int j0 = 0, int nj = 0);
 void launch_phibc(const Dims& d, double* PHI, cudaStream_t s);
+// k_poisson2d.cu: the three-pass solve for NX = NZ = 256 (FP64).  P2S of
+// every plane (one cluster of 8 CTAs per plane), SPN + SP0B partitioned over
+// 16 lanes per system (ny = 16 m, 3 <= m <= 16), S2P + PHIBC.
+bool poisson3_ok(const PoissonPlan& pp);
+bool spn_part_ok(const PoissonPlan& pp);
+void launch_p2s256(const PoissonPlan& pp, const Dims& d, const double* FP, cudaStream_t s);
+void launch_spn_part(const PoissonPlan& pp, cudaStream_t s);
+void launch_s2p256_phibc(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s);
 // spectrum <-> reference PHIT layout (0:nx/2,0:ny+1,0:nz+1)
 void launch_spec_to_phit(const PoissonPlan& pp, double* phit, cudaStream_t s);
 void launch_phit_to_spec(const PoissonPlan& pp, const double* phit, cudaStream_t s);

@@ -1797,37 +1797,78 @@ int nse_start(nse_ctx* x) {
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
 
-// MKP in the mixed-precision form: FP32 u*, v*, w*; FP32 spectral solve with
-// FP64 residual refinement (or, with NSE_FLAG_POISSON64, the FP64 solve of
-// the FP64 divergence); FP64 correction of the FP64 state
+// the three-pass Poisson solve (k_poisson2d.cu) of the fast forms: NX = NZ
+// = 256 and ny = 16 m, unless NSE_FLAG_POISSON5 asks for the five passes
+static bool poisson3(const nse_ctx* x) {
+  return !(x->cfg.flags & (NSE_FLAG_EXACT | NSE_FLAG_POISSON5)) && poisson3_ok(x->pb.pp);
+}
+
+// P2S -> SPN/SP0B -> S2P -> PHIBC on phi (FP64), phase-marked
+static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
+  const Dims& d = x->d;
+  cudaStream_t s = x->stream;
+  const PoissonPlan& pp = x->pb.pp;
+  if (!div_marked) mark(x, PH_FFTX_F);
+  if (poisson3(x)) {
+    launch_p2s256(pp, d, phi, s);
+    mark(x, PH_FFTZ_F);
+    mark(x, PH_SPN);
+    launch_spn_part(pp, s);
+    mark(x, PH_FFTZ_I);
+    mark(x, PH_FFTX_I);
+    launch_s2p256_phibc(pp, d, phi, s);
+    mark(x, PH_PHIBC);
+    return;
+  }
+  launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
+  mark(x, PH_FFTZ_F);
+  launch_fft_z(pp, false, s);
+  mark(x, PH_SPN);
+  launch_spn_fast(pp, s);
+  mark(x, PH_FFTZ_I);
+  launch_fft_z(pp, true, s);
+  mark(x, PH_FFTX_I);
+  launch_fft_inv_x(pp, d, phi, s);
+  mark(x, PH_PHIBC);
+  launch_phibc(d, phi, s);
+}
+
+// MKP in the mixed-precision form: FP32 u*, v*, w*; the FP64 solve of their
+// FP64 divergence (or, with NSE_FLAG_POISSON32, the FP32 spectral solve with
+// FP64 residual refinement); FP64 correction of the FP64 state
 static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const float* wt) {
   const Dims& d = x->d;
   cudaStream_t s = x->stream;
   const PoissonPlan& pp = x->pb.pp;
   double* phi = F(x, NSE_PHI);
   const double dt = x->cfg.dt, dx = x->hdx[1], dz = x->hdz[1];
-  const bool p64 = (x->cfg.flags & NSE_FLAG_POISSON64) != 0;
+  const bool p64 = (x->cfg.flags & NSE_FLAG_POISSON32) == 0;
   mark(x, PH_FFTX_F);
-  if (p64) {
+  if (p64 && poisson3(x)) {
+    launch_div_src32(d, x->rg, ut, vt, wt, dt, phi, s);
+    ctx_poisson64(x, phi, true);
+  } else if (p64) {
     launch_div_src32(d, x->rg, ut, vt, wt, dt, phi, s);
     launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
   } else {
     launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, nullptr, dx, dz, 1, s);
   }
-  mark(x, PH_FFTZ_F);
-  if (p64) launch_fft_z(pp, false, s);
-  else launch_fft_z_f32(pp, false, s);
-  mark(x, PH_SPN);
-  if (p64) launch_spn_fast(pp, s);
-  else launch_spn_fast_f32(pp, s);
-  mark(x, PH_FFTZ_I);
-  if (p64) launch_fft_z(pp, true, s);
-  else launch_fft_z_f32(pp, true, s);
-  mark(x, PH_FFTX_I);
-  if (p64) launch_fft_inv_x(pp, d, phi, s);
-  else launch_fft_inv_x_f32(pp, d, phi, false, s);
-  mark(x, PH_PHIBC);
-  launch_phibc(d, phi, s);
+  if (!(p64 && poisson3(x))) {
+    mark(x, PH_FFTZ_F);
+    if (p64) launch_fft_z(pp, false, s);
+    else launch_fft_z_f32(pp, false, s);
+    mark(x, PH_SPN);
+    if (p64) launch_spn_fast(pp, s);
+    else launch_spn_fast_f32(pp, s);
+    mark(x, PH_FFTZ_I);
+    if (p64) launch_fft_z(pp, true, s);
+    else launch_fft_z_f32(pp, true, s);
+    mark(x, PH_FFTX_I);
+    if (p64) launch_fft_inv_x(pp, d, phi, s);
+    else launch_fft_inv_x_f32(pp, d, phi, false, s);
+    mark(x, PH_PHIBC);
+    launch_phibc(d, phi, s);
+  }
   mark(x, PH_REFINE);
   for (int r = 0; !p64 && r < x->refine; ++r) {
     launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, phi, dx, dz, 2, s);
@@ -1854,23 +1895,28 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
   const PoissonPlan& pp = x->pb.pp;
   const GridRcp* rg = (x->cfg.flags & NSE_FLAG_EXACT) ? nullptr : &x->rg;
   mark(x, PH_FFTX_F);
-  if (rg) {
+  if (rg && poisson3(x)) {
+    launch_div_src(d, *rg, ut, vt, wt, x->cfg.dt, phi, s);
+    ctx_poisson64(x, phi, true);
+  } else if (rg) {
     // phi is free until the inverse x pass: it holds the divergence samples
     launch_div_src(d, *rg, ut, vt, wt, x->cfg.dt, phi, s);
     launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
   } else {
     launch_fft_fwd_x(pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s, rg);
   }
-  mark(x, PH_FFTZ_F);
-  launch_fft_z(pp, false, s);
-  mark(x, PH_SPN);
-  launch_spn_fast(pp, s);
-  mark(x, PH_FFTZ_I);
-  launch_fft_z(pp, true, s);
-  mark(x, PH_FFTX_I);
-  launch_fft_inv_x(pp, d, phi, s);
-  mark(x, PH_PHIBC);
-  launch_phibc(d, phi, s);
+  if (!(rg && poisson3(x))) {
+    mark(x, PH_FFTZ_F);
+    launch_fft_z(pp, false, s);
+    mark(x, PH_SPN);
+    launch_spn_fast(pp, s);
+    mark(x, PH_FFTZ_I);
+    launch_fft_z(pp, true, s);
+    mark(x, PH_FFTX_I);
+    launch_fft_inv_x(pp, d, phi, s);
+    mark(x, PH_PHIBC);
+    launch_phibc(d, phi, s);
+  }
   mark(x, PH_REFINE);
   mark(x, PH_CORRECT);
   if (x->cfg.flags & NSE_FLAG_EXACT)
@@ -1915,16 +1961,7 @@ int nse_project(nse_ctx* x) {
 
 int nse_poisson(nse_ctx* x) {
   if (!x) return NSE_ERR_ARG;
-  const Dims& d = x->d;
-  cudaStream_t s = x->stream;
-  double* phi = F(x, NSE_PHI);
-  const PoissonPlan& pp = x->pb.pp;
-  launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
-  launch_fft_z(pp, false, s);
-  launch_spn_fast(pp, s);
-  launch_fft_z(pp, true, s);
-  launch_fft_inv_x(pp, d, phi, s);
-  launch_phibc(d, phi, s);
+  ctx_poisson64(x, F(x, NSE_PHI), false);
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
 

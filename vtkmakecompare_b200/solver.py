@@ -24,6 +24,8 @@ FLAG_POISSON64 = 16
 FLAG_MATH64 = 32
 FLAG_LINES64 = 64
 FLAG_ONE_STREAM = 128
+FLAG_POISSON5 = 256
+FLAG_POISSON32 = 512
 
 
 class Config(C.Structure):
