@@ -273,6 +273,89 @@ def run_mixed(S, W, torch, stream, args, fp64_ms):
     return out
 
 
+def run_big(S, W, torch, stream, args):
+    """The 512x256x512 mixed-precision workload: the sphere geometry of the
+    main workload on the finer grid, the mixed form (default: FP64 Poisson
+    solve) and the FP64 form stepped args.big_steps penalised steps from the
+    same projected seeded field and the same mask; per-step divergence of
+    both, relative L2 of u, v, w, T and of the joint velocity of the mixed run
+    against the FP64 run, and the speed of both.  Then the seeded N(0,1)
+    right-hand side (dy-weighted mean removed) solved by the FP64 Poisson
+    solve, with the relative residual of the discrete operator it inverts."""
+    nx, ny, nz = 512, 256, 512
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    f = W.channel_state(g, seed=512, t_bot=0.0, t_top=0.0)
+    dt = W.cfl_dt(g, f["u"], f["v"], f["w"])
+    c1 = W.smoothed_mask(g, W.sphere_phi0(g, *SPHERE), WIDTH)
+    res = {"grid": [nx, ny, nz], "steps": args.big_steps, "dt": dt,
+           "mask": "smoothed Heaviside (1.5 dx) of the exact sphere signed distance"}
+    out = {}
+    for name, prec in (("fp64", S.FP64), ("mixed", S.MIXED)):
+        cfg = S.Config(nx, ny, nz, dt, RE, PR, ETA, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                       ystretch=2.0, body_force=3.0 / RE, heat_source=0.0, t_bot=0.0,
+                       t_top=0.0, t_solid=1.0, precision=prec)
+        with S.Context(cfg) as ctx:
+            ctx.set_stream(stream.cuda_stream)
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.project()
+            ctx.start()
+            divs = []
+            torch.cuda.synchronize()
+            e0 = torch.cuda.Event(enable_timing=True)
+            e1 = torch.cuda.Event(enable_timing=True)
+            ms = 0.0
+            for _ in range(args.big_steps):
+                e0.record(stream)
+                ctx.step(1)
+                e1.record(stream)
+                d = ctx.monitor()
+                ms += e0.elapsed_time(e1)
+                divs.append(d["max_divu"])
+            out[name] = {k: ctx.download(k) for k in ("u", "v", "w", "T")}
+            res[name] = {"ms_per_step": round(ms / max(1, args.big_steps), 4),
+                         "max_divu": max(divs), "max_divu_step1": divs[0] if divs else None}
+            if prec == S.FP64:
+                rhs = W.poisson_rhs(g, seed=513)
+                ctx.upload("phi", rhs)
+                ctx.poisson()
+                phi = ctx.download("phi")
+                res["poisson_rhs"] = {"seed": 513, "solve": "fp64",
+                                      "relative_residual": poisson_residual(g, phi, rhs)}
+    a, b = out["mixed"], out["fp64"]
+    res["mixed"]["rel_l2_vs_fp64"] = {k: float(np.linalg.norm(a[k] - b[k]) / np.linalg.norm(b[k]))
+                                      for k in a}
+    num = sum(np.linalg.norm(a[k] - b[k]) ** 2 for k in ("u", "v", "w"))
+    den = sum(np.linalg.norm(b[k]) ** 2 for k in ("u", "v", "w"))
+    res["mixed"]["velocity_rel_l2_vs_fp64"] = float(math.sqrt(num / den))
+    res["mixed"]["speedup_vs_fp64"] = round(res["fp64"]["ms_per_step"] /
+                                            res["mixed"]["ms_per_step"], 3)
+    return res
+
+
+def poisson_residual(g, phi, rhs):
+    """||L phi - rhs|| / ||rhs|| on the interior, L the 7-point operator the
+    spectral solve inverts (periodic second differences in x and z, the
+    stretched-grid second difference in y with PHIBC's Neumann ghosts); the
+    plane mean of the residual at J = NY, the mean-mode row that SP0B's
+    marching does not enforce, is left out."""
+    nx, ny, nz = g["nx"], g["ny"], g["nz"]
+    P = phi
+    i, j, k = slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1)
+    dx, dy, dz = g["dx"], g["dy"], g["dz"]
+    dx12, dy12, dz12 = g["dx12"], g["dy12"], g["dz12"]
+    L = ((P[2:nx + 2, j, k] - P[i, j, k]) / dx12[1:nx + 1, None, None] -
+         (P[i, j, k] - P[0:nx, j, k]) / dx12[0:nx, None, None]) / dx[1:nx + 1, None, None]
+    L += ((P[i, 2:ny + 2, k] - P[i, j, k]) / dy12[None, 1:ny + 1, None] -
+          (P[i, j, k] - P[i, 0:ny, k]) / dy12[None, 0:ny, None]) / dy[None, 1:ny + 1, None]
+    L += ((P[i, j, 2:nz + 2] - P[i, j, k]) / dz12[None, None, 1:nz + 1] -
+          (P[i, j, k] - P[i, j, 0:nz]) / dz12[None, None, 0:nz]) / dz[None, None, 1:nz + 1]
+    r = L - rhs[i, j, k]
+    r[:, ny - 1, :] -= r[:, ny - 1, :].mean()
+    return float(np.linalg.norm(r) / np.linalg.norm(rhs[i, j, k]))
+
+
 def replica_rate(ms_local, steps, world, device="cpu"):
     """Whole-job rate of `world` replicas that each timed `steps` steps in
     ms_local: the slowest rank's time (all-reduce MAX over the process group;
@@ -520,6 +603,11 @@ def summary(line):
         out[name] = {"speedup_vs_fp64": rec.get("speedup_vs_fp64"),
                      "max_divu": rec.get("max_divu"),
                      "velocity_rel_l2_vs_fp64": rec.get("velocity_rel_l2_vs_fp64")}
+    big = line.get("mixed_512x256x512")
+    if big:
+        out["mixed_512"] = {"speedup_vs_fp64": big["mixed"]["speedup_vs_fp64"],
+                            "max_divu": big["mixed"]["max_divu"],
+                            "velocity_rel_l2_vs_fp64": big["mixed"]["velocity_rel_l2_vs_fp64"]}
     if line.get("parity"):
         out["parity_max_rel_l2"] = line["parity"]["max_rel_l2"]
         out["parity_pass"] = line["parity"]["pass"]
@@ -645,6 +733,11 @@ def run_ours(args, rank, world, local_rank):
     if args.ens_cases > 0:
         ensemble = run_ensemble(S, W, torch, stream, args, rank, world, dev)
 
+    # ---------------------------------------- 512x256x512 mixed-precision leg
+    big = None
+    if args.big_steps > 0 and rank == 0:
+        big = run_big(S, W, torch, stream, args)
+
     # ------------------------------------------------------ discrete adjoint
     adjoint = None
     if args.adj_steps > 0:
@@ -702,6 +795,7 @@ def run_ours(args, rank, world, local_rank):
                         "pass on one stream in order; the timed steps run the four line "
                         "chains concurrently"),
         "mixed_precision": mixed,
+        "mixed_512x256x512": big,
         "max_divu": mon["max_divu"],
         "poisson": poisson,
         "parity": parity,
@@ -843,6 +937,8 @@ def main():
                     help="forward steps of the adjoint measurement (0 skips it)")
     ap.add_argument("--adj-grid", type=int, default=128)
     ap.add_argument("--adj-dirs", type=int, default=16)
+    ap.add_argument("--big-steps", type=int, default=100,
+                    help="steps of the 512x256x512 FP64-vs-mixed leg (0 skips it)")
     ap.add_argument("--acc-steps", type=int, default=100,
                     help="steps of the mixed-vs-FP64 accuracy comparison")
     args = ap.parse_args()

@@ -188,7 +188,7 @@ __global__ void k_build_yz(Dims d, GridDev g, const double* c1, LineArgs a, cons
     RP[2 * lane + 1] = Be + Ae * QQ[e - 1];
     UU[2 * lane + 1] = Ce;
   }
-  __syncwarp();
+  __syncthreads();
   if (lane == 0) {
     // fold constants: right-hand-side corrections of the first and last rows
     Row r1 = L.ref(1), rn = L.ref(nu);
@@ -235,10 +235,10 @@ __global__ void k_build_yz(Dims d, GridDev g, const double* c1, LineArgs a, cons
       cst[1] = 0.0;
     }
   }
-  __syncwarp();
+  __syncthreads();
   // column c of the inverse: the reduced solve applied to the unit vector e_c
-  if (lane < R) {
-    const int c = lane;
+  // (blockDim >= P; the columns are shared out over the threads)
+  for (int c = lane; c < R; c += blockDim.x) {
     double y = (c == 0) ? 1.0 : 0.0;
     MI[c] = y;
     for (int r = 1; r < R; ++r) {
@@ -689,7 +689,7 @@ __global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yz
 // ============================================================== launchers
 // partitions of a y/z line of nu unknowns: the fewest of 4, 8, 16 that
 // leave at most 16 rows each (rows per thread are registers)
-int yz_partitions(int nu) { return nu <= 64 ? 4 : (nu <= 128 ? 8 : 16); }
+int yz_partitions(int nu) { return nu <= 64 ? 4 : (nu <= 128 ? 8 : (nu <= 256 ? 16 : 32)); }
 static int yz_rows(int nu) {
   int P = yz_partitions(nu);
   int m = (nu + P - 1) / P;
@@ -752,13 +752,14 @@ void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, cons
   }
   int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
   int P = yz_partitions(nu);
+  const int nt = P <= 16 ? 32 : 2 * P;  // one thread per partition and per inverse column
   if (dir == 1) {
-    if (kind == LK_UL_U) k_build_yz<1, LK_UL_U><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
-    else if (kind == LK_UL_V) k_build_yz<1, LK_UL_V><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
-    else k_build_yz<1, LK_UL_T><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    if (kind == LK_UL_U) k_build_yz<1, LK_UL_U><<<count, nt, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    else if (kind == LK_UL_V) k_build_yz<1, LK_UL_V><<<count, nt, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    else k_build_yz<1, LK_UL_T><<<count, nt, 0, s>>>(d, g, c1, a, ids, count, P, out);
   } else {
-    if (kind == LK_CYC_VEL) k_build_yz<2, LK_CYC_VEL><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
-    else k_build_yz<2, LK_CYC_T><<<count, 32, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    if (kind == LK_CYC_VEL) k_build_yz<2, LK_CYC_VEL><<<count, nt, 0, s>>>(d, g, c1, a, ids, count, P, out);
+    else k_build_yz<2, LK_CYC_T><<<count, nt, 0, s>>>(d, g, c1, a, ids, count, P, out);
   }
 }
 
@@ -833,9 +834,11 @@ static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const Li
   else if (MM == 12) NSE_YZ(DIR_, 12, P_); \
   else NSE_YZ(DIR_, 16, P_);
   if (dir == 1) {
-    if (P == 16) { NSE_YZ_MM(1, 16) } else if (P == 8) { NSE_YZ_MM(1, 8) } else { NSE_YZ_MM(1, 4) }
+    if (P == 32) { NSE_YZ_MM(1, 32) } else if (P == 16) { NSE_YZ_MM(1, 16) }
+    else if (P == 8) { NSE_YZ_MM(1, 8) } else { NSE_YZ_MM(1, 4) }
   } else {
-    if (P == 16) { NSE_YZ_MM(2, 16) } else if (P == 8) { NSE_YZ_MM(2, 8) } else { NSE_YZ_MM(2, 4) }
+    if (P == 32) { NSE_YZ_MM(2, 32) } else if (P == 16) { NSE_YZ_MM(2, 16) }
+    else if (P == 8) { NSE_YZ_MM(2, 8) } else { NSE_YZ_MM(2, 4) }
   }
 #undef NSE_YZ_MM
 #undef NSE_YZ

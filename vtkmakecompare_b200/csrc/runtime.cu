@@ -1431,7 +1431,7 @@ static bool build_line_tables(nse_ctx* x) {
   if (x->mixed && !x->part) {
     set_error(NSE_ERR_ARG,
               "nse_ctx_create: the mixed-precision form needs nx = 32*M (M in 3,4,5,6,8,16), "
-              "12 to 256 cells in y and z, and no NSE_FLAG_EXACT");
+              "12 to 512 cells in y and z, and no NSE_FLAG_EXACT");
     return false;
   }
   if (x->part) {
