@@ -284,8 +284,11 @@ enum {
   NSE_FLAG_POISSON5 = 256,   /* FP64 Poisson solve as five launches (x and z transforms
                                 separate) instead of three (each plane's 2-D transform
                                 in one cluster launch; NX = NZ = 256, ny = 16 m) */
-  NSE_FLAG_POISSON32 = 512   /* NSE_MIXED: FP32 Poisson transforms and spectrum with FP64
+  NSE_FLAG_POISSON32 = 512,  /* NSE_MIXED: FP32 Poisson transforms and spectrum with FP64
                                 residual refinement instead of the FP64 solve */
+  NSE_FLAG_LINES_TMA = 1024  /* FP64 fast form: the y and z line passes stream tiles of
+                                16 lines through shared memory by TMA copies (persistent
+                                CTAs, next tile in flight while one is solved) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

@@ -250,3 +250,27 @@ def test_concurrent_line_chains_equal_serial(n, prec, base):
     for k in STATE:
         assert np.array_equal(out[0][k], out[1][k]), k
 
+
+
+@pytest.mark.parametrize("n", [(96, 48, 64), (128, 40, 96), (256, 64, 256), (160, 128, 160)])
+def test_tma_line_tiles_equal_default_lines(n):
+    """NSE_FLAG_LINES_TMA (y and z line passes streamed through shared memory
+    by TMA tile copies, persistent CTAs) gives the default form's fields
+    after 4 steps of a penalised case (same arithmetic, same tables)."""
+    g, f, c1, par = make_case(*n)
+    out = []
+    for flags in (0, S.FLAG_LINES_TMA):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"], flags=flags)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.start()
+            ctx.step(4)
+            ctx.sync()
+            out.append({k: ctx.download(k) for k in STATE})
+    for k in STATE:
+        assert rel_l2(out[1][k], out[0][k]) < 1e-13, k

@@ -29,6 +29,7 @@ SOURCES = {
     "k_fft.cu": [],
     "k_poisson2d.cu": [],
     "noalloc.cu": [],
+    "tma.cu": [],
     "fortran_io.cu": [],
     "k_adjoint.cu": ["--fmad=false"],
     "adjoint.cu": [],
@@ -52,7 +53,7 @@ def _needs(obj, deps):
 def build(verbose=False, extra=()):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "k_lines.cuh"),
-               os.path.join(CSRC, "fft_core.cuh"),
+               os.path.join(CSRC, "fft_core.cuh"), os.path.join(CSRC, "tma.cuh"),
                os.path.join(CSRC, "k_adjoint.cuh"),
                os.path.join(HERE, "..", "include", "nsegpu.h")]
     jobs = []

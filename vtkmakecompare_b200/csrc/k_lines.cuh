@@ -92,6 +92,7 @@ struct LineArgs {
   double beta, dt, eta, ft, fb, r0, l0;
   int comp;  // 0 c2, 1 c3, 2 c4, 3 c1
   int jtop;  // lines along j for z and x tiles (ny, or ny-1 for v)
+  int tma = 0;  // FP64 y/z lines of the fast form through TMA tiles (k_yzlines_tma)
 };
 
 __device__ __forceinline__ double mask_at(const Dims& d, const double* c1, int comp, int i,

@@ -32,6 +32,7 @@
 #include <algorithm>
 
 #include "k_lines.cuh"
+#include "tma.cuh"
 
 // launch shapes (compile-time): x lines per warp iteration, y/z lines per CTA
 #ifndef NSE_XL_NL
@@ -686,6 +687,121 @@ __global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yz
     if (r < m) dst[r * es] = (RO)x[r];
 }
 
+// ------------------------------------------ y / z lines through TMA tiles
+// FP64 form.  A persistent CTA (16 lines x P partitions) walks tiles of 16
+// x-adjacent lines: the tile's nu rows (16 x nu doubles) come into shared
+// memory by one TMA copy (tensor map over the padded field, box 16 x nu at
+// x = 16 t, so the box starts 16-byte aligned: tile t covers i = 16t..16t+15,
+// the ghost columns i = 0 and nx+1 are carried along unchanged and columns
+// past nx+1 fall outside the map), the solution is written back into the
+// tile and leaves by one TMA store.  Two tile buffers: the next tile's load
+// is in flight while this one is solved.  The mask-free table sits in shared
+// memory; a line that touches the mask reads its own table from global
+// memory.  The arithmetic is k_yzlines' (same values).
+__host__ __device__ __forceinline__ size_t yzt_tile_bytes(int nu) {
+  return (((size_t)nu * 16 * 8) + 127) & ~(size_t)127;
+}
+// set when a wait on a tile copy gave up (read by the host: line_wait_error)
+__device__ int g_line_wait_err = 0;
+
+template <int DIR, int MM, int P>
+__global__ void __launch_bounds__(16 * P, 2)
+    k_yzlines_tma(const __grid_constant__ CUtensorMap tm, Dims d, int nu, int nother, int ntx,
+                  const double* __restrict__ tab, const int* __restrict__ slots,
+                  const double* __restrict__ mtab, double ft, double fb, int periodic) {
+  constexpr int LPB = 16, R2 = 2 * P;
+  extern __shared__ __align__(128) unsigned char ysm[];
+  const size_t tb_bytes = yzt_tile_bytes(nu);
+  double* buf0 = reinterpret_cast<double*>(ysm);
+  double* buf1 = reinterpret_cast<double*>(ysm + tb_bytes);
+  double* red = reinterpret_cast<double*>(ysm + 2 * tb_bytes);  // [R2][LPB]
+  const size_t stride = yz_table_stride(nu, P);
+  double* stab = red + R2 * LPB;  // mask-free table
+  uint64_t* bar = reinterpret_cast<uint64_t*>(stab + ((stride + 1) & ~(size_t)1));
+  const int lane = threadIdx.x % LPB, k = threadIdx.x / LPB;
+  const long ntiles = (long)ntx * nother;
+  const unsigned tile_tx = (unsigned)nu * LPB * 8;
+  for (size_t t = threadIdx.x; t < stride; t += blockDim.x) stab[t] = __ldg(tab + t);
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](long q, double* dst, uint64_t* b) {
+    const int x0 = (int)(q % ntx) * LPB, o = 1 + (int)(q / ntx);
+    mbar_expect_tx(b, tile_tx);
+    if (DIR == 1) tma_load_3d(dst, &tm, x0, 1, o, b);
+    else tma_load_3d(dst, &tm, x0, o, 1, b);
+  };
+  long q = blockIdx.x;
+  if (threadIdx.x == 0 && q < ntiles) issue(q, buf0, &bar[0]);
+  const int s = (int)((long)k * nu / P), e = (int)((long)(k + 1) * nu / P) - 1;
+  const int m = e - s + 1;
+  for (int it = 0; q < ntiles; q += gridDim.x, ++it) {
+    double* cur = (it & 1) ? buf1 : buf0;
+    double* nxt = (it & 1) ? buf0 : buf1;
+    const long qn = q + gridDim.x;
+    if (threadIdx.x == 0 && qn < ntiles) {
+      tma_store_wait_read();  // the previous tile's store has read its buffer
+      issue(qn, nxt, &bar[(it + 1) & 1]);
+    }
+    if (!tma_wait(&bar[it & 1], (unsigned)((it >> 1) & 1)) && threadIdx.x == 0)
+      atomicExch(&g_line_wait_err, 1);
+    const int i = (int)(q % ntx) * LPB + lane;
+    const int o = 1 + (int)(q / ntx);
+    const bool valid = i >= 1 && i <= d.nx;
+    const double* T = stab;
+    if (valid) {
+      const long lineid = (long)(i - 1) + (long)d.nx * (o - 1);
+      const int slot = slots[lineid];
+      if (slot >= 0) T = mtab + (size_t)slot * stride;
+    }
+    YZTab<double> tb{T, nu, s};
+    double x[MM];
+    const double* col = cur + (size_t)s * LPB + lane;
+    const double c0 = (!periodic && k == 0) ? T[5 * nu + 10 * P + 2] * ft : 0.0;
+    const double cN = (!periodic && k == P - 1) ? T[5 * nu + 10 * P + 3] * fb : 0.0;
+#pragma unroll
+    for (int r = 0; r < MM; ++r) x[r] = col[(size_t)min(r, m - 1) * LPB];
+    x[0] = x[0] - c0;
+    const double xe = col[(size_t)(m - 1) * LPB] - cN;
+    const double xe1 = interior_solve<MM>(x, m, tb);
+    red[(2 * k) * LPB + lane] = x[0] - T[5 * nu + k] * x[1];
+    red[(2 * k + 1) * LPB + lane] = xe - T[5 * nu + P + k] * xe1;
+    __syncthreads();
+    const double* MI = T + 5 * nu + 10 * P + 4;
+    double F = 0.0, E = 0.0;
+#pragma unroll
+    for (int c = 0; c < R2; ++c) {
+      const double rc = red[c * LPB + lane];
+      F = F + MI[(2 * k) * R2 + c] * rc;
+      E = E + MI[(2 * k + 1) * R2 + c] * rc;
+    }
+#pragma unroll
+    for (int r = 1; r < MM; ++r) {
+      if (r < m - 1) x[r] = x[r] + tb.pp(r) * F + tb.qq(r) * E;
+      if (r == m - 1) x[r] = E;
+    }
+    x[0] = F;
+    double* dst = cur + (size_t)s * LPB + lane;
+    if (valid) {
+#pragma unroll
+      for (int r = 0; r < MM; ++r)
+        if (r < m) dst[(size_t)r * LPB] = x[r];
+    }
+    fence_async_smem();
+    __syncthreads();  // the tile is complete; red may be rewritten
+    if (threadIdx.x == 0) {
+      const int x0 = (int)(q % ntx) * LPB;
+      if (DIR == 1) tma_store_3d(&tm, x0, 1, o, cur);
+      else tma_store_3d(&tm, x0, o, 1, cur);
+      tma_store_commit();
+    }
+  }
+  if (threadIdx.x == 0) tma_store_wait_all();
+}
+
 // ============================================================== launchers
 // partitions of a y/z line of nu unknowns: the fewest of 4, 8, 16 that
 // leave at most 16 rows each (rows per thread are registers)
@@ -794,6 +910,58 @@ static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, 
   }
 }
 
+// the TMA tile path of the FP64 y/z lines; false when it does not apply or
+// the tensor map cannot be made (the caller then launches k_yzlines)
+static bool yz_tma_lines(int dir, const Dims& d, double* f, int nu, int P, int MM, int nother,
+                         const double* tab, const int* slots, const double* mtab, double ft,
+                         double fb, bool periodic, cudaStream_t s) {
+  CUtensorMap tm;
+  const long p1 = (long)(d.nx + 2) * 8, p2 = p1 * (d.ny + 2);
+  if (p1 % 16 != 0 || ((uintptr_t)f & 15) != 0) return false;
+  const bool ok = dir == 1 ? tma_encode_3d(&tm, f, true, d.nx + 2, d.ny + 2, d.nz + 2, p1, p2, 16,
+                                           nu, 1)
+                           : tma_encode_3d(&tm, f, true, d.nx + 2, d.ny + 2, d.nz + 2, p1, p2, 16,
+                                           1, nu);
+  if (!ok) return false;
+  const int ntx = (d.nx + 2 + 15) / 16;
+  const long ntiles = (long)ntx * nother;
+  const size_t stride = yz_table_stride(nu, P);
+  const size_t smem = 2 * yzt_tile_bytes(nu) + (size_t)2 * P * 16 * 8 +
+                      ((stride + 1) & ~(size_t)1) * 8 + 16;
+  const int grid = (int)std::min<long>(ntiles, 2L * sm_count());
+  const int per = periodic ? 1 : 0;
+#define NSE_YZT(DIR_, MM_, P_)                                                                \
+  {                                                                                           \
+    auto kern = k_yzlines_tma<DIR_, MM_, P_>;                                                 \
+    cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize,      \
+                         (int)smem);                                                          \
+    count_launch();                                                                           \
+    kern<<<grid, 16 * P_, smem, s>>>(tm, d, nu, nother, ntx, tab, slots, mtab, ft, fb, per);  \
+  }
+#define NSE_YZT_MM(DIR_, P_)                 \
+  if (MM == 8) NSE_YZT(DIR_, 8, P_)          \
+  else if (MM == 12) NSE_YZT(DIR_, 12, P_)   \
+  else NSE_YZT(DIR_, 16, P_)
+  if (dir == 1) {
+    if (P == 16) { NSE_YZT_MM(1, 16) } else if (P == 8) { NSE_YZT_MM(1, 8) } else { NSE_YZT_MM(1, 4) }
+  } else {
+    if (P == 16) { NSE_YZT_MM(2, 16) } else if (P == 8) { NSE_YZT_MM(2, 8) } else { NSE_YZT_MM(2, 4) }
+  }
+#undef NSE_YZT_MM
+#undef NSE_YZT
+  return true;
+}
+
+int line_wait_error() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_line_wait_err, sizeof(int)) != cudaSuccess) return 0;
+  if (v) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_line_wait_err, &z, sizeof(int));
+  }
+  return v;
+}
+
 template <class S, class R, class RO>
 static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const LineArgs& a,
                        const R* tab, const int* slots, const int* ids, int nmasked,
@@ -821,6 +989,13 @@ static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const Li
   int P = yz_partitions(nu);
   int MM = yz_rows(nu);
   int nother = dir == 1 ? d.nz : a.jtop;
+  if constexpr (sizeof(S) == 8 && sizeof(R) == 8 && sizeof(RO) == 8) {
+    if (a.tma && !out && P <= 16 &&
+        yz_tma_lines(dir, d, reinterpret_cast<double*>(f), nu, P, MM, nother,
+                     reinterpret_cast<const double*>(tab), slots,
+                     reinterpret_cast<const double*>(mtab), a.ft, a.fb, kind >= LK_CYC_VEL, s))
+      return;
+  }
   constexpr int LPB = NSE_YZ_LPB;
   dim3 grid((d.nx + LPB - 1) / LPB, nother);
   int periodic = kind >= LK_CYC_VEL ? 1 : 0;

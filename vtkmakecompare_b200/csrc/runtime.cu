@@ -34,6 +34,7 @@ void launch_line_tables_masked(int dir, int kind, const Dims& d, const GridDev& 
                                double* out, cudaStream_t s);
 // k_lines_part.cu
 bool part_lines_supported(const Dims& d);
+int line_wait_error();  // k_lines_part.cu: a TMA tile wait gave up since the last call
 size_t part_table_stride(int dir, int kind, const Dims& d);
 void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, const double* c1,
                         const LineArgs& a, const int* ids, int count, double* out,
@@ -1478,6 +1479,7 @@ static LineArgs line_args(nse_ctx* x, int comp) {
   a.dt = c.dt; a.eta = c.eta; a.r0 = c.rho_cp; a.l0 = c.thc;
   a.comp = comp;
   a.jtop = comp == 1 ? x->d.ny - 1 : x->d.ny;
+  a.tma = (c.flags & NSE_FLAG_LINES_TMA) ? 1 : 0;
   return a;
 }
 
@@ -2411,7 +2413,12 @@ int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
 
 int nse_sync(nse_ctx* x) {
   if (!x) return NSE_ERR_ARG;
-  return NSE_CUDA(cudaStreamSynchronize(x->stream)) ? NSE_OK : status_or(NSE_ERR_CUDA);
+  if (!NSE_CUDA(cudaStreamSynchronize(x->stream))) return status_or(NSE_ERR_CUDA);
+  if (line_wait_error()) {
+    set_error(NSE_ERR_CUDA, "nse_sync: a line kernel's wait for its tile copy gave up");
+    return NSE_ERR_CUDA;
+  }
+  return NSE_OK;
 }
 
 }  // extern "C"

@@ -26,6 +26,7 @@ FLAG_LINES64 = 64
 FLAG_ONE_STREAM = 128
 FLAG_POISSON5 = 256
 FLAG_POISSON32 = 512
+FLAG_LINES_TMA = 1024
 
 
 class Config(C.Structure):
