@@ -499,6 +499,60 @@ def run_ensemble(S, W, torch, stream, args, rank=0, world=1, device="cpu"):
     return res
 
 
+def run_dft_gemm(S, W, torch, stream, n=64, reps=50):
+    """The tensor-core question for small transforms (the smallest ensemble grid,
+    n^3 with n = 64): one Poisson solve of the library (its own radix FFTs in
+    x and z, SPN, inverse) against the four transform passes of a solve done
+    as dense DFT matrix products through cuBLAS (torch.matmul): the x passes
+    as a real (n^2 x n) by (n x 2(n/2+1)) product, the z passes as a complex
+    (n x n) by (n x (n/2+1) n) product, each twice (forward and inverse), in
+    FP64 (the form's precision) and in TF32 (the tensor-core precision the
+    FP32 form would use).  CUDA events on one stream, after warm-up."""
+    g = W.grid_arrays(n, n, n, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    cfg = S.Config(n, n, n, 1.0, 1.0, 1.0, 0.0, 2 * math.pi, 2.0, math.pi, y0=-1.0, ystretch=2.0)
+    dev = torch.device("cuda")
+
+    def timed(fn):
+        for _ in range(5):
+            fn()
+        torch.cuda.synchronize()
+        e0 = torch.cuda.Event(enable_timing=True)
+        e1 = torch.cuda.Event(enable_timing=True)
+        with torch.cuda.stream(stream):
+            e0.record(stream)
+            for _ in range(reps):
+                fn()
+            e1.record(stream)
+        torch.cuda.synchronize()
+        return e0.elapsed_time(e1) / reps
+
+    with S.Context(cfg) as ctx:
+        ctx.set_stream(stream.cuda_stream)
+        ctx.upload("phi", W.poisson_rhs(g, 3))
+        ours = timed(ctx.poisson)
+    h = n // 2 + 1
+    out = {"n": n, "reps": reps, "library_solve_ms": round(ours, 5)}
+    for name, dt in (("fp64", torch.float64), ("tf32", torch.float32)):
+        torch.backends.cuda.matmul.allow_tf32 = name == "tf32"
+        with torch.cuda.stream(stream):
+            xr = torch.randn(n * n, n, dtype=dt, device=dev)
+            fr = torch.randn(n, 2 * h, dtype=dt, device=dev)
+            zc = torch.randn(2 * n, h * n, dtype=dt, device=dev)
+            fz = torch.randn(2 * n, 2 * n, dtype=dt, device=dev)
+
+        def passes():
+            torch.matmul(xr, fr)   # x pass (real samples -> half spectrum)
+            torch.matmul(fz, zc)   # z pass (complex as a 2n x 2n real block)
+
+        t = 2 * timed(passes)
+        out[f"gemm_{name}_ms"] = round(t, 5)
+        out[f"gemm_{name}_flop"] = 2 * (2 * n * n * n * 2 * h + 2 * (2 * n) ** 2 * h * n)
+    torch.backends.cuda.matmul.allow_tf32 = False
+    out["note"] = ("GEMM times cover the four transform passes only (no SPN, no sample "
+                   "packing); the library time is a whole solve")
+    return out
+
+
 def run_adjoint(S, W, torch, stream, args):
     """Discrete adjoint at args.adj_grid^3: the sphere of the main workload at
     the same physical size, walls at T = 1 (y = -1) and T = 0 (y = 1), sphere
@@ -733,6 +787,10 @@ def run_ours(args, rank, world, local_rank):
     if args.ens_cases > 0:
         ensemble = run_ensemble(S, W, torch, stream, args, rank, world, dev)
 
+    dft_gemm = None
+    if args.dft_gemm and rank == 0:
+        dft_gemm = run_dft_gemm(S, W, torch, stream)
+
     # ---------------------------------------- 512x256x512 mixed-precision leg
     big = None
     if args.big_steps > 0 and rank == 0:
@@ -796,6 +854,7 @@ def run_ours(args, rank, world, local_rank):
                         "chains concurrently"),
         "mixed_precision": mixed,
         "mixed_512x256x512": big,
+        "dft_as_gemm_64": dft_gemm,
         "max_divu": mon["max_divu"],
         "poisson": poisson,
         "parity": parity,
@@ -936,6 +995,9 @@ def main():
     ap.add_argument("--adj-steps", type=int, default=400,
                     help="forward steps of the adjoint measurement (0 skips it)")
     ap.add_argument("--adj-grid", type=int, default=128)
+    ap.add_argument("--dft-gemm", action="store_true",
+                    help="also time 64-point transforms as dense DFT GEMMs (cuBLAS) "
+                         "against the library's own transform")
     ap.add_argument("--adj-dirs", type=int, default=16)
     ap.add_argument("--big-steps", type=int, default=100,
                     help="steps of the 512x256x512 FP64-vs-mixed leg (0 skips it)")
