@@ -286,9 +286,11 @@ enum {
                                 in one cluster launch; NX = NZ = 256, ny = 16 m) */
   NSE_FLAG_POISSON32 = 512,  /* NSE_MIXED: FP32 Poisson transforms and spectrum with FP64
                                 residual refinement instead of the FP64 solve */
-  NSE_FLAG_LINES_TMA = 1024  /* FP64 fast form: the y and z line passes stream tiles of
+  NSE_FLAG_LINES_TMA = 1024, /* FP64 fast form: the y and z line passes stream tiles of
                                 16 lines through shared memory by TMA copies (persistent
                                 CTAs, next tile in flight while one is solved) */
+  NSE_FLAG_NO_AUTOTUNE = 2048 /* keep the fixed line launch shapes instead of timing the
+                                candidates before the first step (same values either way) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */
@@ -344,6 +346,12 @@ int nse_ctx_read_field(nse_ctx* ctx, const char* path);
  * out[3]=sum|w|dz, out[4]=sum T dx dy dz (all cells), out[5]=non-finite count */
 int nse_monitor(nse_ctx* ctx, double out[6]);
 int nse_sync(nse_ctx* ctx);
+/* Launch shapes the autotuner chose for the partitioned line passes (set
+ * before the context's first step; no counterpart in the reference):
+ * yz[(dir-1)*4 + comp] for y (dir 1) and z (dir 2) lines of u, v, w, T:
+ * 0 = 16 lines per CTA, 1 = 8, 3 = 32, 2 = TMA tiles of 16 lines; xnl[comp] =
+ * x lines per warp iteration. */
+int nse_ctx_line_shapes(nse_ctx* ctx, int* yz, int* xnl);
 /* Per-phase timing of the next max_steps steps with CUDA events on the
  * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the
  * summed milliseconds over the profiled steps; phases in launch order:

@@ -253,13 +253,15 @@ def test_concurrent_line_chains_equal_serial(n, prec, base):
 
 
 @pytest.mark.parametrize("n", [(96, 48, 64), (128, 40, 96), (256, 64, 256), (160, 128, 160)])
-def test_tma_line_tiles_equal_default_lines(n):
-    """NSE_FLAG_LINES_TMA (y and z line passes streamed through shared memory
-    by TMA tile copies, persistent CTAs) gives the default form's fields
-    after 4 steps of a penalised case (same arithmetic, same tables)."""
+def test_line_launch_shapes_give_the_same_fields(n):
+    """The line passes' launch shapes give the same fields after 4 steps of a
+    penalised case (same arithmetic, same tables): the fixed shapes
+    (NSE_FLAG_NO_AUTOTUNE), the TMA tiles for every FP64 y/z pass
+    (NSE_FLAG_LINES_TMA) and the autotuner's choice (the default)."""
     g, f, c1, par = make_case(*n)
     out = []
-    for flags in (0, S.FLAG_LINES_TMA):
+    shapes = None
+    for flags in (S.FLAG_NO_AUTOTUNE, S.FLAG_LINES_TMA, 0):
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                        g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
                        body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
@@ -272,5 +274,10 @@ def test_tma_line_tiles_equal_default_lines(n):
             ctx.step(4)
             ctx.sync()
             out.append({k: ctx.download(k) for k in STATE})
+            if flags == 0:
+                shapes = ctx.line_shapes()
     for k in STATE:
         assert rel_l2(out[1][k], out[0][k]) < 1e-13, k
+        assert rel_l2(out[2][k], out[0][k]) < 1e-13, k
+    assert all(v in (0, 1, 2, 3) for v in shapes["y"] + shapes["z"]), shapes
+    assert all(v in (1, 2) for v in shapes["x"]), shapes

@@ -92,7 +92,12 @@ struct LineArgs {
   double beta, dt, eta, ft, fb, r0, l0;
   int comp;  // 0 c2, 1 c3, 2 c4, 3 c1
   int jtop;  // lines along j for z and x tiles (ny, or ny-1 for v)
-  int tma = 0;  // FP64 y/z lines of the fast form through TMA tiles (k_yzlines_tma)
+  // launch shape of the partitioned solver (chosen by the context's autotuner;
+  // every shape gives the same values): y/z lines 0 = 16 lines per CTA, 1 = 8,
+  // 3 = 32, 2 = TMA tiles of 16 lines (FP64); x lines per warp iteration 1 or
+  // 2 (0: the default, 2)
+  int yzshape = 0;
+  int xnl = 0;
 };
 
 __device__ __forceinline__ double mask_at(const Dims& d, const double* c1, int comp, int i,

@@ -890,11 +890,11 @@ static int sm_count() {
   return cached;
 }
 
-template <int M, class S, class R, int PL = 32>
+template <int M, class S, class R, int PL = 32, int NLW = 0>
 static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, const int* ids,
                  int nmasked, const R* mtab, cudaStream_t s) {
   const int sms = sm_count();
-  constexpr int NL = M <= 8 ? NSE_XL_NL : 2;
+  constexpr int NL = NLW > 0 ? NLW : (M <= 8 ? NSE_XL_NL : 2);
   constexpr int HW = 32 / PL;
   long nlines = (long)jtop * d.nz;
   long per_blk = 8L * NL * HW;
@@ -962,44 +962,12 @@ int line_wait_error() {
   return v;
 }
 
-template <class S, class R, class RO>
-static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const LineArgs& a,
-                       const R* tab, const int* slots, const int* ids, int nmasked,
-                       const R* mtab, cudaStream_t s) {
-  if (dir == 0) {
-    int M, PL;
-    x_shape(d.nx, M, PL);
-    if (PL == 16) {
-      if (M == 3) go_x<3, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
-      else if (M == 4) go_x<4, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
-      else go_x<5, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
-      return;
-    }
-    switch (M) {
-      case 3: go_x<3>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
-      case 4: go_x<4>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
-      case 5: go_x<5>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
-      case 6: go_x<6>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
-      case 8: go_x<8>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
-      default: go_x<16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
-    }
-    return;
-  }
-  int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
-  int P = yz_partitions(nu);
-  int MM = yz_rows(nu);
-  int nother = dir == 1 ? d.nz : a.jtop;
-  if constexpr (sizeof(S) == 8 && sizeof(R) == 8 && sizeof(RO) == 8) {
-    if (a.tma && !out && P <= 16 &&
-        yz_tma_lines(dir, d, reinterpret_cast<double*>(f), nu, P, MM, nother,
-                     reinterpret_cast<const double*>(tab), slots,
-                     reinterpret_cast<const double*>(mtab), a.ft, a.fb, kind >= LK_CYC_VEL, s))
-      return;
-  }
-  constexpr int LPB = NSE_YZ_LPB;
+template <int LPB, class S, class R, class RO>
+static void yz_launch(int dir, const Dims& d, S* f, RO* out, int nu, int P, int MM, int nother,
+                      const R* tab, const int* slots, const R* mtab, R ft, R fb, bool per,
+                      cudaStream_t s) {
   dim3 grid((d.nx + LPB - 1) / LPB, nother);
-  int periodic = kind >= LK_CYC_VEL ? 1 : 0;
-  const R ft = (R)a.ft, fb = (R)a.fb;
+  const int periodic = per ? 1 : 0;
   count_launch();
 #define NSE_YZ(DIR_, MM_, P_)                                                               \
   k_yzlines<DIR_, MM_, P_, LPB, S, R, RO><<<grid, LPB * P_, 0, s>>>(                        \
@@ -1017,6 +985,72 @@ static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const Li
   }
 #undef NSE_YZ_MM
 #undef NSE_YZ
+}
+
+template <class S, class R, class RO>
+static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const LineArgs& a,
+                       const R* tab, const int* slots, const int* ids, int nmasked,
+                       const R* mtab, cudaStream_t s) {
+  if (dir == 0) {
+    int M, PL;
+    x_shape(d.nx, M, PL);
+    if (PL == 16) {
+      if (M == 3) go_x<3, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+      else if (M == 4) go_x<4, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+      else go_x<5, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+      return;
+    }
+    // one line per warp iteration is the autotuner's alternative to two (same values)
+    if constexpr (sizeof(S) == sizeof(R)) {
+      if (a.xnl == 1) {
+        switch (M) {
+          case 3: go_x<3, S, R, 32, 1>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); return;
+          case 4: go_x<4, S, R, 32, 1>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); return;
+          case 5: go_x<5, S, R, 32, 1>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); return;
+          case 6: go_x<6, S, R, 32, 1>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); return;
+          case 8: go_x<8, S, R, 32, 1>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); return;
+          default: break;
+        }
+      }
+    }
+    switch (M) {
+      case 3: go_x<3>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 4: go_x<4>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 5: go_x<5>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 6: go_x<6>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      case 8: go_x<8>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+      default: go_x<16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); break;
+    }
+    return;
+  }
+  int nu = dir == 1 ? (kind == LK_UL_V ? d.ny - 1 : d.ny) : d.nz;
+  int P = yz_partitions(nu);
+  int MM = yz_rows(nu);
+  int nother = dir == 1 ? d.nz : a.jtop;
+  if constexpr (sizeof(S) == 8 && sizeof(R) == 8 && sizeof(RO) == 8) {
+    if (a.yzshape == 2 && !out && P <= 16 &&
+        yz_tma_lines(dir, d, reinterpret_cast<double*>(f), nu, P, MM, nother,
+                     reinterpret_cast<const double*>(tab), slots,
+                     reinterpret_cast<const double*>(mtab), a.ft, a.fb, kind >= LK_CYC_VEL, s))
+      return;
+  }
+  // lines per CTA: 16, or the autotuner's alternatives 8 and 32 (same values)
+  // for the uniform storage/arithmetic types
+  constexpr bool uni = sizeof(S) == sizeof(R) && sizeof(R) == sizeof(RO);
+  if constexpr (uni) {
+    if (a.yzshape == 1 && !out) {
+      yz_launch<8>(dir, d, f, out, nu, P, MM, nother, tab, slots, mtab, (R)a.ft, (R)a.fb,
+                   kind >= LK_CYC_VEL, s);
+      return;
+    }
+    if (a.yzshape == 3 && !out) {
+      yz_launch<32>(dir, d, f, out, nu, P, MM, nother, tab, slots, mtab, (R)a.ft, (R)a.fb,
+                    kind >= LK_CYC_VEL, s);
+      return;
+    }
+  }
+  yz_launch<NSE_YZ_LPB>(dir, d, f, out, nu, P, MM, nother, tab, slots, mtab, (R)a.ft, (R)a.fb,
+                        kind >= LK_CYC_VEL, s);
 }
 
 void launch_lines_part(int dir, int kind, const Dims& d, double* f, const LineArgs& a,

@@ -9,6 +9,8 @@
 
 #include <algorithm>
 #include <atomic>
+#include <map>
+#include <mutex>
 #include <string>
 #include <vector>
 
@@ -35,6 +37,7 @@ void launch_line_tables_masked(int dir, int kind, const Dims& d, const GridDev& 
 // k_lines_part.cu
 bool part_lines_supported(const Dims& d);
 int line_wait_error();  // k_lines_part.cu: a TMA tile wait gave up since the last call
+int x_rows_per_lane(int nx);  // k_lines_part.cu: rows per lane of the x solver (0: none)
 size_t part_table_stride(int dir, int kind, const Dims& d);
 void launch_part_tables(int dir, int kind, const Dims& d, const GridDev& g, const double* c1,
                         const LineArgs& a, const int* ids, int count, double* out,
@@ -1391,6 +1394,12 @@ struct nse_ctx {
   // y/z/x chains beside u's, forked from and joined back into `stream`
   cudaStream_t side[3] = {};
   cudaEvent_t lfork = nullptr, ljoin[3] = {};
+  // launch shapes of the partitioned line passes (LineArgs::yzshape per
+  // direction and component, x lines per warp iteration per component),
+  // chosen by autotune_lines before the first step
+  int yzshape[3][4] = {};
+  int xnl[4] = {};
+  bool tuned = false;
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1479,8 +1488,12 @@ static LineArgs line_args(nse_ctx* x, int comp) {
   a.dt = c.dt; a.eta = c.eta; a.r0 = c.rho_cp; a.l0 = c.thc;
   a.comp = comp;
   a.jtop = comp == 1 ? x->d.ny - 1 : x->d.ny;
-  a.tma = (c.flags & NSE_FLAG_LINES_TMA) ? 1 : 0;
   return a;
+}
+
+static void line_shape(const nse_ctx* x, int dir, int comp, LineArgs& la) {
+  la.yzshape = x->yzshape[dir][comp];
+  la.xnl = x->xnl[comp];
 }
 
 // after a mask change: flag the lines that touch the mask, give each of them
@@ -1967,6 +1980,116 @@ int nse_poisson(nse_ctx* x) {
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
 
+// ------------------------------------------------------------- autotuner --
+// The partitioned line passes have several launch shapes that give the same
+// values: y/z lines 16, 8 or 32 lines per CTA (the y/z line-to-warp mapping:
+// a warp holds 32/L lines x L partitions... of one CTA), or, in FP64, TMA
+// tiles of 16 lines with persistent CTAs; x lines one or two per warp
+// iteration.  Before a context's first step (outside any stream capture)
+// every candidate of every pass is timed on a scratch copy of the pass's
+// field (CUDA events, one warm-up and three timed runs, the fastest kept).
+// Choices are kept per grid and form for the process, so the cases of an
+// ensemble that share a grid are timed once.  NSE_FLAG_NO_AUTOTUNE keeps
+// the fixed shapes (16 lines per CTA, two x lines per warp iteration);
+// NSE_FLAG_LINES_TMA sets the TMA tiles for every FP64 y/z pass.
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tune;
+
+static int x_nl_candidates(const nse_ctx* x) { return x_rows_per_lane(x->d.nx) <= 8 ? 2 : 1; }
+
+static void autotune_lines(nse_ctx* x) {
+  if (x->tuned || !x->part) return;
+  const int flags = x->cfg.flags;
+  if (flags & NSE_FLAG_LINES_TMA) {
+    for (int dir = 1; dir <= 2; ++dir)
+      for (int comp = 0; comp < 4; ++comp) x->yzshape[dir][comp] = x->mixed ? 0 : 2;
+    x->tuned = true;
+    return;
+  }
+  if (flags & NSE_FLAG_NO_AUTOTUNE) {
+    x->tuned = true;
+    return;
+  }
+  cudaStream_t s = x->stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  const Dims& d = x->d;
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  const int form = x->mixed ? (x->lines64 ? 2 : 1) : 0;
+  size_t fbytes = d.ntot * (x->mixed ? sizeof(float) : sizeof(double));
+  for (int comp = 0; comp < 4; ++comp) {
+    void* src = comp == 0 ? x->ua.p : comp == 1 ? x->va.p : comp == 2 ? x->wa.p : x->uT.p;
+    for (int dir = 0; dir < 3; ++dir) {
+      char key[96];
+      snprintf(key, sizeof(key), "%d %d %d %d %d %d", d.nx, d.ny, d.nz, dir,
+               line_kind(dir, comp), form);
+      {
+        std::lock_guard<std::mutex> lk(g_tune_mu);
+        auto it = g_tune.find(key);
+        if (it != g_tune.end()) {
+          if (dir == 0) x->xnl[comp] = it->second;
+          else x->yzshape[dir][comp] = it->second;
+          continue;
+        }
+      }
+      std::vector<int> cand;
+      if (dir == 0) {
+        if (x_nl_candidates(x) < 2) continue;
+        cand = {2, 1};
+      } else {
+        cand = {0, 1, 3};
+        if (!x->mixed) cand.push_back(2);
+      }
+      int best = cand[0];
+      float best_ms = 1e30f;
+      for (int c : cand) {
+        cudaMemcpyAsync(x->sa.p, src, fbytes, cudaMemcpyDeviceToDevice, s);
+        LineArgs la = line_args(x, comp);
+        la.ft = 0.0;
+        la.fb = 0.0;
+        if (dir == 0) la.xnl = c;
+        else la.yzshape = c;
+        auto run = [&]() {
+          if (x->mixed)
+            launch_lines_part_f32(dir, line_kind(dir, comp), d, x->sa.as<float>(), nullptr, la,
+                                  x->ptab_f[dir][comp].as<float>(),
+                                  x->slots[dir][comp].as<int>(), x->ids[dir][comp].as<int>(),
+                                  x->nmasked[dir][comp], x->pmtab_f[dir][comp].as<float>(),
+                                  x->lines64 ? x->ptab[dir][comp].as<double>() : nullptr,
+                                  x->lines64 ? x->pmtab[dir][comp].as<double>() : nullptr, s);
+          else
+            launch_lines_part(dir, line_kind(dir, comp), d, x->sa.as<double>(), la,
+                              x->ptab[dir][comp].as<double>(), x->slots[dir][comp].as<int>(),
+                              x->ids[dir][comp].as<int>(), x->nmasked[dir][comp],
+                              x->pmtab[dir][comp].as<double>(), s);
+        };
+        run();
+        cudaEventRecord(e0, s);
+        for (int r = 0; r < 3; ++r) run();
+        cudaEventRecord(e1, s);
+        float ms = 1e30f;
+        if (cudaEventSynchronize(e1) == cudaSuccess && cudaEventElapsedTime(&ms, e0, e1) ==
+                                                           cudaSuccess && ms < best_ms) {
+          best_ms = ms;
+          best = c;
+        }
+      }
+      if (dir == 0) x->xnl[comp] = best;
+      else x->yzshape[dir][comp] = best;
+      std::lock_guard<std::mutex> lk(g_tune_mu);
+      g_tune[key] = best;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  x->tuned = true;
+}
+
 // one time step in the mixed-precision form: FP64 state u, v, w, T, p;
 // FP32 right-hand side, line sweeps and transforms
 static void ctx_step_f32(nse_ctx* x) {
@@ -1990,10 +2113,12 @@ static void ctx_step_f32(nse_ctx* x) {
                  F32(x, NSE_W_TA), F32(x, NSE_U_PRE), F32(x, NSE_V_PRE), F32(x, NSE_W_PRE),
                  F32(x, NSE_T_PRE), c1, ua, va, wa, uT, x->math64, s);
   refresh_line_flags(x, s);
+  autotune_lines(x);
   float* fa[3] = {ua, va, wa};
   auto run_on = [&](cudaStream_t st, int dir, int comp, float* f, double* out, double ft,
                     double fb) {
     LineArgs la = line_args(x, comp);
+    line_shape(x, dir, comp, la);
     la.ft = ft;
     la.fb = fb;
     launch_lines_part_f32(dir, line_kind(dir, comp), d, f, out, la,
@@ -2093,6 +2218,7 @@ static void ctx_step(nse_ctx* x) {
   // the fields are independent, so this order gives the same values as
   // the reference's per-field y, z, x order)
   refresh_line_flags(x, s);
+  if (!x->rec) autotune_lines(x);
   const bool exact = (c.flags & NSE_FLAG_EXACT) != 0;
   auto lines = exact ? launch_lines_exact : launch_lines_fast;
   double* fa[3] = {ua, va, wa};
@@ -2109,6 +2235,7 @@ static void ctx_step(nse_ctx* x) {
               comp == 3 ? (dir == 1 ? 0 : (dir == 0 ? 1 : 2)) : (dir == 1 ? 0 : (dir == 2 ? 1 : 2)),
               f);
     LineArgs la = line_args(x, comp);
+    line_shape(x, dir, comp, la);
     la.ft = ft;
     la.fb = fb;
     if (x->part)
@@ -2214,6 +2341,7 @@ void ctx_step_rec(nse_ctx* x, double* const* rec) {
 void ctx_line_solve(nse_ctx* x, int dir, int comp, double* f, cudaStream_t s) {
   refresh_line_flags(x, s);
   LineArgs la = line_args(x, comp);
+    line_shape(x, dir, comp, la);
   la.ft = 0.0;
   la.fb = 0.0;
   const Dims& d = x->d;
@@ -2408,6 +2536,14 @@ int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
     }
   if (nsteps) *nsteps = x->prof_n;
   x->prof_n = 0;
+  return NSE_OK;
+}
+
+int nse_ctx_line_shapes(nse_ctx* x, int* yz, int* xnl) {
+  if (!x || !yz || !xnl) return NSE_ERR_ARG;
+  for (int dir = 1; dir <= 2; ++dir)
+    for (int comp = 0; comp < 4; ++comp) yz[(dir - 1) * 4 + comp] = x->yzshape[dir][comp];
+  for (int comp = 0; comp < 4; ++comp) xnl[comp] = x->xnl[comp] ? x->xnl[comp] : 2;
   return NSE_OK;
 }
 

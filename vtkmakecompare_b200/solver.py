@@ -27,6 +27,7 @@ FLAG_ONE_STREAM = 128
 FLAG_POISSON5 = 256
 FLAG_POISSON32 = 512
 FLAG_LINES_TMA = 1024
+FLAG_NO_AUTOTUNE = 2048
 
 
 class Config(C.Structure):
@@ -75,6 +76,7 @@ def _sig():
     L.nse_levelset.argtypes = [vp, vp, vp, C.c_int, C.c_double, C.c_double]
     L.nse_ctx_grid.argtypes = [vp] + [vp] * 12
     L.nse_ctx_profile.argtypes = [vp, C.c_int]
+    L.nse_ctx_line_shapes.argtypes = [vp, vp, vp]
     L.nse_ctx_phase_times.argtypes = [vp, vp, C.c_int, vp]
     L.nse_launch_count.restype = C.c_longlong
     L.nse_ensemble_create.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp)]
@@ -182,6 +184,15 @@ class Context:
 
     def sync(self):
         check(self.L.nse_sync(self.h))
+
+    def line_shapes(self):
+        """Launch shapes the autotuner chose for the line passes (after the first
+        step): {"y": [u, v, w, T], "z": [...], "x": [...]}; y/z codes 0 = 16 lines
+        per CTA, 1 = 8, 3 = 32, 2 = TMA tiles; x = lines per warp iteration."""
+        yz = (C.c_int * 8)()
+        xn = (C.c_int * 4)()
+        check(self.L.nse_ctx_line_shapes(self.h, yz, xn))
+        return {"y": list(yz[:4]), "z": list(yz[4:]), "x": list(xn)}
 
     def levelset(self, phi0, nnn=2000, dtau=1.0e-3, width=1.0, want_phi=True):
         a = np.asfortranarray(phi0, dtype=np.float64)
