@@ -446,7 +446,7 @@ def run_ensemble(S, W, torch, stream, args, rank=0, world=1, device="cpu"):
     shapes = gather_case_scalars({i: (g["nx"], g["ny"], g["nz"]) for i, (g, *_) in zip(mine, cases)},
                                  args.ens_cases, 3, world, device)
     cells = int(sum(a * b * c for a, b, c in shapes))
-    res = {"cases": args.ens_cases, "cells": cells,
+    res = {"cases": args.ens_cases, "cells": cells, "streams": args.ens_streams,
            "grids": sorted({tuple(int(x) for x in sh) for sh in shapes})}
     if world > 1:
         res["ranks"] = world
@@ -461,7 +461,7 @@ def run_ensemble(S, W, torch, stream, args, rank=0, world=1, device="cpu"):
             c.step(1)  # Euler start and the mask tables, outside the timing
         seq_ms = timed(lambda: [c.step(args.steps) for c in ctxs])
         if ctxs:
-            with S.Ensemble(ctxs, nstreams=8) as ens:
+            with S.Ensemble(ctxs, nstreams=args.ens_streams) as ens:
                 ens.set_stream(stream.cuda_stream)
                 ens.step(2)
                 ens.sync()
@@ -992,6 +992,8 @@ def main():
     ap.add_argument("--no-mixed", action="store_true")
     ap.add_argument("--ens-cases", type=int, default=32,
                     help="cases of the batched-ensemble measurement (0 skips it)")
+    ap.add_argument("--ens-streams", type=int, default=8,
+                    help="streams the batched ensemble's cases are spread over")
     ap.add_argument("--adj-steps", type=int, default=400,
                     help="forward steps of the adjoint measurement (0 skips it)")
     ap.add_argument("--adj-grid", type=int, default=128)
