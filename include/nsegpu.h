@@ -281,9 +281,9 @@ enum {
   NSE_FLAG_ONE_STREAM = 128, /* everything on the context's stream, in the reference's
                                 order (default: the line passes of u, v, w, T as four
                                 concurrent chains on side streams; same results) */
-  NSE_FLAG_POISSON5 = 256,   /* FP64 Poisson solve as five launches (x and z transforms
-                                separate) instead of three (each plane's 2-D transform
-                                in one cluster launch; NX = NZ = 256, ny = 16 m) */
+  NSE_FLAG_POISSON3 = 256,   /* FP64 Poisson solve in three launches (each plane's 2-D
+                                transform in one cluster launch, partitioned SPN; NX =
+                                NZ = 256, ny = 16 m) instead of the five-launch default */
   NSE_FLAG_POISSON32 = 512,  /* NSE_MIXED: FP32 Poisson transforms and spectrum with FP64
                                 residual refinement instead of the FP64 solve */
   NSE_FLAG_LINES_TMA = 1024, /* FP64 fast form: the y and z line passes stream tiles of

@@ -1812,10 +1812,11 @@ int nse_start(nse_ctx* x) {
   return NSE_CUDA(cudaGetLastError()) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
 
-// the three-pass Poisson solve (k_poisson2d.cu) of the fast forms: NX = NZ
-// = 256 and ny = 16 m, unless NSE_FLAG_POISSON5 asks for the five passes
+// the three-pass Poisson solve (k_poisson2d.cu) of the fast forms, when asked
+// for with NSE_FLAG_POISSON3 (NX = NZ = 256 and ny = 16 m)
 static bool poisson3(const nse_ctx* x) {
-  return !(x->cfg.flags & (NSE_FLAG_EXACT | NSE_FLAG_POISSON5)) && poisson3_ok(x->pb.pp);
+  return (x->cfg.flags & NSE_FLAG_POISSON3) && !(x->cfg.flags & NSE_FLAG_EXACT) &&
+         poisson3_ok(x->pb.pp);
 }
 
 // P2S -> SPN/SP0B -> S2P -> PHIBC on phi (FP64), phase-marked

@@ -27,6 +27,8 @@ def main():
     ap.add_argument("--poisson", type=int, default=0)
     ap.add_argument("--exact", action="store_true")
     ap.add_argument("--adjoint", type=int, default=0)
+    ap.add_argument("--flags", type=int, default=0,
+                    help="extra nse_config flags (e.g. 256 = NSE_FLAG_POISSON3)")
     a = ap.parse_args()
     nx, ny, nz = a.grid
     g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
@@ -35,7 +37,7 @@ def main():
     Re = 3000.0
     cfg = S.Config(nx, ny, nz, dt, Re, 0.71, 1.0e4, 2 * math.pi, 2.0, math.pi, y0=-1.0,
                    ystretch=2.0, body_force=3.0 / Re, heat_source=0.0, t_solid=1.0,
-                   flags=S.FLAG_EXACT if a.exact else 0)
+                   flags=(S.FLAG_EXACT if a.exact else 0) | a.flags)
     with S.Context(cfg) as ctx:
         for k in ("u", "v", "w", "T"):
             ctx.upload(k, f[k])

@@ -24,7 +24,7 @@ FLAG_POISSON64 = 16
 FLAG_MATH64 = 32
 FLAG_LINES64 = 64
 FLAG_ONE_STREAM = 128
-FLAG_POISSON5 = 256
+FLAG_POISSON3 = 256
 FLAG_POISSON32 = 512
 FLAG_LINES_TMA = 1024
 FLAG_NO_AUTOTUNE = 2048
