@@ -289,8 +289,11 @@ enum {
   NSE_FLAG_LINES_TMA = 1024, /* FP64 fast form: the y and z line passes stream tiles of
                                 16 lines through shared memory by TMA copies (persistent
                                 CTAs, next tile in flight while one is solved) */
-  NSE_FLAG_NO_AUTOTUNE = 2048 /* keep the fixed line launch shapes instead of timing the
+  NSE_FLAG_NO_AUTOTUNE = 2048, /* keep the fixed line launch shapes instead of timing the
                                 candidates before the first step (same values either way) */
+  NSE_FLAG_SPN_TMA = 4096    /* FP64 spectral tridiagonal solve (SPN + SP0B) through TMA
+                                tiles of 16 kx columns, partitioned over 16 warps
+                                (ny = 16 m), instead of the two-ended solver */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

@@ -187,3 +187,46 @@ def test_three_pass_poisson_matches_five_pass_and_oracle(ny):
     # the entries PHIBC and S2P never write keep the uploaded values
     assert np.array_equal(out[0][nx + 1, 0, :], rhs[nx + 1, 0, :])
     assert np.array_equal(out[0][:, ny + 1, 0], rhs[:, ny + 1, 0])
+
+
+@pytest.mark.parametrize("n", [(256, 192, 256), (96, 64, 96), (160, 128, 160), (64, 48, 60)])
+def test_tma_tile_spn_matches_default_and_oracle(n):
+    """NSE_FLAG_SPN_TMA (SPN + SP0B through TMA tiles of 16 kx columns,
+    partitioned over 16 warps) against the default two-ended solver and the
+    oracle on the seeded right-hand side, and through 3 steps of the
+    penalised step."""
+    nx, ny, nz = n
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    rhs = W.poisson_rhs(g, seed=nx + ny)
+    out = []
+    for flags in (S.FLAG_SPN_TMA, 0):
+        cfg = S.Config(nx, ny, nz, 1.0, 1.0, 1.0, 0.0, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                       ystretch=2.0, flags=flags)
+        with S.Context(cfg) as ctx:
+            ctx.upload("phi", rhs)
+            ctx.poisson()
+            ctx.sync()
+            out.append(ctx.download("phi"))
+    I = (slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1))
+    assert rel_l2(out[0][I], out[1][I]) < 1e-12
+    ref, _, _ = oracle_poisson(g, rhs)
+    assert rel_l2(out[0][I], ref[I]) < 1e-12
+    gg, f, dt = channel(*n, seed=5, t_bot=1.0, t_top=0.0)
+    c1 = W.smoothed_mask(gg, W.sphere_phi0(gg, (math.pi, 0.0, math.pi / 2), 0.25), 1.5)
+    res = []
+    for flags in (S.FLAG_SPN_TMA, 0):
+        cfg = S.Config(nx, ny, nz, dt, 3000.0, 0.71, 1.0e4, gg["xl"], gg["yl"], gg["zl"],
+                       y0=-1.0, ystretch=2.0, body_force=1e-3, heat_source=0.0, t_bot=1.0,
+                       t_solid=1.0, flags=flags)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.project()
+            ctx.start()
+            ctx.step(3)
+            ctx.sync()
+            res.append({k: ctx.download(k) for k in ("u", "v", "w", "p", "T")})
+            assert ctx.monitor()["max_divu"] < 1e-10
+    for k in res[0]:
+        assert rel_l2(res[0][k], res[1][k]) < 1e-10, k

@@ -265,6 +265,9 @@ bool spn_part_ok(const PoissonPlan& pp);
 void launch_p2s256(const PoissonPlan& pp, const Dims& d, const double* FP, cudaStream_t s);
 void launch_spn_part(const PoissonPlan& pp, cudaStream_t s);
 void launch_s2p256_phibc(const PoissonPlan& pp, const Dims& d, double* FP, cudaStream_t s);
+// SPN + SP0B through TMA tiles (ny = 16 m); false when it does not apply
+bool launch_spn_tma(const PoissonPlan& pp, cudaStream_t s);
+int spn_wait_error();
 // spectrum <-> reference PHIT layout (0:nx/2,0:ny+1,0:nz+1)
 void launch_spec_to_phit(const PoissonPlan& pp, double* phit, cudaStream_t s);
 void launch_phit_to_spec(const PoissonPlan& pp, const double* phit, cudaStream_t s);

@@ -27,8 +27,11 @@
 // algorithm from FFTW's in any case).
 #include <cooperative_groups.h>
 
+#include <algorithm>
+
 #include "common.cuh"
 #include "fft_core.cuh"
+#include "tma.cuh"
 
 namespace cg = cooperative_groups;
 
@@ -429,6 +432,214 @@ __global__ void __launch_bounds__(256, 2)
   }
 }
 
+// ------------------------------------------- SPN + SP0B through TMA tiles
+// The spectrum as a real array [kz][J][2 Hp] (re, im interleaved): a tile is
+// 32 reals (16 kx columns) x the ny rows of one kz, brought into shared memory
+// by one TMA copy (box at x = 32 t, 16-byte aligned), next tile in flight on a
+// second buffer.  Thread (lane, k): lane = real column (kx = 16 t + lane/2,
+// re or im), k = partition (warp) of m = ny/16 rows; the re and im columns
+// of a system run the same coefficient recurrence.  Each partition is
+// eliminated in registers as in k_spn_part; the reduced system (F eliminated
+// with the next partition's first row, then cyclic reduction over the 16
+// partitions) goes through shared memory, one column per lane, so every
+// shared-memory access of a warp is 32 consecutive reals.  The mean mode's
+// two columns are skipped by the partitioned solve and marched by SP0B
+// (mkp.f:263-290) afterwards, from the tile.  The solved tile leaves by one
+// TMA store (columns past NX/2 are carried along unchanged).
+__device__ int g_spn_wait_err = 0;
+
+template <int M>
+__global__ void __launch_bounds__(512, 1)
+    k_spn_tma(const __grid_constant__ CUtensorMap tm, int H, int ny, int nz, int ntx,
+              const double* __restrict__ AC, const double* __restrict__ KXZ) {
+  constexpr int NL = 32;  // real columns per tile
+  extern __shared__ __align__(128) unsigned char ssm[];
+  const size_t tb_bytes = (((size_t)ny * NL * 8) + 127) & ~(size_t)127;
+  double* buf0 = reinterpret_cast<double*>(ssm);
+  double* buf1 = reinterpret_cast<double*>(ssm + tb_bytes);
+  double* acs = reinterpret_cast<double*>(ssm + 2 * tb_bytes);  // AC1, AC2, AC3 [ny] each
+  double* rs = acs + 3 * ny;          // [4][16][NL] first-row values of each partition
+  double* pc = rs + 4 * 16 * NL;      // [4][16][NL] cyclic-reduction rows
+  uint64_t* bar = reinterpret_cast<uint64_t*>(pc + 4 * 16 * NL);
+  const int lane = threadIdx.x & 31, k = threadIdx.x >> 5;
+  const long ntiles = (long)ntx * nz;
+  const unsigned tile_tx = (unsigned)ny * NL * 8;
+  for (int r = threadIdx.x; r < 3 * ny; r += blockDim.x)
+    acs[r] = AC[r];
+  if (threadIdx.x == 0) {
+    mbar_init(&bar[0], 1);
+    mbar_init(&bar[1], 1);
+    mbar_fence_init();
+  }
+  __syncthreads();
+  auto issue = [&](long q, double* dst, uint64_t* b) {
+    mbar_expect_tx(b, tile_tx);
+    tma_load_3d(dst, &tm, (int)(q % ntx) * NL, 0, (int)(q / ntx), b);
+  };
+  long q = blockIdx.x;
+  if (threadIdx.x == 0 && q < ntiles) issue(q, buf0, &bar[0]);
+  const int r0 = k * M;
+  auto RS = [&](int v, int kk) -> double& { return rs[(v * 16 + kk) * NL + lane]; };
+  auto PC = [&](int v, int kk) -> double& { return pc[(v * 16 + kk) * NL + lane]; };
+  for (int it = 0; q < ntiles; q += gridDim.x, ++it) {
+    double* cur = (it & 1) ? buf1 : buf0;
+    double* nxt = (it & 1) ? buf0 : buf1;
+    const long qn = q + gridDim.x;
+    if (threadIdx.x == 0 && qn < ntiles) {
+      tma_store_wait_read();
+      issue(qn, nxt, &bar[(it + 1) & 1]);
+    }
+    if (!tma_wait(&bar[it & 1], (unsigned)((it >> 1) & 1)) && threadIdx.x == 0)
+      atomicExch(&g_spn_wait_err, 1);
+    const int kx = (int)(q % ntx) * (NL / 2) + (lane >> 1);
+    const int kz = (int)(q / ntx);
+    const bool mean = kx == 0 && kz == 0;
+    const bool valid = kx < H && !mean;
+    const double kxz = valid ? KXZ[kx + (long)H * kz] : 1.0;
+    auto coef = [&](int r, double& a, double& b, double& c) {
+      a = acs[r];
+      b = acs[ny + r] - kxz;
+      c = acs[2 * ny + r];
+      if (r == 0) { b = b + a; a = 0.0; }
+      if (r == ny - 1) { b = b + c; c = 0.0; }
+    };
+    double dv[M], cp[M], pp[M];
+    const double* col = cur + (size_t)r0 * NL + lane;
+#pragma unroll
+    for (int t = 0; t < M; ++t) dv[t] = col[(size_t)t * NL];
+    {
+      double cprev = 0.0, pprev = 0.0, gprev = 0.0;
+#pragma unroll
+      for (int t = 1; t <= M - 2; ++t) {
+        double a, b, c;
+        coef(r0 + t, a, b, c);
+        const double inv = 1.0 / (b - a * cprev);
+        const double g = (dv[t] - a * gprev) * inv;
+        const double p = (t == 1 ? -a : -a * pprev) * inv;
+        cp[t] = c * inv;
+        pp[t] = p;
+        dv[t] = g;
+        gprev = g;
+        pprev = p;
+        cprev = cp[t];
+      }
+    }
+    const double gL = dv[M - 2], pL = pp[M - 2], qL = -cp[M - 2];
+    double g1 = gL, p1 = pL, q1 = qL;
+#pragma unroll
+    for (int t = M - 3; t >= 1; --t) {
+      g1 = dv[t] - cp[t] * g1;
+      p1 = pp[t] - cp[t] * p1;
+      q1 = -cp[t] * q1;
+    }
+    double as, bs, cs, ae, be, ce;
+    coef(r0, as, bs, cs);
+    coef(r0 + M - 1, ae, be, ce);
+    const double sub_s = as, diag_s = bs + cs * p1, sup_s = cs * q1, rhs_s = dv[0] - cs * g1;
+    const double sub_e = ae * pL, diag_e = be + ae * qL, sup_e = ce, rhs_e = dv[M - 1] - ae * gL;
+    RS(0, k) = sub_s;
+    RS(1, k) = diag_s;
+    RS(2, k) = sup_s;
+    RS(3, k) = rhs_s;
+    __syncthreads();
+    // F eliminated: al E(k-1) + be E(k) + ga E(k+1) = rho
+    const double f = sub_e / diag_s;
+    double al = -f * sub_s, bb = diag_e - f * sup_s, ga = 0.0, rho = rhs_e - f * rhs_s;
+    if (k < 15) {
+      const double hh = sup_e / RS(1, k + 1);
+      bb -= hh * RS(0, k + 1);
+      ga = -hh * RS(2, k + 1);
+      rho -= hh * RS(3, k + 1);
+    }
+#pragma unroll
+    for (int st = 1; st < 16; st <<= 1) {
+      PC(0, k) = al;
+      PC(1, k) = bb;
+      PC(2, k) = ga;
+      PC(3, k) = rho;
+      __syncthreads();
+      double nal = 0.0, nga = 0.0, nbb = bb, nrho = rho;
+      if (k >= st) {
+        const double k1 = al / PC(1, k - st);
+        nal = -k1 * PC(0, k - st);
+        nbb -= k1 * PC(2, k - st);
+        nrho -= k1 * PC(3, k - st);
+      }
+      if (k + st < 16) {
+        const double k2 = ga / PC(1, k + st);
+        nga = -k2 * PC(2, k + st);
+        nbb -= k2 * PC(0, k + st);
+        nrho -= k2 * PC(3, k + st);
+      }
+      __syncthreads();
+      al = nal;
+      ga = nga;
+      bb = nbb;
+      rho = nrho;
+    }
+    const double E = rho / bb;
+    PC(0, k) = E;
+    __syncthreads();
+    const double Em = k > 0 ? PC(0, k - 1) : 0.0;
+    const double F = (rhs_s - sub_s * Em - sup_s * E) / diag_s;
+    double* dst = cur + (size_t)r0 * NL + lane;
+    if (valid) {
+      dst[0] = F;
+      dst[(size_t)(M - 1) * NL] = E;
+      double xn = dv[M - 2] + F * pp[M - 2] + E * qL;
+      dst[(size_t)(M - 2) * NL] = xn;
+#pragma unroll
+      for (int t = M - 3; t >= 1; --t) {
+        xn = dv[t] + F * pp[t] - cp[t] * xn;
+        dst[(size_t)t * NL] = xn;
+      }
+    }
+    __syncthreads();
+    if (kz == 0 && k == 0 && lane < 2 && (q % ntx) == 0) {
+      // SP0B on column `lane` (re | im) of the mean mode, from the tile
+      double* m0 = cur + lane;
+      double pm = 0.0, pcur = 0.0, Dj = m0[0];
+      m0[0] = 0.0;
+      for (int J = 1; J <= ny - 1; ++J) {
+        const double Dn = m0[(size_t)J * NL];
+        const double pn = (Dj - acs[J - 1] * pm - acs[ny + J - 1] * pcur) / acs[2 * ny + J - 1];
+        m0[(size_t)J * NL] = pn;
+        pm = pcur;
+        pcur = pn;
+        Dj = Dn;
+      }
+    }
+    fence_async_smem();
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      tma_store_3d(&tm, (int)(q % ntx) * NL, 0, kz, cur);
+      tma_store_commit();
+    }
+  }
+  if (threadIdx.x == 0) tma_store_wait_all();
+}
+
+template <int M>
+bool spn_tma_launch(const PoissonPlan& pp, cudaStream_t s) {
+  CUtensorMap tm;
+  const long e0 = 2L * pp.Hp, p1 = e0 * 8, p2 = p1 * pp.ny;
+  if (p1 % 16 != 0 || ((uintptr_t)pp.spec & 15) != 0 || pp.ny > 256) return false;
+  if (!tma_encode_3d(&tm, pp.spec, true, e0, pp.ny, pp.nz, p1, p2, 32, pp.ny, 1)) return false;
+  const int ntx = (2 * pp.H + 31) / 32;
+  const long ntiles = (long)ntx * pp.nz;
+  const size_t tb = (((size_t)pp.ny * 32 * 8) + 127) & ~(size_t)127;
+  const size_t smem = 2 * tb + (3 * (size_t)pp.ny + 8 * 16 * 32) * 8 + 16;
+  int sms = 148, dev = 0;
+  cudaGetDevice(&dev);
+  cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev);
+  cudaFuncSetAttribute((const void*)k_spn_tma<M>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+                       (int)smem);
+  count_launch();
+  k_spn_tma<M><<<(int)std::min<long>(ntiles, sms), 512, smem, s>>>(tm, pp.H, pp.ny, pp.nz, ntx,
+                                                                  pp.AC, pp.KXZ);
+  return true;
+}
+
 template <int M>
 void spn_part_launch(const PoissonPlan& pp, cudaStream_t s) {
   const int nsys = pp.H * pp.nz;
@@ -474,6 +685,36 @@ void launch_spn_part(const PoissonPlan& pp, cudaStream_t s) {
     case 15: spn_part_launch<15>(pp, s); break;
     default: spn_part_launch<16>(pp, s); break;
   }
+}
+
+bool launch_spn_tma(const PoissonPlan& pp, cudaStream_t s) {
+  if (!spn_part_ok(pp)) return false;
+  switch (pp.ny / 16) {
+    case 3: return spn_tma_launch<3>(pp, s);
+    case 4: return spn_tma_launch<4>(pp, s);
+    case 5: return spn_tma_launch<5>(pp, s);
+    case 6: return spn_tma_launch<6>(pp, s);
+    case 7: return spn_tma_launch<7>(pp, s);
+    case 8: return spn_tma_launch<8>(pp, s);
+    case 9: return spn_tma_launch<9>(pp, s);
+    case 10: return spn_tma_launch<10>(pp, s);
+    case 11: return spn_tma_launch<11>(pp, s);
+    case 12: return spn_tma_launch<12>(pp, s);
+    case 13: return spn_tma_launch<13>(pp, s);
+    case 14: return spn_tma_launch<14>(pp, s);
+    case 15: return spn_tma_launch<15>(pp, s);
+    default: return spn_tma_launch<16>(pp, s);
+  }
+}
+
+int spn_wait_error() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_spn_wait_err, sizeof(int)) != cudaSuccess) return 0;
+  if (v) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_spn_wait_err, &z, sizeof(int));
+  }
+  return v;
 }
 
 void launch_p2s256(const PoissonPlan& pp, const Dims& d, const double* FP, cudaStream_t s) {

@@ -1819,6 +1819,15 @@ static bool poisson3(const nse_ctx* x) {
          poisson3_ok(x->pb.pp);
 }
 
+// SPN + SP0B of the fast forms (FP64 spectrum): the TMA-tile solver with
+// NSE_FLAG_SPN_TMA, else the two-ended solver
+static void ctx_spn(nse_ctx* x, bool part) {
+  const PoissonPlan& pp = x->pb.pp;
+  if ((x->cfg.flags & NSE_FLAG_SPN_TMA) && launch_spn_tma(pp, x->stream)) return;
+  if (part) launch_spn_part(pp, x->stream);
+  else launch_spn_fast(pp, x->stream);
+}
+
 // P2S -> SPN/SP0B -> S2P -> PHIBC on phi (FP64), phase-marked
 static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
   const Dims& d = x->d;
@@ -1829,7 +1838,7 @@ static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
     launch_p2s256(pp, d, phi, s);
     mark(x, PH_FFTZ_F);
     mark(x, PH_SPN);
-    launch_spn_part(pp, s);
+    ctx_spn(x, true);
     mark(x, PH_FFTZ_I);
     mark(x, PH_FFTX_I);
     launch_s2p256_phibc(pp, d, phi, s);
@@ -1840,7 +1849,7 @@ static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
   mark(x, PH_FFTZ_F);
   launch_fft_z(pp, false, s);
   mark(x, PH_SPN);
-  launch_spn_fast(pp, s);
+  ctx_spn(x, false);
   mark(x, PH_FFTZ_I);
   launch_fft_z(pp, true, s);
   mark(x, PH_FFTX_I);
@@ -1874,7 +1883,7 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
     if (p64) launch_fft_z(pp, false, s);
     else launch_fft_z_f32(pp, false, s);
     mark(x, PH_SPN);
-    if (p64) launch_spn_fast(pp, s);
+    if (p64) ctx_spn(x, false);
     else launch_spn_fast_f32(pp, s);
     mark(x, PH_FFTZ_I);
     if (p64) launch_fft_z(pp, true, s);
@@ -1925,7 +1934,8 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
     mark(x, PH_FFTZ_F);
     launch_fft_z(pp, false, s);
     mark(x, PH_SPN);
-    launch_spn_fast(pp, s);
+    if (rg) ctx_spn(x, false);
+    else launch_spn_fast(pp, s);
     mark(x, PH_FFTZ_I);
     launch_fft_z(pp, true, s);
     mark(x, PH_FFTX_I);
@@ -2551,6 +2561,10 @@ int nse_ctx_line_shapes(nse_ctx* x, int* yz, int* xnl) {
 int nse_sync(nse_ctx* x) {
   if (!x) return NSE_ERR_ARG;
   if (!NSE_CUDA(cudaStreamSynchronize(x->stream))) return status_or(NSE_ERR_CUDA);
+  if (spn_wait_error()) {
+    set_error(NSE_ERR_CUDA, "nse_sync: the spectral solve's wait for its tile copy gave up");
+    return NSE_ERR_CUDA;
+  }
   if (line_wait_error()) {
     set_error(NSE_ERR_CUDA, "nse_sync: a line kernel's wait for its tile copy gave up");
     return NSE_ERR_CUDA;

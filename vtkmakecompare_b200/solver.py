@@ -28,6 +28,7 @@ FLAG_POISSON3 = 256
 FLAG_POISSON32 = 512
 FLAG_LINES_TMA = 1024
 FLAG_NO_AUTOTUNE = 2048
+FLAG_SPN_TMA = 4096
 
 
 class Config(C.Structure):
