@@ -727,15 +727,24 @@ __global__ void __launch_bounds__(16 * P, 2)
     mbar_init(&bar[1], 1);
     mbar_fence_init();
   }
+  // the copies need the tensor map 64-byte aligned and the tile buffers
+  // 128-byte aligned in shared memory; a launch that finds otherwise records
+  // the error and copies nothing (its tiles are then left as they are)
+  const bool aligned = ((reinterpret_cast<uintptr_t>(&tm) & 63) == 0) &&
+                       ((smem_u32(buf0) & 127) == 0) && ((smem_u32(buf1) & 127) == 0) &&
+                       ((smem_u32(bar) & 7) == 0);
+  if (!aligned) {
+    if (threadIdx.x == 0) atomicExch(&g_line_wait_err, 2);
+    return;
+  }
   __syncthreads();
-  auto issue = [&](long q, double* dst, uint64_t* b) {
-    const int x0 = (int)(q % ntx) * LPB, o = 1 + (int)(q / ntx);
-    mbar_expect_tx(b, tile_tx);
-    if (DIR == 1) tma_load_3d(dst, &tm, x0, 1, o, b);
-    else tma_load_3d(dst, &tm, x0, o, 1, b);
-  };
   long q = blockIdx.x;
-  if (threadIdx.x == 0 && q < ntiles) issue(q, buf0, &bar[0]);
+  if (threadIdx.x == 0 && q < ntiles) {
+    mbar_expect_tx(&bar[0], tile_tx);
+    const int x0 = (int)(q % ntx) * LPB, o = 1 + (int)(q / ntx);
+    if (DIR == 1) tma_load_3d(buf0, &tm, x0, 1, o, &bar[0]);
+    else tma_load_3d(buf0, &tm, x0, o, 1, &bar[0]);
+  }
   const int s = (int)((long)k * nu / P), e = (int)((long)(k + 1) * nu / P) - 1;
   const int m = e - s + 1;
   for (int it = 0; q < ntiles; q += gridDim.x, ++it) {
@@ -744,7 +753,11 @@ __global__ void __launch_bounds__(16 * P, 2)
     const long qn = q + gridDim.x;
     if (threadIdx.x == 0 && qn < ntiles) {
       tma_store_wait_read();  // the previous tile's store has read its buffer
-      issue(qn, nxt, &bar[(it + 1) & 1]);
+      uint64_t* nb = &bar[(it + 1) & 1];
+      mbar_expect_tx(nb, tile_tx);
+      const int x0 = (int)(qn % ntx) * LPB, o = 1 + (int)(qn / ntx);
+      if (DIR == 1) tma_load_3d(nxt, &tm, x0, 1, o, nb);
+      else tma_load_3d(nxt, &tm, x0, o, 1, nb);
     }
     if (!tma_wait(&bar[it & 1], (unsigned)((it >> 1) & 1)) && threadIdx.x == 0)
       atomicExch(&g_line_wait_err, 1);

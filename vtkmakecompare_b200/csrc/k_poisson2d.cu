@@ -471,13 +471,22 @@ __global__ void __launch_bounds__(512, 1)
     mbar_init(&bar[1], 1);
     mbar_fence_init();
   }
+  // the copies need the tensor map 64-byte aligned and the tile buffers
+  // 128-byte aligned in shared memory; a launch that finds otherwise records
+  // the error and copies nothing
+  const bool aligned = ((reinterpret_cast<uintptr_t>(&tm) & 63) == 0) &&
+                       ((smem_u32(buf0) & 127) == 0) && ((smem_u32(buf1) & 127) == 0) &&
+                       ((smem_u32(bar) & 7) == 0);
+  if (!aligned) {
+    if (threadIdx.x == 0) atomicExch(&g_spn_wait_err, 2);
+    return;
+  }
   __syncthreads();
-  auto issue = [&](long q, double* dst, uint64_t* b) {
-    mbar_expect_tx(b, tile_tx);
-    tma_load_3d(dst, &tm, (int)(q % ntx) * NL, 0, (int)(q / ntx), b);
-  };
   long q = blockIdx.x;
-  if (threadIdx.x == 0 && q < ntiles) issue(q, buf0, &bar[0]);
+  if (threadIdx.x == 0 && q < ntiles) {
+    mbar_expect_tx(&bar[0], tile_tx);
+    tma_load_3d(buf0, &tm, (int)(q % ntx) * NL, 0, (int)(q / ntx), &bar[0]);
+  }
   const int r0 = k * M;
   auto RS = [&](int v, int kk) -> double& { return rs[(v * 16 + kk) * NL + lane]; };
   auto PC = [&](int v, int kk) -> double& { return pc[(v * 16 + kk) * NL + lane]; };
@@ -487,7 +496,9 @@ __global__ void __launch_bounds__(512, 1)
     const long qn = q + gridDim.x;
     if (threadIdx.x == 0 && qn < ntiles) {
       tma_store_wait_read();
-      issue(qn, nxt, &bar[(it + 1) & 1]);
+      uint64_t* nb = &bar[(it + 1) & 1];
+      mbar_expect_tx(nb, tile_tx);
+      tma_load_3d(nxt, &tm, (int)(qn % ntx) * NL, 0, (int)(qn / ntx), nb);
     }
     if (!tma_wait(&bar[it & 1], (unsigned)((it >> 1) & 1)) && threadIdx.x == 0)
       atomicExch(&g_spn_wait_err, 1);

@@ -1994,9 +1994,9 @@ int nse_poisson(nse_ctx* x) {
 // ------------------------------------------------------------- autotuner --
 // The partitioned line passes have several launch shapes that give the same
 // values: y/z lines 16, 8 or 32 lines per CTA (the y/z line-to-warp mapping:
-// a warp holds 32/L lines x L partitions... of one CTA), or, in FP64, TMA
-// tiles of 16 lines with persistent CTAs; x lines one or two per warp
-// iteration.  Before a context's first step (outside any stream capture)
+// with L lines per CTA a warp holds min(L, 32) lines of 32/L partitions), and
+// x lines one or two per warp iteration.  (The TMA tiles of the FP64 y/z
+// lines are a further shape, set only by NSE_FLAG_LINES_TMA.)  Before a context's first step (outside any stream capture)
 // every candidate of every pass is timed on a scratch copy of the pass's
 // field (CUDA events, one warm-up and three timed runs, the fastest kept).
 // Choices are kept per grid and form for the process, so the cases of an
@@ -2054,7 +2054,6 @@ static void autotune_lines(nse_ctx* x) {
         cand = {2, 1};
       } else {
         cand = {0, 1, 3};
-        if (!x->mixed) cand.push_back(2);
       }
       int best = cand[0];
       float best_ms = 1e30f;
