@@ -349,12 +349,14 @@ int nse_ctx_read_field(nse_ctx* ctx, const char* path);
  * out[3]=sum|w|dz, out[4]=sum T dx dy dz (all cells), out[5]=non-finite count */
 int nse_monitor(nse_ctx* ctx, double out[6]);
 int nse_sync(nse_ctx* ctx);
-/* Launch shapes the autotuner chose for the partitioned line passes (set
- * before the context's first step; no counterpart in the reference):
- * yz[(dir-1)*4 + comp] for y (dir 1) and z (dir 2) lines of u, v, w, T:
- * 0 = 16 lines per CTA, 1 = 8, 3 = 32, 2 = TMA tiles of 16 lines; xnl[comp] =
- * x lines per warp iteration. */
-int nse_ctx_line_shapes(nse_ctx* ctx, int* yz, int* xnl);
+/* Launch shapes the autotuner chose (set before the context's first step;
+ * no counterpart in the reference), out[13]: out[(dir-1)*4 + comp] for the y
+ * (dir 1) and z (dir 2) line passes of u, v, w, T (0 = 16 lines per CTA, 1 =
+ * 8, 3 = 32, 2 = TMA tiles of 16 lines), out[8 + comp] the x lines per warp
+ * iteration, out[12] the right-hand-side kernel's shape (0 = 32x4 tiles with a
+ * 5-plane ring in FP64 / 32x8 in FP32, 1 = 32x4 with 4 planes, 2 = 32x8 with
+ * 5, 3 = 32x8 with 4). */
+int nse_ctx_launch_shapes(nse_ctx* ctx, int* out);
 /* Per-phase timing of the next max_steps steps with CUDA events on the
  * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the
  * summed milliseconds over the profiled steps; phases in launch order:

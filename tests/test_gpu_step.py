@@ -281,3 +281,4 @@ def test_line_launch_shapes_give_the_same_fields(n):
         assert rel_l2(out[2][k], out[0][k]) < 1e-13, k
     assert all(v in (0, 1, 2, 3) for v in shapes["y"] + shapes["z"]), shapes
     assert all(v in (1, 2) for v in shapes["x"]), shapes
+    assert shapes["rhs"] in (0, 1, 2, 3), shapes

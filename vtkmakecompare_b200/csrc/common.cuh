@@ -156,7 +156,7 @@ void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
                      const double* u_ta, const double* v_ta, const double* w_ta,
                      double* u_pre, double* v_pre, double* w_pre, double* T_pre,
                      const double* c1, double* u_a, double* v_a, double* w_a, double* u_T,
-                     cudaStream_t s);
+                     cudaStream_t s, int shape = 0);
 
 // ADI line solves; mask is c1 (nx,ny,nz); comp: 0 u (c2), 1 v (c3), 2 w (c4)
 struct LineScratch {

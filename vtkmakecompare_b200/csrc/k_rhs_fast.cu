@@ -167,31 +167,26 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       const R dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
       const R rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
       const R rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
-      // neighbourhood from shared memory (field f at offset f*PLANE)
+      // neighbourhood from shared memory (field f at offset f*PLANE), each
+      // component's values loaded where they are used: short live ranges keep
+      // the register count low
 #define AT(pl, f, dxo, dyo) (R)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
-      const R uc = AT(pc, 0, 0, 0), uxp = AT(pc, 0, 1, 0), uxm = AT(pc, 0, -1, 0),
-                   uyp = AT(pc, 0, 0, 1), uym = AT(pc, 0, 0, -1), uzp = AT(pp, 0, 0, 0),
-                   uzm = AT(pm, 0, 0, 0), uxmyp = AT(pc, 0, -1, 1), uxmzp = AT(pp, 0, -1, 0);
-      const R vc = AT(pc, 1, 0, 0), vxp = AT(pc, 1, 1, 0), vxm = AT(pc, 1, -1, 0),
-                   vyp = AT(pc, 1, 0, 1), vym = AT(pc, 1, 0, -1), vzp = AT(pp, 1, 0, 0),
-                   vzm = AT(pm, 1, 0, 0), vxpym = AT(pc, 1, 1, -1), vymzp = AT(pp, 1, 0, -1);
-      const R wc = AT(pc, 2, 0, 0), wxp = AT(pc, 2, 1, 0), wxm = AT(pc, 2, -1, 0),
-                   wyp = AT(pc, 2, 0, 1), wym = AT(pc, 2, 0, -1), wzp = AT(pp, 2, 0, 0),
-                   wzm = AT(pm, 2, 0, 0), wxpzm = AT(pm, 2, 1, 0), wypzm = AT(pm, 2, 0, 1);
-      const R tc = AT(pc, 3, 0, 0), txp = AT(pc, 3, 1, 0), txm = AT(pc, 3, -1, 0),
-                   typ = AT(pc, 3, 0, 1), tym = AT(pc, 3, 0, -1), tzp = AT(pp, 3, 0, 0),
-                   tzm = AT(pm, 3, 0, 0);
       // masks (set_immersed_boundary :1037-1080) and AB2 histories
       const R cc1 = AT(pc, 4, 0, 0);
       const R c2 = (I < d.nx) ? (cc1 + AT(pc, 4, 1, 0)) * R(0.5) : cc1;
       const R c3 = (J < d.ny) ? (cc1 + AT(pc, 4, 0, 1)) * R(0.5) : cc1;
       const R c4 = (K < d.nz) ? (cc1 + AT(pp, 4, 0, 0)) * R(0.5) : cc1;
-#undef AT
       const H* hist = reinterpret_cast<const H*>(pc + 5 * PLANE) + t0;
-      const R upre = hist[0], vpre = hist[TILE], wpre = hist[2 * TILE], tpre = hist[3 * TILE];
-    const bool solid = (c2 != R(0)) || (c3 != R(0)) || (c4 != R(0)) || (cc1 != R(0));
+      const bool solid = (c2 != R(0)) || (c3 != R(0)) || (c4 != R(0)) || (cc1 != R(0));
     // u
     {
+      const R uc = AT(pc, 0, 0, 0), uxp = AT(pc, 0, 1, 0), uxm = AT(pc, 0, -1, 0),
+              uyp = AT(pc, 0, 0, 1), uym = AT(pc, 0, 0, -1), uzp = AT(pp, 0, 0, 0),
+              uzm = AT(pm, 0, 0, 0);
+      const R vc = AT(pc, 1, 0, 0), vxp = AT(pc, 1, 1, 0), vym = AT(pc, 1, 0, -1),
+              vxpym = AT(pc, 1, 1, -1);
+      const R wc = AT(pc, 2, 0, 0), wxp = AT(pc, 2, 1, 0), wzm = AT(pm, 2, 0, 0),
+              wxpzm = AT(pm, 2, 1, 0);
       R s1 = uc + uxp, s2 = uc + uxm;
       R U1 = (s1 * s1 - s2 * s2) * rx12;
       R U2 = ((vxp * dxp + vc * dx) * (uyp + uc) - (vxpym * dxp + vym * dx) * (uc + uym)) *
@@ -202,7 +197,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       R L = ((uxp - uc) * rxp - (uc - uxm) * rx) * rx12 +
                  ((uyp - uc) * ry12 - (uc - uym) * ry12m) * ry +
                  ((uzp - uc) * rz12 - (uc - uzm) * rz12m) * rz;
-      R ua = a1 * uv + a2 * upre + kd * L;
+      R ua = a1 * uv + a2 * (R)hist[0] + kd * L;
       U_PRE[c] = uv;
       if (solid && c2 != R(0)) {
         ua += (R)sp.eta * c2 * LD(U_TA, c) * DT;
@@ -213,6 +208,13 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     }
     // v
     {
+      const R uc = AT(pc, 0, 0, 0), uyp = AT(pc, 0, 0, 1), uxm = AT(pc, 0, -1, 0),
+              uxmyp = AT(pc, 0, -1, 1);
+      const R vc = AT(pc, 1, 0, 0), vxp = AT(pc, 1, 1, 0), vxm = AT(pc, 1, -1, 0),
+              vyp = AT(pc, 1, 0, 1), vym = AT(pc, 1, 0, -1), vzp = AT(pp, 1, 0, 0),
+              vzm = AT(pm, 1, 0, 0);
+      const R wc = AT(pc, 2, 0, 0), wyp = AT(pc, 2, 0, 1), wzm = AT(pm, 2, 0, 0),
+              wypzm = AT(pm, 2, 0, 1);
       R V1 = ((uyp * dyp + uc * dy) * (vxp + vc) - (uxmyp * dyp + uxm * dy) * (vc + vxm)) *
                   ry12 * rx;
       R s1 = vc + vyp, s2 = vc + vym;
@@ -223,7 +225,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       R L = ((vxp - vc) * rx12 - (vc - vxm) * rx12m) * rx +
                  ((vyp - vc) * ryp - (vc - vym) * ry) * ry12 +
                  ((vzp - vc) * rz12 - (vc - vzm) * rz12m) * rz;
-      R va = a1 * vv + a2 * vpre + kd * L;
+      R va = a1 * vv + a2 * (R)hist[TILE] + kd * L;
       V_PRE[c] = vv;
       if (solid && c3 != R(0)) va += (R)sp.eta * c3 * LD(V_TA, c) * DT;
       if (J == d.ny) va = R(0);  // set_bc(u_a,v_a,...) zeroes v_a(:,ny,:)
@@ -232,6 +234,13 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     }
     // w
     {
+      const R uc = AT(pc, 0, 0, 0), uzp = AT(pp, 0, 0, 0), uxm = AT(pc, 0, -1, 0),
+              uxmzp = AT(pp, 0, -1, 0);
+      const R vc = AT(pc, 1, 0, 0), vzp = AT(pp, 1, 0, 0), vym = AT(pc, 1, 0, -1),
+              vymzp = AT(pp, 1, 0, -1);
+      const R wc = AT(pc, 2, 0, 0), wxp = AT(pc, 2, 1, 0), wxm = AT(pc, 2, -1, 0),
+              wyp = AT(pc, 2, 0, 1), wym = AT(pc, 2, 0, -1), wzp = AT(pp, 2, 0, 0),
+              wzm = AT(pm, 2, 0, 0);
       R W1 = ((uzp * dzp + uc * dz) * (wxp + wc) - (uxmzp * dzp + uxm * dz) * (wc + wxm)) *
                   rz12 * rx;
       R W2 = ((vzp * dzp + vc * dz) * (wyp + wc) - (vymzp * dzp + vym * dz) * (wc + wym)) *
@@ -242,7 +251,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       R L = ((wxp - wc) * rx12 - (wc - wxm) * rx12m) * rx +
                  ((wyp - wc) * ry12 - (wc - wym) * ry12m) * ry +
                  ((wzp - wc) * rzp - (wc - wzm) * rz) * rz12;
-      R wa = a1 * wv + a2 * wpre + kd * L;
+      R wa = a1 * wv + a2 * (R)hist[2 * TILE] + kd * L;
       W_PRE[c] = wv;
       if (solid && c4 != R(0)) {
         wa += (R)sp.eta * c4 * LD(W_TA, c) * DT;
@@ -253,6 +262,12 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     }
     // T
     {
+      const R uc = AT(pc, 0, 0, 0), uxm = AT(pc, 0, -1, 0);
+      const R vc = AT(pc, 1, 0, 0), vym = AT(pc, 1, 0, -1);
+      const R wc = AT(pc, 2, 0, 0), wzm = AT(pm, 2, 0, 0);
+      const R tc = AT(pc, 3, 0, 0), txp = AT(pc, 3, 1, 0), txm = AT(pc, 3, -1, 0),
+              typ = AT(pc, 3, 0, 1), tym = AT(pc, 3, 0, -1), tzp = AT(pp, 3, 0, 0),
+              tzm = AT(pm, 3, 0, 0);
       R UT = (-((r0 * txm * dx + r0 * tc * dxm) * uxm) * R(0.5) * rx12m +
                    ((r0 * tc * dxp + r0 * txp * dx) * uc) * R(0.5) * rx12) *
                   rx;
@@ -266,7 +281,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       R D1 = (l0 * (txp - tc) * rx12 - l0 * (tc - txm) * rx12m) * rx;
       R D2 = (l0 * (typ - tc) * ry12 - l0 * (tc - tym) * ry12m) * ry;
       R D3 = (l0 * (tzp - tc) * rz12 - l0 * (tc - tzm) * rz12m) * rz;
-      R ut = a1 * vt + a2 * tpre + kT * (D1 + D2 + D3);
+      R ut = a1 * vt + a2 * (R)hist[3 * TILE] + kT * (D1 + D2 + D3);
       T_PRE[c] = vt;
       if (cc1 != R(0)) {
         R pen = (R)sp.eta * cc1 * DT;
@@ -275,28 +290,49 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
         U_T[c] = tc + ut;
       }
     }
+#undef AT
     }  // valid
     cp_async_wait<F - 1>();
     __syncthreads();
   }
 }
 
+template <class H, class CT, int TY, int NS, int MINB>
+static void rhs_go(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
+                   const double* u, const double* v, const double* w, const double* T,
+                   const H* u_ta, const H* v_ta, const H* w_ta, H* u_pre, H* v_pre, H* w_pre,
+                   H* T_pre, const double* c1, H* u_a, H* v_a, H* w_a, H* u_T, cudaStream_t s) {
+  dim3 block(TXW, TY, 1);
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KCHUNK - 1) / KCHUNK);
+  size_t smem = (size_t)NS * slot_bytes<H, TY>();
+  auto kern = k_rhs_fast<H, CT, TY, NS, MINB>;
+  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+  count_launch();
+  kern<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
+                                 T_pre, c1, u_a, v_a, w_a, u_T);
+}
+
+// launch shape: 0 the storage type's default (RhsShape), 1 32x4 tiles with a
+// 4-plane ring and four CTAs per SM, 2 32x8 tiles with a 5-plane ring and two
+// CTAs per SM, 3 32x8 tiles with a 4-plane ring and two CTAs per SM (every
+// shape computes each cell the same way; the context's autotuner picks one)
 template <class H, class CT>
 static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                      const double* u, const double* v, const double* w, const double* T,
                      const H* u_ta, const H* v_ta, const H* w_ta, H* u_pre, H* v_pre, H* w_pre,
                      H* T_pre, const double* c1, H* u_a, H* v_a, H* w_a, H* u_T,
-                     cudaStream_t s) {
+                     cudaStream_t s, int shape) {
   using Sh = RhsShape<H, CT>;
-  constexpr int TY = Sh::TY, NS = Sh::NS;
-  dim3 block(TXW, TY, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KCHUNK - 1) / KCHUNK);
-  size_t smem = (size_t)NS * slot_bytes<H, TY>();
-  auto kern = k_rhs_fast<H, CT, TY, NS, Sh::MINB>;
-  cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-  count_launch();
-  kern<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
-                                 T_pre, c1, u_a, v_a, w_a, u_T);
+#define NSE_RHS_GO(TY_, NS_, MB_)                                                           \
+  rhs_go<H, CT, TY_, NS_, MB_>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre,    \
+                               w_pre, T_pre, c1, u_a, v_a, w_a, u_T, s)
+  switch (shape) {
+    case 1: NSE_RHS_GO(4, 4, 4); break;
+    case 2: NSE_RHS_GO(8, 5, 2); break;
+    case 3: NSE_RHS_GO(8, 4, 2); break;
+    default: NSE_RHS_GO(Sh::TY, Sh::NS, Sh::MINB); break;
+  }
+#undef NSE_RHS_GO
 }
 
 void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
@@ -304,9 +340,9 @@ void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
                      const double* u_ta, const double* v_ta, const double* w_ta,
                      double* u_pre, double* v_pre, double* w_pre, double* T_pre,
                      const double* c1, double* u_a, double* v_a, double* w_a, double* u_T,
-                     cudaStream_t s) {
+                     cudaStream_t s, int shape) {
   rhs_fast<double, double>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
-                           T_pre, c1, u_a, v_a, w_a, u_T, s);
+                           T_pre, c1, u_a, v_a, w_a, u_T, s, shape);
 }
 
 // FP32 storage; arithmetic in FP32, or FP64 with math64
@@ -314,13 +350,14 @@ void launch_rhs_f32(const Dims& d, const GridDev& g, const GridRcp& rg, const St
                     const double* u, const double* v, const double* w, const double* T,
                     const float* u_ta, const float* v_ta, const float* w_ta, float* u_pre,
                     float* v_pre, float* w_pre, float* T_pre, const double* c1, float* u_a,
-                    float* v_a, float* w_a, float* u_T, bool math64, cudaStream_t s) {
+                    float* v_a, float* w_a, float* u_T, bool math64, cudaStream_t s,
+                    int shape) {
   if (math64)
     rhs_fast<float, double>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
-                            T_pre, c1, u_a, v_a, w_a, u_T, s);
+                            T_pre, c1, u_a, v_a, w_a, u_T, s, shape);
   else
     rhs_fast<float, float>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
-                           T_pre, c1, u_a, v_a, w_a, u_T, s);
+                           T_pre, c1, u_a, v_a, w_a, u_T, s, shape);
 }
 
 }  // namespace nse

@@ -59,7 +59,8 @@ void launch_rhs_f32(const Dims& d, const GridDev& g, const GridRcp& rg, const St
                     const double* u, const double* v, const double* w, const double* T,
                     const float* u_ta, const float* v_ta, const float* w_ta, float* u_pre,
                     float* v_pre, float* w_pre, float* T_pre, const double* c1, float* u_a,
-                    float* v_a, float* w_a, float* u_T, bool math64, cudaStream_t s);
+                    float* v_a, float* w_a, float* u_T, bool math64, cudaStream_t s,
+                    int shape = 0);
 void launch_correct_f32(const Dims& d, const GridRcp& rg, const double* PHI, const float* ut,
                         const float* vt, const float* wt, double* p, double* u, double* v,
                         double* w, float* u_ta, float* v_ta, float* w_ta, float* u_ep2,
@@ -1400,6 +1401,9 @@ struct nse_ctx {
   int yzshape[3][4] = {};
   int xnl[4] = {};
   bool tuned = false;
+  // launch shape of the fast right-hand-side kernel (autotune_rhs)
+  int rhs_shape = 0;
+  bool rhs_tuned = false;
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -2100,6 +2104,81 @@ static void autotune_lines(nse_ctx* x) {
   x->tuned = true;
 }
 
+// The fast right-hand-side kernel's launch shapes (tile height, ring depth,
+// CTAs per SM; every shape computes each cell the same way) are timed the same
+// way before the first step: the four AB2 histories, which the kernel reads
+// and rewrites, are copied to scratch fields first, so the timing runs change
+// no state (their outputs go to the step's work fields, which the step's own
+// right-hand side then overwrites).
+static void autotune_rhs(nse_ctx* x, const StepParams& sp) {
+  if (x->rhs_tuned) return;
+  if (x->cfg.flags & (NSE_FLAG_NO_AUTOTUNE | NSE_FLAG_EXACT)) {
+    x->rhs_tuned = true;
+    return;
+  }
+  cudaStream_t s = x->stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  const Dims& d = x->d;
+  char key[96];
+  snprintf(key, sizeof(key), "rhs %d %d %d %d %d", d.nx, d.ny, d.nz, x->mixed ? 1 : 0,
+           x->math64 ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      x->rhs_shape = it->second;
+      x->rhs_tuned = true;
+      return;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  const size_t hb = d.ntot * (x->mixed ? sizeof(float) : sizeof(double));
+  void* hist[4] = {x->sa.p, x->sb.p, x->tmp.p, x->f[NSE_PHI].p};
+  const int hid[4] = {NSE_U_PRE, NSE_V_PRE, NSE_W_PRE, NSE_T_PRE};
+  for (int q = 0; q < 4; ++q)
+    cudaMemcpyAsync(hist[q], x->f[hid[q]].p, hb, cudaMemcpyDeviceToDevice, s);
+  const double *u = F(x, NSE_U), *v = F(x, NSE_V), *w = F(x, NSE_W), *T = F(x, NSE_T);
+  const double* c1 = F(x, NSE_CELLVALUE);
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int shape = 0; shape < 4; ++shape) {
+    auto run = [&]() {
+      if (x->mixed)
+        launch_rhs_f32(d, x->g, x->rg, sp, u, v, w, T, F32(x, NSE_U_TA), F32(x, NSE_V_TA),
+                       F32(x, NSE_W_TA), (float*)hist[0], (float*)hist[1], (float*)hist[2],
+                       (float*)hist[3], c1, x->ua.as<float>(), x->va.as<float>(),
+                       x->wa.as<float>(), x->uT.as<float>(), x->math64, s, shape);
+      else
+        launch_rhs_fast(d, x->g, x->rg, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA),
+                        F(x, NSE_W_TA), (double*)hist[0], (double*)hist[1], (double*)hist[2],
+                        (double*)hist[3], c1, x->ua.as<double>(), x->va.as<double>(),
+                        x->wa.as<double>(), x->uT.as<double>(), s, shape);
+    };
+    run();
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r) run();
+    cudaEventRecord(e1, s);
+    float ms = 1e30f;
+    if (cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = shape;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  x->rhs_shape = best;
+  x->rhs_tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+}
+
 // one time step in the mixed-precision form: FP64 state u, v, w, T, p;
 // FP32 right-hand side, line sweeps and transforms
 static void ctx_step_f32(nse_ctx* x) {
@@ -2119,9 +2198,10 @@ static void ctx_step_f32(nse_ctx* x) {
   mark(x, PH_BC);
   launch_set_bc(d, u, v, w, p, T, c.t_bot, c.t_top, 31, s);
   mark(x, PH_RHS);
+  autotune_rhs(x, sp);
   launch_rhs_f32(d, x->g, x->rg, sp, u, v, w, T, F32(x, NSE_U_TA), F32(x, NSE_V_TA),
                  F32(x, NSE_W_TA), F32(x, NSE_U_PRE), F32(x, NSE_V_PRE), F32(x, NSE_W_PRE),
-                 F32(x, NSE_T_PRE), c1, ua, va, wa, uT, x->math64, s);
+                 F32(x, NSE_T_PRE), c1, ua, va, wa, uT, x->math64, s, x->rhs_shape);
   refresh_line_flags(x, s);
   autotune_lines(x);
   float* fa[3] = {ua, va, wa};
@@ -2215,6 +2295,7 @@ static void ctx_step(nse_ctx* x) {
   launch_set_bc(d, u, v, w, p, T, c.t_bot, c.t_top, 31, s);
   mark(x, PH_RHS);
   // :299-396 explicit terms, AB2, set_bc(u_a,...) and the penalised updates
+  if (!(c.flags & NSE_FLAG_EXACT) && !x->rec) autotune_rhs(x, sp);
   if (c.flags & NSE_FLAG_EXACT)
     launch_rhs_fused(d, x->g, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA),
                      F(x, NSE_U_PRE), F(x, NSE_V_PRE), F(x, NSE_W_PRE), F(x, NSE_T_PRE), c1,
@@ -2222,7 +2303,7 @@ static void ctx_step(nse_ctx* x) {
   else
     launch_rhs_fast(d, x->g, x->rg, sp, u, v, w, T, F(x, NSE_U_TA), F(x, NSE_V_TA),
                     F(x, NSE_W_TA), F(x, NSE_U_PRE), F(x, NSE_V_PRE), F(x, NSE_W_PRE),
-                    F(x, NSE_T_PRE), c1, ua, va, wa, uT, s);
+                    F(x, NSE_T_PRE), c1, ua, va, wa, uT, s, x->rhs_shape);
   // :397 solve_u_temp: per component y, z, x line solves
   // (timed per direction: all y solves, then z, then x of the three fields;
   // the fields are independent, so this order gives the same values as
@@ -2549,11 +2630,12 @@ int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
   return NSE_OK;
 }
 
-int nse_ctx_line_shapes(nse_ctx* x, int* yz, int* xnl) {
-  if (!x || !yz || !xnl) return NSE_ERR_ARG;
+int nse_ctx_launch_shapes(nse_ctx* x, int* out) {
+  if (!x || !out) return NSE_ERR_ARG;
   for (int dir = 1; dir <= 2; ++dir)
-    for (int comp = 0; comp < 4; ++comp) yz[(dir - 1) * 4 + comp] = x->yzshape[dir][comp];
-  for (int comp = 0; comp < 4; ++comp) xnl[comp] = x->xnl[comp] ? x->xnl[comp] : 2;
+    for (int comp = 0; comp < 4; ++comp) out[(dir - 1) * 4 + comp] = x->yzshape[dir][comp];
+  for (int comp = 0; comp < 4; ++comp) out[8 + comp] = x->xnl[comp] ? x->xnl[comp] : 2;
+  out[12] = x->rhs_shape;
   return NSE_OK;
 }
 

@@ -77,7 +77,7 @@ def _sig():
     L.nse_levelset.argtypes = [vp, vp, vp, C.c_int, C.c_double, C.c_double]
     L.nse_ctx_grid.argtypes = [vp] + [vp] * 12
     L.nse_ctx_profile.argtypes = [vp, C.c_int]
-    L.nse_ctx_line_shapes.argtypes = [vp, vp, vp]
+    L.nse_ctx_launch_shapes.argtypes = [vp, vp]
     L.nse_ctx_phase_times.argtypes = [vp, vp, C.c_int, vp]
     L.nse_launch_count.restype = C.c_longlong
     L.nse_ensemble_create.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp)]
@@ -187,13 +187,13 @@ class Context:
         check(self.L.nse_sync(self.h))
 
     def line_shapes(self):
-        """Launch shapes the autotuner chose for the line passes (after the first
-        step): {"y": [u, v, w, T], "z": [...], "x": [...]}; y/z codes 0 = 16 lines
-        per CTA, 1 = 8, 3 = 32, 2 = TMA tiles; x = lines per warp iteration."""
-        yz = (C.c_int * 8)()
-        xn = (C.c_int * 4)()
-        check(self.L.nse_ctx_line_shapes(self.h, yz, xn))
-        return {"y": list(yz[:4]), "z": list(yz[4:]), "x": list(xn)}
+        """Launch shapes the autotuner chose (after the first step): {"y": [u, v,
+        w, T], "z": [...], "x": [...], "rhs": shape}; y/z codes 0 = 16 lines per
+        CTA, 1 = 8, 3 = 32, 2 = TMA tiles; x = lines per warp iteration; rhs 0-3
+        (nsegpu.h, nse_ctx_launch_shapes)."""
+        o = (C.c_int * 13)()
+        check(self.L.nse_ctx_launch_shapes(self.h, o))
+        return {"y": list(o[:4]), "z": list(o[4:8]), "x": list(o[8:12]), "rhs": o[12]}
 
     def levelset(self, phi0, nnn=2000, dtau=1.0e-3, width=1.0, want_phi=True):
         a = np.asfortranarray(phi0, dtype=np.float64)
