@@ -350,12 +350,13 @@ int nse_ctx_read_field(nse_ctx* ctx, const char* path);
 int nse_monitor(nse_ctx* ctx, double out[6]);
 int nse_sync(nse_ctx* ctx);
 /* Launch shapes the autotuner chose (set before the context's first step;
- * no counterpart in the reference), out[13]: out[(dir-1)*4 + comp] for the y
+ * no counterpart in the reference), out[14]: out[(dir-1)*4 + comp] for the y
  * (dir 1) and z (dir 2) line passes of u, v, w, T (0 = 16 lines per CTA, 1 =
  * 8, 3 = 32, 2 = TMA tiles of 16 lines), out[8 + comp] the x lines per warp
  * iteration, out[12] the right-hand-side kernel's shape (0 = 32x4 tiles with a
  * 5-plane ring in FP64 / 32x8 in FP32, 1 = 32x4 with 4 planes, 2 = 32x8 with
- * 5, 3 = 32x8 with 4). */
+ * 5, 3 = 32x8 with 4), out[13] the pipelined correction's shape (0 = the
+ * default, 1 = 32x8 tiles with 5 planes, 2 = 32x4 with 4, 3 = 32x8 with 4). */
 int nse_ctx_launch_shapes(nse_ctx* ctx, int* out);
 /* Per-phase timing of the next max_steps steps with CUDA events on the
  * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the

@@ -285,7 +285,8 @@ void launch_correct_fast(const Dims& d, const GridRcp& rg, const double* PHI, co
 void launch_correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const double* ut,
                          const double* vt, const double* wt, double* p, double* u, double* v,
                          double* w, double* u_ta, double* v_ta, double* w_ta, double* u_ep2,
-                         double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s);
+                         double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s,
+                         int shape = 0);
 
 // level set (set_levelset.f)
 void launch_levelset_iter(const Dims& d, const GridDev& g, const double* phi0,

@@ -575,21 +575,40 @@ __global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ P
   w_ta[c] = (H)(dt * gz);
 }
 
-template <class H>
-static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
-                         const H* vt, const H* wt, double* p, double* u, double* v, double* w,
-                         H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
-                         double dt, cudaStream_t s) {
-  using Sh = CorrShape<H>;
-  constexpr int TY = Sh::TY, NS = Sh::NS;
+template <class H, int TY, int NS, int MINB>
+static void correct_go(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
+                       const H* vt, const H* wt, double* p, double* u, double* v, double* w,
+                       H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
+                       double dt, cudaStream_t s) {
   dim3 block(TXW, TY, 1);
   dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + CKCHUNK - 1) / CKCHUNK);
   size_t smem = (size_t)NS * cslot_bytes<H, TY>();
-  auto kern = k_correct_pipe<H, TY, NS, Sh::MINB>;
+  auto kern = k_correct_pipe<H, TY, NS, MINB>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   kern<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,
                                  v_ep2, w_ep2, divu, dt);
+}
+
+// launch shape: 0 the storage type's default (CorrShape), 1 32x8 tiles with a
+// 5-plane ring and two CTAs per SM, 2 32x4 tiles with 4 planes and four CTAs,
+// 3 32x8 tiles with 4 planes and three CTAs (each cell computed the same way)
+template <class H>
+static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
+                         const H* vt, const H* wt, double* p, double* u, double* v, double* w,
+                         H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
+                         double dt, cudaStream_t s, int shape) {
+  using Sh = CorrShape<H>;
+#define NSE_CORR_GO(TY_, NS_, MB_)                                                           \
+  correct_go<H, TY_, NS_, MB_>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,  \
+                               v_ep2, w_ep2, divu, dt, s)
+  switch (shape) {
+    case 1: NSE_CORR_GO(8, 5, 2); break;
+    case 2: NSE_CORR_GO(4, 4, 4); break;
+    case 3: NSE_CORR_GO(8, 4, 3); break;
+    default: NSE_CORR_GO(Sh::TY, Sh::NS, Sh::MINB); break;
+  }
+#undef NSE_CORR_GO
   long nf = (long)(d.ny + 1) * (d.nz + 1) + (long)d.nx * (d.nz + 1) + (long)d.nx * d.ny;
   count_launch();
   k_correct_faces<H><<<(unsigned)((nf + 255) / 256), 256, 0, s>>>(d, rg, PHI, ut, vt, wt, u, v,
@@ -599,17 +618,19 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
 void launch_correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const double* ut,
                          const double* vt, const double* wt, double* p, double* u, double* v,
                          double* w, double* u_ta, double* v_ta, double* w_ta, double* u_ep2,
-                         double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s) {
+                         double* v_ep2, double* w_ep2, double* divu, double dt, cudaStream_t s,
+                         int shape) {
   correct_pipe<double>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2, v_ep2,
-                       w_ep2, divu, dt, s);
+                       w_ep2, divu, dt, s, shape);
 }
 
 void launch_correct_f32(const Dims& d, const GridRcp& rg, const double* PHI, const float* ut,
                         const float* vt, const float* wt, double* p, double* u, double* v,
                         double* w, float* u_ta, float* v_ta, float* w_ta, float* u_ep2,
-                        float* v_ep2, float* w_ep2, float* divu, double dt, cudaStream_t s) {
+                        float* v_ep2, float* w_ep2, float* divu, double dt, cudaStream_t s,
+                        int shape) {
   correct_pipe<float>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2, v_ep2, w_ep2,
-                      divu, dt, s);
+                      divu, dt, s, shape);
 }
 
 }  // namespace nse

@@ -64,7 +64,8 @@ void launch_rhs_f32(const Dims& d, const GridDev& g, const GridRcp& rg, const St
 void launch_correct_f32(const Dims& d, const GridRcp& rg, const double* PHI, const float* ut,
                         const float* vt, const float* wt, double* p, double* u, double* v,
                         double* w, float* u_ta, float* v_ta, float* w_ta, float* u_ep2,
-                        float* v_ep2, float* w_ep2, float* divu, double dt, cudaStream_t s);
+                        float* v_ep2, float* w_ep2, float* divu, double dt, cudaStream_t s,
+                        int shape = 0);
 void launch_set_bc_f32(const Dims& d, float* u, float* v, float* w, double* p, double* T,
                        double tbot, double ttop, int which, cudaStream_t s);
 void launch_fft_fwd_x_f32(const PoissonPlan& pp, const Dims& d, const GridDev& g,
@@ -1351,6 +1352,10 @@ void readgrid3d_(const int* nx, const int* ny, const int* nz, double* phi0) {
 }  // extern "C"
 
 // ============================================================ tier 3 =======
+// launch-shape choices of the autotuner, per grid and form, for the process
+static std::mutex g_tune_mu;
+static std::map<std::string, int> g_tune;
+
 struct nse_ctx {
   nse_config cfg;
   Dims d;
@@ -1404,6 +1409,9 @@ struct nse_ctx {
   // launch shape of the fast right-hand-side kernel (autotune_rhs)
   int rhs_shape = 0;
   bool rhs_tuned = false;
+  // launch shape of the pipelined correction (autotune_correct)
+  int corr_shape = 0;
+  bool corr_tuned = false;
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1862,6 +1870,79 @@ static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
   launch_phibc(d, phi, s);
 }
 
+// The pipelined correction's launch shapes, timed inside the first step's
+// MKP with the solved phi: the kernel reads the old u_ta and writes the new
+// one in place, so the timing runs read and write scratch copies of u_ta (its
+// other outputs are rewritten by the step's own correction right after).
+extern "C++" {
+template <class H>
+static void autotune_correct(nse_ctx* x, const H* ut, const H* vt, const H* wt) {
+  if (x->corr_tuned) return;
+  if (x->cfg.flags & (NSE_FLAG_NO_AUTOTUNE | NSE_FLAG_EXACT)) {
+    x->corr_tuned = true;
+    return;
+  }
+  cudaStream_t s = x->stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  const Dims& d = x->d;
+  char key[96];
+  snprintf(key, sizeof(key), "corr %d %d %d %d", d.nx, d.ny, d.nz, x->mixed ? 1 : 0);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      x->corr_shape = it->second;
+      x->corr_tuned = true;
+      return;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  const size_t hb = d.ntot * sizeof(H);
+  H* ta[3] = {x->sa.as<H>(), x->sb.as<H>(), x->tmp.as<H>()};
+  const int tid[3] = {NSE_U_TA, NSE_V_TA, NSE_W_TA};
+  for (int q = 0; q < 3; ++q)
+    cudaMemcpyAsync(ta[q], x->f[tid[q]].p, hb, cudaMemcpyDeviceToDevice, s);
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int shape = 0; shape < 4; ++shape) {
+    auto run = [&]() {
+      if constexpr (sizeof(H) == 4)
+        launch_correct_f32(d, x->rg, F(x, NSE_PHI), ut, vt, wt, F(x, NSE_P), F(x, NSE_U),
+                           F(x, NSE_V), F(x, NSE_W), ta[0], ta[1], ta[2], F32(x, NSE_U_EP2),
+                           F32(x, NSE_V_EP2), F32(x, NSE_W_EP2), F32(x, NSE_DIVU), x->cfg.dt, s,
+                           shape);
+      else
+        launch_correct_pipe(d, x->rg, F(x, NSE_PHI), ut, vt, wt, F(x, NSE_P), F(x, NSE_U),
+                            F(x, NSE_V), F(x, NSE_W), ta[0], ta[1], ta[2], F(x, NSE_U_EP2),
+                            F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU), x->cfg.dt, s,
+                            shape);
+    };
+    run();
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r) run();
+    cudaEventRecord(e1, s);
+    float ms = 1e30f;
+    if (cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = shape;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  x->corr_shape = best;
+  x->corr_tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+}
+}  // extern "C++"
+
 // MKP in the mixed-precision form: FP32 u*, v*, w*; the FP64 solve of their
 // FP64 divergence (or, with NSE_FLAG_POISSON32, the FP32 spectral solve with
 // FP64 residual refinement); FP64 correction of the FP64 state
@@ -1907,11 +1988,12 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
     launch_fft_inv_x_f32(pp, d, phi, true, s);
     launch_phibc(d, phi, s);
   }
+  if (!x->rec) autotune_correct<float>(x, ut, vt, wt);
   mark(x, PH_CORRECT);
   launch_correct_f32(d, x->rg, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V),
                      F(x, NSE_W), F32(x, NSE_U_TA), F32(x, NSE_V_TA), F32(x, NSE_W_TA),
                      F32(x, NSE_U_EP2), F32(x, NSE_V_EP2), F32(x, NSE_W_EP2), F32(x, NSE_DIVU),
-                     dt, s);
+                     dt, s, x->corr_shape);
   mark(x, PH_COUNT);
 }
 
@@ -1953,11 +2035,13 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
     launch_correct(d, x->g, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V), F(x, NSE_W),
                    F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA), F(x, NSE_U_EP2),
                    F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU), x->cfg.dt, s);
-  else
+  else {
+    if (!x->rec) autotune_correct<double>(x, ut, vt, wt);
     launch_correct_pipe(d, x->rg, phi, ut, vt, wt, F(x, NSE_P), F(x, NSE_U), F(x, NSE_V),
                         F(x, NSE_W), F(x, NSE_U_TA), F(x, NSE_V_TA), F(x, NSE_W_TA),
                         F(x, NSE_U_EP2), F(x, NSE_V_EP2), F(x, NSE_W_EP2), F(x, NSE_DIVU),
-                        x->cfg.dt, s);
+                        x->cfg.dt, s, x->corr_shape);
+  }
   mark(x, PH_COUNT);
 }
 
@@ -2007,8 +2091,6 @@ int nse_poisson(nse_ctx* x) {
 // ensemble that share a grid are timed once.  NSE_FLAG_NO_AUTOTUNE keeps
 // the fixed shapes (16 lines per CTA, two x lines per warp iteration);
 // NSE_FLAG_LINES_TMA sets the TMA tiles for every FP64 y/z pass.
-static std::mutex g_tune_mu;
-static std::map<std::string, int> g_tune;
 
 static int x_nl_candidates(const nse_ctx* x) { return x_rows_per_lane(x->d.nx) <= 8 ? 2 : 1; }
 
@@ -2636,6 +2718,7 @@ int nse_ctx_launch_shapes(nse_ctx* x, int* out) {
     for (int comp = 0; comp < 4; ++comp) out[(dir - 1) * 4 + comp] = x->yzshape[dir][comp];
   for (int comp = 0; comp < 4; ++comp) out[8 + comp] = x->xnl[comp] ? x->xnl[comp] : 2;
   out[12] = x->rhs_shape;
+  out[13] = x->corr_shape;
   return NSE_OK;
 }
 
