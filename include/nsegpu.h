@@ -291,9 +291,12 @@ enum {
                                 CTAs, next tile in flight while one is solved) */
   NSE_FLAG_NO_AUTOTUNE = 2048, /* keep the fixed line launch shapes instead of timing the
                                 candidates before the first step (same values either way) */
-  NSE_FLAG_SPN_TMA = 4096    /* FP64 spectral tridiagonal solve (SPN + SP0B) through TMA
+  NSE_FLAG_SPN_TMA = 4096,   /* FP64 spectral tridiagonal solve (SPN + SP0B) through TMA
                                 tiles of 16 kx columns, partitioned over 16 warps
                                 (ny = 16 m), instead of the two-ended solver */
+  NSE_FLAG_MID_SLICES = 8192 /* FP64 five-launch solve with NZ = 256: run the z
+                                transforms and the SPN in 3 kx slices without timing the
+                                slice counts (same values either way) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */
@@ -350,13 +353,15 @@ int nse_ctx_read_field(nse_ctx* ctx, const char* path);
 int nse_monitor(nse_ctx* ctx, double out[6]);
 int nse_sync(nse_ctx* ctx);
 /* Launch shapes the autotuner chose (set before the context's first step;
- * no counterpart in the reference), out[14]: out[(dir-1)*4 + comp] for the y
+ * no counterpart in the reference), out[15]: out[(dir-1)*4 + comp] for the y
  * (dir 1) and z (dir 2) line passes of u, v, w, T (0 = 16 lines per CTA, 1 =
  * 8, 3 = 32, 2 = TMA tiles of 16 lines), out[8 + comp] the x lines per warp
  * iteration, out[12] the right-hand-side kernel's shape (0 = 32x4 tiles with a
  * 5-plane ring in FP64 / 32x8 in FP32, 1 = 32x4 with 4 planes, 2 = 32x8 with
  * 5, 3 = 32x8 with 4), out[13] the pipelined correction's shape (0 = the
- * default, 1 = 32x8 tiles with 5 planes, 2 = 32x4 with 4, 3 = 32x8 with 4). */
+ * default, 1 = 32x8 tiles with 5 planes, 2 = 32x4 with 4, 3 = 32x8 with 4),
+ * out[14] the kx slices the FP64 solve's z transforms and SPN run in (1 =
+ * unsliced). */
 int nse_ctx_launch_shapes(nse_ctx* ctx, int* out);
 /* Per-phase timing of the next max_steps steps with CUDA events on the
  * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the

@@ -230,3 +230,52 @@ def test_tma_tile_spn_matches_default_and_oracle(n):
             assert ctx.monitor()["max_divu"] < 1e-10
     for k in res[0]:
         assert rel_l2(res[0][k], res[1][k]) < 1e-10, k
+
+
+@pytest.mark.parametrize("n", [(256, 192, 256), (64, 48, 256)])
+def test_sliced_middle_passes_are_bit_identical(n):
+    """The z transforms and SPN in kx slices (NSE_FLAG_MID_SLICES: 3 slices,
+    each slice's three passes back to back) give the same bits as the
+    unsliced passes (NSE_FLAG_NO_AUTOTUNE), in the solve on the seeded
+    right-hand side and through 2 penalised steps, FP64 and mixed; the
+    autotuned default agrees too and reports a slice count."""
+    nx, ny, nz = n
+    g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
+    rhs = W.poisson_rhs(g, seed=nx + 7)
+    out = []
+    for flags in (S.FLAG_NO_AUTOTUNE, S.FLAG_MID_SLICES, 0):
+        cfg = S.Config(nx, ny, nz, 1.0, 1.0, 1.0, 0.0, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                       ystretch=2.0, flags=flags)
+        with S.Context(cfg) as ctx:
+            ctx.upload("phi", rhs)
+            ctx.poisson()
+            ctx.sync()
+            out.append(ctx.download("phi"))
+            if flags == S.FLAG_MID_SLICES:
+                assert ctx.line_shapes()["mid"] == 3
+            if flags == 0:
+                assert ctx.line_shapes()["mid"] in (1, 2, 3, 5, 9)
+    assert np.array_equal(out[0], out[1])
+    assert np.array_equal(out[0], out[2])
+    ref, _, _ = oracle_poisson(g, rhs)
+    I = (slice(1, nx + 1), slice(1, ny + 1), slice(1, nz + 1))
+    assert rel_l2(out[1][I], ref[I]) < 1e-12
+    gg, f, dt = channel(*n, seed=9, t_bot=1.0, t_top=0.0)
+    c1 = W.smoothed_mask(gg, W.sphere_phi0(gg, (math.pi, 0.0, math.pi / 2), 0.25), 1.5)
+    for prec in (S.FP64, S.MIXED):
+        res = []
+        for flags in (S.FLAG_NO_AUTOTUNE, S.FLAG_MID_SLICES | S.FLAG_NO_AUTOTUNE):
+            cfg = S.Config(nx, ny, nz, dt, 3000.0, 0.71, 1.0e4, gg["xl"], gg["yl"], gg["zl"],
+                           y0=-1.0, ystretch=2.0, body_force=1e-3, heat_source=0.0,
+                           t_bot=1.0, t_solid=1.0, precision=prec, flags=flags)
+            with S.Context(cfg) as ctx:
+                for k in ("u", "v", "w", "T"):
+                    ctx.upload(k, f[k])
+                ctx.upload("cellvalue", c1)
+                ctx.project()
+                ctx.start()
+                ctx.step(2)
+                ctx.sync()
+                res.append({k: ctx.download(k) for k in ("u", "v", "w", "p", "T")})
+        for k in res[0]:
+            assert np.array_equal(res[0][k], res[1][k]), (prec, k)

@@ -246,6 +246,8 @@ void launch_spn(const PoissonPlan& pp, bool do_spn, bool do_sp0b, cudaStream_t s
 int spn_split(const PoissonPlan& pp);
 void launch_spn_tables(const PoissonPlan& pp, double* im, cudaStream_t s);
 void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s);
+int poisson_mid_groups(const PoissonPlan& pp);
+void launch_poisson_mid(const PoissonPlan& pp, int nchunk, cudaStream_t s);
 bool launch_spn_transposed(const PoissonPlan& pp, const double* rdy, const double* dy,
                            cudaStream_t s);
 

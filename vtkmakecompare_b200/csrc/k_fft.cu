@@ -421,19 +421,20 @@ __global__ void __launch_bounds__(128) k_fft256_inv_x(Dims d, SpecViewT<CT> sv, 
   }
 }
 
-// z pass, N = 256: a CTA transforms 16 adjacent kx columns of one plane;
-// thread (col, b) holds x[16a + b] of its column (loads coalesced over col)
+// z pass, N = 256: a CTA transforms 16 adjacent kx columns of one plane
+// (column group g0 + blockIdx.x); thread (col, b) holds x[16a + b] of its
+// column (loads coalesced over col)
 template <class CT>
 __global__ void __launch_bounds__(256) k_fft256_z(int H, SpecViewT<CT> sv,
                                                   const CT* __restrict__ tw, int inv,
-                                                  double nrm) {
+                                                  double nrm, int g0) {
   using RT = typename CReal<CT>::T;
   constexpr int FS = 17;
   extern __shared__ __align__(16) char fsm[];
   CT* S_ = reinterpret_cast<CT*>(fsm);  // [c][b][col], col stride 1, b stride 17
   const int col = threadIdx.x & 15, b = threadIdx.x >> 4;
   const int jj = sv.j0 + blockIdx.y;
-  const int kx = blockIdx.x * 16 + col;
+  const int kx = (g0 + blockIdx.x) * 16 + col;
   const bool ok = kx < H;
   CT* base = sv.base + kx + sv.sj * jj;
   CT v[16];
@@ -675,7 +676,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
                                                  const double* __restrict__ im, long tj,
                                                  long tk, const double* __restrict__ AC,
                                                  const double* __restrict__ pre,
-                                                 const double* __restrict__ post) {
+                                                 const double* __restrict__ post, int g0) {
   extern __shared__ __align__(16) unsigned char spn_sm[];
   const int rmax = ny - m;  // rows of the longer (bottom) half
   RT* vs = reinterpret_cast<RT*>(spn_sm);                                  // [rmax][64]
@@ -688,7 +689,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
   }
   __syncthreads();
   const int comp = lt & 1, part = (lt >> 1) & 1, hs = lt >> 1;
-  const int kx = blockIdx.x * 16 + (lt >> 2);
+  const int kx = (g0 + blockIdx.x) * 16 + (lt >> 2);
   const int kz = blockIdx.y;
   const bool mean = (kx == 0 && kz == 0);
   const bool valid = kx < H && !mean;
@@ -914,18 +915,22 @@ void launch_div_src32(const Dims& d, const GridRcp& rg, const float* ut, const f
   div_src<float>(d, rg, ut, vt, wt, dt, out, s);
 }
 
+// g0, ng: the groups of 16 kx columns to transform (ng = 0: all; only the
+// NZ = 256 kernel takes a subset)
 template <class CT>
-static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 0, int nj = 0) {
+static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 0, int nj = 0,
+                  int g0 = 0, int ng = 0) {
   if (nj <= 0) { j0 = 0; nj = pp.ny; }
   SpecViewT<CT> sv = spec_internal_t<CT>(pp);
   sv.j0 = j0;
   if (pp.nz == 256) {
-    dim3 grid((pp.H + 15) / 16, nj);
+    if (ng <= 0) { g0 = 0; ng = (pp.H + 15) / 16; }
+    dim3 grid(ng, nj);
     size_t sm = 16 * 16 * 17 * sizeof(CT);
     smem_optin((const void*)k_fft256_z<CT>, sm);
     count_launch();
     k_fft256_z<CT><<<grid, 256, sm, s>>>(pp.H, sv, twz_of<CT>(pp), inverse ? 1 : 0,
-                                         (double)pp.nx * (double)pp.nz);
+                                         (double)pp.nx * (double)pp.nz, g0);
     return;
   }
   FFTShape sh = make_shape(pp.nz);
@@ -965,16 +970,18 @@ static size_t spn_smem(int ny, int m) {
          2 * (size_t)ny * sizeof(double);
 }
 
+// g0, ng: the groups of 16 kx columns to solve (ng = 0: all)
 template <class RT>
-static void spn_babe(const PoissonPlan& pp, RT* spec, cudaStream_t s) {
+static void spn_babe(const PoissonPlan& pp, RT* spec, cudaStream_t s, int g0 = 0, int ng = 0) {
   const int m = spn_split(pp);
   const size_t sm = spn_smem(pp.ny, m);
   smem_optin((const void*)k_spn_babe<RT>, sm);
-  dim3 grid((pp.H + 15) / 16, pp.nz);
+  if (ng <= 0) { g0 = 0; ng = (pp.H + 15) / 16; }
+  dim3 grid(ng, pp.nz);
   count_launch();
   k_spn_babe<RT><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, spec, pp.Hp, (long)pp.Hp * pp.ny,
                                       pp.spn_im, pp.Hp, (long)pp.Hp * pp.ny, pp.AC, nullptr,
-                                      nullptr);
+                                      nullptr, g0);
 }
 
 // transposed SPN + SP0B (the discrete adjoint) on the FP64 spectrum: rdy, dy
@@ -990,7 +997,7 @@ bool launch_spn_transposed(const PoissonPlan& pp, const double* rdy, const doubl
   count_launch();
   k_spn_babe<double><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, pp.spec, pp.Hp,
                                           (long)pp.Hp * pp.ny, pp.spn_im, pp.Hp,
-                                          (long)pp.Hp * pp.ny, pp.AC, rdy, dy);
+                                          (long)pp.Hp * pp.ny, pp.AC, rdy, dy, 0);
   return true;
 }
 
@@ -1002,6 +1009,33 @@ void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s) {
     return;
   }
   spn_babe<double>(pp, pp.spec, s);
+}
+
+// The z transforms and the SPN between them, in nchunk slices of the kx
+// column groups: z forward, SPN and z inverse of one slice run back to back,
+// so the slice's spectrum (107 MB / nchunk at 256x192x256) is re-read from
+// L2 instead of HBM by the second and third pass.  Every column sees the
+// same operations as in the unsliced order (the passes act on disjoint
+// columns), so the result is bit-identical.  Slicing needs the N = 256 z
+// kernel and the tabulated SPN; otherwise the three passes run whole.
+int poisson_mid_groups(const PoissonPlan& pp) {
+  return (pp.nz == 256 && pp.spn_im) ? (pp.H + 15) / 16 : 0;
+}
+void launch_poisson_mid(const PoissonPlan& pp, int nchunk, cudaStream_t s) {
+  const int G = poisson_mid_groups(pp);
+  if (G == 0 || nchunk <= 1) {
+    fft_z<double2>(pp, false, s);
+    launch_spn_fast(pp, s);
+    fft_z<double2>(pp, true, s);
+    return;
+  }
+  if (nchunk > G) nchunk = G;
+  for (int c = 0; c < nchunk; ++c) {
+    const int ga = (int)((long)c * G / nchunk), gb = (int)((long)(c + 1) * G / nchunk);
+    fft_z<double2>(pp, false, s, 0, 0, ga, gb - ga);
+    spn_babe<double>(pp, pp.spec, s, ga, gb - ga);
+    fft_z<double2>(pp, true, s, 0, 0, ga, gb - ga);
+  }
 }
 
 void launch_spn_f32(const PoissonPlan& pp, cudaStream_t s);

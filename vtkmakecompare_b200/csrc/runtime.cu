@@ -1412,6 +1412,9 @@ struct nse_ctx {
   // launch shape of the pipelined correction (autotune_correct)
   int corr_shape = 0;
   bool corr_tuned = false;
+  // kx slices of the z transforms and SPN of the FP64 solve (autotune_mid)
+  int mid_chunks = 1;
+  bool mid_tuned = false;
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1840,6 +1843,90 @@ static void ctx_spn(nse_ctx* x, bool part) {
   else launch_spn_fast(pp, x->stream);
 }
 
+// z forward -> SPN/SP0B -> z inverse of the FP64 five-pass solve, phase-
+// marked; in kx slices (launch_poisson_mid) when the autotuner chose them,
+// all three passes then counted as the SPN phase
+static void ctx_poisson_mid(nse_ctx* x, bool part) {
+  const PoissonPlan& pp = x->pb.pp;
+  cudaStream_t s = x->stream;
+  if (x->mid_chunks > 1 && !part && !(x->cfg.flags & NSE_FLAG_SPN_TMA)) {
+    mark(x, PH_FFTZ_F);
+    mark(x, PH_SPN);
+    launch_poisson_mid(pp, x->mid_chunks, s);
+    mark(x, PH_FFTZ_I);
+    return;
+  }
+  mark(x, PH_FFTZ_F);
+  launch_fft_z(pp, false, s);
+  mark(x, PH_SPN);
+  ctx_spn(x, part);
+  mark(x, PH_FFTZ_I);
+  launch_fft_z(pp, true, s);
+}
+
+// The number of kx slices of the middle passes, timed before the first FP64
+// solve of a context while the spectrum holds nothing the solve needs (the
+// forward x pass overwrites all of it next): the candidates run the three
+// passes on whatever the spectrum holds, which costs the same time as on a
+// real spectrum and changes no state.
+static void autotune_mid(nse_ctx* x) {
+  if (x->mid_tuned) return;
+  const PoissonPlan& pp = x->pb.pp;
+  const int G = poisson_mid_groups(pp);
+  if (G < 2 || (x->cfg.flags & (NSE_FLAG_EXACT | NSE_FLAG_SPN_TMA))) {
+    x->mid_tuned = true;
+    return;
+  }
+  if (x->cfg.flags & (NSE_FLAG_MID_SLICES | NSE_FLAG_NO_AUTOTUNE)) {
+    x->mid_chunks = (x->cfg.flags & NSE_FLAG_MID_SLICES) ? (G < 3 ? G : 3) : 1;
+    x->mid_tuned = true;
+    return;
+  }
+  cudaStream_t s = x->stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  char key[96];
+  snprintf(key, sizeof(key), "mid %d %d %d", x->d.nx, x->d.ny, x->d.nz);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      x->mid_chunks = it->second;
+      x->mid_tuned = true;
+      return;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  int best = 1;
+  float best_ms = 1e30f;
+  const int cand[5] = {1, 2, 3, 5, 9};
+  for (int ci = 0; ci < 5; ++ci) {
+    const int nc = cand[ci];
+    if (nc > G) break;
+    launch_poisson_mid(pp, nc, s);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r) launch_poisson_mid(pp, nc, s);
+    cudaEventRecord(e1, s);
+    float ms = 1e30f;
+    if (cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = nc;
+    }
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  x->mid_chunks = best;
+  x->mid_tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+}
+
 // P2S -> SPN/SP0B -> S2P -> PHIBC on phi (FP64), phase-marked
 static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
   const Dims& d = x->d;
@@ -1857,13 +1944,9 @@ static void ctx_poisson64(nse_ctx* x, double* phi, bool div_marked) {
     mark(x, PH_PHIBC);
     return;
   }
+  if (!div_marked) autotune_mid(x);
   launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
-  mark(x, PH_FFTZ_F);
-  launch_fft_z(pp, false, s);
-  mark(x, PH_SPN);
-  ctx_spn(x, false);
-  mark(x, PH_FFTZ_I);
-  launch_fft_z(pp, true, s);
+  ctx_poisson_mid(x, false);
   mark(x, PH_FFTX_I);
   launch_fft_inv_x(pp, d, phi, s);
   mark(x, PH_PHIBC);
@@ -1958,21 +2041,23 @@ static void ctx_mkp_f32(nse_ctx* x, const float* ut, const float* vt, const floa
     launch_div_src32(d, x->rg, ut, vt, wt, dt, phi, s);
     ctx_poisson64(x, phi, true);
   } else if (p64) {
+    autotune_mid(x);
     launch_div_src32(d, x->rg, ut, vt, wt, dt, phi, s);
     launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
   } else {
     launch_fft_fwd_x_f32(pp, d, x->g, x->rg, ut, vt, wt, dt, nullptr, dx, dz, 1, s);
   }
   if (!(p64 && poisson3(x))) {
-    mark(x, PH_FFTZ_F);
-    if (p64) launch_fft_z(pp, false, s);
-    else launch_fft_z_f32(pp, false, s);
-    mark(x, PH_SPN);
-    if (p64) ctx_spn(x, false);
-    else launch_spn_fast_f32(pp, s);
-    mark(x, PH_FFTZ_I);
-    if (p64) launch_fft_z(pp, true, s);
-    else launch_fft_z_f32(pp, true, s);
+    if (p64) {
+      ctx_poisson_mid(x, false);
+    } else {
+      mark(x, PH_FFTZ_F);
+      launch_fft_z_f32(pp, false, s);
+      mark(x, PH_SPN);
+      launch_spn_fast_f32(pp, s);
+      mark(x, PH_FFTZ_I);
+      launch_fft_z_f32(pp, true, s);
+    }
     mark(x, PH_FFTX_I);
     if (p64) launch_fft_inv_x(pp, d, phi, s);
     else launch_fft_inv_x_f32(pp, d, phi, false, s);
@@ -2010,6 +2095,7 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
     launch_div_src(d, *rg, ut, vt, wt, x->cfg.dt, phi, s);
     ctx_poisson64(x, phi, true);
   } else if (rg) {
+    autotune_mid(x);
     // phi is free until the inverse x pass: it holds the divergence samples
     launch_div_src(d, *rg, ut, vt, wt, x->cfg.dt, phi, s);
     launch_fft_fwd_x(pp, d, phi, nullptr, nullptr, nullptr, x->g, 1.0, 0, s);
@@ -2017,13 +2103,16 @@ static void ctx_mkp(nse_ctx* x, const double* ut, const double* vt, const double
     launch_fft_fwd_x(pp, d, nullptr, ut, vt, wt, x->g, x->cfg.dt, 1, s, rg);
   }
   if (!(rg && poisson3(x))) {
-    mark(x, PH_FFTZ_F);
-    launch_fft_z(pp, false, s);
-    mark(x, PH_SPN);
-    if (rg) ctx_spn(x, false);
-    else launch_spn_fast(pp, s);
-    mark(x, PH_FFTZ_I);
-    launch_fft_z(pp, true, s);
+    if (rg) {
+      ctx_poisson_mid(x, false);
+    } else {
+      mark(x, PH_FFTZ_F);
+      launch_fft_z(pp, false, s);
+      mark(x, PH_SPN);
+      launch_spn_fast(pp, s);
+      mark(x, PH_FFTZ_I);
+      launch_fft_z(pp, true, s);
+    }
     mark(x, PH_FFTX_I);
     launch_fft_inv_x(pp, d, phi, s);
     mark(x, PH_PHIBC);
@@ -2719,6 +2808,7 @@ int nse_ctx_launch_shapes(nse_ctx* x, int* out) {
   for (int comp = 0; comp < 4; ++comp) out[8 + comp] = x->xnl[comp] ? x->xnl[comp] : 2;
   out[12] = x->rhs_shape;
   out[13] = x->corr_shape;
+  out[14] = x->mid_chunks;
   return NSE_OK;
 }
 

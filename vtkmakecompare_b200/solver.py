@@ -29,6 +29,7 @@ FLAG_POISSON32 = 512
 FLAG_LINES_TMA = 1024
 FLAG_NO_AUTOTUNE = 2048
 FLAG_SPN_TMA = 4096
+FLAG_MID_SLICES = 8192
 
 
 class Config(C.Structure):
@@ -188,13 +189,14 @@ class Context:
 
     def line_shapes(self):
         """Launch shapes the autotuner chose (after the first step): {"y": [u, v,
-        w, T], "z": [...], "x": [...], "rhs": shape, "correct": shape}; y/z codes 0 = 16 lines per
-        CTA, 1 = 8, 3 = 32, 2 = TMA tiles; x = lines per warp iteration; rhs 0-3
-        (nsegpu.h, nse_ctx_launch_shapes)."""
-        o = (C.c_int * 14)()
+        w, T], "z": [...], "x": [...], "rhs": shape, "correct": shape, "mid": slices};
+        y/z codes 0 = 16 lines per CTA, 1 = 8, 3 = 32, 2 = TMA tiles; x = lines per
+        warp iteration; rhs, correct 0-3; mid = kx slices of the FP64 solve's z
+        transforms and SPN (nsegpu.h, nse_ctx_launch_shapes)."""
+        o = (C.c_int * 15)()
         check(self.L.nse_ctx_launch_shapes(self.h, o))
         return {"y": list(o[:4]), "z": list(o[4:8]), "x": list(o[8:12]), "rhs": o[12],
-                "correct": o[13]}
+                "correct": o[13], "mid": o[14]}
 
     def levelset(self, phi0, nnn=2000, dtau=1.0e-3, width=1.0, want_phi=True):
         a = np.asfortranarray(phi0, dtype=np.float64)
