@@ -577,6 +577,19 @@ struct YZTab {
   __device__ R pp(int r) const { return __ldg(T + 3 * nu + s + r); }
   __device__ R qq(int r) const { return __ldg(T + 4 * nu + s + r); }
 };
+// the same table through generic loads, for a table that may sit in shared
+// memory (__ldg is a global-memory load: on a shared-memory address it fails
+// with "operation not supported on global/shared address space")
+template <class R>
+struct YZTabAny {
+  const R* T;
+  int nu, s;
+  __device__ R w(int r) const { return T[s + r]; }
+  __device__ R rb(int r) const { return T[nu + s + r]; }
+  __device__ R cc(int r) const { return T[2 * nu + s + r]; }
+  __device__ R pp(int r) const { return T[3 * nu + s + r]; }
+  __device__ R qq(int r) const { return T[4 * nu + s + r]; }
+};
 
 // LPB lines per CTA (adjacent in x; 16 lines keep two CTAs resident per SM).
 // The solution goes to `out` (type RO) when given, else back into f.
@@ -770,7 +783,7 @@ __global__ void __launch_bounds__(16 * P, 2)
       const int slot = slots[lineid];
       if (slot >= 0) T = mtab + (size_t)slot * stride;
     }
-    YZTab<double> tb{T, nu, s};
+    YZTabAny<double> tb{T, nu, s};
     double x[MM];
     const double* col = cur + (size_t)s * LPB + lane;
     const double c0 = (!periodic && k == 0) ? T[5 * nu + 10 * P + 2] * ft : 0.0;
