@@ -281,4 +281,46 @@ def test_line_launch_shapes_give_the_same_fields(n):
         assert rel_l2(out[2][k], out[0][k]) < 1e-13, k
     assert all(v in (0, 1, 2, 3) for v in shapes["y"] + shapes["z"]), shapes
     assert all(v in (1, 2) for v in shapes["x"]), shapes
-    assert shapes["rhs"] in (0, 1, 2, 3), shapes
+    assert shapes["rhs"] in range(7), shapes
+    assert shapes["correct"] in range(7), shapes
+
+
+@pytest.mark.parametrize("n", [(96, 64, 96), (80, 40, 48)])
+def test_rhs_and_correction_shapes_give_the_same_bits(n):
+    """Every launch shape of the right-hand side and of the pipelined
+    correction, the cp.async rings (0-3) and the TMA rings (4-6), gives the
+    same bits after 3 penalised FP64 steps (partial x and y tiles in the
+    80x40x48 case), with no ring wait reported by nse_sync."""
+    g, f, c1, par = make_case(*n)
+    out = []
+    for rhs, corr in ((0, 0), (1, 2), (2, 1), (3, 3), (4, 4), (5, 5), (6, 6)):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"])
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.set_shapes(rhs, corr)
+            ctx.project()
+            ctx.start()
+            ctx.step(3)
+            ctx.sync()
+            sh = ctx.line_shapes()
+            assert (sh["rhs"], sh["correct"]) == (rhs, corr)
+            out.append({k: ctx.download(k) for k in STATE})
+    for o in out[1:]:
+        for k in STATE:
+            assert np.array_equal(o[k], out[0][k]), k
+
+
+def test_set_shapes_rejects_bad_codes():
+    g, f, c1, par = make_case(64, 48, 64)
+    cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                   g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0)
+    with S.Context(cfg) as ctx:
+        with pytest.raises(Exception):
+            ctx.set_shapes(7, 0)
+        with pytest.raises(Exception):
+            ctx.set_shapes(0, -2)

@@ -151,6 +151,9 @@ void launch_rhs_fused(const Dims& d, const GridDev& g, const StepParams& sp,
 
 // same terms in the fast form (reciprocal metrics, FMA, mask-free cells skip
 // the immersed-boundary loads); k_rhs_fast.cu
+// nonzero (and cleared) when a TMA ring wait of the RHS or correction gave up
+// (1) or a launch found its buffers misaligned (2)
+int ring_wait_error();
 void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                      const double* u, const double* v, const double* w, const double* T,
                      const double* u_ta, const double* v_ta, const double* w_ta,

@@ -20,7 +20,10 @@
 // height, ring depth and CTAs per SM are chosen per storage type (RhsShape):
 // the FP64 kernel needs ~150 registers per thread without spilling, so it
 // runs 32 x 4 tiles, three CTAs per SM.
+#include <string.h>
+
 #include "common.cuh"
+#include "tma.cuh"
 
 namespace nse {
 
@@ -108,20 +111,88 @@ __device__ __forceinline__ void load_plane(char* sm, const Dims& d, int i0, int 
   cp_async_commit();
 }
 
+// ------------------------------------------------ TMA ring (FP64 form)
+// The same ring filled by tensor-memory-accelerator copies: one thread issues,
+// per plane, one box copy per field (u, v, w, T: 34 x (TY+2) halo boxes at
+// x = i0-1, which is a multiple of 32 and so 16-byte aligned; c1, whose
+// (nx,ny,nz) layout puts cell I at x = I-1, a 36 x (TY+2) box at c1-x = i0-3;
+// the four histories 34 x TY boxes at x = i0-1) and the plane's mbarrier
+// counts the bytes in.  Boxes reaching past the arrays read zeros, which no
+// valid cell uses.  Fields sit in 128-byte aligned sub-buffers of the slot.
+// Only plain (non-multicast) loads of this GPU's own fields are issued, and
+// every wait is bounded (g_ring_wait_err, read by the host).
+constexpr int ru16(int n) { return (n + 15) & ~15; }  // doubles, rounded to 128 bytes
+struct alignas(64) RhsMaps {
+  CUtensorMap m[9];  // u, v, w, T, c1, u_pre, v_pre, w_pre, T_pre
+};
+struct alignas(64) CorrMaps {
+  CUtensorMap m[7];  // phi, u*, v*, w*, u_ta, v_ta, w_ta
+};
+__device__ int g_ring_wait_err = 0;
+
+// shared-memory layout of one RHS ring slot (in doubles); TMA selects the
+// padded sub-buffers and box pitches of the TMA ring
+template <class H, int TY, bool TMA>
+struct RhsLay {
+  static constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+  static constexpr int FP = TMA ? ru16(PLANE) : PLANE;            // field stride
+  static constexpr int C1W = TMA ? 36 : SXW;                      // c1 row pitch
+  static constexpr int C1P = TMA ? ru16(36 * (TY + 2)) : PLANE;   // c1 buffer
+  static constexpr int HW = TMA ? SXW : TXW;                      // history row pitch
+  static constexpr int HS = TMA ? ru16(SXW * TY) : TILE;          // history stride
+  static constexpr int HOFF = 4 * FP + C1P;                        // first history
+  static constexpr int SLOT = TMA ? (HOFF + 4 * HS) * 8 : slot_bytes<H, TY>();
+  // this thread's cell in the c1 buffer and in a history tile
+  static __device__ __forceinline__ int c1e(int tx, int ty) {
+    return TMA ? (ty + 1) * 36 + tx + 2 : (ty + 1) * SXW + tx + 1;
+  }
+  static __device__ __forceinline__ int he(int tx, int ty) {
+    return TMA ? ty * SXW + tx + 1 : ty * TXW + tx;
+  }
+};
+
+// wait for plane P of the TMA ring (slot and phase counted from plane k0-1)
+template <int NS>
+__device__ __forceinline__ void ring_wait(uint64_t* bars, int P, int k0) {
+  const int r = P - (k0 - 1);
+  if (!tma_wait(&bars[r % NS], (unsigned)((r / NS) & 1)) && threadIdx.x == 0 && threadIdx.y == 0)
+    atomicExch(&g_ring_wait_err, 1);
+}
+
+// plane K of u, v, w, T, c1 and the histories into its slot by TMA (one
+// issuing thread)
+template <int TY, int NS>
+__device__ __forceinline__ void load_plane_tma(char* sm, uint64_t* bars, const RhsMaps& tm,
+                                               int i0, int j0, int K, int k0, int kmax) {
+  using L = RhsLay<double, TY, true>;
+  if (K > kmax) return;
+  const int r = K - (k0 - 1);
+  double* slot = reinterpret_cast<double*>(sm + (r % NS) * L::SLOT);
+  uint64_t* bar = &bars[r % NS];
+  constexpr unsigned HALO = SXW * (TY + 2) * 8, C1B = 36 * (TY + 2) * 8, HB = SXW * TY * 8;
+  mbar_expect_tx(bar, 4 * HALO + C1B + 4 * HB);
+  for (int f = 0; f < 4; ++f) tma_load_3d(slot + f * L::FP, &tm.m[f], i0 - 1, j0 - 1, K, bar);
+  tma_load_3d(slot + 4 * L::FP, &tm.m[4], i0 - 3, j0 - 2, K - 1, bar);
+  for (int f = 0; f < 4; ++f)
+    tma_load_3d(slot + L::HOFF + f * L::HS, &tm.m[5 + f], i0 - 1, j0, K, bar);
+}
+
 // H: storage type of the histories, u_ta and the outputs (double; float in
 // the mixed-precision form); CT: arithmetic type (FP32 arithmetic rounds the
-// FP64 state as it is read from the ring)
-template <class H, class CT, int TY, int NS, int MINB>
+// FP64 state as it is read from the ring).  TMA: the ring is filled by tensor
+// copies (FP64 form only; tm holds the maps), else by cp.async.
+template <class H, class CT, int TY, int NS, int MINB, bool TMA>
 __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     Dims d, GridDev g, GridRcp rg, StepParams sp, const double* __restrict__ U,
     const double* __restrict__ V, const double* __restrict__ W, const double* __restrict__ T,
     const H* __restrict__ U_TA, const H* __restrict__ V_TA, const H* __restrict__ W_TA,
     H* __restrict__ U_PRE, H* __restrict__ V_PRE, H* __restrict__ W_PRE, H* __restrict__ T_PRE,
     const double* __restrict__ C1, H* __restrict__ U_A, H* __restrict__ V_A,
-    H* __restrict__ W_A, H* __restrict__ U_T) {
-  extern __shared__ __align__(16) char smc[];
+    H* __restrict__ W_A, H* __restrict__ U_T, const __grid_constant__ RhsMaps tm) {
+  extern __shared__ __align__(128) char smc[];
   char* sm = smc;
-  constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+  using Lay = RhsLay<H, TY, TMA>;
+  constexpr int PLANE = Lay::FP, TILE = Lay::HS;
   constexpr int F = NS - 3;  // planes in flight
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
@@ -129,12 +200,34 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
   const int k0 = 1 + blockIdx.z * KCHUNK;
   const int k1 = min(d.nz, k0 + KCHUNK - 1);
   const int kmax = k1 + 1;  // last plane any iteration reads
-  // prologue: planes k0-1 .. k0+F (the last F-1 stay in flight)
-  for (int q = -1; q <= F; ++q)
-    load_plane<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE,
-                          T_PRE);
-  cp_async_wait<F - 1>();
-  __syncthreads();
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + NS * Lay::SLOT);
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  if constexpr (TMA) {
+    // the copies need 128-byte aligned buffers and a 64-byte aligned map; a
+    // launch that finds otherwise records the error (its cells then read
+    // zeros from the never-filled ring, and the host reports the error)
+    const bool aligned = ((smem_u32(sm) & 127) == 0) &&
+                         ((reinterpret_cast<uintptr_t>(&tm.m[0]) & 63) == 0);
+    if (lead) {
+      for (int q = 0; q < NS; ++q) mbar_init(&bars[q], 1);
+      mbar_fence_init();
+      if (!aligned) atomicExch(&g_ring_wait_err, 2);
+    }
+    __syncthreads();
+    if (!aligned) return;
+    // prologue: planes k0-1 .. k0+F
+    if (lead)
+      for (int q = -1; q <= F; ++q) load_plane_tma<TY, NS>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
+    ring_wait<NS>(bars, k0 - 1, k0);
+    ring_wait<NS>(bars, k0, k0);
+  } else {
+    // prologue: planes k0-1 .. k0+F (the last F-1 stay in flight)
+    for (int q = -1; q <= F; ++q)
+      load_plane<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE,
+                            T_PRE);
+    cp_async_wait<F - 1>();
+    __syncthreads();
+  }
   using R = CT;  // arithmetic type
   const R DT = (R)sp.dt;
   const R a1 = (sp.l == 1) ? R(1) : R(1.5), a2 = (sp.l == 1) ? R(0) : R(-0.5);
@@ -152,17 +245,25 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     ry12 = LD(rg.rdy12, J); ry12m = LD(rg.rdy12, J - 1);
   }
   const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;  // this cell in a halo plane
-  const int t0 = threadIdx.y * TXW + threadIdx.x;            // this cell in a tile
+  const int t0 = Lay::he(threadIdx.x, threadIdx.y);          // this cell in a history tile
+  const int ec = Lay::c1e(threadIdx.x, threadIdx.y);         // this cell in the c1 plane
   for (int K = k0; K <= k1; ++K) {
     // plane K+1+F goes into the slot of plane K-2, free since the barrier
     // that ended the previous iteration
-    load_plane<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE,
-                          T_PRE);
+    if constexpr (TMA) {
+      if (lead) load_plane_tma<TY, NS>(sm, bars, tm, i0, j0, K + 1 + F, k0, kmax);
+      ring_wait<NS>(bars, K + 1, k0);
+    } else {
+      load_plane<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, U, V, W, T, C1, U_PRE, V_PRE,
+                            W_PRE, T_PRE);
+    }
     if (valid) {
-      constexpr int SB = slot_bytes<H, TY>();
-      const double* pm = reinterpret_cast<const double*>(sm + ((K - 1) % NS) * SB);
-      const double* pc = reinterpret_cast<const double*>(sm + (K % NS) * SB);
-      const double* pp = reinterpret_cast<const double*>(sm + ((K + 1) % NS) * SB);
+      constexpr int SB = Lay::SLOT;
+      // ring slot of plane K: K mod NS, or counted from k0-1 in the TMA ring
+      auto slot_of = [&](int P) { return TMA ? (P - (k0 - 1)) % NS : P % NS; };
+      const double* pm = reinterpret_cast<const double*>(sm + slot_of(K - 1) * SB);
+      const double* pc = reinterpret_cast<const double*>(sm + slot_of(K) * SB);
+      const double* pp = reinterpret_cast<const double*>(sm + slot_of(K + 1) * SB);
       const long c = d.P(I, J, K);
       const R dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
       const R rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
@@ -171,12 +272,13 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       // component's values loaded where they are used: short live ranges keep
       // the register count low
 #define AT(pl, f, dxo, dyo) (R)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
+#define C1AT(pl, dxo, dyo) (R)(pl)[4 * PLANE + ec + (dyo) * Lay::C1W + (dxo)]
       // masks (set_immersed_boundary :1037-1080) and AB2 histories
-      const R cc1 = AT(pc, 4, 0, 0);
-      const R c2 = (I < d.nx) ? (cc1 + AT(pc, 4, 1, 0)) * R(0.5) : cc1;
-      const R c3 = (J < d.ny) ? (cc1 + AT(pc, 4, 0, 1)) * R(0.5) : cc1;
-      const R c4 = (K < d.nz) ? (cc1 + AT(pp, 4, 0, 0)) * R(0.5) : cc1;
-      const H* hist = reinterpret_cast<const H*>(pc + 5 * PLANE) + t0;
+      const R cc1 = C1AT(pc, 0, 0);
+      const R c2 = (I < d.nx) ? (cc1 + C1AT(pc, 1, 0)) * R(0.5) : cc1;
+      const R c3 = (J < d.ny) ? (cc1 + C1AT(pc, 0, 1)) * R(0.5) : cc1;
+      const R c4 = (K < d.nz) ? (cc1 + C1AT(pp, 0, 0)) * R(0.5) : cc1;
+      const H* hist = reinterpret_cast<const H*>(pc + Lay::HOFF) + t0;
       const bool solid = (c2 != R(0)) || (c3 != R(0)) || (c4 != R(0)) || (cc1 != R(0));
     // u
     {
@@ -291,31 +393,63 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       }
     }
 #undef AT
+#undef C1AT
     }  // valid
-    cp_async_wait<F - 1>();
+    if constexpr (!TMA) cp_async_wait<F - 1>();
     __syncthreads();
   }
 }
 
-template <class H, class CT, int TY, int NS, int MINB>
-static void rhs_go(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
+// tensor maps of the TMA ring: the padded FP64 fields (box 34 x (TY+2) or
+// 34 x TY) and the (nx,ny,nz) mask (box 36 x (TY+2)); false when a field is
+// not 16-byte aligned or the driver rejects a map
+static bool ring_map(CUtensorMap* m, const Dims& d, const void* p, int bx, int by) {
+  if (((uintptr_t)p & 15) != 0 || ((d.nx + 2) * 8) % 16 != 0) return false;
+  return tma_encode_3d(m, p, true, d.nx + 2, d.ny + 2, d.nz + 2, (long)(d.nx + 2) * 8,
+                       (long)(d.nx + 2) * (d.ny + 2) * 8, bx, by, 1);
+}
+static bool mask_map(CUtensorMap* m, const Dims& d, const void* p, int by) {
+  if (((uintptr_t)p & 15) != 0 || (d.nx * 8) % 16 != 0) return false;
+  return tma_encode_3d(m, p, true, d.nx, d.ny, d.nz, (long)d.nx * 8, (long)d.nx * d.ny * 8, 36,
+                       by, 1);
+}
+
+template <class H, class CT, int TY, int NS, int MINB, bool TMA = false>
+static bool rhs_go(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                    const double* u, const double* v, const double* w, const double* T,
                    const H* u_ta, const H* v_ta, const H* w_ta, H* u_pre, H* v_pre, H* w_pre,
                    H* T_pre, const double* c1, H* u_a, H* v_a, H* w_a, H* u_T, cudaStream_t s) {
+  RhsMaps tm;
+  size_t smem = (size_t)NS * RhsLay<H, TY, TMA>::SLOT;
+  if constexpr (TMA) {
+    const void* f[4] = {u, v, w, T};
+    const void* h[4] = {u_pre, v_pre, w_pre, T_pre};
+    bool ok = mask_map(&tm.m[4], d, c1, TY + 2);
+    for (int q = 0; q < 4; ++q)
+      ok = ok && ring_map(&tm.m[q], d, f[q], SXW, TY + 2) && ring_map(&tm.m[5 + q], d, h[q], SXW, TY);
+    if (!ok) return false;
+    smem += NS * sizeof(uint64_t);
+  } else {
+    memset(&tm, 0, sizeof(tm));
+  }
   dim3 block(TXW, TY, 1);
   dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KCHUNK - 1) / KCHUNK);
-  size_t smem = (size_t)NS * slot_bytes<H, TY>();
-  auto kern = k_rhs_fast<H, CT, TY, NS, MINB>;
+  auto kern = k_rhs_fast<H, CT, TY, NS, MINB, TMA>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   kern<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
-                                 T_pre, c1, u_a, v_a, w_a, u_T);
+                                 T_pre, c1, u_a, v_a, w_a, u_T, tm);
+  return true;
 }
 
 // launch shape: 0 the storage type's default (RhsShape), 1 32x4 tiles with a
 // 4-plane ring and four CTAs per SM, 2 32x8 tiles with a 5-plane ring and two
-// CTAs per SM, 3 32x8 tiles with a 4-plane ring and two CTAs per SM (every
-// shape computes each cell the same way; the context's autotuner picks one)
+// CTAs per SM, 3 32x8 tiles with a 4-plane ring and two CTAs per SM; FP64
+// storage and arithmetic also the TMA ring: 4 32x4 tiles with 5 planes and
+// three CTAs per SM, 5 32x4 with 4 planes and four CTAs, 6 32x8 with 4
+// planes and two CTAs (every shape computes each cell the same way; the
+// context's autotuner picks one; a TMA shape whose maps cannot be made runs
+// the default)
 template <class H, class CT>
 static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                      const double* u, const double* v, const double* w, const double* T,
@@ -326,6 +460,18 @@ static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
 #define NSE_RHS_GO(TY_, NS_, MB_)                                                           \
   rhs_go<H, CT, TY_, NS_, MB_>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre,    \
                                w_pre, T_pre, c1, u_a, v_a, w_a, u_T, s)
+#define NSE_RHS_TMA(TY_, NS_, MB_)                                                              \
+  done = rhs_go<H, CT, TY_, NS_, MB_, true>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre,  \
+                                            v_pre, w_pre, T_pre, c1, u_a, v_a, w_a, u_T, s)
+  if constexpr (sizeof(H) == 8 && sizeof(CT) == 8) {
+    bool done = false;
+    if (shape == 4) NSE_RHS_TMA(4, 5, 3);
+    else if (shape == 5) NSE_RHS_TMA(4, 4, 4);
+    else if (shape == 6) NSE_RHS_TMA(8, 4, 2);
+    if (done) return;
+    if (shape >= 4) shape = 0;
+  }
+#undef NSE_RHS_TMA
   switch (shape) {
     case 1: NSE_RHS_GO(4, 4, 4); break;
     case 2: NSE_RHS_GO(8, 5, 2); break;
@@ -333,6 +479,16 @@ static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
     default: NSE_RHS_GO(Sh::TY, Sh::NS, Sh::MINB); break;
   }
 #undef NSE_RHS_GO
+}
+
+int ring_wait_error() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_ring_wait_err, sizeof(int)) != cudaSuccess) return 0;
+  if (v) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_ring_wait_err, &z, sizeof(int));
+  }
+  return v;
 }
 
 void launch_rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
@@ -468,40 +624,97 @@ __device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, in
   cp_async_commit();
 }
 
-template <class H, int TY, int NS, int MINB>
+// ring slot of the correction (in doubles): phi, then u*, v*, w* halo planes
+// and the old u_ta, v_ta, w_ta tiles; the TMA ring (FP64 storage) keeps every
+// buffer 128-byte aligned and its tiles 34 wide (box from x = i0-1)
+template <class H, int TY, bool TMA>
+struct CorrLay {
+  static constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
+  static constexpr int FP = TMA ? ru16(PLANE) : PLANE;
+  static constexpr int HS = TMA ? ru16(SXW * TY) : TILE;
+  static constexpr int SLOT = TMA ? (4 * FP + 3 * HS) * 8 : cslot_bytes<H, TY>();
+  static __device__ __forceinline__ int he(int tx, int ty) {
+    return TMA ? ty * SXW + tx + 1 : ty * TXW + tx;
+  }
+};
+
+template <int TY, int NS>
+__device__ __forceinline__ void load_plane_c_tma(char* sm, uint64_t* bars, const CorrMaps& tm,
+                                                 int i0, int j0, int K, int k0, int kmax) {
+  using L = CorrLay<double, TY, true>;
+  if (K > kmax) return;
+  const int r = K - (k0 - 1);
+  double* slot = reinterpret_cast<double*>(sm + (r % NS) * L::SLOT);
+  uint64_t* bar = &bars[r % NS];
+  constexpr unsigned HALO = SXW * (TY + 2) * 8, HB = SXW * TY * 8;
+  mbar_expect_tx(bar, 4 * HALO + 3 * HB);
+  for (int f = 0; f < 4; ++f) tma_load_3d(slot + f * L::FP, &tm.m[f], i0 - 1, j0 - 1, K, bar);
+  for (int f = 0; f < 3; ++f)
+    tma_load_3d(slot + 4 * L::FP + f * L::HS, &tm.m[4 + f], i0 - 1, j0, K, bar);
+}
+
+template <class H, int TY, int NS, int MINB, bool TMA>
 __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     Dims d, GridRcp rg, const double* __restrict__ PHI, const H* __restrict__ UT,
     const H* __restrict__ VT, const H* __restrict__ WT, double* __restrict__ p,
     double* __restrict__ u, double* __restrict__ v, double* __restrict__ w,
     H* __restrict__ u_ta, H* __restrict__ v_ta, H* __restrict__ w_ta, H* __restrict__ u_ep2,
-    H* __restrict__ v_ep2, H* __restrict__ w_ep2, H* __restrict__ divu, double dt) {
-  extern __shared__ __align__(16) char smc[];
+    H* __restrict__ v_ep2, H* __restrict__ w_ep2, H* __restrict__ divu, double dt,
+    const __grid_constant__ CorrMaps tm) {
+  extern __shared__ __align__(128) char smc[];
   char* sm = smc;
-  constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY, F = NS - 3;
+  using Lay = CorrLay<H, TY, TMA>;
+  constexpr int PLANE = Lay::FP, TILE = Lay::HS, F = NS - 3;
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
   const int k0 = 1 + blockIdx.z * CKCHUNK;
   const int k1 = min(d.nz, k0 + CKCHUNK - 1);
   const int kmax = k1 + 1;
-  for (int q = -1; q <= F; ++q)
-    load_plane_c<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
-  cp_async_wait<F - 1>();
-  __syncthreads();
+  uint64_t* bars = reinterpret_cast<uint64_t*>(sm + NS * Lay::SLOT);
+  const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  if constexpr (TMA) {
+    const bool aligned = ((smem_u32(sm) & 127) == 0) &&
+                         ((reinterpret_cast<uintptr_t>(&tm.m[0]) & 63) == 0);
+    if (lead) {
+      for (int q = 0; q < NS; ++q) mbar_init(&bars[q], 1);
+      mbar_fence_init();
+      if (!aligned) atomicExch(&g_ring_wait_err, 2);
+    }
+    __syncthreads();
+    if (!aligned) return;
+    if (lead)
+      for (int q = -1; q <= F; ++q)
+        load_plane_c_tma<TY, NS>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
+    ring_wait<NS>(bars, k0 - 1, k0);
+    ring_wait<NS>(bars, k0, k0);
+  } else {
+    for (int q = -1; q <= F; ++q)
+      load_plane_c<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    cp_async_wait<F - 1>();
+    __syncthreads();
+  }
   double rx = 0, rx12 = 0, rx12m = 0, ry = 0, ry12 = 0, ry12m = 0;
   if (valid) {
     rx = LD(rg.rdx, I); rx12 = LD(rg.rdx12, I); rx12m = LD(rg.rdx12, I - 1);
     ry = LD(rg.rdy, J); ry12 = LD(rg.rdy12, J); ry12m = LD(rg.rdy12, J - 1);
   }
   const int e0 = (threadIdx.y + 1) * SXW + threadIdx.x + 1;
-  const int t0 = threadIdx.y * TXW + threadIdx.x;
+  const int t0 = Lay::he(threadIdx.x, threadIdx.y);
   for (int K = k0; K <= k1; ++K) {
-    load_plane_c<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    if constexpr (TMA) {
+      if (lead) load_plane_c_tma<TY, NS>(sm, bars, tm, i0, j0, K + 1 + F, k0, kmax);
+      ring_wait<NS>(bars, K + 1, k0);
+    } else {
+      load_plane_c<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, PHI, UT, VT, WT, u_ta, v_ta,
+                              w_ta);
+    }
     if (valid) {
-      constexpr int SB = cslot_bytes<H, TY>();
-      const char* sm_m = sm + ((K - 1) % NS) * SB;
-      const char* sm_c = sm + (K % NS) * SB;
-      const char* sm_p = sm + ((K + 1) % NS) * SB;
+      constexpr int SB = Lay::SLOT;
+      auto slot_of = [&](int P) { return TMA ? (P - (k0 - 1)) % NS : P % NS; };
+      const char* sm_m = sm + slot_of(K - 1) * SB;
+      const char* sm_c = sm + slot_of(K) * SB;
+      const char* sm_p = sm + slot_of(K + 1) * SB;
       const double* qm = reinterpret_cast<const double*>(sm_m);
       const double* qc = reinterpret_cast<const double*>(sm_c);
       const double* qp = reinterpret_cast<const double*>(sm_p);
@@ -538,7 +751,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
       v_ta[c] = (H)(dt * gy);
       w_ta[c] = (H)(dt * gz);
     }
-    cp_async_wait<F - 1>();
+    if constexpr (!TMA) cp_async_wait<F - 1>();
     __syncthreads();
   }
 }
@@ -575,24 +788,38 @@ __global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ P
   w_ta[c] = (H)(dt * gz);
 }
 
-template <class H, int TY, int NS, int MINB>
-static void correct_go(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
+template <class H, int TY, int NS, int MINB, bool TMA = false>
+static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                        const H* vt, const H* wt, double* p, double* u, double* v, double* w,
                        H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
                        double dt, cudaStream_t s) {
+  CorrMaps tm;
+  size_t smem = (size_t)NS * CorrLay<H, TY, TMA>::SLOT;
+  if constexpr (TMA) {
+    const void* f[7] = {PHI, ut, vt, wt, u_ta, v_ta, w_ta};
+    bool ok = true;
+    for (int q = 0; q < 7; ++q) ok = ok && ring_map(&tm.m[q], d, f[q], SXW, q < 4 ? TY + 2 : TY);
+    if (!ok) return false;
+    smem += NS * sizeof(uint64_t);
+  } else {
+    memset(&tm, 0, sizeof(tm));
+  }
   dim3 block(TXW, TY, 1);
   dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + CKCHUNK - 1) / CKCHUNK);
-  size_t smem = (size_t)NS * cslot_bytes<H, TY>();
-  auto kern = k_correct_pipe<H, TY, NS, MINB>;
+  auto kern = k_correct_pipe<H, TY, NS, MINB, TMA>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   kern<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,
-                                 v_ep2, w_ep2, divu, dt);
+                                 v_ep2, w_ep2, divu, dt, tm);
+  return true;
 }
 
 // launch shape: 0 the storage type's default (CorrShape), 1 32x8 tiles with a
 // 5-plane ring and two CTAs per SM, 2 32x4 tiles with 4 planes and four CTAs,
-// 3 32x8 tiles with 4 planes and three CTAs (each cell computed the same way)
+// 3 32x8 tiles with 4 planes and three CTAs; FP64 storage also the TMA ring:
+// 4 32x4 tiles with 4 planes and five CTAs per SM, 5 32x4 with 5 planes and
+// four CTAs, 6 32x8 with 4 planes and three CTAs (each cell computed the same
+// way; a TMA shape whose maps cannot be made runs the default)
 template <class H>
 static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                          const H* vt, const H* wt, double* p, double* u, double* v, double* w,
@@ -602,7 +829,18 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
 #define NSE_CORR_GO(TY_, NS_, MB_)                                                           \
   correct_go<H, TY_, NS_, MB_>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,  \
                                v_ep2, w_ep2, divu, dt, s)
-  switch (shape) {
+#define NSE_CORR_TMA(TY_, NS_, MB_)                                                          \
+  done = correct_go<H, TY_, NS_, MB_, true>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
+                                            w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
+  bool done = false;
+  if constexpr (sizeof(H) == 8) {
+    if (shape == 4) NSE_CORR_TMA(4, 4, 5);
+    else if (shape == 5) NSE_CORR_TMA(4, 5, 4);
+    else if (shape == 6) NSE_CORR_TMA(8, 4, 3);
+  }
+#undef NSE_CORR_TMA
+  if (!done && shape >= 4) shape = 0;
+  if (!done) switch (shape) {
     case 1: NSE_CORR_GO(8, 5, 2); break;
     case 2: NSE_CORR_GO(4, 4, 4); break;
     case 3: NSE_CORR_GO(8, 4, 3); break;

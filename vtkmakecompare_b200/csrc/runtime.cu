@@ -1355,6 +1355,11 @@ void readgrid3d_(const int* nx, const int* ny, const int* nz, double* phi0) {
 // launch-shape choices of the autotuner, per grid and form, for the process
 static std::mutex g_tune_mu;
 static std::map<std::string, int> g_tune;
+// NSEGPU_TUNE_LOG set: every autotuner candidate's time goes to stderr
+static void tune_log(const char* key, int cand, float ms) {
+  static const bool on = getenv("NSEGPU_TUNE_LOG") != nullptr;
+  if (on) fprintf(stderr, "nsegpu tune [%s] candidate %d: %.4f ms\n", key, cand, ms);
+}
 
 struct nse_ctx {
   nse_config cfg;
@@ -1918,6 +1923,7 @@ static void autotune_mid(nse_ctx* x) {
       best_ms = ms;
       best = nc;
     }
+    tune_log(key, nc, ms);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -1993,7 +1999,8 @@ static void autotune_correct(nse_ctx* x, const H* ut, const H* vt, const H* wt) 
     cudaMemcpyAsync(ta[q], x->f[tid[q]].p, hb, cudaMemcpyDeviceToDevice, s);
   int best = 0;
   float best_ms = 1e30f;
-  for (int shape = 0; shape < 4; ++shape) {
+  const int nshape = sizeof(H) == 4 ? 4 : 7;  // shapes 4-6: the FP64 TMA ring
+  for (int shape = 0; shape < nshape; ++shape) {
     auto run = [&]() {
       if constexpr (sizeof(H) == 4)
         launch_correct_f32(d, x->rg, F(x, NSE_PHI), ut, vt, wt, F(x, NSE_P), F(x, NSE_U),
@@ -2016,6 +2023,7 @@ static void autotune_correct(nse_ctx* x, const H* ut, const H* vt, const H* wt) 
       best_ms = ms;
       best = shape;
     }
+    tune_log(key, shape, ms);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2263,6 +2271,7 @@ static void autotune_lines(nse_ctx* x) {
           best_ms = ms;
           best = c;
         }
+        tune_log(key, c, ms);
       }
       if (dir == 0) x->xnl[comp] = best;
       else x->yzshape[dir][comp] = best;
@@ -2318,7 +2327,8 @@ static void autotune_rhs(nse_ctx* x, const StepParams& sp) {
   const double* c1 = F(x, NSE_CELLVALUE);
   int best = 0;
   float best_ms = 1e30f;
-  for (int shape = 0; shape < 4; ++shape) {
+  const int nshape = x->mixed ? 4 : 7;  // shapes 4-6: the FP64 TMA ring
+  for (int shape = 0; shape < nshape; ++shape) {
     auto run = [&]() {
       if (x->mixed)
         launch_rhs_f32(d, x->g, x->rg, sp, u, v, w, T, F32(x, NSE_U_TA), F32(x, NSE_V_TA),
@@ -2341,6 +2351,7 @@ static void autotune_rhs(nse_ctx* x, const StepParams& sp) {
       best_ms = ms;
       best = shape;
     }
+    tune_log(key, shape, ms);
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
@@ -2801,6 +2812,20 @@ int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
   return NSE_OK;
 }
 
+int nse_ctx_set_shapes(nse_ctx* x, int rhs_shape, int corr_shape) {
+  if (!x || rhs_shape < -1 || rhs_shape > 6 || corr_shape < -1 || corr_shape > 6)
+    return NSE_ERR_ARG;
+  if (rhs_shape >= 0) {
+    x->rhs_shape = rhs_shape;
+    x->rhs_tuned = true;
+  }
+  if (corr_shape >= 0) {
+    x->corr_shape = corr_shape;
+    x->corr_tuned = true;
+  }
+  return NSE_OK;
+}
+
 int nse_ctx_launch_shapes(nse_ctx* x, int* out) {
   if (!x || !out) return NSE_ERR_ARG;
   for (int dir = 1; dir <= 2; ++dir)
@@ -2821,6 +2846,10 @@ int nse_sync(nse_ctx* x) {
   }
   if (line_wait_error()) {
     set_error(NSE_ERR_CUDA, "nse_sync: a line kernel's wait for its tile copy gave up");
+    return NSE_ERR_CUDA;
+  }
+  if (ring_wait_error()) {
+    set_error(NSE_ERR_CUDA, "nse_sync: a right-hand-side or correction ring wait gave up");
     return NSE_ERR_CUDA;
   }
   return NSE_OK;

@@ -79,6 +79,7 @@ def _sig():
     L.nse_ctx_grid.argtypes = [vp] + [vp] * 12
     L.nse_ctx_profile.argtypes = [vp, C.c_int]
     L.nse_ctx_launch_shapes.argtypes = [vp, vp]
+    L.nse_ctx_set_shapes.argtypes = [vp, C.c_int, C.c_int]
     L.nse_ctx_phase_times.argtypes = [vp, vp, C.c_int, vp]
     L.nse_launch_count.restype = C.c_longlong
     L.nse_ensemble_create.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp)]
@@ -197,6 +198,11 @@ class Context:
         check(self.L.nse_ctx_launch_shapes(self.h, o))
         return {"y": list(o[:4]), "z": list(o[4:8]), "x": list(o[8:12]), "rhs": o[12],
                 "correct": o[13], "mid": o[14]}
+
+    def set_shapes(self, rhs=-1, correct=-1):
+        """Fix the right-hand-side and correction launch shapes (-1: autotuned);
+        nsegpu.h, nse_ctx_set_shapes."""
+        check(self.L.nse_ctx_set_shapes(self.h, int(rhs), int(correct)))
 
     def levelset(self, phi0, nnn=2000, dtau=1.0e-3, width=1.0, want_phi=True):
         a = np.asfortranarray(phi0, dtype=np.float64)
