@@ -324,3 +324,60 @@ def test_set_shapes_rejects_bad_codes():
             ctx.set_shapes(7, 0)
         with pytest.raises(Exception):
             ctx.set_shapes(0, -2)
+
+
+@pytest.mark.parametrize("prec,flags", [(S.FP64, 0), (S.MIXED, 64)])
+def test_autotuning_context_matches_fixed_shapes(prec, flags):
+    """The first context of a grid runs every autotuner inside its first
+    step (right-hand side, lines, correction); its fields after 4 penalised
+    steps agree with a context that keeps the fixed shapes.  A grid no other
+    test uses, so the tuning is not skipped by the per-process table."""
+    g, f, c1, par = make_case(80, 48, 112, seed=11)
+    out = []
+    for fl in (flags, flags | S.FLAG_NO_AUTOTUNE):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"], precision=prec, flags=fl)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.project()
+            ctx.start()
+            ctx.step(4)
+            ctx.sync()
+            out.append({k: ctx.download(k) for k in ("u", "v", "w", "p", "T")})
+    for k in out[0]:
+        assert rel_l2(out[0][k], out[1][k]) < 1e-13, k
+
+
+def test_levelset_leaves_the_poisson_work_field_clean():
+    """A context whose mask comes from nse_levelset steps exactly like one
+    given the same mask by upload: the level set does not stay behind in the
+    Poisson work field, whose never-written ghost entries the correction's
+    face pass reads (zero, as in the oracle)."""
+    g, f, c1, par = make_case(96, 48, 64, seed=5)
+    phi0 = W.sphere_phi0(g, (math.pi, 0.0, math.pi / 2), 0.4)
+    out = []
+    mask = None
+    for use_levelset in (True, False):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"])
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            if use_levelset:
+                ctx.levelset(phi0, nnn=50, width=1.5, want_phi=False)
+                mask = ctx.download("cellvalue")
+            else:
+                ctx.upload("cellvalue", mask)
+            ctx.project()
+            ctx.start()
+            ctx.step(5)
+            ctx.sync()
+            out.append({k: ctx.download(k) for k in STATE})
+    for k in STATE:
+        assert np.array_equal(out[0][k], out[1][k]), k

@@ -2235,8 +2235,10 @@ static void autotune_lines(nse_ctx* x) {
       if (dir == 0) {
         if (x_nl_candidates(x) < 2) continue;
         cand = {2, 1};
-      } else {
+      } else if (x->mixed) {
         cand = {0, 1, 3};
+      } else {
+        cand = {0, 1, 3, 2};  // 2: the FP64 TMA tiles
       }
       int best = cand[0];
       float best_ms = 1e30f;
@@ -2319,7 +2321,20 @@ static void autotune_rhs(nse_ctx* x, const StepParams& sp) {
     return;
   }
   const size_t hb = d.ntot * (x->mixed ? sizeof(float) : sizeof(double));
-  void* hist[4] = {x->sa.p, x->sb.p, x->tmp.p, x->f[NSE_PHI].p};
+  // the fourth history copy gets a buffer of its own, released after the
+  // timing: phi must not serve as scratch, because the Poisson solve never
+  // writes some of its ghost entries (as in the reference) and the
+  // correction's face pass reads them
+  DBuf extra;
+  if (!extra.ensure(hb)) {  // no room: keep the default shape, report nothing
+    nse_clear_error();
+    cudaGetLastError();
+    cudaEventDestroy(e0);
+    cudaEventDestroy(e1);
+    x->rhs_tuned = true;
+    return;
+  }
+  void* hist[4] = {x->sa.p, x->sb.p, x->tmp.p, extra.p};
   const int hid[4] = {NSE_U_PRE, NSE_V_PRE, NSE_W_PRE, NSE_T_PRE};
   for (int q = 0; q < 4; ++q)
     cudaMemcpyAsync(hist[q], x->f[hid[q]].p, hb, cudaMemcpyDeviceToDevice, s);
@@ -2355,6 +2370,7 @@ static void autotune_rhs(nse_ctx* x, const StepParams& sp) {
   }
   cudaEventDestroy(e0);
   cudaEventDestroy(e1);
+  extra.release();
   x->rhs_shape = best;
   x->rhs_tuned = true;
   std::lock_guard<std::mutex> lk(g_tune_mu);
@@ -2675,6 +2691,11 @@ int nse_levelset(nse_ctx* x, const double* phi0, double* phi_out, int nnn, doubl
   if (phi_out &&
       !NSE_CUDA(cudaMemcpyAsync(phi_out, x->f[NSE_PHI].p, d.ntot * sizeof(double),
                                 cudaMemcpyDeviceToHost, s)))
+    return status_or(NSE_ERR_CUDA);
+  // the Poisson work field goes back to zero: MKP's PHI is a separate array
+  // in the reference (mkp.f:21), and the ghost entries its solve never writes
+  // (read by the correction's face pass) must not keep level-set values
+  if (!NSE_CUDA(cudaMemsetAsync(x->f[NSE_PHI].p, 0, d.ntot * sizeof(double), s)))
     return status_or(NSE_ERR_CUDA);
   return NSE_CUDA(cudaStreamSynchronize(s)) ? NSE_OK : status_or(NSE_ERR_CUDA);
 }
