@@ -358,8 +358,9 @@ int nse_sync(nse_ctx* ctx);
  * 8, 3 = 32, 2 = TMA tiles of 16 lines), out[8 + comp] the x lines per warp
  * iteration, out[12] the right-hand-side kernel's shape (0 = 32x4 tiles with a
  * 5-plane ring in FP64 / 32x8 in FP32, 1 = 32x4 with 4 planes, 2 = 32x8 with
- * 5, 3 = 32x8 with 4; FP64 only, the ring filled by TMA copies: 4 = 32x4 with
- * 5 planes, 5 = 32x4 with 4, 6 = 32x8 with 4), out[13] the pipelined
+ * 5, 3 = 32x8 with 4; the ring filled by TMA copies (FP32 storage: the FP64
+ * halo planes by TMA, the history tiles by cp.async): 4 = 32x4 with 5 planes,
+ * 5 = 32x4 with 4, 6 = 32x8 with 4), out[13] the pipelined
  * correction's shape (0 = the default, 1 = 32x8 tiles with 5 planes, 2 = 32x4
  * with 4, 3 = 32x8 with 4; FP64 TMA ring: 4 = 32x4 with 4 planes, 5 = 32x4
  * with 5, 6 = 32x8 with 4), out[14] the kx slices the FP64 solve's z

@@ -285,19 +285,23 @@ def test_line_launch_shapes_give_the_same_fields(n):
     assert shapes["correct"] in range(7), shapes
 
 
-@pytest.mark.parametrize("n", [(96, 64, 96), (80, 40, 48)])
-def test_rhs_and_correction_shapes_give_the_same_bits(n):
+@pytest.mark.parametrize("n,prec,flags", [((96, 64, 96), S.FP64, 0), ((80, 40, 48), S.FP64, 0),
+                                          ((96, 64, 96), S.MIXED, 0),
+                                          ((80, 40, 48), S.MIXED, 32)])
+def test_rhs_and_correction_shapes_give_the_same_bits(n, prec, flags):
     """Every launch shape of the right-hand side and of the pipelined
-    correction, the cp.async rings (0-3) and the TMA rings (4-6), gives the
-    same bits after 3 penalised FP64 steps (partial x and y tiles in the
-    80x40x48 case), with no ring wait reported by nse_sync."""
+    correction, the cp.async rings (0-3) and the TMA rings (4-6; FP32
+    storage: FP64 halo planes by TMA, history tiles by cp.async), gives the
+    same bits after 3 penalised steps (partial x and y tiles in the 80x40x48
+    case; FP64, mixed, and mixed with FP64 stencil arithmetic), with no ring
+    wait reported by nse_sync."""
     g, f, c1, par = make_case(*n)
     out = []
     for rhs, corr in ((0, 0), (1, 2), (2, 1), (3, 3), (4, 4), (5, 5), (6, 6)):
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                        g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
                        body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
-                       t_top=par["ttop"], t_solid=par["tsolid"])
+                       t_top=par["ttop"], t_solid=par["tsolid"], precision=prec, flags=flags)
         with S.Context(cfg) as ctx:
             for k in ("u", "v", "w", "T"):
                 ctx.upload(k, f[k])
@@ -332,7 +336,7 @@ def test_autotuning_context_matches_fixed_shapes(prec, flags):
     step (right-hand side, lines, correction); its fields after 4 penalised
     steps agree with a context that keeps the fixed shapes.  A grid no other
     test uses, so the tuning is not skipped by the per-process table."""
-    g, f, c1, par = make_case(80, 48, 112, seed=11)
+    g, f, c1, par = make_case(80, 48, 120, seed=11)
     out = []
     for fl in (flags, flags | S.FLAG_NO_AUTOTUNE):
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],

@@ -353,6 +353,16 @@ template <> struct Vec2T<float> { using T = float2; };
 // (which every step would repeat).  FP64 tables hold the values themselves.
 __device__ __forceinline__ double mul1(double a, double v) { return a * v; }
 __device__ __forceinline__ float mul1(float a, float dv) { return a + a * dv; }
+// one term of the reduced inverse's row sum, F + m rc (the diagonal term
+// through mul1); in FP64 the product and the sum are rounded separately
+// (no contraction), so every y/z line kernel forms the same bits
+__device__ __forceinline__ double red_acc(double F, double rc, double m, bool diag) {
+  (void)diag;
+  return __dadd_rn(F, __dmul_rn(rc, m));
+}
+__device__ __forceinline__ float red_acc(float F, float rc, float m, bool diag) {
+  return F + (diag ? mul1(rc, m) : m * rc);
+}
 
 // interior Thomas on registers: g <- solution of the interior rows with
 // zero end values; rows r = 1..m-2 of the partition, table rows at tb(r).
@@ -681,8 +691,8 @@ __global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yz
   for (int c = 0; c < R2; ++c) {
     const R rc = red[c * LPB + lane];
     const R mf = __ldg(MI + (2 * k) * R2 + c), me = __ldg(MI + (2 * k + 1) * R2 + c);
-    F = F + (c == 2 * k ? mul1(rc, mf) : mf * rc);
-    E = E + (c == 2 * k + 1 ? mul1(rc, me) : me * rc);
+    F = red_acc(F, rc, mf, c == 2 * k);
+    E = red_acc(E, rc, me, c == 2 * k + 1);
   }
 #pragma unroll
   for (int r = 1; r < MM; ++r) {
@@ -801,8 +811,8 @@ __global__ void __launch_bounds__(16 * P, 2)
 #pragma unroll
     for (int c = 0; c < R2; ++c) {
       const double rc = red[c * LPB + lane];
-      F = F + MI[(2 * k) * R2 + c] * rc;
-      E = E + MI[(2 * k + 1) * R2 + c] * rc;
+      F = red_acc(F, rc, MI[(2 * k) * R2 + c], c == 2 * k);
+      E = red_acc(E, rc, MI[(2 * k + 1) * R2 + c], c == 2 * k + 1);
     }
 #pragma unroll
     for (int r = 1; r < MM; ++r) {

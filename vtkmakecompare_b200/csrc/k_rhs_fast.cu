@@ -130,24 +130,29 @@ struct alignas(64) CorrMaps {
 };
 __device__ int g_ring_wait_err = 0;
 
-// shared-memory layout of one RHS ring slot (in doubles); TMA selects the
-// padded sub-buffers and box pitches of the TMA ring
-template <class H, int TY, bool TMA>
+// shared-memory layout of one RHS ring slot (in doubles).  TM, the ring's
+// fill: 0 cp.async for every field; 1 TMA for every field (FP64 storage);
+// 2 TMA for the five FP64 halo planes and cp.async for the FP32 history
+// tiles (mixed form: a padded FP32 field's row pitch, (nx+2)*4 bytes, is not
+// the multiple of 16 bytes a tensor map needs).  TMA buffers are padded to
+// 128 bytes and use the boxes' pitches.
+template <class H, int TY, int TM>
 struct RhsLay {
   static constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
-  static constexpr int FP = TMA ? ru16(PLANE) : PLANE;            // field stride
-  static constexpr int C1W = TMA ? 36 : SXW;                      // c1 row pitch
-  static constexpr int C1P = TMA ? ru16(36 * (TY + 2)) : PLANE;   // c1 buffer
-  static constexpr int HW = TMA ? SXW : TXW;                      // history row pitch
-  static constexpr int HS = TMA ? ru16(SXW * TY) : TILE;          // history stride
+  static constexpr int FP = TM ? ru16(PLANE) : PLANE;             // field stride
+  static constexpr int C1W = TM ? 36 : SXW;                       // c1 row pitch
+  static constexpr int C1P = TM ? ru16(36 * (TY + 2)) : PLANE;    // c1 buffer
+  static constexpr int HS = TM == 1 ? ru16(SXW * TY) : TILE;      // history stride (H)
   static constexpr int HOFF = 4 * FP + C1P;                        // first history
-  static constexpr int SLOT = TMA ? (HOFF + 4 * HS) * 8 : slot_bytes<H, TY>();
+  static constexpr int SLOT = TM == 1 ? (HOFF + 4 * HS) * 8
+                              : TM == 2 ? HOFF * 8 + ((4 * TILE * (int)sizeof(H) + 127) & ~127)
+                                        : slot_bytes<H, TY>();
   // this thread's cell in the c1 buffer and in a history tile
   static __device__ __forceinline__ int c1e(int tx, int ty) {
-    return TMA ? (ty + 1) * 36 + tx + 2 : (ty + 1) * SXW + tx + 1;
+    return TM ? (ty + 1) * 36 + tx + 2 : (ty + 1) * SXW + tx + 1;
   }
   static __device__ __forceinline__ int he(int tx, int ty) {
-    return TMA ? ty * SXW + tx + 1 : ty * TXW + tx;
+    return TM == 1 ? ty * SXW + tx + 1 : ty * TXW + tx;
   }
 };
 
@@ -159,29 +164,51 @@ __device__ __forceinline__ void ring_wait(uint64_t* bars, int P, int k0) {
     atomicExch(&g_ring_wait_err, 1);
 }
 
-// plane K of u, v, w, T, c1 and the histories into its slot by TMA (one
-// issuing thread)
-template <int TY, int NS>
+// plane K of u, v, w, T, c1 (and with TM = 1 the histories) into its slot
+// by TMA (one issuing thread)
+template <class H, int TY, int NS, int TM>
 __device__ __forceinline__ void load_plane_tma(char* sm, uint64_t* bars, const RhsMaps& tm,
                                                int i0, int j0, int K, int k0, int kmax) {
-  using L = RhsLay<double, TY, true>;
+  using L = RhsLay<H, TY, TM>;
   if (K > kmax) return;
   const int r = K - (k0 - 1);
   double* slot = reinterpret_cast<double*>(sm + (r % NS) * L::SLOT);
   uint64_t* bar = &bars[r % NS];
   constexpr unsigned HALO = SXW * (TY + 2) * 8, C1B = 36 * (TY + 2) * 8, HB = SXW * TY * 8;
-  mbar_expect_tx(bar, 4 * HALO + C1B + 4 * HB);
+  mbar_expect_tx(bar, 4 * HALO + C1B + (TM == 1 ? 4 * HB : 0));
   for (int f = 0; f < 4; ++f) tma_load_3d(slot + f * L::FP, &tm.m[f], i0 - 1, j0 - 1, K, bar);
   tma_load_3d(slot + 4 * L::FP, &tm.m[4], i0 - 3, j0 - 2, K - 1, bar);
-  for (int f = 0; f < 4; ++f)
-    tma_load_3d(slot + L::HOFF + f * L::HS, &tm.m[5 + f], i0 - 1, j0, K, bar);
+  if constexpr (TM == 1)
+    for (int f = 0; f < 4; ++f)
+      tma_load_3d(slot + L::HOFF + f * L::HS, &tm.m[5 + f], i0 - 1, j0, K, bar);
+}
+// TM = 2: the history tiles of plane K by cp.async (one commit group, empty
+// past kmax or outside the interior)
+template <class H, int TY, int NS>
+__device__ __forceinline__ void load_hist_async(char* sm, const Dims& d, int i0, int j0, int K,
+                                                int k0, int kmax, const H* UP, const H* VP,
+                                                const H* WP, const H* TP) {
+  using L = RhsLay<H, TY, 2>;
+  constexpr int TILE = TXW * TY;
+  const int i = i0 + threadIdx.x, j = j0 + threadIdx.y;
+  if (K <= kmax && i <= d.nx && j <= d.ny && K >= 1 && K <= d.nz) {
+    const int r = K - (k0 - 1);
+    H* h = reinterpret_cast<H*>(reinterpret_cast<double*>(sm + (r % NS) * L::SLOT) + L::HOFF) +
+           threadIdx.y * TXW + threadIdx.x;
+    const long c = d.P(i, j, K);
+    cp_async8(h, UP + c);
+    cp_async8(h + TILE, VP + c);
+    cp_async8(h + 2 * TILE, WP + c);
+    cp_async8(h + 3 * TILE, TP + c);
+  }
+  cp_async_commit();
 }
 
 // H: storage type of the histories, u_ta and the outputs (double; float in
 // the mixed-precision form); CT: arithmetic type (FP32 arithmetic rounds the
-// FP64 state as it is read from the ring).  TMA: the ring is filled by tensor
-// copies (FP64 form only; tm holds the maps), else by cp.async.
-template <class H, class CT, int TY, int NS, int MINB, bool TMA>
+// FP64 state as it is read from the ring).  TM: how the ring is filled (see
+// RhsLay; tm holds the tensor maps of a TMA fill).
+template <class H, class CT, int TY, int NS, int MINB, int TM>
 __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     Dims d, GridDev g, GridRcp rg, StepParams sp, const double* __restrict__ U,
     const double* __restrict__ V, const double* __restrict__ W, const double* __restrict__ T,
@@ -191,7 +218,8 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     H* __restrict__ W_A, H* __restrict__ U_T, const __grid_constant__ RhsMaps tm) {
   extern __shared__ __align__(128) char smc[];
   char* sm = smc;
-  using Lay = RhsLay<H, TY, TMA>;
+  using Lay = RhsLay<H, TY, TM>;
+  constexpr bool TMA = TM != 0;
   constexpr int PLANE = Lay::FP, TILE = Lay::HS;
   constexpr int F = NS - 3;  // planes in flight
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
@@ -217,7 +245,14 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     if (!aligned) return;
     // prologue: planes k0-1 .. k0+F
     if (lead)
-      for (int q = -1; q <= F; ++q) load_plane_tma<TY, NS>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
+      for (int q = -1; q <= F; ++q)
+        load_plane_tma<H, TY, NS, TM>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
+    if constexpr (TM == 2) {
+      for (int q = -1; q <= F; ++q)
+        load_hist_async<H, TY, NS>(sm, d, i0, j0, k0 + q, k0, kmax, U_PRE, V_PRE, W_PRE, T_PRE);
+      cp_async_wait<F - 1>();
+      __syncthreads();
+    }
     ring_wait<NS>(bars, k0 - 1, k0);
     ring_wait<NS>(bars, k0, k0);
   } else {
@@ -251,7 +286,10 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     // plane K+1+F goes into the slot of plane K-2, free since the barrier
     // that ended the previous iteration
     if constexpr (TMA) {
-      if (lead) load_plane_tma<TY, NS>(sm, bars, tm, i0, j0, K + 1 + F, k0, kmax);
+      if (lead) load_plane_tma<H, TY, NS, TM>(sm, bars, tm, i0, j0, K + 1 + F, k0, kmax);
+      if constexpr (TM == 2)
+        load_hist_async<H, TY, NS>(sm, d, i0, j0, K + 1 + F, k0, kmax, U_PRE, V_PRE, W_PRE,
+                                   T_PRE);
       ring_wait<NS>(bars, K + 1, k0);
     } else {
       load_plane<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, U, V, W, T, C1, U_PRE, V_PRE,
@@ -395,7 +433,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
 #undef AT
 #undef C1AT
     }  // valid
-    if constexpr (!TMA) cp_async_wait<F - 1>();
+    if constexpr (TM != 1) cp_async_wait<F - 1>();
     __syncthreads();
   }
 }
@@ -414,27 +452,28 @@ static bool mask_map(CUtensorMap* m, const Dims& d, const void* p, int by) {
                        by, 1);
 }
 
-template <class H, class CT, int TY, int NS, int MINB, bool TMA = false>
+template <class H, class CT, int TY, int NS, int MINB, int TM = 0>
 static bool rhs_go(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                    const double* u, const double* v, const double* w, const double* T,
                    const H* u_ta, const H* v_ta, const H* w_ta, H* u_pre, H* v_pre, H* w_pre,
                    H* T_pre, const double* c1, H* u_a, H* v_a, H* w_a, H* u_T, cudaStream_t s) {
   RhsMaps tm;
-  size_t smem = (size_t)NS * RhsLay<H, TY, TMA>::SLOT;
-  if constexpr (TMA) {
+  memset(&tm, 0, sizeof(tm));
+  size_t smem = (size_t)NS * RhsLay<H, TY, TM>::SLOT;
+  if constexpr (TM != 0) {
     const void* f[4] = {u, v, w, T};
     const void* h[4] = {u_pre, v_pre, w_pre, T_pre};
     bool ok = mask_map(&tm.m[4], d, c1, TY + 2);
-    for (int q = 0; q < 4; ++q)
-      ok = ok && ring_map(&tm.m[q], d, f[q], SXW, TY + 2) && ring_map(&tm.m[5 + q], d, h[q], SXW, TY);
+    for (int q = 0; q < 4; ++q) {
+      ok = ok && ring_map(&tm.m[q], d, f[q], SXW, TY + 2);
+      if constexpr (TM == 1) ok = ok && ring_map(&tm.m[5 + q], d, h[q], SXW, TY);
+    }
     if (!ok) return false;
     smem += NS * sizeof(uint64_t);
-  } else {
-    memset(&tm, 0, sizeof(tm));
   }
   dim3 block(TXW, TY, 1);
   dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KCHUNK - 1) / KCHUNK);
-  auto kern = k_rhs_fast<H, CT, TY, NS, MINB, TMA>;
+  auto kern = k_rhs_fast<H, CT, TY, NS, MINB, TM>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   kern<<<grid, block, smem, s>>>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre, w_pre,
@@ -444,12 +483,12 @@ static bool rhs_go(const Dims& d, const GridDev& g, const GridRcp& rg, const Ste
 
 // launch shape: 0 the storage type's default (RhsShape), 1 32x4 tiles with a
 // 4-plane ring and four CTAs per SM, 2 32x8 tiles with a 5-plane ring and two
-// CTAs per SM, 3 32x8 tiles with a 4-plane ring and two CTAs per SM; FP64
-// storage and arithmetic also the TMA ring: 4 32x4 tiles with 5 planes and
-// three CTAs per SM, 5 32x4 with 4 planes and four CTAs, 6 32x8 with 4
-// planes and two CTAs (every shape computes each cell the same way; the
-// context's autotuner picks one; a TMA shape whose maps cannot be made runs
-// the default)
+// CTAs per SM, 3 32x8 tiles with a 4-plane ring and two CTAs per SM; the TMA
+// ring (every field in FP64 storage; the halo planes, with cp.async history
+// tiles, in FP32 storage): 4 32x4 tiles with 5 planes and three CTAs per SM,
+// 5 32x4 with 4 planes and four CTAs, 6 32x8 with 4 planes and two CTAs
+// (every shape computes each cell the same way; the context's autotuner
+// picks one; a TMA shape whose maps cannot be made runs the default)
 template <class H, class CT>
 static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const StepParams& sp,
                      const double* u, const double* v, const double* w, const double* T,
@@ -460,10 +499,11 @@ static void rhs_fast(const Dims& d, const GridDev& g, const GridRcp& rg, const S
 #define NSE_RHS_GO(TY_, NS_, MB_)                                                           \
   rhs_go<H, CT, TY_, NS_, MB_>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre, v_pre,    \
                                w_pre, T_pre, c1, u_a, v_a, w_a, u_T, s)
+  constexpr int TM = sizeof(H) == 8 ? 1 : 2;
 #define NSE_RHS_TMA(TY_, NS_, MB_)                                                              \
-  done = rhs_go<H, CT, TY_, NS_, MB_, true>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre,  \
-                                            v_pre, w_pre, T_pre, c1, u_a, v_a, w_a, u_T, s)
-  if constexpr (sizeof(H) == 8 && sizeof(CT) == 8) {
+  done = rhs_go<H, CT, TY_, NS_, MB_, TM>(d, g, rg, sp, u, v, w, T, u_ta, v_ta, w_ta, u_pre,    \
+                                          v_pre, w_pre, T_pre, c1, u_a, v_a, w_a, u_T, s)
+  {
     bool done = false;
     if (shape == 4) NSE_RHS_TMA(4, 5, 3);
     else if (shape == 5) NSE_RHS_TMA(4, 4, 4);

@@ -2342,7 +2342,7 @@ static void autotune_rhs(nse_ctx* x, const StepParams& sp) {
   const double* c1 = F(x, NSE_CELLVALUE);
   int best = 0;
   float best_ms = 1e30f;
-  const int nshape = x->mixed ? 4 : 7;  // shapes 4-6: the FP64 TMA ring
+  const int nshape = 7;  // shapes 4-6: the TMA rings
   for (int shape = 0; shape < nshape; ++shape) {
     auto run = [&]() {
       if (x->mixed)
