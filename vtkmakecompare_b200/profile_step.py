@@ -29,6 +29,9 @@ def main():
     ap.add_argument("--adjoint", type=int, default=0)
     ap.add_argument("--flags", type=int, default=0,
                     help="extra nse_config flags (e.g. 256 = NSE_FLAG_POISSON3)")
+    ap.add_argument("--shapes", type=int, nargs=2, default=[-1, -1],
+                    help="right-hand-side and correction launch shapes (nse_ctx_set_shapes; "
+                         "-1: autotuned), so a profiler sees no tuning launches of them")
     a = ap.parse_args()
     nx, ny, nz = a.grid
     g = W.grid_arrays(nx, ny, nz, 2 * math.pi, 2.0, math.pi, y0=-1.0, gamma=2.0)
@@ -43,6 +46,7 @@ def main():
             ctx.upload(k, f[k])
         ctx.levelset(W.sphere_phi0(g, (math.pi, 0.0, math.pi / 2), 0.25), width=1.5,
                      want_phi=False)
+        ctx.set_shapes(*a.shapes)
         ctx.project()
         ctx.start()
         ctx.step(a.warmup)
