@@ -858,8 +858,9 @@ static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, cons
 // 5-plane ring and two CTAs per SM, 2 32x4 tiles with 4 planes and four CTAs,
 // 3 32x8 tiles with 4 planes and three CTAs; FP64 storage also the TMA ring:
 // 4 32x4 tiles with 4 planes and five CTAs per SM, 5 32x4 with 5 planes and
-// four CTAs, 6 32x8 with 4 planes and three CTAs (each cell computed the same
-// way; a TMA shape whose maps cannot be made runs the default)
+// four CTAs, 6 32x8 with 4 planes and three CTAs, 7 32x4 with 7 planes and
+// three CTAs, 8 32x4 with 6 planes and three CTAs (each cell computed the
+// same way; a TMA shape whose maps cannot be made runs the default)
 template <class H>
 static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                          const H* vt, const H* wt, double* p, double* u, double* v, double* w,
@@ -877,6 +878,8 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
     if (shape == 4) NSE_CORR_TMA(4, 4, 5);
     else if (shape == 5) NSE_CORR_TMA(4, 5, 4);
     else if (shape == 6) NSE_CORR_TMA(8, 4, 3);
+    else if (shape == 7) NSE_CORR_TMA(4, 7, 3);
+    else if (shape == 8) NSE_CORR_TMA(4, 6, 3);
   }
 #undef NSE_CORR_TMA
   if (!done && shape >= 4) shape = 0;
