@@ -26,6 +26,7 @@ SOURCES = {
     "k_lines_fast.cu": [],
     "k_lines_part.cu": [],
     "k_rhs_fast.cu": [],
+    "k_rhs_f32.cu": ["--fmad=false"],
     "k_fft.cu": [],
     "k_poisson2d.cu": [],
     "noalloc.cu": [],
@@ -54,6 +55,7 @@ def build(verbose=False, extra=()):
     os.makedirs(BUILD, exist_ok=True)
     headers = [os.path.join(CSRC, "common.cuh"), os.path.join(CSRC, "k_lines.cuh"),
                os.path.join(CSRC, "fft_core.cuh"), os.path.join(CSRC, "tma.cuh"),
+               os.path.join(CSRC, "k_rhs_fast.cuh"),
                os.path.join(CSRC, "k_adjoint.cuh"),
                os.path.join(HERE, "..", "include", "nsegpu.h")]
     jobs = []

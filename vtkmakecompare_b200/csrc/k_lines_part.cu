@@ -401,6 +401,21 @@ struct XTab {
   __device__ R qq(int r) const { return v(XT_ROW + 5 * (r - 1) + 4); }
 };
 
+// The x solver's arithmetic with every rounding spelled out: products and
+// sums the compiler may fuse differently in each template instantiation
+// (one or two lines per warp iteration schedule differently) are written as
+// explicit fused or separately rounded operations, so every NL gives the
+// same bits.
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+// mul1 (see above) with its rounding spelled out
+__device__ __forceinline__ double xmul1(double a, double v) { return __dmul_rn(a, v); }
+__device__ __forceinline__ float xmul1(float a, float dv) { return __fmaf_rn(a, dv, a); }
+
 // NL lines per warp iteration share every table load (the table reads, not
 // the line data, dominate the L1 traffic of this kernel)
 // (with PL = 16 the two half-warps work on different lines)
@@ -482,8 +497,8 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
         for (int r = 0; r < M; ++r) {
           const R xm = r == 0 ? left : xr[q][r > 0 ? r - 1 : 0];
           const R xp = r == M - 1 ? right : xr[q][r + 1 < M ? r + 1 : M - 1];
-          x[q][r] = -(tb.v(NV + 3 * r) * xm + tb.v(NV + 3 * r + 1) * xr[q][r] +
-                      tb.v(NV + 3 * r + 2) * xp);
+          x[q][r] = -xfma(tb.v(NV + 3 * r + 2), xp,
+                          xfma(tb.v(NV + 3 * r + 1), xr[q][r], xmul(tb.v(NV + 3 * r), xm)));
         }
       }
     }
@@ -495,14 +510,14 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
     for (int r = 2; r <= M - 2; ++r) {
       const R w = tb.w(r);
 #pragma unroll
-      for (int q = 0; q < NL; ++q) { gp[q] = x[q][r] - w * gp[q]; x[q][r] = gp[q]; }
+      for (int q = 0; q < NL; ++q) { gp[q] = xfma(-w, gp[q], x[q][r]); x[q][r] = gp[q]; }
     }
 #pragma unroll
     for (int r = M - 2; r >= 1; --r) {
       const R rb = tb.rb(r), cc = tb.cc(r);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        R v = (r == M - 2) ? mul1(x[q][r], rb) : mul1(x[q][r] - cc * gp[q], rb);
+        R v = xmul1((r == M - 2) ? x[q][r] : xfma(-cc, gp[q], x[q][r]), rb);
         x[q][r] = v;
         gp[q] = v;
       }
@@ -513,9 +528,10 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
       const R cf = tb.v(XT_CF), ae = tb.v(XT_AE), mu = tb.v(XT_MU), nu = tb.v(XT_NU);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        rhsF[q] = x[q][0] - cf * x[q][1];
-        const R rhsE = x[q][M - 1] - ae * x[q][M - 2];
-        rho[q] = rhsE + mu * rhsF[q] + nu * __shfl_sync(FULL, rhsF[q], (lane + 1) & (PL - 1), PL);
+        rhsF[q] = xfma(-cf, x[q][1], x[q][0]);
+        const R rhsE = xfma(-ae, x[q][M - 2], x[q][M - 1]);
+        rho[q] = xfma(nu, __shfl_sync(FULL, rhsF[q], (lane + 1) & (PL - 1), PL),
+                      xfma(mu, rhsF[q], rhsE));
       }
     }
 #pragma unroll
@@ -526,7 +542,7 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
       for (int q = 0; q < NL; ++q) {
         const R rm = __shfl_sync(FULL, rho[q], (lane - sft) & (PL - 1), PL);
         const R rp = __shfl_sync(FULL, rho[q], (lane + sft) & (PL - 1), PL);
-        rho[q] = rho[q] + k1 * rm + k2 * rp;
+        rho[q] = xfma(k2, rp, xfma(k1, rm, rho[q]));
       }
     }
     {
@@ -534,9 +550,10 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
       const R lfr = tb.v(XT_LFR), ufr = tb.v(XT_UFR);
 #pragma unroll
       for (int q = 0; q < NL; ++q) {
-        const R E = mul1(rho[q], lam) + kap * __shfl_sync(FULL, rho[q], lane ^ (PL / 2), PL);
+        const R E = xfma(kap, __shfl_sync(FULL, rho[q], lane ^ (PL / 2), PL),
+                         xmul1(rho[q], lam));
         const R Em = __shfl_sync(FULL, E, (lane - 1) & (PL - 1), PL);
-        const R F = mul1(rhsF[q], rdf) + lfr * Em + ufr * E;
+        const R F = xfma(ufr, E, xfma(lfr, Em, xmul1(rhsF[q], rdf)));
         rhsF[q] = F;
         rho[q] = E;
       }
@@ -545,7 +562,7 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
     for (int r = 1; r < M - 1; ++r) {
       const R pp = tb.pp(r), qq = tb.qq(r);
 #pragma unroll
-      for (int q = 0; q < NL; ++q) x[q][r] = x[q][r] + pp * rhsF[q] + qq * rho[q];
+      for (int q = 0; q < NL; ++q) x[q][r] = xfma(qq, rho[q], xfma(pp, rhsF[q], x[q][r]));
     }
 #pragma unroll
     for (int q = 0; q < NL; ++q) {
@@ -553,7 +570,7 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
       x[q][M - 1] = rho[q];
       if constexpr (INC) {
 #pragma unroll
-        for (int r = 0; r < M; ++r) x[q][r] = xr[q][r] + x[q][r];
+        for (int r = 0; r < M; ++r) x[q][r] = xadd(xr[q][r], x[q][r]);
       }
       if (!ok[q]) continue;
       if (M % 2 == 0) {
