@@ -736,6 +736,27 @@ def run_ours(args, rank, world, local_rank):
     pms = max_over_ranks(p0.elapsed_time(p1)) / npois
     Hs = (NX // 2 + 1) * NY * NZ
     BP = 2 * 8 * NX * NY * NZ + 4 * 16 * Hs
+    # the opt-in solves on the same right-hand side (one GPU only): the SPN
+    # through TMA tiles and the three-pass solve
+    pvar = {}
+    if world == 1:
+        for name, flag in (("spn_tma", S.FLAG_SPN_TMA), ("three_pass", S.FLAG_POISSON3)):
+            vcfg = S.Config(NX, NY, NZ, 1.0, 1.0, 1.0, 0.0, 2 * math.pi, 2.0, math.pi, y0=-1.0,
+                            ystretch=2.0, flags=flag)
+            with S.Context(vcfg) as vc:
+                vc.set_stream(stream.cuda_stream)
+                vc.upload("phi", W.poisson_rhs(g, 7))
+                vc.poisson()
+                torch.cuda.synchronize()
+                p0.record(stream)
+                for _ in range(npois):
+                    vc.poisson()
+                p1.record(stream)
+                torch.cuda.synchronize()
+                vms = p0.elapsed_time(p1) / npois
+                vc.sync()
+            pvar[name] = {"ms_per_solve": round(vms, 4),
+                          "frac_of_hbm": round(BP / (vms / 1e3) / 1e9 / peaks()[0], 4)}
 
     # ------------------------------------------------------------------ e2e
     # the job through the public API from pinned host buffers: upload the
@@ -827,6 +848,8 @@ def run_ours(args, rank, world, local_rank):
     poisson = {"solves_per_s": round(world * 1e3 / pms, 2), "ms_per_solve": round(pms, 4),
                "algorithmic_bytes": BP, "gbs": round(BP / (pms / 1e3) / 1e9, 1),
                "frac_of_hbm": round(BP / (pms / 1e3) / 1e9 / peak, 4)}
+    if pvar:
+        poisson["opt_in_solves"] = pvar
     line = {
         "metric": METRIC,
         "value": round(steps_s, 3),
