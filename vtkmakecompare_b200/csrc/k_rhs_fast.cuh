@@ -245,6 +245,14 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
   const int kmax = k1 + 1;  // last plane any iteration reads
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + NS * Lay::SLOT);
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
+  // the chunk's z spacings and reciprocals (planes k0-1 .. k0+KCHUNK), staged
+  // once instead of loaded per plane; the barrier before the march publishes
+  // them
+  __shared__ double zt[3][KCHUNK + 2];
+  for (int t = threadIdx.y * TXW + threadIdx.x; t < 3 * (KCHUNK + 2); t += TXW * TY) {
+    const int q = t / (KCHUNK + 2), kk = k0 - 1 + t % (KCHUNK + 2);
+    if (kk <= d.nz + 1) zt[q][t % (KCHUNK + 2)] = q == 0 ? g.dz[kk] : q == 1 ? rg.rdz[kk] : rg.rdz12[kk];
+  }
   if constexpr (TMA) {
     // the copies need 128-byte aligned buffers and a 64-byte aligned map; a
     // launch that finds otherwise records the error (its cells then read
@@ -318,9 +326,10 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
       const double* pc = reinterpret_cast<const double*>(sm + slot_of(K) * SB);
       const double* pp = reinterpret_cast<const double*>(sm + slot_of(K + 1) * SB);
       const long c = d.P(I, J, K);
-      const R dz = LD(g.dz, K), dzp = LD(g.dz, K + 1), dzm = LD(g.dz, K - 1);
-      const R rz = LD(rg.rdz, K), rzp = LD(rg.rdz, K + 1);
-      const R rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
+      const int kz = K - k0 + 1;  // plane K in the staged z tables
+      const R dz = zt[0][kz], dzp = zt[0][kz + 1], dzm = zt[0][kz - 1];
+      const R rz = zt[1][kz], rzp = zt[1][kz + 1];
+      const R rz12 = zt[2][kz], rz12m = zt[2][kz - 1];
       // neighbourhood from shared memory (field f at offset f*PLANE), each
       // component's values loaded where they are used: short live ranges keep
       // the register count low
