@@ -180,10 +180,14 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
   // the chunk's z reciprocals (planes k0-1 .. k0+CKCHUNK), staged once; the
   // barrier before the march publishes them
   __shared__ double zt[2][CKCHUNK + 2];
-  for (int t = threadIdx.y * TXW + threadIdx.x; t < 2 * (CKCHUNK + 2); t += TXW * TY) {
-    const int q = t / (CKCHUNK + 2), kk = k0 - 1 + t % (CKCHUNK + 2);
-    if (kk <= d.nz + 1) zt[q][t % (CKCHUNK + 2)] = q == 0 ? rg.rdz[kk] : rg.rdz12[kk];
-  }
+  // (issued after the prologue's copies, so the ring fills while these
+  // few loads are in flight)
+  auto stage_z = [&]() {
+    for (int t = threadIdx.y * TXW + threadIdx.x; t < 2 * (CKCHUNK + 2); t += TXW * TY) {
+      const int q = t / (CKCHUNK + 2), kk = k0 - 1 + t % (CKCHUNK + 2);
+      if (kk <= d.nz + 1) zt[q][t % (CKCHUNK + 2)] = q == 0 ? rg.rdz[kk] : rg.rdz12[kk];
+    }
+  };
   if constexpr (TMA) {
     const bool aligned = ((smem_u32(sm) & 127) == 0) &&
                          ((reinterpret_cast<uintptr_t>(&tm.m[0]) & 63) == 0);
@@ -197,11 +201,14 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     if (lead)
       for (int q = -1; q <= F; ++q)
         load_plane_c_tma<TY, NS>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
+    stage_z();
+    __syncthreads();
     ring_wait<NS>(bars, k0 - 1, k0);
     ring_wait<NS>(bars, k0, k0);
   } else {
     for (int q = -1; q <= F; ++q)
       load_plane_c<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
+    stage_z();
     cp_async_wait<F - 1>();
     __syncthreads();
   }

@@ -249,10 +249,14 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
   // once instead of loaded per plane; the barrier before the march publishes
   // them
   __shared__ double zt[3][KCHUNK + 2];
-  for (int t = threadIdx.y * TXW + threadIdx.x; t < 3 * (KCHUNK + 2); t += TXW * TY) {
-    const int q = t / (KCHUNK + 2), kk = k0 - 1 + t % (KCHUNK + 2);
-    if (kk <= d.nz + 1) zt[q][t % (KCHUNK + 2)] = q == 0 ? g.dz[kk] : q == 1 ? rg.rdz[kk] : rg.rdz12[kk];
-  }
+  // (issued after the prologue's copies, so the ring fills while these
+  // few loads are in flight)
+  auto stage_z = [&]() {
+    for (int t = threadIdx.y * TXW + threadIdx.x; t < 3 * (KCHUNK + 2); t += TXW * TY) {
+      const int q = t / (KCHUNK + 2), kk = k0 - 1 + t % (KCHUNK + 2);
+      if (kk <= d.nz + 1) zt[q][t % (KCHUNK + 2)] = q == 0 ? g.dz[kk] : q == 1 ? rg.rdz[kk] : rg.rdz12[kk];
+    }
+  };
   if constexpr (TMA) {
     // the copies need 128-byte aligned buffers and a 64-byte aligned map; a
     // launch that finds otherwise records the error (its cells then read
@@ -270,12 +274,12 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     if (lead)
       for (int q = -1; q <= F; ++q)
         load_plane_tma<H, TY, NS, TM>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
-    if constexpr (TM == 2) {
+    if constexpr (TM == 2)
       for (int q = -1; q <= F; ++q)
         load_hist_async<H, TY, NS>(sm, d, i0, j0, k0 + q, k0, kmax, U_PRE, V_PRE, W_PRE, T_PRE);
-      cp_async_wait<F - 1>();
-      __syncthreads();
-    }
+    stage_z();
+    if constexpr (TM == 2) cp_async_wait<F - 1>();
+    __syncthreads();
     ring_wait<NS>(bars, k0 - 1, k0);
     ring_wait<NS>(bars, k0, k0);
   } else {
@@ -283,6 +287,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_rhs_fast(
     for (int q = -1; q <= F; ++q)
       load_plane<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, U, V, W, T, C1, U_PRE, V_PRE, W_PRE,
                             T_PRE);
+    stage_z();
     cp_async_wait<F - 1>();
     __syncthreads();
   }
