@@ -151,11 +151,21 @@ __device__ void partition_rows(const Line& L, int s, int e, double* W, double* R
 }  // namespace
 
 // ===================================================== y and z line tables
-// layout (nu unknowns, P partitions, R = 2P reduced unknowns):
-//   W, RB, CC, PP, QQ [nu] | CF, AE [P] | LL, RP, UU, ZZ [R] | bg, rden, fold0, foldN |
-//   MI [R x R] (inverse of the reduced system, row-major)
+// layout (nu unknowns, P partitions; value v of partition k at
+// T[5 nu + v P + k]):
+//   W, RB, CC, PP, QQ [nu] | CF, AE, MU, NU, K1 [4], K2 [4], LAM, KAP, RDF,
+//   LFR, UFR (per partition) | bg, rden, fold0, foldN
+// The reduced system of the partition end unknowns F(k) (first row) and E(k)
+// (last row) is solved as in the x tables: F eliminated, cyclic reduction
+// over the partitions on E (strides 1, 2, ..., P/4; the non-periodic lines
+// have zero couplings past their ends), the pair k, k ^ P/2 solved directly,
+// then F from E.
+enum {
+  YT_CF = 0, YT_AE, YT_MU, YT_NU, YT_K1, YT_K2 = YT_K1 + 4, YT_LAM = YT_K2 + 4, YT_KAP, YT_RDF,
+  YT_LFR, YT_UFR, YT_NV
+};
 __host__ __device__ size_t yz_table_stride(int nu, int P) {
-  return 5 * (size_t)nu + 2 * (size_t)P + 8 * (size_t)P + 4 + 4 * (size_t)P * P;
+  return 5 * (size_t)nu + (size_t)YT_NV * P + 4;
 }
 
 template <int DIR, int KIND>
@@ -163,99 +173,84 @@ __global__ void k_build_yz(Dims d, GridDev g, const double* c1, LineArgs a, cons
                            int count, int P, double* out) {
   const int line = blockIdx.x;
   const int lane = threadIdx.x;
-  if (line >= count) return;
+  if (line >= count || threadIdx.x >= 32) return;  // warp 0 builds the table (P <= 32)
   const bool masked = ids != nullptr;
   auto L = folded_line<DIR, KIND>(d, g, c1, a, masked ? ids[line] : 0, masked, false);
-  const int nu = L.nu, R = 2 * P;
+  const int nu = L.nu;
   double* T = out + (size_t)line * yz_table_stride(nu, P);
   double *W = T, *RB = T + nu, *CC = T + 2 * nu, *PP = T + 3 * nu, *QQ = T + 4 * nu;
-  double *CF = T + 5 * nu, *AE = CF + P, *LL = AE + P, *RP = LL + R, *UU = RP + R, *ZZ = UU + R;
-  double* cst = ZZ + R;
-  double* MI = cst + 4;
+  double* V = T + 5 * nu;  // V[v * P + k]
+  double* cst = V + YT_NV * P;
   const bool periodic = KIND >= LK_CYC_VEL;
-  if (lane < P) {
-    const int s = (int)((long)lane * nu / P), e = (int)((long)(lane + 1) * nu / P) - 1;
-    partition_rows(L, s, e, W, RB, CC, PP, QQ, 1);
-    double As, Bs, Cs, Ae, Be, Ce;
-    L.coef(s, As, Bs, Cs);
-    L.coef(e, Ae, Be, Ce);
-    CF[lane] = Cs;
-    AE[lane] = Ae;
-    // reduced rows: F row (couples E(k-1), F(k), E(k)), E row (F(k), E(k), F(k+1))
-    LL[2 * lane] = As;
-    RP[2 * lane] = Bs + Cs * PP[s + 1];
-    UU[2 * lane] = Cs * QQ[s + 1];
-    LL[2 * lane + 1] = Ae * PP[e - 1];
-    RP[2 * lane + 1] = Be + Ae * QQ[e - 1];
-    UU[2 * lane + 1] = Ce;
+  // lanes past P repeat partition P-1 (every lane takes part in the
+  // shuffles; only lanes < P store)
+  const bool own = lane < P;
+  const int k = own ? lane : P - 1;
+  const int s = (int)((long)k * nu / P), e = (int)((long)(k + 1) * nu / P) - 1;
+  if (own) partition_rows(L, s, e, W, RB, CC, PP, QQ, 1);
+  __syncwarp();
+  double As, Bs, Cs, Ae, Be, Ce;
+  L.coef(s, As, Bs, Cs);
+  L.coef(e, Ae, Be, Ce);
+  // F row: LF E(k-1) + DF F(k) + UF E(k); E row: LE F(k) + DE E(k) + UE F(k+1)
+  // (A of the first and C of the last unknown are zero on non-periodic lines)
+  const double LF = As, DF = Bs + Cs * PP[s + 1], UF = Cs * QQ[s + 1];
+  const double LE = Ae * PP[e - 1], DE = Be + Ae * QQ[e - 1], UE = Ce;
+  const unsigned FULL = 0xffffffffu;
+  const int kp = (k + 1) % P;
+  const double LF1 = __shfl_sync(FULL, LF, kp), DF1 = __shfl_sync(FULL, DF, kp);
+  const double UF1 = __shfl_sync(FULL, UF, kp);
+  // eliminate the F unknowns: al E(k-1) + be E(k) + ga E(k+1) = rho
+  double al = -LE * LF / DF;
+  double be = DE - LE * UF / DF - UE * LF1 / DF1;
+  double ga = -UE * UF1 / DF1;
+  if (own) {
+    V[YT_CF * P + k] = Cs;
+    V[YT_AE * P + k] = Ae;
+    V[YT_MU * P + k] = -LE / DF;
+    V[YT_NU * P + k] = -UE / DF1;
   }
-  __syncthreads();
+  for (int lv = 0; lv < 4; ++lv) {
+    if ((1 << lv) >= P / 2) {
+      if (own) V[(YT_K1 + lv) * P + k] = V[(YT_K2 + lv) * P + k] = 0.0;
+      continue;
+    }
+    const int sft = 1 << lv;
+    const int km = (k - sft + P) % P, kq = (k + sft) % P;
+    const double alm = __shfl_sync(FULL, al, km), bem = __shfl_sync(FULL, be, km);
+    const double gam = __shfl_sync(FULL, ga, km);
+    const double alp = __shfl_sync(FULL, al, kq), bep = __shfl_sync(FULL, be, kq);
+    const double gap = __shfl_sync(FULL, ga, kq);
+    const double k1 = -al / bem, k2 = -ga / bep;
+    if (own) {
+      V[(YT_K1 + lv) * P + k] = k1;
+      V[(YT_K2 + lv) * P + k] = k2;
+    }
+    const double nal = k1 * alm, nga = k2 * gap, nbe = be + k1 * gam + k2 * alp;
+    al = nal;
+    ga = nga;
+    be = nbe;
+  }
+  // rows k and k ^ P/2 now couple only each other
+  const int kx = k ^ (P / 2);
+  const double alx = __shfl_sync(FULL, al, kx), bex = __shfl_sync(FULL, be, kx);
+  const double gax = __shfl_sync(FULL, ga, kx);
+  const double a2 = al + ga;
+  const double det = be * bex - a2 * (alx + gax);
+  if (own) {
+    V[YT_LAM * P + k] = bex / det;
+    V[YT_KAP * P + k] = -a2 / det;
+    V[YT_RDF * P + k] = 1.0 / DF;
+    V[YT_LFR * P + k] = -LF / DF;
+    V[YT_UFR * P + k] = -UF / DF;
+  }
   if (lane == 0) {
     // fold constants: right-hand-side corrections of the first and last rows
     Row r1 = L.ref(1), rn = L.ref(nu);
+    cst[0] = 0.0;
+    cst[1] = 0.0;
     cst[2] = periodic ? 0.0 : r1.lo;
     cst[3] = periodic ? 0.0 : rn.up;
-    // factorisation of the reduced system (in place: LL <- multipliers,
-    // RP <- reciprocal pivots); periodic: Sherman-Morrison with gamma = -b0
-    double gam = 0.0, bcorner = 0.0, acorner = 0.0;
-    if (periodic) {
-      bcorner = LL[0];      // row 0 couples y(R-1)
-      acorner = UU[R - 1];  // row R-1 couples y(0)
-      gam = -RP[0];
-      RP[0] = RP[0] - gam;
-      RP[R - 1] = RP[R - 1] - acorner * bcorner / gam;
-    }
-    double piv = RP[0];
-    LL[0] = 0.0;
-    RP[0] = 1.0 / piv;
-    for (int r = 1; r < R; ++r) {
-      double l = LL[r] / piv;
-      piv = RP[r] - l * UU[r - 1];
-      LL[r] = l;
-      RP[r] = 1.0 / piv;
-    }
-    if (periodic) {
-      // z solves the modified system for u = (gam, 0, ..., 0, acorner)
-      double zf = gam;
-      ZZ[0] = zf;
-      for (int r = 1; r < R; ++r) {
-        zf = (r == R - 1 ? acorner : 0.0) - LL[r] * zf;
-        ZZ[r] = zf;
-      }
-      double zb = ZZ[R - 1] * RP[R - 1];
-      ZZ[R - 1] = zb;
-      for (int r = R - 2; r >= 0; --r) {
-        zb = (ZZ[r] - UU[r] * zb) * RP[r];
-        ZZ[r] = zb;
-      }
-      cst[0] = bcorner / gam;
-      cst[1] = 1.0 / (1.0 + ZZ[0] + bcorner * ZZ[R - 1] / gam);
-    } else {
-      for (int r = 0; r < R; ++r) ZZ[r] = 0.0;
-      cst[0] = 0.0;
-      cst[1] = 0.0;
-    }
-  }
-  __syncthreads();
-  // column c of the inverse: the reduced solve applied to the unit vector e_c
-  // (blockDim >= P; the columns are shared out over the threads)
-  for (int c = lane; c < R; c += blockDim.x) {
-    double y = (c == 0) ? 1.0 : 0.0;
-    MI[c] = y;
-    for (int r = 1; r < R; ++r) {
-      y = (r == c ? 1.0 : 0.0) - LL[r] * y;
-      MI[r * R + c] = y;
-    }
-    y = y * RP[R - 1];
-    MI[(R - 1) * R + c] = y;
-    for (int r = R - 2; r >= 0; --r) {
-      y = (MI[r * R + c] - UU[r] * y) * RP[r];
-      MI[r * R + c] = y;
-    }
-    if (periodic) {
-      const double fact = (y + cst[0] * MI[(R - 1) * R + c]) * cst[1];
-      for (int r = 0; r < R; ++r) MI[r * R + c] = MI[r * R + c] - fact * ZZ[r];
-    }
   }
 }
 
@@ -345,24 +340,27 @@ template <> struct Vec2T<double> { using T = double2; };
 template <> struct Vec2T<float> { using T = float2; };
 
 // Products with the table entries that are close to 1 (the reciprocal pivots
-// RB, the reduced-system factors LAM and RDF and the diagonal of the reduced
-// inverse: near-identity systems, dt/Re/dx^2 ~ 1e-3).  The FP32 tables hold
+// RB and the reduced-system factors LAM and RDF: near-identity systems,
+// dt/Re/dx^2 ~ 1e-3).  The FP32 tables hold
 // these entries as their deviation from 1, so a * v is formed as a + a * dv:
 // a table rounded to FP32 then carries a relative error of 6e-8 of the
 // deviation, not of 1, and the solve has no systematic bias of that size
 // (which every step would repeat).  FP64 tables hold the values themselves.
 __device__ __forceinline__ double mul1(double a, double v) { return a * v; }
 __device__ __forceinline__ float mul1(float a, float dv) { return a + a * dv; }
-// one term of the reduced inverse's row sum, F + m rc (the diagonal term
-// through mul1); in FP64 the product and the sum are rounded separately
-// (no contraction), so every y/z line kernel forms the same bits
-__device__ __forceinline__ double red_acc(double F, double rc, double m, bool diag) {
-  (void)diag;
-  return __dadd_rn(F, __dmul_rn(rc, m));
-}
-__device__ __forceinline__ float red_acc(float F, float rc, float m, bool diag) {
-  return F + (diag ? mul1(rc, m) : m * rc);
-}
+// The line solvers' arithmetic with every rounding spelled out: products and
+// sums the compiler may fuse differently in each template instantiation (the
+// launch shapes schedule differently) are written as explicit fused or
+// separately rounded operations, so every launch shape gives the same bits.
+__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
+__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
+__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
+__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
+__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
+__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
+// mul1 with its rounding spelled out
+__device__ __forceinline__ double xmul1(double a, double v) { return __dmul_rn(a, v); }
+__device__ __forceinline__ float xmul1(float a, float dv) { return __fmaf_rn(a, dv, a); }
 
 // interior Thomas on registers: g <- solution of the interior rows with
 // zero end values; rows r = 1..m-2 of the partition, table rows at tb(r).
@@ -373,13 +371,13 @@ __device__ __forceinline__ R interior_solve(R (&x)[MM], int m, const TB& tb) {
   R gp = x[1];
 #pragma unroll
   for (int r = 2; r < MM - 1; ++r)
-    if (r <= m - 2) { gp = x[r] - tb.w(r) * gp; x[r] = gp; }
+    if (r <= m - 2) { gp = xfma(-tb.w(r), gp, x[r]); x[r] = gp; }
   R gn = R(0), glast = R(0);
 #pragma unroll
   for (int r = MM - 2; r >= 1; --r)
     if (r <= m - 2) {
       // gn is still 0 at r = m-2, so this is x(m-2) * rb there
-      R v = mul1(x[r] - tb.cc(r) * gn, tb.rb(r));
+      R v = xmul1(xfma(-tb.cc(r), gn, x[r]), tb.rb(r));
       if (r == m - 2) glast = v;
       x[r] = v;
       gn = v;
@@ -400,21 +398,6 @@ struct XTab {
   __device__ R pp(int r) const { return v(XT_ROW + 5 * (r - 1) + 3); }
   __device__ R qq(int r) const { return v(XT_ROW + 5 * (r - 1) + 4); }
 };
-
-// The x solver's arithmetic with every rounding spelled out: products and
-// sums the compiler may fuse differently in each template instantiation
-// (one or two lines per warp iteration schedule differently) are written as
-// explicit fused or separately rounded operations, so every NL gives the
-// same bits.
-__device__ __forceinline__ double xfma(double a, double b, double c) { return __fma_rn(a, b, c); }
-__device__ __forceinline__ float xfma(float a, float b, float c) { return __fmaf_rn(a, b, c); }
-__device__ __forceinline__ double xmul(double a, double b) { return __dmul_rn(a, b); }
-__device__ __forceinline__ float xmul(float a, float b) { return __fmul_rn(a, b); }
-__device__ __forceinline__ double xadd(double a, double b) { return __dadd_rn(a, b); }
-__device__ __forceinline__ float xadd(float a, float b) { return __fadd_rn(a, b); }
-// mul1 (see above) with its rounding spelled out
-__device__ __forceinline__ double xmul1(double a, double v) { return __dmul_rn(a, v); }
-__device__ __forceinline__ float xmul1(float a, float dv) { return __fmaf_rn(a, dv, a); }
 
 // NL lines per warp iteration share every table load (the table reads, not
 // the line data, dominate the L1 traffic of this kernel)
@@ -617,6 +600,49 @@ struct YZTabAny {
   __device__ R pp(int r) const { return T[3 * nu + s + r]; }
   __device__ R qq(int r) const { return T[4 * nu + s + r]; }
 };
+// the reduced-system values of partition k (YT_* of the table layout)
+template <class R, bool LDG>
+struct YZRed {
+  const R* V;  // T + 5 nu
+  int P, k;
+  __device__ R v(int q) const { return LDG ? __ldg(V + q * P + k) : V[q * P + k]; }
+};
+
+// F and E of partition k for the LPB lines of a CTA (lane = line), from the
+// partition's reduced right-hand sides rhsF (first row) and rhsE (last row):
+// cyclic reduction over the P partitions through shared memory, xs two
+// buffers of P x LPB values.  Every thread of the CTA calls it (it holds the
+// CTA's barriers); lanes of invalid lines carry values nothing reads.
+template <int P, int LPB, class R, class RV>
+__device__ __forceinline__ void yz_reduced(R* xs, const RV& rv, int k, int lane, R rhsF, R rhsE,
+                                           R& F, R& E) {
+  R* b0 = xs;
+  R* b1 = xs + P * LPB;
+  b0[k * LPB + lane] = rhsF;
+  __syncthreads();
+  const R rhsF1 = b0[((k + 1) % P) * LPB + lane];
+  R rho = xfma(rv.v(YT_NU), rhsF1, xfma(rv.v(YT_MU), rhsF, rhsE));
+  R* cur = b1;
+#pragma unroll
+  for (int lv = 0; (1 << lv) < P / 2; ++lv) {
+    const int sft = 1 << lv;
+    cur[k * LPB + lane] = rho;
+    __syncthreads();
+    const R rm = cur[((k - sft + P) % P) * LPB + lane];
+    const R rp = cur[((k + sft) % P) * LPB + lane];
+    rho = xfma(rv.v(YT_K2 + lv), rp, xfma(rv.v(YT_K1 + lv), rm, rho));
+    cur = (cur == b0) ? b1 : b0;
+  }
+  cur[k * LPB + lane] = rho;
+  __syncthreads();
+  const R rx = cur[(k ^ (P / 2)) * LPB + lane];
+  E = xfma(rv.v(YT_KAP), rx, xmul1(rho, rv.v(YT_LAM)));
+  cur = (cur == b0) ? b1 : b0;
+  cur[k * LPB + lane] = E;
+  __syncthreads();
+  const R Em = cur[((k - 1 + P) % P) * LPB + lane];
+  F = xfma(rv.v(YT_UFR), E, xfma(rv.v(YT_LFR), Em, xmul1(rhsF, rv.v(YT_RDF))));
+}
 
 // LPB lines per CTA (adjacent in x; 16 lines keep two CTAs resident per SM).
 // The solution goes to `out` (type RO) when given, else back into f.
@@ -627,11 +653,10 @@ __global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yz
                                                       const int* __restrict__ slots,
                                                       const R* __restrict__ mtab, R ft, R fb,
                                                       int periodic) {
-  constexpr int R2 = 2 * P;
   // FP32 tables (mixed form): increment form, row coefficients after the
   // factorisation values (see line_coef_values)
   constexpr bool INC = sizeof(R) == 4;
-  __shared__ R red[R2 * LPB];
+  __shared__ R xs[2 * P * LPB];
   const int lane = threadIdx.x % LPB, k = threadIdx.x / LPB;
   const int i = 1 + blockIdx.x * LPB + lane;
   const int o = 1 + blockIdx.y;  // k of a y line, j of a z line
@@ -654,8 +679,8 @@ __global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yz
   YZTab<R> tb{T, nu, s};
   if (valid) {
     // right-hand-side folds of the boundary rows (zero for periodic lines)
-    const R c0 = (!periodic && k == 0) ? __ldg(T + 5 * nu + 10 * P + 2) * ft : R(0);
-    const R cN = (!periodic && k == P - 1) ? __ldg(T + 5 * nu + 10 * P + 3) * fb : R(0);
+    const R c0 = (!periodic && k == 0) ? __ldg(T + 5 * nu + YT_NV * P + 2) * ft : R(0);
+    const R cN = (!periodic && k == P - 1) ? __ldg(T + 5 * nu + YT_NV * P + 3) * fb : R(0);
     // every load is issued up front (rows past m re-read row m-1); the
     // right-hand side of row m-1 is loaded once more on its own, so no
     // register is selected by the run-time m
@@ -687,39 +712,32 @@ __global__ void __launch_bounds__(LPB * P, (YZMinB<LPB * P, MM, R>::value)) k_yz
           const R xm = r == 0 ? left : xr[r > 0 ? r - 1 : 0];
           const R xc = r == m - 1 ? xe : xr[r];
           const R xp = r == m - 1 ? right : xr[r + 1 < MM ? r + 1 : MM - 1];
-          const R sv = -(__ldg(CA + r) * xm + __ldg(CB + r) * xc + __ldg(CC + r) * xp);
+          const R sv = -xfma(__ldg(CC + r), xp, xfma(__ldg(CB + r), xc, xmul(__ldg(CA + r), xm)));
           if (r == m - 1) xe = sv;
           else x[r] = sv;
         }
       }
     }
   }
+  const YZRed<R, true> rv{T + 5 * nu, P, k};
+  R rhsF = R(0), rhsE = R(0);
   if (valid) {
     const R xe1 = interior_solve<MM>(x, m, tb);
-    red[(2 * k) * LPB + lane] = x[0] - __ldg(T + 5 * nu + k) * x[1];
-    red[(2 * k + 1) * LPB + lane] = xe - __ldg(T + 5 * nu + P + k) * xe1;
+    rhsF = xfma(-rv.v(YT_CF), x[1], x[0]);
+    rhsE = xfma(-rv.v(YT_AE), xe1, xe);
   }
-  __syncthreads();
+  R F, E;
+  yz_reduced<P, LPB>(xs, rv, k, lane, rhsF, rhsE, F, E);
   if (!valid) return;
-  // F and E of this partition: rows 2k and 2k+1 of the reduced inverse
-  const R* MI = T + 5 * nu + 10 * P + 4;
-  R F = R(0), E = R(0);
-#pragma unroll
-  for (int c = 0; c < R2; ++c) {
-    const R rc = red[c * LPB + lane];
-    const R mf = __ldg(MI + (2 * k) * R2 + c), me = __ldg(MI + (2 * k + 1) * R2 + c);
-    F = red_acc(F, rc, mf, c == 2 * k);
-    E = red_acc(E, rc, me, c == 2 * k + 1);
-  }
 #pragma unroll
   for (int r = 1; r < MM; ++r) {
-    if (r < m - 1) x[r] = x[r] + tb.pp(r) * F + tb.qq(r) * E;
+    if (r < m - 1) x[r] = xfma(tb.qq(r), E, xfma(tb.pp(r), F, x[r]));
     if (r == m - 1) x[r] = E;
   }
   x[0] = F;
   if constexpr (INC) {
 #pragma unroll
-    for (int r = 0; r < MM; ++r) x[r] = (r == m - 1 ? xer : xr[r]) + x[r];
+    for (int r = 0; r < MM; ++r) x[r] = xadd(r == m - 1 ? xer : xr[r], x[r]);
   }
   RO* dst = out ? out + off : reinterpret_cast<RO*>(f + off);
 #pragma unroll
@@ -749,14 +767,14 @@ __global__ void __launch_bounds__(16 * P, 2)
     k_yzlines_tma(const __grid_constant__ CUtensorMap tm, Dims d, int nu, int nother, int ntx,
                   const double* __restrict__ tab, const int* __restrict__ slots,
                   const double* __restrict__ mtab, double ft, double fb, int periodic) {
-  constexpr int LPB = 16, R2 = 2 * P;
+  constexpr int LPB = 16;
   extern __shared__ __align__(128) unsigned char ysm[];
   const size_t tb_bytes = yzt_tile_bytes(nu);
   double* buf0 = reinterpret_cast<double*>(ysm);
   double* buf1 = reinterpret_cast<double*>(ysm + tb_bytes);
-  double* red = reinterpret_cast<double*>(ysm + 2 * tb_bytes);  // [R2][LPB]
+  double* xs = reinterpret_cast<double*>(ysm + 2 * tb_bytes);  // [2][P][LPB]
   const size_t stride = yz_table_stride(nu, P);
-  double* stab = red + R2 * LPB;  // mask-free table
+  double* stab = xs + 2 * P * LPB;  // mask-free table
   uint64_t* bar = reinterpret_cast<uint64_t*>(stab + ((stride + 1) & ~(size_t)1));
   const int lane = threadIdx.x % LPB, k = threadIdx.x / LPB;
   const long ntiles = (long)ntx * nother;
@@ -813,27 +831,21 @@ __global__ void __launch_bounds__(16 * P, 2)
     YZTabAny<double> tb{T, nu, s};
     double x[MM];
     const double* col = cur + (size_t)s * LPB + lane;
-    const double c0 = (!periodic && k == 0) ? T[5 * nu + 10 * P + 2] * ft : 0.0;
-    const double cN = (!periodic && k == P - 1) ? T[5 * nu + 10 * P + 3] * fb : 0.0;
+    const double c0 = (!periodic && k == 0) ? T[5 * nu + YT_NV * P + 2] * ft : 0.0;
+    const double cN = (!periodic && k == P - 1) ? T[5 * nu + YT_NV * P + 3] * fb : 0.0;
 #pragma unroll
     for (int r = 0; r < MM; ++r) x[r] = col[(size_t)min(r, m - 1) * LPB];
     x[0] = x[0] - c0;
     const double xe = col[(size_t)(m - 1) * LPB] - cN;
     const double xe1 = interior_solve<MM>(x, m, tb);
-    red[(2 * k) * LPB + lane] = x[0] - T[5 * nu + k] * x[1];
-    red[(2 * k + 1) * LPB + lane] = xe - T[5 * nu + P + k] * xe1;
-    __syncthreads();
-    const double* MI = T + 5 * nu + 10 * P + 4;
-    double F = 0.0, E = 0.0;
-#pragma unroll
-    for (int c = 0; c < R2; ++c) {
-      const double rc = red[c * LPB + lane];
-      F = red_acc(F, rc, MI[(2 * k) * R2 + c], c == 2 * k);
-      E = red_acc(E, rc, MI[(2 * k + 1) * R2 + c], c == 2 * k + 1);
-    }
+    const YZRed<double, false> rv{T + 5 * nu, P, k};
+    const double rhsF = xfma(-rv.v(YT_CF), x[1], x[0]);
+    const double rhsE = xfma(-rv.v(YT_AE), xe1, xe);
+    double F, E;
+    yz_reduced<P, LPB>(xs, rv, k, lane, rhsF, rhsE, F, E);
 #pragma unroll
     for (int r = 1; r < MM; ++r) {
-      if (r < m - 1) x[r] = x[r] + tb.pp(r) * F + tb.qq(r) * E;
+      if (r < m - 1) x[r] = xfma(tb.qq(r), E, xfma(tb.pp(r), F, x[r]));
       if (r == m - 1) x[r] = E;
     }
     x[0] = F;
@@ -844,7 +856,7 @@ __global__ void __launch_bounds__(16 * P, 2)
         if (r < m) dst[(size_t)r * LPB] = x[r];
     }
     fence_async_smem();
-    __syncthreads();  // the tile is complete; red may be rewritten
+    __syncthreads();  // the tile is complete; the exchange buffers may be rewritten
     if (threadIdx.x == 0) {
       const int x0 = (int)(q % ntx) * LPB;
       if (DIR == 1) tma_store_3d(&tm, x0, 1, o, cur);
@@ -1150,8 +1162,8 @@ void launch_round_table(const double* in, float* out, long n, cudaStream_t s) {
 
 // FP32 line tables of the mixed form.  Each FP32 table is the FP64 table
 // rounded, with the entries close to 1 stored as their deviation from 1 (see
-// mul1: x tables RB of every row, LAM, RDF; y/z tables RB of every unknown and
-// the reduced inverse's diagonal), followed by the row coefficients of the
+// mul1: x tables RB of every row, LAM, RDF; y/z tables RB of every unknown,
+// LAM and RDF of every partition), followed by the row coefficients of the
 // increment form: A (to the previous unknown), B - 1, C (to the next) of
 // every unknown, FP64 values rounded once.  x tables: value NV + 3r + c of
 // lane k (unknown k*M + r) at [(NV + 3r + c) * PL + k]; y/z tables:
@@ -1171,8 +1183,8 @@ __global__ void k_round_line_table(const double* __restrict__ in, float* __restr
       const int v = (int)(o / PL);
       near1 = v == XT_LAM || v == XT_RDF || (v >= XT_ROW && (v - XT_ROW) % 5 == 1);
     } else {
-      const long mi = 5L * nu + 10L * P + 4, r2 = 2L * P;
-      near1 = (o >= nu && o < 2L * nu) || (o >= mi && (o - mi) / r2 == (o - mi) % r2);
+      const long vl = 5L * nu + (long)YT_LAM * P, vr = 5L * nu + (long)YT_RDF * P;
+      near1 = (o >= nu && o < 2L * nu) || (o >= vl && o < vl + P) || (o >= vr && o < vr + P);
     }
     out[line * stride32 + o] = near1 ? (float)(in[t] - 1.0) : (float)in[t];
   }

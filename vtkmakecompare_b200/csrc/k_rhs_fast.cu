@@ -177,17 +177,6 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
   const int kmax = k1 + 1;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + NS * Lay::SLOT);
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
-  // the chunk's z reciprocals (planes k0-1 .. k0+CKCHUNK), staged once; the
-  // barrier before the march publishes them
-  __shared__ double zt[2][CKCHUNK + 2];
-  // (issued after the prologue's copies, so the ring fills while these
-  // few loads are in flight)
-  auto stage_z = [&]() {
-    for (int t = threadIdx.y * TXW + threadIdx.x; t < 2 * (CKCHUNK + 2); t += TXW * TY) {
-      const int q = t / (CKCHUNK + 2), kk = k0 - 1 + t % (CKCHUNK + 2);
-      if (kk <= d.nz + 1) zt[q][t % (CKCHUNK + 2)] = q == 0 ? rg.rdz[kk] : rg.rdz12[kk];
-    }
-  };
   if constexpr (TMA) {
     const bool aligned = ((smem_u32(sm) & 127) == 0) &&
                          ((reinterpret_cast<uintptr_t>(&tm.m[0]) & 63) == 0);
@@ -201,14 +190,11 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     if (lead)
       for (int q = -1; q <= F; ++q)
         load_plane_c_tma<TY, NS>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
-    stage_z();
-    __syncthreads();
     ring_wait<NS>(bars, k0 - 1, k0);
     ring_wait<NS>(bars, k0, k0);
   } else {
     for (int q = -1; q <= F; ++q)
       load_plane_c<H, TY, NS>(sm, d, i0, j0, k0 + q, kmax, PHI, UT, VT, WT, u_ta, v_ta, w_ta);
-    stage_z();
     cp_async_wait<F - 1>();
     __syncthreads();
   }
@@ -241,8 +227,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
 #define PH(pl, dxo, dyo) (pl)[e0 + (dyo) * SXW + (dxo)]
 #define FL(pl, f, dxo, dyo) (double)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
       const long c = d.P(I, J, K);
-      const int kz = K - k0 + 1;  // plane K in the staged z tables
-      const double rz = zt[0][kz], rz12 = zt[1][kz], rz12m = zt[1][kz - 1];
+      const double rz = LD(rg.rdz, K), rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
       const double ph = PH(qc, 0, 0), phx = PH(qc, 1, 0), phy = PH(qc, 0, 1), phz = PH(qp, 0, 0),
                    phxm = PH(qc, -1, 0), phym = PH(qc, 0, -1), phzm = PH(qm, 0, 0);
       const double gx = (phx - ph) * rx12, gy = (phy - ph) * ry12, gz = (phz - ph) * rz12;
