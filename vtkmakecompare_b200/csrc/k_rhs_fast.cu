@@ -157,7 +157,7 @@ __device__ __forceinline__ void load_plane_c_tma(char* sm, uint64_t* bars, const
     tma_load_3d(slot + 4 * L::FP + f * L::HS, &tm.m[4 + f], i0 - 1, j0, K, bar);
 }
 
-template <class H, int TY, int NS, int MINB, bool TMA>
+template <class H, int TY, int NS, int MINB, bool TMA, int KC = CKCHUNK>
 __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     Dims d, GridRcp rg, const double* __restrict__ PHI, const H* __restrict__ UT,
     const H* __restrict__ VT, const H* __restrict__ WT, double* __restrict__ p,
@@ -172,8 +172,8 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
   const bool valid = (I <= d.nx) && (J <= d.ny);
-  const int k0 = 1 + blockIdx.z * CKCHUNK;
-  const int k1 = min(d.nz, k0 + CKCHUNK - 1);
+  const int k0 = 1 + blockIdx.z * KC;
+  const int k1 = min(d.nz, k0 + KC - 1);
   const int kmax = k1 + 1;
   uint64_t* bars = reinterpret_cast<uint64_t*>(sm + NS * Lay::SLOT);
   const bool lead = threadIdx.x == 0 && threadIdx.y == 0;
@@ -292,7 +292,7 @@ __global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ P
   w_ta[c] = (H)(dt * gz);
 }
 
-template <class H, int TY, int NS, int MINB, bool TMA = false>
+template <class H, int TY, int NS, int MINB, bool TMA = false, int KC = CKCHUNK>
 static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                        const H* vt, const H* wt, double* p, double* u, double* v, double* w,
                        H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
@@ -309,8 +309,8 @@ static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, cons
     memset(&tm, 0, sizeof(tm));
   }
   dim3 block(TXW, TY, 1);
-  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + CKCHUNK - 1) / CKCHUNK);
-  auto kern = k_correct_pipe<H, TY, NS, MINB, TMA>;
+  dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KC - 1) / KC);
+  auto kern = k_correct_pipe<H, TY, NS, MINB, TMA, KC>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   kern<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,
@@ -323,8 +323,10 @@ static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, cons
 // 3 32x8 tiles with 4 planes and three CTAs; FP64 storage also the TMA ring:
 // 4 32x4 tiles with 4 planes and five CTAs per SM, 5 32x4 with 5 planes and
 // four CTAs, 6 32x8 with 4 planes and three CTAs, 7 32x4 with 7 planes and
-// three CTAs, 8 32x4 with 6 planes and three CTAs (each cell computed the
-// same way; a TMA shape whose maps cannot be made runs the default)
+// three CTAs, 8 32x4 with 6 planes and three CTAs, and with 16 z planes per
+// CTA instead of 8: 9 32x4 with 5 planes and four CTAs, 10 32x4 with 4 planes
+// and five CTAs (each cell computed the same way; a TMA shape whose maps
+// cannot be made runs the default)
 template <class H>
 static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                          const H* vt, const H* wt, double* p, double* u, double* v, double* w,
@@ -337,6 +339,9 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
 #define NSE_CORR_TMA(TY_, NS_, MB_)                                                          \
   done = correct_go<H, TY_, NS_, MB_, true>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
                                             w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
+#define NSE_CORR_TMA16(TY_, NS_, MB_)                                                            \
+  done = correct_go<H, TY_, NS_, MB_, true, 16>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
+                                                w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
   bool done = false;
   if constexpr (sizeof(H) == 8) {
     if (shape == 4) NSE_CORR_TMA(4, 4, 5);
@@ -344,8 +349,11 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
     else if (shape == 6) NSE_CORR_TMA(8, 4, 3);
     else if (shape == 7) NSE_CORR_TMA(4, 7, 3);
     else if (shape == 8) NSE_CORR_TMA(4, 6, 3);
+    else if (shape == 9) NSE_CORR_TMA16(4, 5, 4);
+    else if (shape == 10) NSE_CORR_TMA16(4, 4, 5);
   }
 #undef NSE_CORR_TMA
+#undef NSE_CORR_TMA16
   if (!done && shape >= 4) shape = 0;
   if (!done) switch (shape) {
     case 1: NSE_CORR_GO(8, 5, 2); break;
