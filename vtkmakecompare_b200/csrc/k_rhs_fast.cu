@@ -128,36 +128,66 @@ __device__ __forceinline__ void load_plane_c(char* sm, const Dims& d, int i0, in
   cp_async_commit();
 }
 
-// ring slot of the correction (in doubles): phi, then u*, v*, w* halo planes
-// and the old u_ta, v_ta, w_ta tiles; the TMA ring (FP64 storage) keeps every
-// buffer 128-byte aligned and its tiles 34 wide (box from x = i0-1)
-template <class H, int TY, bool TMA>
+// ring slot of the correction (in doubles): phi, then u*, v*, w* and the old
+// u_ta, v_ta, w_ta.  TM, the ring's fill: 0 cp.async (u*, v*, w* as halo
+// planes, the old u_ta as interior tiles); 1 TMA with the same buffers,
+// 128-byte aligned and 34 wide (boxes from x = i0-1); 2 TMA with each buffer
+// holding only what the correction reads of it: phi with its full halo, u*
+// the tile rows with the x halo, v* the rows j0-1..j0+TY-1, w* and the old
+// u_ta the tile rows (13 % less shared memory than 1, so more CTAs fit).
+// Offsets of u*, v*, w* and the old u_ta from the start of u* (in elements
+// of H) and the index of this thread's cell (its neighbour at x or y offset
+// o) in each.
+template <class H, int TY, int TM>
 struct CorrLay {
   static constexpr int PLANE = SXW * (TY + 2), TILE = TXW * TY;
-  static constexpr int FP = TMA ? ru16(PLANE) : PLANE;
-  static constexpr int HS = TMA ? ru16(SXW * TY) : TILE;
-  static constexpr int SLOT = TMA ? (4 * FP + 3 * HS) * 8 : cslot_bytes<H, TY>();
+  static constexpr int FP = TM ? ru16(PLANE) : PLANE;            // phi buffer (doubles)
+  static constexpr int US = TM == 2 ? ru16(SXW * TY) : FP;        // u* and w* buffers
+  static constexpr int VS = TM == 2 ? ru16(SXW * (TY + 1)) : FP;  // v* buffer
+  static constexpr int HS = TM ? ru16(SXW * TY) : TILE;           // old u_ta tiles
+  static constexpr int VO = US, WO = US + VS, HO = 2 * US + VS;
+  static constexpr int SLOT = TM ? (FP + HO + 3 * HS) * 8 : cslot_bytes<H, TY>();
+  static __device__ __forceinline__ int ui(int tx, int ty, int o) {
+    return TM == 2 ? ty * SXW + tx + 1 + o : (ty + 1) * SXW + tx + 1 + o;
+  }
+  static __device__ __forceinline__ int vi(int tx, int ty, int o) {
+    return (ty + 1 + o) * SXW + tx + 1;
+  }
+  static __device__ __forceinline__ int wi(int tx, int ty) {
+    return TM == 2 ? ty * SXW + tx + 1 : (ty + 1) * SXW + tx + 1;
+  }
   static __device__ __forceinline__ int he(int tx, int ty) {
-    return TMA ? ty * SXW + tx + 1 : ty * TXW + tx;
+    return TM ? ty * SXW + tx + 1 : ty * TXW + tx;
   }
 };
 
-template <int TY, int NS>
+template <int TY, int NS, int TM>
 __device__ __forceinline__ void load_plane_c_tma(char* sm, uint64_t* bars, const CorrMaps& tm,
                                                  int i0, int j0, int K, int k0, int kmax) {
-  using L = CorrLay<double, TY, true>;
+  using L = CorrLay<double, TY, TM>;
   if (K > kmax) return;
   const int r = K - (k0 - 1);
   double* slot = reinterpret_cast<double*>(sm + (r % NS) * L::SLOT);
   uint64_t* bar = &bars[r % NS];
-  constexpr unsigned HALO = SXW * (TY + 2) * 8, HB = SXW * TY * 8;
-  mbar_expect_tx(bar, 4 * HALO + 3 * HB);
-  for (int f = 0; f < 4; ++f) tma_load_3d(slot + f * L::FP, &tm.m[f], i0 - 1, j0 - 1, K, bar);
+  double* fl = slot + L::FP;
+  if constexpr (TM == 1) {
+    constexpr unsigned HALO = SXW * (TY + 2) * 8, HB = SXW * TY * 8;
+    mbar_expect_tx(bar, 4 * HALO + 3 * HB);
+    tma_load_3d(slot, &tm.m[0], i0 - 1, j0 - 1, K, bar);
+    for (int f = 0; f < 3; ++f) tma_load_3d(fl + f * L::FP, &tm.m[1 + f], i0 - 1, j0 - 1, K, bar);
+  } else {
+    constexpr unsigned B = SXW * 8;  // bytes of one box row
+    mbar_expect_tx(bar, B * ((TY + 2) + TY + (TY + 1) + TY + 3 * TY));
+    tma_load_3d(slot, &tm.m[0], i0 - 1, j0 - 1, K, bar);
+    tma_load_3d(fl, &tm.m[1], i0 - 1, j0, K, bar);
+    tma_load_3d(fl + L::VO, &tm.m[2], i0 - 1, j0 - 1, K, bar);
+    tma_load_3d(fl + L::WO, &tm.m[3], i0 - 1, j0, K, bar);
+  }
   for (int f = 0; f < 3; ++f)
-    tma_load_3d(slot + 4 * L::FP + f * L::HS, &tm.m[4 + f], i0 - 1, j0, K, bar);
+    tma_load_3d(fl + L::HO + f * L::HS, &tm.m[4 + f], i0 - 1, j0, K, bar);
 }
 
-template <class H, int TY, int NS, int MINB, bool TMA, int KC = CKCHUNK>
+template <class H, int TY, int NS, int MINB, int TM, int KC = CKCHUNK>
 __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     Dims d, GridRcp rg, const double* __restrict__ PHI, const H* __restrict__ UT,
     const H* __restrict__ VT, const H* __restrict__ WT, double* __restrict__ p,
@@ -167,7 +197,8 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     const __grid_constant__ CorrMaps tm) {
   extern __shared__ __align__(128) char smc[];
   char* sm = smc;
-  using Lay = CorrLay<H, TY, TMA>;
+  using Lay = CorrLay<H, TY, TM>;
+  constexpr bool TMA = TM != 0;
   constexpr int PLANE = Lay::FP, TILE = Lay::HS, F = NS - 3;
   const int i0 = 1 + blockIdx.x * TXW, j0 = 1 + blockIdx.y * TY;
   const int I = i0 + threadIdx.x, J = j0 + threadIdx.y;
@@ -189,7 +220,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
     if (!aligned) return;
     if (lead)
       for (int q = -1; q <= F; ++q)
-        load_plane_c_tma<TY, NS>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
+        load_plane_c_tma<TY, NS, TM>(sm, bars, tm, i0, j0, k0 + q, k0, kmax);
     ring_wait<NS>(bars, k0 - 1, k0);
     ring_wait<NS>(bars, k0, k0);
   } else {
@@ -207,7 +238,7 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
   const int t0 = Lay::he(threadIdx.x, threadIdx.y);
   for (int K = k0; K <= k1; ++K) {
     if constexpr (TMA) {
-      if (lead) load_plane_c_tma<TY, NS>(sm, bars, tm, i0, j0, K + 1 + F, k0, kmax);
+      if (lead) load_plane_c_tma<TY, NS, TM>(sm, bars, tm, i0, j0, K + 1 + F, k0, kmax);
       ring_wait<NS>(bars, K + 1, k0);
     } else {
       load_plane_c<H, TY, NS>(sm, d, i0, j0, K + 1 + F, kmax, PHI, UT, VT, WT, u_ta, v_ta,
@@ -225,21 +256,20 @@ __global__ void __launch_bounds__(TXW * TY, MINB) k_correct_pipe(
       const H* fm = reinterpret_cast<const H*>(sm_m + PLANE * 8);
       const H* fc = reinterpret_cast<const H*>(sm_c + PLANE * 8);
 #define PH(pl, dxo, dyo) (pl)[e0 + (dyo) * SXW + (dxo)]
-#define FL(pl, f, dxo, dyo) (double)(pl)[(f) * PLANE + e0 + (dyo) * SXW + (dxo)]
+      const int tx = threadIdx.x, ty = threadIdx.y;
       const long c = d.P(I, J, K);
       const double rz = LD(rg.rdz, K), rz12 = LD(rg.rdz12, K), rz12m = LD(rg.rdz12, K - 1);
       const double ph = PH(qc, 0, 0), phx = PH(qc, 1, 0), phy = PH(qc, 0, 1), phz = PH(qp, 0, 0),
                    phxm = PH(qc, -1, 0), phym = PH(qc, 0, -1), phzm = PH(qm, 0, 0);
       const double gx = (phx - ph) * rx12, gy = (phy - ph) * ry12, gz = (phz - ph) * rz12;
-      const double un = FL(fc, 0, 0, 0) - dt * gx;
-      const double vn = FL(fc, 1, 0, 0) - dt * gy;
-      const double wn = FL(fc, 2, 0, 0) - dt * gz;
-      const double um = FL(fc, 0, -1, 0) - dt * ((ph - phxm) * rx12m);
-      const double vm = FL(fc, 1, 0, -1) - dt * ((ph - phym) * ry12m);
-      const double wm = FL(fm, 2, 0, 0) - dt * ((ph - phzm) * rz12m);
+      const double un = (double)fc[Lay::ui(tx, ty, 0)] - dt * gx;
+      const double vn = (double)fc[Lay::VO + Lay::vi(tx, ty, 0)] - dt * gy;
+      const double wn = (double)fc[Lay::WO + Lay::wi(tx, ty)] - dt * gz;
+      const double um = (double)fc[Lay::ui(tx, ty, -1)] - dt * ((ph - phxm) * rx12m);
+      const double vm = (double)fc[Lay::VO + Lay::vi(tx, ty, -1)] - dt * ((ph - phym) * ry12m);
+      const double wm = (double)fm[Lay::WO + Lay::wi(tx, ty)] - dt * ((ph - phzm) * rz12m);
 #undef PH
-#undef FL
-      const H* old = fc + 3 * PLANE + t0;
+      const H* old = fc + Lay::HO + t0;
       u[c] = un;
       v[c] = vn;
       w[c] = wn;
@@ -292,17 +322,21 @@ __global__ void k_correct_faces(Dims d, GridRcp rg, const double* __restrict__ P
   w_ta[c] = (H)(dt * gz);
 }
 
-template <class H, int TY, int NS, int MINB, bool TMA = false, int KC = CKCHUNK>
+template <class H, int TY, int NS, int MINB, int TM = 0, int KC = CKCHUNK>
 static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                        const H* vt, const H* wt, double* p, double* u, double* v, double* w,
                        H* u_ta, H* v_ta, H* w_ta, H* u_ep2, H* v_ep2, H* w_ep2, H* divu,
                        double dt, cudaStream_t s) {
   CorrMaps tm;
-  size_t smem = (size_t)NS * CorrLay<H, TY, TMA>::SLOT;
-  if constexpr (TMA) {
+  size_t smem = (size_t)NS * CorrLay<H, TY, TM>::SLOT;
+  if constexpr (TM != 0) {
     const void* f[7] = {PHI, ut, vt, wt, u_ta, v_ta, w_ta};
+    // box rows per field: phi, u*, v*, w* with the y halo (TM 1), or phi
+    // with it, u* and w* the tile rows, v* the row below too (TM 2)
+    const int rows[7] = {TY + 2, TM == 1 ? TY + 2 : TY, TM == 1 ? TY + 2 : TY + 1,
+                         TM == 1 ? TY + 2 : TY, TY, TY, TY};
     bool ok = true;
-    for (int q = 0; q < 7; ++q) ok = ok && ring_map(&tm.m[q], d, f[q], SXW, q < 4 ? TY + 2 : TY);
+    for (int q = 0; q < 7; ++q) ok = ok && ring_map(&tm.m[q], d, f[q], SXW, rows[q]);
     if (!ok) return false;
     smem += NS * sizeof(uint64_t);
   } else {
@@ -310,7 +344,7 @@ static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, cons
   }
   dim3 block(TXW, TY, 1);
   dim3 grid((d.nx + TXW - 1) / TXW, (d.ny + TY - 1) / TY, (d.nz + KC - 1) / KC);
-  auto kern = k_correct_pipe<H, TY, NS, MINB, TMA, KC>;
+  auto kern = k_correct_pipe<H, TY, NS, MINB, TM, KC>;
   cudaFuncSetAttribute((const void*)kern, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
   count_launch();
   kern<<<grid, block, smem, s>>>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,
@@ -325,7 +359,9 @@ static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, cons
 // four CTAs, 6 32x8 with 4 planes and three CTAs, 7 32x4 with 7 planes and
 // three CTAs, 8 32x4 with 6 planes and three CTAs, and with 16 z planes per
 // CTA instead of 8: 9 32x4 with 5 planes and four CTAs, 10 32x4 with 4 planes
-// and five CTAs (each cell computed the same way; a TMA shape whose maps
+// and five CTAs; the trimmed TMA ring (CorrLay, TM 2): 11 32x4 with 5 planes
+// and five CTAs, 12 32x4 with 4 planes and six CTAs, 13 as 11 with 16 z
+// planes per CTA (each cell computed the same way; a TMA shape whose maps
 // cannot be made runs the default)
 template <class H>
 static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
@@ -337,11 +373,14 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
   correct_go<H, TY_, NS_, MB_>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta, w_ta, u_ep2,  \
                                v_ep2, w_ep2, divu, dt, s)
 #define NSE_CORR_TMA(TY_, NS_, MB_)                                                          \
-  done = correct_go<H, TY_, NS_, MB_, true>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
-                                            w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
+  done = correct_go<H, TY_, NS_, MB_, 1>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
+                                         w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
 #define NSE_CORR_TMA16(TY_, NS_, MB_)                                                            \
-  done = correct_go<H, TY_, NS_, MB_, true, 16>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
-                                                w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
+  done = correct_go<H, TY_, NS_, MB_, 1, 16>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
+                                             w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
+#define NSE_CORR_TRIM(TY_, NS_, MB_, KC_)                                                       \
+  done = correct_go<H, TY_, NS_, MB_, 2, KC_>(d, rg, PHI, ut, vt, wt, p, u, v, w, u_ta, v_ta,  \
+                                              w_ta, u_ep2, v_ep2, w_ep2, divu, dt, s)
   bool done = false;
   if constexpr (sizeof(H) == 8) {
     if (shape == 4) NSE_CORR_TMA(4, 4, 5);
@@ -351,9 +390,13 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
     else if (shape == 8) NSE_CORR_TMA(4, 6, 3);
     else if (shape == 9) NSE_CORR_TMA16(4, 5, 4);
     else if (shape == 10) NSE_CORR_TMA16(4, 4, 5);
+    else if (shape == 11) NSE_CORR_TRIM(4, 5, 5, 8);
+    else if (shape == 12) NSE_CORR_TRIM(4, 4, 6, 8);
+    else if (shape == 13) NSE_CORR_TRIM(4, 5, 5, 16);
   }
 #undef NSE_CORR_TMA
 #undef NSE_CORR_TMA16
+#undef NSE_CORR_TRIM
   if (!done && shape >= 4) shape = 0;
   if (!done) switch (shape) {
     case 1: NSE_CORR_GO(8, 5, 2); break;
