@@ -366,14 +366,15 @@ int nse_sync(nse_ctx* ctx);
  * with 5, 6 = 32x8 with 4, 7 = 32x4 with 7, 8 = 32x4 with 6; 16 z planes per
  * CTA: 9 = 32x4 with 5, 10 = 32x4 with 4; the TMA ring holding only what the
  * correction reads: 11 = 32x4 with 5, 12 = 32x4 with 4, 13 = as 11 with 16 z
- * planes per CTA), out[14] the kx
+ * planes per CTA, 14 = 32x4 with 5 and four CTAs per SM; 15 = the full TMA
+ * ring with 5 planes and three CTAs), out[14] the kx
  * slices the FP64 solve's z
  * transforms and SPN run in (1 = unsliced). */
 int nse_ctx_launch_shapes(nse_ctx* ctx, int* out);
 /* Fix the right-hand-side and correction launch shapes (codes as above; -1
  * leaves that one to the autotuner) before the first step; every shape gives
  * the same values.  NSE_ERR_ARG for a code outside -1..6 (right-hand side)
- * or -1..13 (correction). */
+ * or -1..15 (correction). */
 int nse_ctx_set_shapes(nse_ctx* ctx, int rhs_shape, int corr_shape);
 /* Per-phase timing of the next max_steps steps with CUDA events on the
  * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the

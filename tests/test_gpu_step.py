@@ -282,7 +282,7 @@ def test_line_launch_shapes_give_the_same_fields(n):
     assert all(v in (0, 1, 2, 3) for v in shapes["y"] + shapes["z"]), shapes
     assert all(v in (1, 2) for v in shapes["x"]), shapes
     assert shapes["rhs"] in range(7), shapes
-    assert shapes["correct"] in range(14), shapes
+    assert shapes["correct"] in range(16), shapes
 
 
 @pytest.mark.parametrize("n,prec,flags", [((96, 64, 96), S.FP64, 0), ((80, 40, 48), S.FP64, 0),
@@ -298,7 +298,7 @@ def test_rhs_and_correction_shapes_give_the_same_bits(n, prec, flags):
     g, f, c1, par = make_case(*n)
     out = []
     for rhs, corr in ((0, 0), (1, 2), (2, 1), (3, 3), (4, 4), (5, 5), (6, 6), (4, 7), (5, 8),
-                      (4, 9), (5, 10), (4, 11), (5, 12), (4, 13)):
+                      (4, 9), (5, 10), (4, 11), (5, 12), (4, 13), (5, 14), (4, 15)):
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                        g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
                        body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
@@ -328,7 +328,7 @@ def test_set_shapes_rejects_bad_codes():
         with pytest.raises(Exception):
             ctx.set_shapes(7, 0)
         with pytest.raises(Exception):
-            ctx.set_shapes(0, 14)
+            ctx.set_shapes(0, 16)
         with pytest.raises(Exception):
             ctx.set_shapes(0, -2)
 

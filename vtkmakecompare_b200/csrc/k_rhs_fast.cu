@@ -361,8 +361,9 @@ static bool correct_go(const Dims& d, const GridRcp& rg, const double* PHI, cons
 // CTA instead of 8: 9 32x4 with 5 planes and four CTAs, 10 32x4 with 4 planes
 // and five CTAs; the trimmed TMA ring (CorrLay, TM 2): 11 32x4 with 5 planes
 // and five CTAs, 12 32x4 with 4 planes and six CTAs, 13 as 11 with 16 z
-// planes per CTA (each cell computed the same way; a TMA shape whose maps
-// cannot be made runs the default)
+// planes per CTA, 14 32x4 with 5 planes and four CTAs; 15 the full TMA ring,
+// 32x4 with 5 planes and three CTAs (each cell computed the same way; a TMA
+// shape whose maps cannot be made runs the default)
 template <class H>
 static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, const H* ut,
                          const H* vt, const H* wt, double* p, double* u, double* v, double* w,
@@ -393,6 +394,8 @@ static void correct_pipe(const Dims& d, const GridRcp& rg, const double* PHI, co
     else if (shape == 11) NSE_CORR_TRIM(4, 5, 5, 8);
     else if (shape == 12) NSE_CORR_TRIM(4, 4, 6, 8);
     else if (shape == 13) NSE_CORR_TRIM(4, 5, 5, 16);
+    else if (shape == 14) NSE_CORR_TRIM(4, 5, 4, 8);
+    else if (shape == 15) NSE_CORR_TMA(4, 5, 3);
   }
 #undef NSE_CORR_TMA
 #undef NSE_CORR_TMA16

@@ -1999,7 +1999,7 @@ static void autotune_correct(nse_ctx* x, const H* ut, const H* vt, const H* wt) 
     cudaMemcpyAsync(ta[q], x->f[tid[q]].p, hb, cudaMemcpyDeviceToDevice, s);
   int best = 0;
   float best_ms = 1e30f;
-  const int nshape = sizeof(H) == 4 ? 4 : 14;  // shapes 4-13: the FP64 TMA rings
+  const int nshape = sizeof(H) == 4 ? 4 : 16;  // shapes 4-15: the FP64 TMA rings
   for (int shape = 0; shape < nshape; ++shape) {
     auto run = [&]() {
       if constexpr (sizeof(H) == 4)
@@ -2834,7 +2834,7 @@ int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
 }
 
 int nse_ctx_set_shapes(nse_ctx* x, int rhs_shape, int corr_shape) {
-  if (!x || rhs_shape < -1 || rhs_shape > 6 || corr_shape < -1 || corr_shape > 13)
+  if (!x || rhs_shape < -1 || rhs_shape > 6 || corr_shape < -1 || corr_shape > 15)
     return NSE_ERR_ARG;
   if (rhs_shape >= 0) {
     x->rhs_shape = rhs_shape;
