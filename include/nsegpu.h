@@ -356,7 +356,7 @@ int nse_sync(nse_ctx* ctx);
  * no counterpart in the reference), out[15]: out[(dir-1)*4 + comp] for the y
  * (dir 1) and z (dir 2) line passes of u, v, w, T (0 = 16 lines per CTA, 1 =
  * 8, 3 = 32, 2 = TMA tiles of 16 lines), out[8 + comp] the x lines per warp
- * iteration, out[12] the right-hand-side kernel's shape (0 = 32x4 tiles with a
+ * iteration (1 or 2; 3 and 4 the same through shared-memory staged loads), out[12] the right-hand-side kernel's shape (0 = 32x4 tiles with a
  * 5-plane ring in FP64 / 32x8 in FP32, 1 = 32x4 with 4 planes, 2 = 32x8 with
  * 5, 3 = 32x8 with 4; the ring filled by TMA copies (FP32 storage: the FP64
  * halo planes by TMA, the history tiles by cp.async): 4 = 32x4 with 5 planes,
@@ -376,6 +376,11 @@ int nse_ctx_launch_shapes(nse_ctx* ctx, int* out);
  * the same values.  NSE_ERR_ARG for a code outside -1..6 (right-hand side)
  * or -1..15 (correction). */
 int nse_ctx_set_shapes(nse_ctx* ctx, int rhs_shape, int corr_shape);
+/* Fix the launch shapes of every partitioned line pass (y/z: 0..3 as in
+ * nse_ctx_launch_shapes; x: 1..4 lines per warp iteration / staged loads)
+ * before the first step instead of the autotuner's choice; every shape gives
+ * the same values.  NSE_ERR_ARG outside those ranges. */
+int nse_ctx_set_line_shapes(nse_ctx* ctx, int yz_shape, int x_lines);
 /* Per-phase timing of the next max_steps steps with CUDA events on the
  * context stream (0 disables).  nse_ctx_phase_times returns, per phase, the
  * summed milliseconds over the profiled steps; phases in launch order:

@@ -280,7 +280,7 @@ def test_line_launch_shapes_give_the_same_fields(n):
         assert np.array_equal(out[1][k], out[0][k]), k
         assert np.array_equal(out[2][k], out[0][k]), k
     assert all(v in (0, 1, 2, 3) for v in shapes["y"] + shapes["z"]), shapes
-    assert all(v in (1, 2) for v in shapes["x"]), shapes
+    assert all(v in (1, 2, 3, 4) for v in shapes["x"]), shapes
     assert shapes["rhs"] in range(7), shapes
     assert shapes["correct"] in range(16), shapes
 
@@ -388,3 +388,37 @@ def test_levelset_leaves_the_poisson_work_field_clean():
             out.append({k: ctx.download(k) for k in STATE})
     for k in STATE:
         assert np.array_equal(out[0][k], out[1][k]), k
+
+
+@pytest.mark.parametrize("n,prec,flags", [((256, 48, 64), S.FP64, 0), ((128, 40, 96), S.FP64, 0),
+                                          ((192, 48, 64), S.MIXED, 0),
+                                          ((256, 48, 64), S.MIXED, 64)])
+def test_every_line_shape_gives_the_same_bits(n, prec, flags):
+    """Every fixed line launch shape (nse_ctx_set_line_shapes: y/z 16, 8, 32
+    lines per CTA or the FP64 TMA tiles; x one or two lines per warp
+    iteration, direct or through shared memory) gives the same bits after 3
+    penalised steps, in FP64, mixed, and mixed with FP64 line arithmetic
+    (nx = 256, 128, 192: 8, 4 and 6 rows per lane in x)."""
+    g, f, c1, par = make_case(*n)
+    out = []
+    combos = [(0, 2), (1, 1), (3, 3), (0, 4)] + ([(2, 2)] if prec == S.FP64 else [])
+    for yz, xl in combos:
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"], precision=prec, flags=flags)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.set_line_shapes(yz, xl)
+            ctx.project()
+            ctx.start()
+            ctx.step(3)
+            ctx.sync()
+            sh = ctx.line_shapes()
+            assert sh["x"] == [xl] * 4 and sh["y"] == [yz] * 4 and sh["z"] == [yz] * 4
+            out.append({k: ctx.download(k) for k in STATE})
+    for o in out[1:]:
+        for k in STATE:
+            assert np.array_equal(o[k], out[0][k]), k

@@ -95,7 +95,7 @@ struct LineArgs {
   // launch shape of the partitioned solver (chosen by the context's autotuner;
   // every shape gives the same values): y/z lines 0 = 16 lines per CTA, 1 = 8,
   // 3 = 32, 2 = TMA tiles of 16 lines (FP64); x lines per warp iteration 1 or
-  // 2 (0: the default, 2)
+  // 2 (0: the default, 2), or 3 / 4: two / one with the staged loads
   int yzshape = 0;
   int xnl = 0;
 };

@@ -401,13 +401,26 @@ struct XTab {
 
 // NL lines per warp iteration share every table load (the table reads, not
 // the line data, dominate the L1 traffic of this kernel)
-// (with PL = 16 the two half-warps work on different lines)
-template <int M, int NL, bool MASKED, class S, class R, int PL>
+// (with PL = 16 the two half-warps work on different lines).  STG (PL = 32,
+// even M <= 8): a warp reads and writes its lines with consecutive lanes on
+// consecutive 16-byte pairs (512 bytes per instruction) and moves them to and
+// from its lanes' partitions through shared memory, with an XOR swizzle of
+// the pair index so both sides stay free of bank conflicts; unstaged, each
+// lane reads its own M values (pairs at a 16 M-byte lane stride, several
+// sectors per request).
+template <int M, int NL, bool MASKED, class S, class R, int PL, bool STG = false>
 __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __restrict__ f, int jtop,
                                                 const R* __restrict__ tab,
                                                 const int* __restrict__ slots,
                                                 const int* __restrict__ ids, int count) {
   using V2 = typename Vec2T<S>::T;
+  static_assert(!STG || (PL == 32 && M % 2 == 0 && M <= 8), "staged x lines: PL 32, even M <= 8");
+  constexpr int CH = STG ? 16 * M : 1;       // pairs of one line
+  constexpr int WV = 128 / (int)sizeof(V2);  // pairs per 128-byte row of banks
+  __shared__ V2 xsb[STG ? 8 * NL * CH : 1];  // [warp of the CTA][line][pair]
+  V2* wb = xsb + (STG ? (threadIdx.x >> 5) * NL * CH : 0);
+  // swizzled pair index (M = 6 reads conflict-free without it)
+  auto sw = [](int c) { return (M % 4 == 0) ? (c ^ ((c / WV) % WV)) : c; };
   constexpr int NV = x_table_values(M);
   // FP32 tables (mixed form) carry the row coefficients of the increment
   // form after the factorisation values (see line_coef_values)
@@ -446,6 +459,7 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
       }
       const int j = 1 + (int)(id % jtop), k = 1 + (int)(id / jtop);
       line[q] = f + d.P(0, j, k);
+      if constexpr (STG) continue;
       // unknowns t = lane*M + r at positions t (t = 0 stands for x(n))
       if (ok[q]) {
         if (M % 2 == 0) {
@@ -465,6 +479,36 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
 #pragma unroll
         for (int r = 0; r < M; ++r) x[q][r] = R(0);
       }
+    }
+    if constexpr (STG) {
+      // each line's pairs through shared memory
+#pragma unroll
+      for (int q = 0; q < NL; ++q)
+        if (ok[q]) {
+          const V2* g2 = reinterpret_cast<const V2*>(line[q]);
+          V2 tmp[M / 2];
+#pragma unroll
+          for (int u = 0; u < M / 2; ++u) tmp[u] = g2[lane + 32 * u];
+#pragma unroll
+          for (int u = 0; u < M / 2; ++u) wb[q * CH + sw(lane + 32 * u)] = tmp[u];
+        }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < NL; ++q) {
+        if (ok[q]) {
+#pragma unroll
+          for (int u = 0; u < M / 2; ++u) {
+            const V2 v = wb[q * CH + sw((M / 2) * lane + u)];
+            x[q][2 * u] = (R)v.x;
+            x[q][2 * u + 1] = (R)v.y;
+          }
+          if (lane == 0) x[q][0] = (R)line[q][n];
+        } else {
+#pragma unroll
+          for (int r = 0; r < M; ++r) x[q][r] = R(0);
+        }
+      }
+      __syncwarp();  // the buffer is rewritten with the solution below
     }
     // increment form (FP32 tables): solve A y = r - A r and return r + y,
     // so the FP32 rounding of the solve scales with |y| ~ |(A - I) r|
@@ -555,7 +599,7 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
 #pragma unroll
         for (int r = 0; r < M; ++r) x[q][r] = xadd(xr[q][r], x[q][r]);
       }
-      if (!ok[q]) continue;
+      if (STG || !ok[q]) continue;
       if (M % 2 == 0) {
         V2* p2 = reinterpret_cast<V2*>(line[q] + lane * M);
 #pragma unroll
@@ -571,6 +615,30 @@ __global__ void __launch_bounds__(256, (M >= 16 ? 2 : 4)) k_xlines(Dims d, S* __
       }
       // position 0 received x(n), the value of the periodic ghost x(0)
       if (lane == 0) line[q][n] = (S)x[q][0];
+    }
+    if constexpr (STG) {
+#pragma unroll
+      for (int q = 0; q < NL; ++q)
+        if (ok[q]) {
+#pragma unroll
+          for (int u = 0; u < M / 2; ++u) {
+            V2 v;
+            v.x = (S)x[q][2 * u];
+            v.y = (S)x[q][2 * u + 1];
+            wb[q * CH + sw((M / 2) * lane + u)] = v;
+          }
+        }
+      __syncwarp();
+#pragma unroll
+      for (int q = 0; q < NL; ++q)
+        if (ok[q]) {
+          V2* g2 = reinterpret_cast<V2*>(line[q]);
+#pragma unroll
+          for (int u = 0; u < M / 2; ++u) g2[lane + 32 * u] = wb[q * CH + sw(lane + 32 * u)];
+          // position 0 received x(n), the value of the periodic ghost x(0)
+          if (lane == 0) line[q][n] = (S)x[q][0];
+        }
+      __syncwarp();  // the next group's loads rewrite the buffer
     }
   }
 }
@@ -955,7 +1023,7 @@ static int sm_count() {
   return cached;
 }
 
-template <int M, class S, class R, int PL = 32, int NLW = 0>
+template <int M, class S, class R, int PL = 32, int NLW = 0, bool STG = false>
 static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, const int* ids,
                  int nmasked, const R* mtab, cudaStream_t s) {
   const int sms = sm_count();
@@ -965,11 +1033,13 @@ static void go_x(const Dims& d, S* f, int jtop, const R* tab, const int* slots, 
   long per_blk = 8L * NL * HW;
   long blocks = std::min<long>((long)sms * 8, (nlines + per_blk - 1) / per_blk);
   count_launch();
-  k_xlines<M, NL, false, S, R, PL><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots,
-                                                                     nullptr, 0);
+  k_xlines<M, NL, false, S, R, PL, STG><<<(unsigned)blocks, 256, 0, s>>>(d, f, jtop, tab, slots,
+                                                                          nullptr, 0);
   if (nmasked > 0) {
     long mb = std::min<long>((long)sms * 8, (nmasked + 8 * HW - 1) / (8 * HW));
     count_launch();
+    // (the pass over the few masked lines keeps the direct loads: staged, its
+    // per-line table pointer pushes it past the 64-register cap)
     k_xlines<M, 1, true, S, R, PL><<<(unsigned)mb, 256, 0, s>>>(d, f, jtop, mtab, slots, ids,
                                                                 nmasked);
   }
@@ -1065,8 +1135,27 @@ static void lines_part(int dir, int kind, const Dims& d, S* f, RO* out, const Li
       else go_x<5, S, R, 16>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
       return;
     }
-    // one line per warp iteration is the autotuner's alternative to two (same values)
+    // one line per warp iteration is the autotuner's alternative to two, and
+    // the staged loads (3: two lines, 4: one line) for even M <= 8 (same values)
     if constexpr (sizeof(S) == sizeof(R)) {
+      if (a.xnl == 3 || a.xnl == 4) {
+        const bool two = a.xnl == 3;
+        switch (M) {
+          case 4:
+            if (two) go_x<4, S, R, 32, 2, true>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+            else go_x<4, S, R, 32, 1, true>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+            return;
+          case 6:
+            if (two) go_x<6, S, R, 32, 2, true>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+            else go_x<6, S, R, 32, 1, true>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+            return;
+          case 8:
+            if (two) go_x<8, S, R, 32, 2, true>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+            else go_x<8, S, R, 32, 1, true>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s);
+            return;
+          default: break;
+        }
+      }
       if (a.xnl == 1) {
         switch (M) {
           case 3: go_x<3, S, R, 32, 1>(d, f, a.jtop, tab, slots, ids, nmasked, mtab, s); return;

@@ -2235,6 +2235,12 @@ static void autotune_lines(nse_ctx* x) {
       if (dir == 0) {
         if (x_nl_candidates(x) < 2) continue;
         cand = {2, 1};
+        // the staged loads (one warp per line, M = nx/32 even)
+        const int M = x_rows_per_lane(d.nx);
+        if (d.nx % 32 == 0 && (M == 4 || M == 6 || M == 8)) {
+          cand.push_back(3);
+          cand.push_back(4);
+        }
       } else if (x->mixed) {
         cand = {0, 1, 3};
       } else {
@@ -2830,6 +2836,15 @@ int nse_ctx_phase_times(nse_ctx* x, double* ms, int nphase, int* nsteps) {
     }
   if (nsteps) *nsteps = x->prof_n;
   x->prof_n = 0;
+  return NSE_OK;
+}
+
+int nse_ctx_set_line_shapes(nse_ctx* x, int yz_shape, int x_lines) {
+  if (!x || yz_shape < 0 || yz_shape > 3 || x_lines < 1 || x_lines > 4) return NSE_ERR_ARG;
+  for (int dir = 1; dir <= 2; ++dir)
+    for (int comp = 0; comp < 4; ++comp) x->yzshape[dir][comp] = yz_shape;
+  for (int comp = 0; comp < 4; ++comp) x->xnl[comp] = x_lines;
+  x->tuned = true;
   return NSE_OK;
 }
 

@@ -80,6 +80,7 @@ def _sig():
     L.nse_ctx_profile.argtypes = [vp, C.c_int]
     L.nse_ctx_launch_shapes.argtypes = [vp, vp]
     L.nse_ctx_set_shapes.argtypes = [vp, C.c_int, C.c_int]
+    L.nse_ctx_set_line_shapes.argtypes = [vp, C.c_int, C.c_int]
     L.nse_ctx_phase_times.argtypes = [vp, vp, C.c_int, vp]
     L.nse_launch_count.restype = C.c_longlong
     L.nse_ensemble_create.argtypes = [vp, C.c_int, C.c_int, C.POINTER(vp)]
@@ -198,6 +199,11 @@ class Context:
         check(self.L.nse_ctx_launch_shapes(self.h, o))
         return {"y": list(o[:4]), "z": list(o[4:8]), "x": list(o[8:12]), "rhs": o[12],
                 "correct": o[13], "mid": o[14]}
+
+    def set_line_shapes(self, yz, x):
+        """Fix every partitioned line pass's launch shape (y/z code 0-3, x code
+        1-4); nsegpu.h, nse_ctx_set_line_shapes."""
+        check(self.L.nse_ctx_set_line_shapes(self.h, int(yz), int(x)))
 
     def set_shapes(self, rhs=-1, correct=-1):
         """Fix the right-hand-side and correction launch shapes (-1: autotuned);
