@@ -331,6 +331,10 @@ def test_set_shapes_rejects_bad_codes():
             ctx.set_shapes(0, 16)
         with pytest.raises(Exception):
             ctx.set_shapes(0, -2)
+        with pytest.raises(Exception):
+            ctx.set_line_shapes(4, 2)
+        with pytest.raises(Exception):
+            ctx.set_line_shapes(0, 5)
 
 
 @pytest.mark.parametrize("prec,flags", [(S.FP64, 0), (S.MIXED, 64)])
