@@ -284,14 +284,16 @@ __device__ __forceinline__ int periodic_pre(int p, int n, int* q) {
 }
 
 // adjoint of the state field F (0 u, 1 v, 2 w, 3 T) at the start of the
-// step, interior cells: the explicit terms transposed and SET_BC folded
+// step, interior cells: the explicit terms transposed and SET_BC folded.
+// A CTA covers an (x, y) tile of one plane, so the y neighbours every cell
+// gathers are mostly the tile's own rows (L1 hits).
 template <int F>
 __global__ void k_adj_explicit(XArgs a, double* __restrict__ out) {
   const Dims& D = a.D;
   const int i = 1 + blockIdx.x * blockDim.x + threadIdx.x;
-  const int j = 1 + blockIdx.y;
+  const int j = 1 + blockIdx.y * blockDim.y + threadIdx.y;
   const int k = 1 + blockIdx.z;
-  if (i > D.nx) return;
+  if (i > D.nx || j > D.ny) return;
   const long c = D.P(i, j, k);
   if (F == 1 && j == D.ny) {  // v(ny) is set to zero by SET_BC
     out[c] = 0.0;
@@ -806,17 +808,17 @@ void launch_adj_explicit(const Dims& D, const AdjGrid& g, const double* const ve
   a.cfac = dt / Re / 2.0;
   a.dfac = dt / (2.0 * Re * Sc * R);
   a.qfac = -dt / R;
-  const int bx = 64;
-  dim3 grid = cell_grid(D, bx);
+  const dim3 block(32, 8, 1);
+  const dim3 grid((D.nx + 31) / 32, (D.ny + 7) / 8, D.nz);
   const cudaStream_t* ss = side ? side : nullptr;
   count_launch();
-  k_adj_explicit<0><<<grid, bx, 0, s>>>(a, out[0]);
+  k_adj_explicit<0><<<grid, block, 0, s>>>(a, out[0]);
   count_launch();
-  k_adj_explicit<1><<<grid, bx, 0, ss ? ss[0] : s>>>(a, out[1]);
+  k_adj_explicit<1><<<grid, block, 0, ss ? ss[0] : s>>>(a, out[1]);
   count_launch();
-  k_adj_explicit<2><<<grid, bx, 0, ss ? ss[1] : s>>>(a, out[2]);
+  k_adj_explicit<2><<<grid, block, 0, ss ? ss[1] : s>>>(a, out[2]);
   count_launch();
-  k_adj_explicit<3><<<grid, bx, 0, ss ? ss[2] : s>>>(a, out[3]);
+  k_adj_explicit<3><<<grid, block, 0, ss ? ss[2] : s>>>(a, out[3]);
 }
 
 void launch_adj_point(const Dims& D, double* const A[4], double* const B[4],
