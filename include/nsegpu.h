@@ -294,9 +294,12 @@ enum {
   NSE_FLAG_SPN_TMA = 4096,   /* FP64 spectral tridiagonal solve (SPN + SP0B) through TMA
                                 tiles of 16 kx columns, partitioned over 16 warps
                                 (ny = 16 m), instead of the two-ended solver */
-  NSE_FLAG_MID_SLICES = 8192 /* FP64 five-launch solve with NZ = 256: run the z
+  NSE_FLAG_MID_SLICES = 8192, /* FP64 five-launch solve with NZ = 256: run the z
                                 transforms and the SPN in 3 kx slices without timing the
                                 slice counts (same values either way) */
+  NSE_FLAG_SPN_CPASYNC = 16384 /* fast forms: the two-ended SPN stages its rows by
+                                per-thread cp.async copies instead of TMA tiles of 16 kx
+                                columns (same values either way) */
 };
 
 /* field ids for upload/download (padded fields unless noted) */

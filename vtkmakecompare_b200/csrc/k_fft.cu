@@ -20,6 +20,7 @@
 
 #include "common.cuh"
 #include "fft_core.cuh"
+#include "tma.cuh"
 
 namespace nse {
 
@@ -657,6 +658,25 @@ __device__ __forceinline__ void cp_async_wait_all() {
   asm volatile("cp.async.commit_group;\ncp.async.wait_all;\n" ::: "memory");
 }
 
+// The recurrences of the two-ended solve with one explicit rounding per
+// operation, shared by k_spn_babe and k_spn_babe_tma so the two give the same
+// bits: elimination y(q) = (d(q) - cf y(q-1)) im(q), back substitution
+// x(r) = y(r) - (cf im) x(r+-1), the 2x2 meeting of the halves and SP0B's
+// marching row (mkp.f:271-288).
+__device__ __forceinline__ double spn_down(bool first, double d, double cf, double y, double w) {
+  return __dmul_rn(first ? d : __fma_rn(-cf, y, d), w);
+}
+__device__ __forceinline__ double spn_up(double y, double cf, double w, double x) {
+  return __fma_rn(-__dmul_rn(cf, w), x, y);
+}
+__device__ __forceinline__ double spn_meet(double ytop, double zbot, double cT, double cB) {
+  return __ddiv_rn(__fma_rn(-cB, ytop, zbot), __fma_rn(-cB, cT, 1.0));
+}
+__device__ __forceinline__ double sp0b_row(double Dj, double pm, double pc, double a1, double a2,
+                                           double a3) {
+  return __ddiv_rn(__fma_rn(-a2, pc, __fma_rn(-a1, pm, Dj)), a3);
+}
+
 // Four threads per (kx, kz): (re | im) x (top | bottom half), 16 systems per
 // 64-thread CTA.  Each thread first issues cp.async copies of all the rows of
 // its half (the spectrum values; the comp-0 thread of each half also the
@@ -726,7 +746,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
     B[0] = (RT)0.0;
     for (int J = 1; J <= ny - 1; ++J) {
       const double Dn = (double)mean_slot(J);
-      const double pn = (Dj - AC1[J - 1] * pm - AC2[J - 1] * pc) / AC3[J - 1];
+      const double pn = sp0b_row(Dj, pm, pc, AC1[J - 1], AC2[J - 1], AC3[J - 1]);
       B[sj * J] = (RT)pn;
       pm = pc;
       pc = pn;
@@ -760,7 +780,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
       const int r = row(q);
       const double cf = cfe[r];
       const double d = pre ? (double)vs[q * 64 + lt] * pre[r + 1] : (double)vs[q * 64 + lt];
-      y = (q == 0 ? d : d - cf * y) * ws[q * 32 + hs];
+      y = spn_down(q == 0, d, cf, y, ws[q * 32 + hs]);
       if (sizeof(RT) == sizeof(double)) ys[q * 64 + lt] = y;
       else vs[q * 64 + lt] = (RT)0;  // FP32 storage: recomputed below
     }
@@ -770,17 +790,133 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
   if (!valid) return;
   const double ytop = part ? other : y;
   const double zbot = part ? y : other;
-  const double cT = AC3[m - 1] * (part ? IM[tj * (m - 1)] : ws[(m - 1) * 32 + hs]);
-  const double cB = AC1[m] * (part ? ws[(ny - 1 - m) * 32 + hs] : IM[tj * m]);
-  const double xm = (zbot - cB * ytop) / (1.0 - cB * cT);
-  double x = part ? xm : ytop - cT * xm;
+  const double cT = __dmul_rn(AC3[m - 1], part ? IM[tj * (m - 1)] : ws[(m - 1) * 32 + hs]);
+  const double cB = __dmul_rn(AC1[m], part ? ws[(ny - 1 - m) * 32 + hs] : IM[tj * m]);
+  const double xm = spn_meet(ytop, zbot, cT, cB);
+  double x = part ? xm : __fma_rn(-cT, xm, ytop);
   B[sj * row(cnt - 1)] = (RT)(post ? x * post[row(cnt - 1) + 1] : x);
 #pragma unroll 4
   for (int q = cnt - 2; q >= 0; --q) {
     const int r = row(q);
-    const double cf = cfb[r] * ws[q * 32 + hs];
-    x = ys[q * 64 + lt] - cf * x;
+    x = spn_up(ys[q * 64 + lt], cfb[r], ws[q * 32 + hs], x);
     B[sj * r] = (RT)(post ? x * post[r + 1] : x);
+  }
+}
+
+// The same two-ended solve on one tile of 16 kx columns x one kz plane, moved
+// by TMA: the tile's spectrum rows (box 32 reals x ny rows) and pivot
+// reciprocals (box 16 x ny) arrive on one mbarrier, one warp solves it in
+// shared memory (lane = 2 kxl + half; each lane runs the re and im
+// recurrences of its half, which share the pivots), the solved values
+// overwrite the tile in place and leave by one TMA store.  Columns kx >= H
+// are outside both tensor maps: zero-filled on load, not stored.  The mean
+// mode's lane marches SP0B on the tile's kx = 0 column.  Forward solve only
+// (the transposed solve keeps k_spn_babe).  Bounded waits: a TMA copy that
+// does not arrive sets g_spn2_wait_err and the tile is not stored.
+__device__ int g_spn2_wait_err = 0;
+
+__global__ void __launch_bounds__(32) k_spn_babe_tma(const __grid_constant__ CUtensorMap tv,
+                                                     const __grid_constant__ CUtensorMap tp,
+                                                     int H, int ny, int m,
+                                                     const double* __restrict__ AC, int g0) {
+  extern __shared__ __align__(128) unsigned char sbt_sm[];
+  double* vs = reinterpret_cast<double*>(sbt_sm);  // [ny][32]: (re, im) of 16 kx
+  double* ws = vs + (size_t)ny * 32;                 // [ny][16]: pivot reciprocals
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ws + (size_t)ny * 16);
+  const int lane = threadIdx.x;
+  const int g = g0 + blockIdx.x, kz = blockIdx.y;
+  const bool aligned = ((reinterpret_cast<uintptr_t>(&tv) & 63) == 0) &&
+                       ((reinterpret_cast<uintptr_t>(&tp) & 63) == 0) &&
+                       ((smem_u32(vs) & 127) == 0) && ((smem_u32(ws) & 127) == 0);
+  if (!aligned) {
+    if (lane == 0) atomicExch(&g_spn2_wait_err, 2);
+    return;
+  }
+  if (lane == 0) {
+    mbar_init(bar, 1);
+    mbar_fence_init();
+    mbar_expect_tx(bar, (unsigned)ny * 48u * 8u);
+    tma_load_3d(vs, &tv, 32 * g, 0, kz, bar);
+    tma_load_3d(ws, &tp, 16 * g, 0, kz, bar);
+  }
+  __syncwarp();
+  if (!tma_wait(bar, 0)) {
+    // the copies of this tile did not arrive: record it, give them one more
+    // bounded wait (the CTA's shared memory must outlive them) and store nothing
+    if (lane == 0) atomicExch(&g_spn2_wait_err, 1);
+    tma_wait(bar, 0);
+    return;
+  }
+  const int kxl = lane >> 1, part = lane & 1;
+  const int kx = 16 * g + kxl;
+  const bool mean = (kx == 0 && kz == 0);
+  const bool valid = kx < H && !mean;
+  const double* AC1 = AC;
+  const double* AC2 = AC + ny;
+  const double* AC3 = AC + 2 * ny;
+  double2* v2 = reinterpret_cast<double2*>(vs) + kxl;  // row r at v2[16 r]
+  const double* w = ws + kxl;                           // row r at w[16 r]
+  if (mean && part == 0) {
+    // SP0B (mkp.f:271-288) on the re and im columns of kx = 0
+    double2 pm = make_double2(0.0, 0.0), pc = pm, Dj = v2[0];
+    v2[0] = make_double2(0.0, 0.0);
+    for (int J = 1; J <= ny - 1; ++J) {
+      const double2 Dn = v2[16 * J];
+      const double a1 = __ldg(AC1 + J - 1), a2 = __ldg(AC2 + J - 1), a3 = __ldg(AC3 + J - 1);
+      const double2 pn = make_double2(sp0b_row(Dj.x, pm.x, pc.x, a1, a2, a3),
+                                      sp0b_row(Dj.y, pm.y, pc.y, a1, a2, a3));
+      v2[16 * J] = pn;
+      pm = pc;
+      pc = pn;
+      Dj = Dn;
+    }
+  }
+  // elimination: part 0 rows 0..m-1 downwards (coefficient AC1), part 1
+  // rows ny-1..m upwards (AC3); y replaces the loaded value in place
+  const int cnt = part ? ny - m : m;
+  const double* cfe = part ? AC3 : AC1;
+  const double* cfb = part ? AC1 : AC3;
+  double2 y = make_double2(0.0, 0.0);
+  if (valid) {
+#pragma unroll 4
+    for (int q = 0; q < cnt; ++q) {
+      const int r = part ? ny - 1 - q : q;
+      const double cf = __ldg(cfe + r), wr = w[16 * r];
+      const double2 d = v2[16 * r];
+      y.x = spn_down(q == 0, d.x, cf, y.x, wr);
+      y.y = spn_down(q == 0, d.y, cf, y.y, wr);
+      v2[16 * r] = y;
+    }
+  }
+  // y(m-1) of the top lane, z(m) of the bottom lane
+  double2 o;
+  o.x = __shfl_xor_sync(0xffffffffu, y.x, 1);
+  o.y = __shfl_xor_sync(0xffffffffu, y.y, 1);
+  if (valid) {
+    const double2 ytop = part ? o : y, zbot = part ? y : o;
+    const double cT = __dmul_rn(__ldg(AC3 + m - 1), w[16 * (m - 1)]);
+    const double cB = __dmul_rn(__ldg(AC1 + m), w[16 * m]);
+    const double2 xm = make_double2(spn_meet(ytop.x, zbot.x, cT, cB),
+                                    spn_meet(ytop.y, zbot.y, cT, cB));
+    double2 x = part ? xm : make_double2(__fma_rn(-cT, xm.x, ytop.x),
+                                         __fma_rn(-cT, xm.y, ytop.y));
+    v2[16 * (part ? m : m - 1)] = x;
+#pragma unroll 4
+    for (int q = cnt - 2; q >= 0; --q) {
+      const int r = part ? ny - 1 - q : q;
+      const double cf = __ldg(cfb + r), wr = w[16 * r];
+      const double2 yy = v2[16 * r];
+      x.x = spn_up(yy.x, cf, wr, x.x);
+      x.y = spn_up(yy.y, cf, wr, x.y);
+      v2[16 * r] = x;
+    }
+  }
+  fence_async_smem();
+  __syncwarp();
+  if (lane == 0) {
+    tma_store_3d(&tv, 32 * g, 0, kz, vs);
+    tma_store_commit();
+    tma_store_wait_read();
   }
 }
 
@@ -984,6 +1120,40 @@ static void spn_babe(const PoissonPlan& pp, RT* spec, cudaStream_t s, int g0 = 0
                                       nullptr, g0);
 }
 
+// the TMA tile form of the two-ended SPN (k_spn_babe_tma) on groups g0 ..
+// g0+ng-1 of 16 kx columns (ng = 0: all); false when the plan cannot use it
+// (no pivot tables, the cp.async form asked for, more than 256 rows for one
+// box, or a tensor map the driver refuses), and nothing is launched then
+static bool spn_babe_tma(const PoissonPlan& pp, cudaStream_t s, int g0 = 0, int ng = 0) {
+  if (!pp.spn_im || pp.spn_cp || pp.ny > 256) return false;
+  const int m = spn_split(pp);
+  if (m == 0) return false;
+  const long sv1 = 16L * pp.Hp, sv2 = sv1 * pp.ny;  // complex rows, planes (bytes)
+  const long sp1 = 8L * pp.Hp, sp2 = sp1 * pp.ny;   // pivot rows, planes
+  if ((sp1 & 15) != 0 || ((uintptr_t)pp.spec & 15) != 0 || ((uintptr_t)pp.spn_im & 15) != 0)
+    return false;
+  CUtensorMap tv, tp;
+  if (!tma_encode_3d(&tv, pp.spec, true, 2L * pp.H, pp.ny, pp.nz, sv1, sv2, 32, pp.ny, 1) ||
+      !tma_encode_3d(&tp, pp.spn_im, true, pp.H, pp.ny, pp.nz, sp1, sp2, 16, pp.ny, 1))
+    return false;
+  const size_t sm = (size_t)pp.ny * 48 * sizeof(double) + 16;
+  smem_optin((const void*)k_spn_babe_tma, sm);
+  if (ng <= 0) { g0 = 0; ng = (pp.H + 15) / 16; }
+  count_launch();
+  k_spn_babe_tma<<<dim3(ng, pp.nz), 32, sm, s>>>(tv, tp, pp.H, pp.ny, m, pp.AC, g0);
+  return true;
+}
+
+int spn2_wait_error() {
+  int v = 0;
+  if (cudaMemcpyFromSymbol(&v, g_spn2_wait_err, sizeof(int)) != cudaSuccess) return 0;
+  if (v) {
+    const int z = 0;
+    cudaMemcpyToSymbol(g_spn2_wait_err, &z, sizeof(int));
+  }
+  return v;
+}
+
 // transposed SPN + SP0B (the discrete adjoint) on the FP64 spectrum: rdy, dy
 // are the reciprocal and plain y spacings (index 0..ny+1); false when the plan
 // has no pivot tables
@@ -1008,7 +1178,7 @@ void launch_spn_fast(const PoissonPlan& pp, cudaStream_t s) {
     launch_spn(pp, true, true, s);
     return;
   }
-  spn_babe<double>(pp, pp.spec, s);
+  if (!spn_babe_tma(pp, s)) spn_babe<double>(pp, pp.spec, s);
 }
 
 // The z transforms and the SPN between them, in nchunk slices of the kx
@@ -1033,7 +1203,7 @@ void launch_poisson_mid(const PoissonPlan& pp, int nchunk, cudaStream_t s) {
   for (int c = 0; c < nchunk; ++c) {
     const int ga = (int)((long)c * G / nchunk), gb = (int)((long)(c + 1) * G / nchunk);
     fft_z<double2>(pp, false, s, 0, 0, ga, gb - ga);
-    spn_babe<double>(pp, pp.spec, s, ga, gb - ga);
+    if (!spn_babe_tma(pp, s, ga, gb - ga)) spn_babe<double>(pp, pp.spec, s, ga, gb - ga);
     fft_z<double2>(pp, true, s, 0, 0, ga, gb - ga);
   }
 }

@@ -718,6 +718,7 @@ bool launch_spn_tma(const PoissonPlan& pp, cudaStream_t s) {
   }
 }
 
+int spn2_wait_error();  // k_spn_babe_tma (k_fft.cu)
 int spn_wait_error() {
   int v = 0;
   if (cudaMemcpyFromSymbol(&v, g_spn_wait_err, sizeof(int)) != cudaSuccess) return 0;
@@ -725,7 +726,8 @@ int spn_wait_error() {
     const int z = 0;
     cudaMemcpyToSymbol(g_spn_wait_err, &z, sizeof(int));
   }
-  return v;
+  const int b = spn2_wait_error();
+  return v ? v : b;
 }
 
 void launch_p2s256(const PoissonPlan& pp, const Dims& d, const double* FP, cudaStream_t s) {

@@ -1707,6 +1707,7 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
   ok = ok && x->pb.build(nx, ny, nz, x->hdx.data(), x->hdy.data(), x->hdz.data(),
                          x->hdy12.data(), c.xl, c.zl, x->own);
   ok = ok && ((c.flags & NSE_FLAG_EXACT) || x->pb.build_tables(x->own));
+  x->pb.pp.spn_cp = (c.flags & NSE_FLAG_SPN_CPASYNC) ? 1 : 0;
   ok = ok && build_line_tables(x);
   if (!ok) {
     nse_ctx_destroy(x);

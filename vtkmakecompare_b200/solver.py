@@ -30,6 +30,7 @@ FLAG_LINES_TMA = 1024
 FLAG_NO_AUTOTUNE = 2048
 FLAG_SPN_TMA = 4096
 FLAG_MID_SLICES = 8192
+FLAG_SPN_CPASYNC = 16384
 
 
 class Config(C.Structure):
