@@ -221,6 +221,7 @@ struct PoissonPlan {
   const float* twz_f;
   const double* spn_im;       // SPN pivot reciprocals [nz][ny][Hp] (null: none)
   int spn_cp = 0;             // 1: the two-ended SPN stages by cp.async, not TMA tiles
+  const double* rAC3 = nullptr;  // 1/AC3 [ny] for SP0B's marching (null: computed inline)
 };
 bool poisson_plan_tables(int nx, int ny, int nz, const double* dx, const double* dy,
                          const double* dz, const double* dy12, double xl, double zl,

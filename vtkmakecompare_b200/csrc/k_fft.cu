@@ -662,7 +662,10 @@ __device__ __forceinline__ void cp_async_wait_all() {
 // operation, shared by k_spn_babe and k_spn_babe_tma so the two give the same
 // bits: elimination y(q) = (d(q) - cf y(q-1)) im(q), back substitution
 // x(r) = y(r) - (cf im) x(r+-1), the 2x2 meeting of the halves and SP0B's
-// marching row (mkp.f:271-288).
+// marching row (mkp.f:271-288).  The marching row multiplies by the
+// reciprocal ra3 = 1/AC3 instead of dividing by AC3: the reciprocals do not
+// depend on the recurrence, so they leave its serial chain (one lane marches
+// all ny rows of the mean mode, the longest chain of the solve).
 __device__ __forceinline__ double spn_down(bool first, double d, double cf, double y, double w) {
   return __dmul_rn(first ? d : __fma_rn(-cf, y, d), w);
 }
@@ -673,8 +676,8 @@ __device__ __forceinline__ double spn_meet(double ytop, double zbot, double cT, 
   return __ddiv_rn(__fma_rn(-cB, ytop, zbot), __fma_rn(-cB, cT, 1.0));
 }
 __device__ __forceinline__ double sp0b_row(double Dj, double pm, double pc, double a1, double a2,
-                                           double a3) {
-  return __ddiv_rn(__fma_rn(-a2, pc, __fma_rn(-a1, pm, Dj)), a3);
+                                           double ra3) {
+  return __dmul_rn(__fma_rn(-a2, pc, __fma_rn(-a1, pm, Dj)), ra3);
 }
 
 // Four threads per (kx, kz): (re | im) x (top | bottom half), 16 systems per
@@ -695,6 +698,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
                                                  long svj, long svk,
                                                  const double* __restrict__ im, long tj,
                                                  long tk, const double* __restrict__ AC,
+                                                 const double* __restrict__ rAC3,
                                                  const double* __restrict__ pre,
                                                  const double* __restrict__ post, int g0) {
   extern __shared__ __align__(16) unsigned char spn_sm[];
@@ -744,9 +748,11 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
     double pm = 0.0, pc = 0.0;
     double Dj = (double)mean_slot(0);
     B[0] = (RT)0.0;
+#pragma unroll 4
     for (int J = 1; J <= ny - 1; ++J) {
       const double Dn = (double)mean_slot(J);
-      const double pn = sp0b_row(Dj, pm, pc, AC1[J - 1], AC2[J - 1], AC3[J - 1]);
+      const double pn = sp0b_row(Dj, pm, pc, AC1[J - 1], AC2[J - 1],
+                                 rAC3 ? rAC3[J - 1] : 1.0 / AC3[J - 1]);
       B[sj * J] = (RT)pn;
       pm = pc;
       pc = pn;
@@ -761,7 +767,7 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
     for (int J = ny - 1; J >= 1; --J) {
       double v = (double)mean_slot(J) - AC2[J] * t1;  // phibar(J+1) is row J
       if (J + 1 <= ny - 1) v -= AC1[J + 1] * t2;
-      const double tj = v / AC3[J - 1];
+      const double tj = __dmul_rn(v, rAC3 ? rAC3[J - 1] : 1.0 / AC3[J - 1]);
       B[sj * (J - 1)] = (RT)tj;
       t2 = t1;
       t1 = tj;
@@ -803,28 +809,101 @@ __global__ void __launch_bounds__(64) k_spn_babe(int H, int ny, int nz, int m, R
   }
 }
 
-// The same two-ended solve on one tile of 16 kx columns x one kz plane, moved
-// by TMA: the tile's spectrum rows (box 32 reals x ny rows) and pivot
-// reciprocals (box 16 x ny) arrive on one mbarrier, one warp solves it in
-// shared memory (lane = 2 kxl + half; each lane runs the re and im
-// recurrences of its half, which share the pivots), the solved values
-// overwrite the tile in place and leave by one TMA store.  Columns kx >= H
-// are outside both tensor maps: zero-filled on load, not stored.  The mean
-// mode's lane marches SP0B on the tile's kx = 0 column.  Forward solve only
-// (the transposed solve keeps k_spn_babe).  Bounded waits: a TMA copy that
-// does not arrive sets g_spn2_wait_err and the tile is not stored.
+// The same two-ended solve on one tile of SPN_KT = 12 kx columns x one kz
+// plane, moved by TMA: the tile's spectrum rows (box 24 reals x ny rows) and
+// pivot reciprocals (box 12 x ny) arrive on one mbarrier, one warp solves it
+// in shared memory and the solved values overwrite the tile in place and
+// leave by one TMA store.  Lane = 16 half + kxl (kxl < 12): each lane runs the
+// re and im recurrences of its half (half 0: rows 0..m-1 downwards, half 1:
+// rows ny-1..m upwards), which share the pivots; a half-warp's accesses to a
+// row are contiguous (no bank conflicts).  The row loads run one block of
+// SPN_U rows ahead of the recurrence (register double buffering), so the
+// shared-memory and L1 latencies overlap the dependent FMA chain.  Four
+// 54 KB tiles fit an SM at ny = 192.  Columns kx >= H are outside both tensor
+// maps (zero-filled on load, not stored); columns kx0 + ... >= kx1 (the end of
+// a kx slice) are not solved and go back unchanged.  The mean mode's lane
+// marches SP0B on the tile's kx = 0 column.  Forward solve only (the
+// transposed solve keeps k_spn_babe).  Bounded waits: a TMA copy that does
+// not arrive sets g_spn2_wait_err and the tile is not stored.
+constexpr int SPN_KT = 12, SPN_U = 8;
+// One sweep of the two-ended recurrence over n rows of a lane's half: row j
+// of the sweep is v[j sv], w[j sv], c[j sc].  DOWN: elimination y(j) =
+// (d(j) - c(j) y(j-1)) w(j); else back substitution x(j) = y(j) - c(j) w(j)
+// x(j-1); each result replaces the row's value.  Loads run one block of
+// SPN_U rows ahead of the recurrence (two register buffers), so their
+// shared-memory and L1 latencies overlap the dependent chain.
+template <bool DOWN>
+__device__ __forceinline__ void spn_sweep(double2* v, const double* w, const double* c, int sv,
+                                          int sc, int n, double2& y) {
+  constexpr int U = SPN_U;
+  double2 dA[U], dB[U];
+  double wA[U], wB[U], cA[U], cB[U];
+  const int nb = n / U;
+  auto load = [&](int b, double2* dd, double* ww, double* cc) {
+    const double2* pv = v + b * U * sv;
+    const double* pw = w + b * U * sv;
+    const double* pc = c + b * U * sc;
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      dd[k] = pv[k * sv];
+      ww[k] = pw[k * sv];
+      cc[k] = __ldg(pc + k * sc);
+    }
+  };
+  auto row = [&](double2 d, double cf, double wr) {
+    if (DOWN) {
+      y.x = spn_down(false, d.x, cf, y.x, wr);
+      y.y = spn_down(false, d.y, cf, y.y, wr);
+    } else {
+      y.x = spn_up(d.x, cf, wr, y.x);
+      y.y = spn_up(d.y, cf, wr, y.y);
+    }
+  };
+  auto step = [&](int b, const double2* dd, const double* ww, const double* cc) {
+    double2* pv = v + b * U * sv;
+#pragma unroll
+    for (int k = 0; k < U; ++k) {
+      row(dd[k], cc[k], ww[k]);
+      pv[k * sv] = y;
+    }
+  };
+  if (nb > 0) load(0, dA, wA, cA);
+  int b = 0;
+  for (; b + 2 <= nb; b += 2) {
+    load(b + 1, dB, wB, cB);
+    step(b, dA, wA, cA);
+    if (b + 2 < nb) load(b + 2, dA, wA, cA);
+    step(b + 1, dB, wB, cB);
+  }
+  if (b < nb) step(b, dA, wA, cA);
+  for (int j = nb * U; j < n; ++j) {
+    row(v[j * sv], __ldg(c + j * sc), w[j * sv]);
+    v[j * sv] = y;
+  }
+}
+
 __device__ int g_spn2_wait_err = 0;
+
+__host__ __device__ inline size_t spn_tile_piv_off(int ny) {
+  return ((size_t)ny * 2 * SPN_KT * sizeof(double) + 127) & ~(size_t)127;
+}
+__host__ __device__ inline size_t spn_tile_smem(int ny) {
+  return spn_tile_piv_off(ny) + (size_t)ny * SPN_KT * sizeof(double) + 16;
+}
 
 __global__ void __launch_bounds__(32) k_spn_babe_tma(const __grid_constant__ CUtensorMap tv,
                                                      const __grid_constant__ CUtensorMap tp,
                                                      int H, int ny, int m,
-                                                     const double* __restrict__ AC, int g0) {
+                                                     const double* __restrict__ AC,
+                                                     const double* __restrict__ rAC3, int kx0,
+                                                     int kx1) {
+  constexpr int KT = SPN_KT;
   extern __shared__ __align__(128) unsigned char sbt_sm[];
-  double* vs = reinterpret_cast<double*>(sbt_sm);  // [ny][32]: (re, im) of 16 kx
-  double* ws = vs + (size_t)ny * 32;                 // [ny][16]: pivot reciprocals
-  uint64_t* bar = reinterpret_cast<uint64_t*>(ws + (size_t)ny * 16);
+  double* vs = reinterpret_cast<double*>(sbt_sm);                        // [ny][2 KT]
+  double* ws = reinterpret_cast<double*>(sbt_sm + spn_tile_piv_off(ny));  // [ny][KT]
+  uint64_t* bar = reinterpret_cast<uint64_t*>(ws + (size_t)ny * KT);
   const int lane = threadIdx.x;
-  const int g = g0 + blockIdx.x, kz = blockIdx.y;
+  const int kb = kx0 + KT * blockIdx.x, kz = blockIdx.y;
   const bool aligned = ((reinterpret_cast<uintptr_t>(&tv) & 63) == 0) &&
                        ((reinterpret_cast<uintptr_t>(&tp) & 63) == 0) &&
                        ((smem_u32(vs) & 127) == 0) && ((smem_u32(ws) & 127) == 0);
@@ -835,9 +914,9 @@ __global__ void __launch_bounds__(32) k_spn_babe_tma(const __grid_constant__ CUt
   if (lane == 0) {
     mbar_init(bar, 1);
     mbar_fence_init();
-    mbar_expect_tx(bar, (unsigned)ny * 48u * 8u);
-    tma_load_3d(vs, &tv, 32 * g, 0, kz, bar);
-    tma_load_3d(ws, &tp, 16 * g, 0, kz, bar);
+    mbar_expect_tx(bar, (unsigned)ny * 3u * KT * 8u);
+    tma_load_3d(vs, &tv, 2 * kb, 0, kz, bar);
+    tma_load_3d(ws, &tp, kb, 0, kz, bar);
   }
   __syncwarp();
   if (!tma_wait(bar, 0)) {
@@ -847,74 +926,72 @@ __global__ void __launch_bounds__(32) k_spn_babe_tma(const __grid_constant__ CUt
     tma_wait(bar, 0);
     return;
   }
-  const int kxl = lane >> 1, part = lane & 1;
-  const int kx = 16 * g + kxl;
+  const int kxl = lane & 15, part = lane >> 4;
+  const int kx = kb + kxl;
   const bool mean = (kx == 0 && kz == 0);
-  const bool valid = kx < H && !mean;
+  const bool valid = kxl < KT && kx < kx1 && kx < H && !mean;
   const double* AC1 = AC;
   const double* AC2 = AC + ny;
   const double* AC3 = AC + 2 * ny;
-  double2* v2 = reinterpret_cast<double2*>(vs) + kxl;  // row r at v2[16 r]
-  const double* w = ws + kxl;                           // row r at w[16 r]
+  double2* v2 = reinterpret_cast<double2*>(vs) + (kxl < KT ? kxl : 0);  // row r at v2[KT r]
+  const double* w = ws + (kxl < KT ? kxl : 0);                           // row r at w[KT r]
   if (mean && part == 0) {
     // SP0B (mkp.f:271-288) on the re and im columns of kx = 0
     double2 pm = make_double2(0.0, 0.0), pc = pm, Dj = v2[0];
     v2[0] = make_double2(0.0, 0.0);
+#pragma unroll 4
     for (int J = 1; J <= ny - 1; ++J) {
-      const double2 Dn = v2[16 * J];
-      const double a1 = __ldg(AC1 + J - 1), a2 = __ldg(AC2 + J - 1), a3 = __ldg(AC3 + J - 1);
+      const double2 Dn = v2[KT * J];
+      const double a1 = __ldg(AC1 + J - 1), a2 = __ldg(AC2 + J - 1);
+      const double a3 = rAC3 ? __ldg(rAC3 + J - 1) : 1.0 / __ldg(AC3 + J - 1);
       const double2 pn = make_double2(sp0b_row(Dj.x, pm.x, pc.x, a1, a2, a3),
                                       sp0b_row(Dj.y, pm.y, pc.y, a1, a2, a3));
-      v2[16 * J] = pn;
+      v2[KT * J] = pn;
       pm = pc;
       pc = pn;
       Dj = Dn;
     }
   }
-  // elimination: part 0 rows 0..m-1 downwards (coefficient AC1), part 1
-  // rows ny-1..m upwards (AC3); y replaces the loaded value in place
+  // this lane's rows: q = 0 .. cnt-1 is row r0 + dr q
   const int cnt = part ? ny - m : m;
-  const double* cfe = part ? AC3 : AC1;
-  const double* cfb = part ? AC1 : AC3;
+  const int r0 = part ? ny - 1 : 0, dr = part ? -1 : 1;
+  const int sv = KT * dr;
   double2 y = make_double2(0.0, 0.0);
   if (valid) {
-#pragma unroll 4
-    for (int q = 0; q < cnt; ++q) {
-      const int r = part ? ny - 1 - q : q;
-      const double cf = __ldg(cfe + r), wr = w[16 * r];
-      const double2 d = v2[16 * r];
-      y.x = spn_down(q == 0, d.x, cf, y.x, wr);
-      y.y = spn_down(q == 0, d.y, cf, y.y, wr);
-      v2[16 * r] = y;
-    }
+    // elimination (coefficient AC1 downwards, AC3 upwards): row q = 0, then
+    // the sweep over q = 1 .. cnt-1
+    const double* cfe = (part ? AC3 : AC1) + r0;
+    double2* vb = v2 + KT * r0;
+    const double* wb = w + KT * r0;
+    const double2 d0 = vb[0];
+    const double w0 = wb[0];
+    y = make_double2(spn_down(true, d0.x, 0.0, 0.0, w0), spn_down(true, d0.y, 0.0, 0.0, w0));
+    vb[0] = y;
+    spn_sweep<true>(vb + sv, wb + sv, cfe + dr, sv, dr, cnt - 1, y);
   }
   // y(m-1) of the top lane, z(m) of the bottom lane
   double2 o;
-  o.x = __shfl_xor_sync(0xffffffffu, y.x, 1);
-  o.y = __shfl_xor_sync(0xffffffffu, y.y, 1);
+  o.x = __shfl_xor_sync(0xffffffffu, y.x, 16);
+  o.y = __shfl_xor_sync(0xffffffffu, y.y, 16);
   if (valid) {
     const double2 ytop = part ? o : y, zbot = part ? y : o;
-    const double cT = __dmul_rn(__ldg(AC3 + m - 1), w[16 * (m - 1)]);
-    const double cB = __dmul_rn(__ldg(AC1 + m), w[16 * m]);
-    const double2 xm = make_double2(spn_meet(ytop.x, zbot.x, cT, cB),
-                                    spn_meet(ytop.y, zbot.y, cT, cB));
+    const double cT = __dmul_rn(__ldg(AC3 + m - 1), w[KT * (m - 1)]);
+    const double cBm = __dmul_rn(__ldg(AC1 + m), w[KT * m]);
+    const double2 xm = make_double2(spn_meet(ytop.x, zbot.x, cT, cBm),
+                                    spn_meet(ytop.y, zbot.y, cT, cBm));
     double2 x = part ? xm : make_double2(__fma_rn(-cT, xm.x, ytop.x),
                                          __fma_rn(-cT, xm.y, ytop.y));
-    v2[16 * (part ? m : m - 1)] = x;
-#pragma unroll 4
-    for (int q = cnt - 2; q >= 0; --q) {
-      const int r = part ? ny - 1 - q : q;
-      const double cf = __ldg(cfb + r), wr = w[16 * r];
-      const double2 yy = v2[16 * r];
-      x.x = spn_up(yy.x, cf, wr, x.x);
-      x.y = spn_up(yy.y, cf, wr, x.y);
-      v2[16 * r] = x;
-    }
+    v2[KT * (part ? m : m - 1)] = x;
+    // back substitution (coefficient AC3 in the top half, AC1 in the bottom
+    // half) over q = cnt-2 .. 0, from the meeting point outwards
+    const int qs = r0 + dr * (cnt - 2);
+    const double* cfb = (part ? AC1 : AC3) + qs;
+    spn_sweep<false>(v2 + KT * qs, w + KT * qs, cfb, -sv, -dr, cnt - 1, x);
   }
   fence_async_smem();
   __syncwarp();
   if (lane == 0) {
-    tma_store_3d(&tv, 32 * g, 0, kz, vs);
+    tma_store_3d(&tv, 2 * kb, 0, kz, vs);
     tma_store_commit();
     tma_store_wait_read();
   }
@@ -1116,14 +1193,14 @@ static void spn_babe(const PoissonPlan& pp, RT* spec, cudaStream_t s, int g0 = 0
   dim3 grid(ng, pp.nz);
   count_launch();
   k_spn_babe<RT><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, spec, pp.Hp, (long)pp.Hp * pp.ny,
-                                      pp.spn_im, pp.Hp, (long)pp.Hp * pp.ny, pp.AC, nullptr,
-                                      nullptr, g0);
+                                      pp.spn_im, pp.Hp, (long)pp.Hp * pp.ny, pp.AC, pp.rAC3,
+                                      nullptr, nullptr, g0);
 }
 
-// the TMA tile form of the two-ended SPN (k_spn_babe_tma) on groups g0 ..
-// g0+ng-1 of 16 kx columns (ng = 0: all); false when the plan cannot use it
-// (no pivot tables, the cp.async form asked for, more than 256 rows for one
-// box, or a tensor map the driver refuses), and nothing is launched then
+// the TMA tile form of the two-ended SPN (k_spn_babe_tma) on the kx columns
+// of groups g0 .. g0+ng-1 of 16 (ng = 0: all); false when the plan cannot use
+// it (no pivot tables, the cp.async form asked for, more than 256 rows for
+// one box, or a tensor map the driver refuses), and nothing is launched then
 static bool spn_babe_tma(const PoissonPlan& pp, cudaStream_t s, int g0 = 0, int ng = 0) {
   if (!pp.spn_im || pp.spn_cp || pp.ny > 256) return false;
   const int m = spn_split(pp);
@@ -1133,14 +1210,18 @@ static bool spn_babe_tma(const PoissonPlan& pp, cudaStream_t s, int g0 = 0, int 
   if ((sp1 & 15) != 0 || ((uintptr_t)pp.spec & 15) != 0 || ((uintptr_t)pp.spn_im & 15) != 0)
     return false;
   CUtensorMap tv, tp;
-  if (!tma_encode_3d(&tv, pp.spec, true, 2L * pp.H, pp.ny, pp.nz, sv1, sv2, 32, pp.ny, 1) ||
-      !tma_encode_3d(&tp, pp.spn_im, true, pp.H, pp.ny, pp.nz, sp1, sp2, 16, pp.ny, 1))
+  if (!tma_encode_3d(&tv, pp.spec, true, 2L * pp.H, pp.ny, pp.nz, sv1, sv2, 2 * SPN_KT, pp.ny,
+                     1) ||
+      !tma_encode_3d(&tp, pp.spn_im, true, pp.H, pp.ny, pp.nz, sp1, sp2, SPN_KT, pp.ny, 1))
     return false;
-  const size_t sm = (size_t)pp.ny * 48 * sizeof(double) + 16;
+  const size_t sm = spn_tile_smem(pp.ny);
   smem_optin((const void*)k_spn_babe_tma, sm);
-  if (ng <= 0) { g0 = 0; ng = (pp.H + 15) / 16; }
+  const int kx0 = ng > 0 ? 16 * g0 : 0;
+  const int kx1 = ng > 0 ? std::min(16 * (g0 + ng), pp.H) : pp.H;
+  if (kx1 <= kx0) return true;
   count_launch();
-  k_spn_babe_tma<<<dim3(ng, pp.nz), 32, sm, s>>>(tv, tp, pp.H, pp.ny, m, pp.AC, g0);
+  k_spn_babe_tma<<<dim3((kx1 - kx0 + SPN_KT - 1) / SPN_KT, pp.nz), 32, sm, s>>>(
+      tv, tp, pp.H, pp.ny, m, pp.AC, pp.rAC3, kx0, kx1);
   return true;
 }
 
@@ -1167,7 +1248,7 @@ bool launch_spn_transposed(const PoissonPlan& pp, const double* rdy, const doubl
   count_launch();
   k_spn_babe<double><<<grid, 64, sm, s>>>(pp.H, pp.ny, pp.nz, m, pp.spec, pp.Hp,
                                           (long)pp.Hp * pp.ny, pp.spn_im, pp.Hp,
-                                          (long)pp.Hp * pp.ny, pp.AC, rdy, dy, 0);
+                                          (long)pp.Hp * pp.ny, pp.AC, pp.rAC3, rdy, dy, 0);
   return true;
 }
 

@@ -1011,10 +1011,12 @@ struct PoissonBufs {
     }
     int H = nx / 2 + 1;
     int Hp = (H + 7) / 8 * 8;
-    std::vector<double> AC(3 * (size_t)ny), KXZ((size_t)H * (nz + 1)), twx(2 * (size_t)nx),
+    // AC (3 ny) followed by the reciprocals of AC3 for SP0B's marching
+    std::vector<double> AC(4 * (size_t)ny), KXZ((size_t)H * (nz + 1)), twx(2 * (size_t)nx),
         twz(2 * (size_t)nz);
     poisson_plan_tables(nx, ny, nz, dx, dy, dz, dy12, xl, zl, AC.data(), KXZ.data(),
                         twx.data(), twz.data());
+    for (int r = 0; r < ny; ++r) AC[3 * (size_t)ny + r] = 1.0 / AC[2 * (size_t)ny + r];
     size_t nspec = (size_t)Hp * ny * nz;
     if (!spec.ensure(2 * nspec * sizeof(double)) || !scr.ensure(nspec * sizeof(double)) ||
         !this->AC.ensure(AC.size() * 8) || !this->KXZ.ensure(KXZ.size() * 8) ||
@@ -1034,6 +1036,7 @@ struct PoissonBufs {
     pp.nx = nx; pp.ny = ny; pp.nz = nz; pp.H = H; pp.Hp = Hp;
     pp.spec = spec.as<double>(); pp.scr = scr.as<double>();
     pp.AC = this->AC.as<double>(); pp.KXZ = this->KXZ.as<double>();
+    pp.rAC3 = pp.AC + 3 * (size_t)ny;
     pp.twx = this->twx.as<double>(); pp.twz = this->twz.as<double>();
     pp.twx_f = twxf.as<float>(); pp.twz_f = twzf.as<float>();
     pp.spn_im = nullptr;
