@@ -1423,6 +1423,9 @@ struct nse_ctx {
   // kx slices of the z transforms and SPN of the FP64 solve (autotune_mid)
   int mid_chunks = 1;
   bool mid_tuned = false;
+  // form of the fast two-ended SPN, TMA tiles or cp.async staging
+  // (autotune_spn_form; the plan's spn_cp)
+  bool spn_tuned = false;
 };
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
@@ -1878,7 +1881,65 @@ static void ctx_poisson_mid(nse_ctx* x, bool part) {
 // forward x pass overwrites all of it next): the candidates run the three
 // passes on whatever the spectrum holds, which costs the same time as on a
 // real spectrum and changes no state.
+// The form of the two-ended SPN (TMA tiles or per-thread cp.async staging;
+// the same bits), timed once per grid before the first FP64 solve of a
+// context: the spectrum is zeroed first (the forward x pass overwrites all of
+// it next), so the candidates time the solve on defined values.
+static void autotune_spn_form(nse_ctx* x) {
+  if (x->spn_tuned) return;
+  PoissonPlan& pp = x->pb.pp;
+  if (!pp.spn_im || (x->cfg.flags & (NSE_FLAG_EXACT | NSE_FLAG_SPN_TMA | NSE_FLAG_SPN_CPASYNC |
+                                     NSE_FLAG_NO_AUTOTUNE))) {
+    x->spn_tuned = true;
+    return;
+  }
+  cudaStream_t s = x->stream;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(s, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone) return;
+  char key[96];
+  snprintf(key, sizeof(key), "spn %d %d %d", x->d.nx, x->d.ny, x->d.nz);
+  {
+    std::lock_guard<std::mutex> lk(g_tune_mu);
+    auto it = g_tune.find(key);
+    if (it != g_tune.end()) {
+      pp.spn_cp = it->second;
+      x->spn_tuned = true;
+      return;
+    }
+  }
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (cudaEventCreate(&e0) != cudaSuccess || cudaEventCreate(&e1) != cudaSuccess) {
+    if (e0) cudaEventDestroy(e0);
+    cudaGetLastError();
+    return;
+  }
+  cudaMemsetAsync(pp.spec, 0, 2 * sizeof(double) * (size_t)pp.Hp * pp.ny * pp.nz, s);
+  int best = 0;
+  float best_ms = 1e30f;
+  for (int form = 0; form < 2; ++form) {
+    pp.spn_cp = form;
+    launch_spn_fast(pp, s);
+    cudaEventRecord(e0, s);
+    for (int r = 0; r < 3; ++r) launch_spn_fast(pp, s);
+    cudaEventRecord(e1, s);
+    float ms = 1e30f;
+    if (cudaEventSynchronize(e1) == cudaSuccess &&
+        cudaEventElapsedTime(&ms, e0, e1) == cudaSuccess && ms < best_ms) {
+      best_ms = ms;
+      best = form;
+    }
+    tune_log(key, form, ms);
+  }
+  cudaEventDestroy(e0);
+  cudaEventDestroy(e1);
+  pp.spn_cp = best;
+  x->spn_tuned = true;
+  std::lock_guard<std::mutex> lk(g_tune_mu);
+  g_tune[key] = best;
+}
+
 static void autotune_mid(nse_ctx* x) {
+  autotune_spn_form(x);
   if (x->mid_tuned) return;
   const PoissonPlan& pp = x->pb.pp;
   const int G = poisson_mid_groups(pp);
