@@ -295,10 +295,14 @@ __global__ void k_fft_inv_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, do
 }
 
 // x forward, N = 256: a half-warp transforms one row pair (two real rows
-// packed as a + ib) of plane J; 8 pairs per 128-thread CTA
-template <class CT, class S>
-__global__ void __launch_bounds__(128) k_fft256_fwd_x(Dims d, SpecViewT<CT> sv, FwdSrc<S> q,
-                                                      int src_mode, const CT* __restrict__ tw) {
+// packed as a + ib) of plane J; 8 pairs per 128-thread CTA.  SRC is the
+// source mode (0 padded samples, 1 divergence, 2 refinement residual) as a
+// template parameter, so the plain-sample pass of the resident step carries
+// none of the other modes' registers: 96 of them, so five CTAs fit an SM.
+template <class CT, class S, int SRC>
+__global__ void __launch_bounds__(128, SRC == 0 ? 5 : 4) k_fft256_fwd_x(Dims d, SpecViewT<CT> sv, FwdSrc<S> q,
+                                                      const CT* __restrict__ tw) {
+  constexpr int src_mode = SRC;
   using RT = typename CReal<CT>::T;
   constexpr int N = 256, FS = 17;
   __shared__ CT sbuf[8][16 * FS];
@@ -362,9 +366,12 @@ __global__ void __launch_bounds__(128) k_fft256_fwd_x(Dims d, SpecViewT<CT> sv, 
   }
 }
 
-// x inverse, N = 256, with the S2P wrap (and `accumulate` as k_fft_inv_x)
+// x inverse, N = 256, with the S2P wrap (and `accumulate` as k_fft_inv_x).
+// Five CTAs per SM (96 registers, a few spilled): 0.059 -> 0.054 ms per pass
+// at 256x192x256 against four CTAs at 124 registers; the forward x pass
+// measured slower with the same cap and keeps four.
 template <class CT>
-__global__ void __launch_bounds__(128) k_fft256_inv_x(Dims d, SpecViewT<CT> sv, double* FP,
+__global__ void __launch_bounds__(128, 5) k_fft256_inv_x(Dims d, SpecViewT<CT> sv, double* FP,
                                                       const CT* __restrict__ tw, int accumulate) {
   using RT = typename CReal<CT>::T;
   constexpr int N = 256, FS = 17;
@@ -1087,7 +1094,12 @@ static void fwd_x(const PoissonPlan& pp, const Dims& d, const FwdSrc<S>& q, int 
   if (pp.nx == 256 && pp.nz % 16 == 0) {
     dim3 grid(nj, pp.nz / 16);
     count_launch();
-    k_fft256_fwd_x<CT, S><<<grid, 128, 0, s>>>(d, sv, q, src_mode, twx_of<CT>(pp));
+    if (src_mode == 0)
+      k_fft256_fwd_x<CT, S, 0><<<grid, 128, 0, s>>>(d, sv, q, twx_of<CT>(pp));
+    else if (src_mode == 1)
+      k_fft256_fwd_x<CT, S, 1><<<grid, 128, 0, s>>>(d, sv, q, twx_of<CT>(pp));
+    else
+      k_fft256_fwd_x<CT, S, 2><<<grid, 128, 0, s>>>(d, sv, q, twx_of<CT>(pp));
     return;
   }
   FFTShape sh = make_shape(pp.nx);
