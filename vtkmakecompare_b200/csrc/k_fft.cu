@@ -431,11 +431,16 @@ __global__ void __launch_bounds__(128, 5) k_fft256_inv_x(Dims d, SpecViewT<CT> s
 
 // z pass, N = 256: a CTA transforms 16 adjacent kx columns of one plane
 // (column group g0 + blockIdx.x); thread (col, b) holds x[16a + b] of its
-// column (loads coalesced over col)
-template <class CT>
+// column (loads coalesced over col).  NORM, the forward pass's division by
+// NX*NZ: 2 divides; 1 multiplies by the reciprocal, which the host passes
+// only when NX*NZ is a power of two (then the product is the correctly
+// rounded quotient, the same bits without a division sequence per value);
+// 0 none (the inverse pass).
+template <class CT, int NORM>
 __global__ void __launch_bounds__(256) k_fft256_z(int H, SpecViewT<CT> sv,
-                                                  const CT* __restrict__ tw, int inv,
-                                                  double nrm, int g0) {
+                                                  const CT* __restrict__ tw, double nrm,
+                                                  int g0) {
+  constexpr bool inv = NORM == 0;
   using RT = typename CReal<CT>::T;
   constexpr int FS = 17;
   extern __shared__ __align__(16) char fsm[];
@@ -461,7 +466,8 @@ __global__ void __launch_bounds__(256) k_fft256_z(int H, SpecViewT<CT> sv,
 #pragma unroll
   for (int e = 0; e < 16; ++e) {
     CT w = v[e];
-    if (!inv) { w.x = w.x / rn; w.y = w.y / rn; }
+    if (NORM == 2) { w.x = w.x / rn; w.y = w.y / rn; }
+    if (NORM == 1) { w.x = w.x * rn; w.y = w.y * rn; }
     base[sv.sk * (c + 16 * e)] = w;
   }
 }
@@ -1152,10 +1158,20 @@ static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 
     if (ng <= 0) { g0 = 0; ng = (pp.H + 15) / 16; }
     dim3 grid(ng, nj);
     size_t sm = 16 * 16 * 17 * sizeof(CT);
-    smem_optin((const void*)k_fft256_z<CT>, sm);
+    const double nrm = (double)pp.nx * (double)pp.nz;
+    int e2 = 0;
+    const bool pow2 = frexp(nrm, &e2) == 0.5;  // nrm = 2^(e2-1)
     count_launch();
-    k_fft256_z<CT><<<grid, 256, sm, s>>>(pp.H, sv, twz_of<CT>(pp), inverse ? 1 : 0,
-                                         (double)pp.nx * (double)pp.nz, g0);
+    if (inverse) {
+      smem_optin((const void*)k_fft256_z<CT, 0>, sm);
+      k_fft256_z<CT, 0><<<grid, 256, sm, s>>>(pp.H, sv, twz_of<CT>(pp), nrm, g0);
+    } else if (pow2) {
+      smem_optin((const void*)k_fft256_z<CT, 1>, sm);
+      k_fft256_z<CT, 1><<<grid, 256, sm, s>>>(pp.H, sv, twz_of<CT>(pp), 1.0 / nrm, g0);
+    } else {
+      smem_optin((const void*)k_fft256_z<CT, 2>, sm);
+      k_fft256_z<CT, 2><<<grid, 256, sm, s>>>(pp.H, sv, twz_of<CT>(pp), nrm, g0);
+    }
     return;
   }
   FFTShape sh = make_shape(pp.nz);
