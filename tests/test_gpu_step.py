@@ -363,6 +363,39 @@ def test_autotuning_context_matches_fixed_shapes(prec, flags):
         assert np.array_equal(out[0][k], out[1][k]), k
 
 
+@pytest.mark.parametrize("prec", [S.FP64, S.MIXED])
+def test_graph_replayed_steps_match_eager_steps(prec):
+    """From the third step on, nse_step replays a captured one-step CUDA graph
+    (one per temperature buffer a step starts from).  Ten steps with a mask
+    change and a launch-shape change in between (each drops the graphs)
+    give the same bits as the same steps run eagerly (profiled steps never
+    replay)."""
+    g, f, c1, par = make_case(64, 48, 64, seed=13)
+    out = []
+    for eager in (False, True):
+        cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
+                       g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
+                       body_force=par["force"], heat_source=par["source"], t_bot=par["tbot"],
+                       t_top=par["ttop"], t_solid=par["tsolid"], precision=prec)
+        with S.Context(cfg) as ctx:
+            for k in ("u", "v", "w", "T"):
+                ctx.upload(k, f[k])
+            ctx.upload("cellvalue", c1)
+            ctx.project()
+            ctx.start()
+            if eager:
+                ctx.profile(20)
+            ctx.step(5)
+            ctx.upload("cellvalue", np.asfortranarray(0.5 * c1))
+            ctx.step(2)
+            ctx.set_shapes(2, 2)
+            ctx.step(3)
+            ctx.sync()
+            out.append({k: ctx.download(k) for k in STATE})
+    for k in STATE:
+        assert np.array_equal(out[0][k], out[1][k]), k
+
+
 def test_levelset_leaves_the_poisson_work_field_clean():
     """A context whose mask comes from nse_levelset steps exactly like one
     given the same mask by upload: the level set does not stay behind in the

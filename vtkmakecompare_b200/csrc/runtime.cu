@@ -1426,7 +1426,50 @@ struct nse_ctx {
   // form of the fast two-ended SPN, TMA tiles or cp.async staging
   // (autotune_spn_form; the plan's spn_cp)
   bool spn_tuned = false;
+  // one-step CUDA graphs of nse_step (step_replay), one per temperature
+  // buffer a step starts from, with the buffer pair the step leaves behind
+  cudaGraphExec_t sg[2] = {nullptr, nullptr};
+  void* sg_t[2] = {nullptr, nullptr};
+  DBuf sg_T[2], sg_uT[2];
+  unsigned long long sg_sig = 0;  // launch shapes the graphs were captured with
+  void* hpin = nullptr;           // pinned staging of the masked line lists
+  size_t hpin_n = 0;              // its capacity (ints)
+  bool sg_off = false;            // a capture failed: step eagerly from now on
 };
+
+namespace {
+// the launch-shape state a step's launches depend on (autotuners, setters)
+unsigned long long shape_sig(const nse_ctx* x) {
+  unsigned long long h = 1469598103934665603ull;
+  auto mix = [&](long long v) { h = (h ^ (unsigned long long)v) * 1099511628211ull; };
+  for (int dir = 0; dir < 3; ++dir)
+    for (int comp = 0; comp < 4; ++comp) mix(x->yzshape[dir][comp]);
+  for (int comp = 0; comp < 4; ++comp) mix(x->xnl[comp]);
+  mix(x->rhs_shape);
+  mix(x->corr_shape);
+  mix(x->mid_chunks);
+  mix(x->pb.pp.spn_cp);
+  mix((x->tuned ? 1 : 0) | (x->rhs_tuned ? 2 : 0) | (x->corr_tuned ? 4 : 0) |
+      (x->mid_tuned ? 8 : 0) | (x->spn_tuned ? 16 : 0));
+  // the masked line lists: their lengths set launch grids, and a longer list
+  // can move its tables
+  for (int dir = 0; dir < 3; ++dir)
+    for (int comp = 0; comp < 4; ++comp) {
+      mix(x->nmasked[dir][comp]);
+      for (const DBuf* b : {&x->slots[dir][comp], &x->ids[dir][comp], &x->mtab[dir][comp],
+                            &x->pmtab[dir][comp], &x->pmtab_f[dir][comp]})
+        mix((long long)(uintptr_t)b->p);
+    }
+  return h;
+}
+void drop_step_graphs(nse_ctx* x) {
+  for (int k = 0; k < 2; ++k) {
+    if (x->sg[k]) cudaGraphExecDestroy(x->sg[k]);
+    x->sg[k] = nullptr;
+    x->sg_t[k] = nullptr;
+  }
+}
+}  // namespace
 
 enum { TB_Y_U = 0, TB_Y_V, TB_Y_T, TB_Z_V, TB_Z_T, TB_X_V, TB_X_T };
 static int line_kind(int dir, int comp);
@@ -1525,65 +1568,111 @@ static void line_shape(const nse_ctx* x, int dir, int comp, LineArgs& la) {
 // after a mask change: flag the lines that touch the mask, give each of them
 // a slot and build its coefficient table (the mask is fixed between changes,
 // so the sweep is reused by every step)
+static bool ensure_side(nse_ctx* x);
 static bool refresh_line_flags(nse_ctx* x, cudaStream_t s) {
   if (!x->mask_dirty) return true;
   const Dims& d = x->d;
   const double* c1 = x->f[NSE_CELLVALUE].as<double>();
+  // the twelve line passes' flag and table kernels are independent and each
+  // is latency-bound (one thread per line), so they run on the context's
+  // stream and its three side streams, forked from and joined back into s
+  // (one stream with NSE_FLAG_ONE_STREAM)
+  cudaStream_t st[4] = {s, s, s, s};
+  const bool fan = !(x->cfg.flags & NSE_FLAG_ONE_STREAM) && ensure_side(x);
+  if (fan)
+    for (int q = 0; q < 3; ++q) st[1 + q] = x->side[q];
+  auto fork = [&]() {
+    if (!fan) return;
+    NSE_CUDA(cudaEventRecord(x->lfork, s));
+    for (int q = 0; q < 3; ++q) NSE_CUDA(cudaStreamWaitEvent(x->side[q], x->lfork, 0));
+  };
+  auto join = [&]() {
+    if (!fan) return;
+    for (int q = 0; q < 3; ++q) {
+      NSE_CUDA(cudaEventRecord(x->ljoin[q], x->side[q]));
+      NSE_CUDA(cudaStreamWaitEvent(s, x->ljoin[q], 0));
+    }
+  };
+  fork();
   for (int comp = 0; comp < 4; ++comp) {
     int jtop = (comp == 1) ? d.ny - 1 : d.ny;
     for (int dir = 0; dir < 3; ++dir)
-      launch_line_flags(d, c1, dir, comp, jtop, flags_of(x, dir, comp), s);
+      launch_line_flags(d, c1, dir, comp, jtop, flags_of(x, dir, comp), st[(dir * 4 + comp) & 3]);
   }
+  join();
   size_t nfl = 4 * ((size_t)d.nx * d.nz + (size_t)d.nx * d.ny + (size_t)d.ny * d.nz);
   std::vector<unsigned char> hf(nfl);
   if (!NSE_CUDA(cudaMemcpyAsync(hf.data(), x->lflags.p, nfl, cudaMemcpyDeviceToHost, s)) ||
       !NSE_CUDA(cudaStreamSynchronize(s)))
     return false;
+  auto lines_of = [&](int dir, int comp) {
+    const LineArgs a = line_args(x, comp);
+    return dir == 1 ? (long)d.nx * d.nz : (dir == 2 ? (long)d.nx * a.jtop : (long)a.jtop * d.nz);
+  };
+  // the slot and id lists of every line pass go through one pinned host
+  // buffer (kept by the context), so their copies are asynchronous and the
+  // refresh waits once, at its end
+  size_t cap = 0;
+  for (int dir = 0; dir < 3; ++dir)
+    for (int comp = 0; comp < 4; ++comp) cap += 2 * (size_t)lines_of(dir, comp);
+  if (x->hpin_n < cap) {
+    if (x->hpin) cudaFreeHost(x->hpin);
+    x->hpin = nullptr;
+    x->hpin_n = 0;
+    if (!NSE_CUDA(cudaMallocHost(&x->hpin, cap * sizeof(int)))) return false;
+    x->hpin_n = cap;
+  }
+  int* hp = static_cast<int*>(x->hpin);
+  fork();
   for (int dir = 0; dir < 3; ++dir)
     for (int comp = 0; comp < 4; ++comp) {
+      cudaStream_t s = st[(dir * 4 + comp) & 3];
       LineArgs a = line_args(x, comp);
-      long nlines = dir == 1 ? (long)d.nx * d.nz : (dir == 2 ? (long)d.nx * a.jtop
-                                                             : (long)a.jtop * d.nz);
+      const long nlines = lines_of(dir, comp);
       const unsigned char* fl = hf.data() + (flags_of(x, dir, comp) - x->lflags.as<unsigned char>());
-      std::vector<int> slot(nlines), ids;
+      int* slot = hp;
+      int* idl = hp + nlines;
+      long nid = 0;
       for (long t = 0; t < nlines; ++t) {
-        slot[t] = fl[t] ? (int)ids.size() : -1;
-        if (fl[t]) ids.push_back((int)t);
+        slot[t] = fl[t] ? (int)nid : -1;
+        if (fl[t]) idl[nid++] = (int)t;
       }
+      hp += nlines + nid;
+      const size_t nids = (size_t)nid;
       int kind = line_kind(dir, comp);
       int n = dir == 0 ? d.nx : (dir == 1 ? d.ny : d.nz);
       size_t stride = line_table_stride(kind, n);
-      x->nmasked[dir][comp] = (int)ids.size();
+      x->nmasked[dir][comp] = (int)nids;
       if (!x->slots[dir][comp].ensure(nlines * sizeof(int)) ||
-          !x->ids[dir][comp].ensure(std::max<size_t>(1, ids.size()) * sizeof(int)) ||
-          !x->mtab[dir][comp].ensure(std::max<size_t>(1, ids.size()) * stride * sizeof(double)))
+          !x->ids[dir][comp].ensure(std::max<size_t>(1, nids) * sizeof(int)) ||
+          !x->mtab[dir][comp].ensure(std::max<size_t>(1, nids) * stride * sizeof(double)))
         return false;
-      if (!NSE_CUDA(cudaMemcpyAsync(x->slots[dir][comp].p, slot.data(), nlines * sizeof(int),
+      if (!NSE_CUDA(cudaMemcpyAsync(x->slots[dir][comp].p, slot, nlines * sizeof(int),
                                     cudaMemcpyHostToDevice, s)))
         return false;
-      if (!ids.empty() &&
-          !NSE_CUDA(cudaMemcpyAsync(x->ids[dir][comp].p, ids.data(), ids.size() * sizeof(int),
+      if (nids > 0 &&
+          !NSE_CUDA(cudaMemcpyAsync(x->ids[dir][comp].p, idl, nids * sizeof(int),
                                     cudaMemcpyHostToDevice, s)))
         return false;
       launch_line_tables_masked(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
-                                (int)ids.size(), x->mtab[dir][comp].as<double>(), s);
+                                (int)nids, x->mtab[dir][comp].as<double>(), s);
       if (x->part) {
         size_t ps = part_table_stride(dir, kind, d);
-        if (!x->pmtab[dir][comp].ensure(std::max<size_t>(1, ids.size()) * ps * sizeof(double)))
+        if (!x->pmtab[dir][comp].ensure(std::max<size_t>(1, nids) * ps * sizeof(double)))
           return false;
         launch_part_tables(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
-                           (int)ids.size(), x->pmtab[dir][comp].as<double>(), s);
+                           (int)nids, x->pmtab[dir][comp].as<double>(), s);
         if (x->mixed) {
-          size_t n = std::max<size_t>(1, ids.size()) * part_table_stride32(dir, kind, d);
+          size_t n = std::max<size_t>(1, nids) * part_table_stride32(dir, kind, d);
           if (!x->pmtab_f[dir][comp].ensure(n * sizeof(float))) return false;
           launch_round_line_table(dir, kind, d, x->g, c1, a, x->ids[dir][comp].as<int>(),
                                   x->pmtab[dir][comp].as<double>(),
-                                  x->pmtab_f[dir][comp].as<float>(), (long)ids.size(), s);
+                                  x->pmtab_f[dir][comp].as<float>(), (long)nids, s);
         }
       }
-      // the host vectors die at the end of this iteration
-      if (!NSE_CUDA(cudaStreamSynchronize(s))) return false;
     }
+  join();
+  if (!NSE_CUDA(cudaStreamSynchronize(s))) return false;
   x->mask_dirty = false;
   return true;
 }
@@ -1726,6 +1815,10 @@ int nse_ctx_create(const nse_config* cfg, nse_ctx** out) {
 int nse_ctx_destroy(nse_ctx* x) {
   if (!x) return NSE_OK;
   if (x->own) cudaStreamSynchronize(x->own);
+  if (x->stream) cudaStreamSynchronize(x->stream);
+  drop_step_graphs(x);
+  if (x->hpin) cudaFreeHost(x->hpin);
+  x->hpin = nullptr;
   for (auto& b : x->f) b.release();
   for (DBuf* b : {&x->grid, &x->ua, &x->va, &x->wa, &x->uT, &x->sa, &x->sb, &x->tmp, &x->mon,
                  &x->ltab, &x->lflags, &x->lsphi})
@@ -2722,10 +2815,86 @@ void ctx_line_solve(nse_ctx* x, int dir, int comp, double* f, cudaStream_t s) {
 
 extern "C" {
 
+// One step as a replay of a captured CUDA graph of one step.  The step's
+// launches depend on the host-side state only through the step counter
+// (l == 1 is the Euler start) and the temperature buffer pair (the FP64 form
+// swaps T and its work buffer every step), so from the third step on a step
+// is the replay of the graph captured from the same starting buffer.  The
+// first two steps, steps after the mask changed, profiled and recorded steps,
+// and steps on a stream that is being captured run eagerly (false).  The
+// capture leaves the host-side state of the step behind (counter, buffer
+// pair) and is launched at once; a replay sets that state the same way.
+// Returns 1 (replayed), 0 (step eagerly) or -1 (a CUDA error).  A launch
+// shape, a masked line list's length or a table's place that differs from
+// the capture drops the graphs (a new mask is tabulated by an eager step).
+static int step_replay(nse_ctx* x) {
+  if (x->sg_off || x->l < 3 || x->mask_dirty || x->prof_n < x->prof_cap || x->rec) return 0;
+  cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(x->stream, &cs) != cudaSuccess || cs != cudaStreamCaptureStatusNone)
+    return 0;
+  const unsigned long long sig = shape_sig(x);
+  if (sig != x->sg_sig) {
+    drop_step_graphs(x);
+    x->sg_sig = sig;
+  }
+  void* t0 = x->f[NSE_T].p;
+  int q = -1;
+  for (int k = 0; k < 2; ++k)
+    if (x->sg[k] && x->sg_t[k] == t0) q = k;
+  if (q >= 0) {
+    if (!NSE_CUDA(cudaGraphLaunch(x->sg[q], x->stream))) return -1;
+    x->f[NSE_T] = x->sg_T[q];
+    x->uT = x->sg_uT[q];
+    x->l += 1;
+    return 1;
+  }
+  q = x->sg[0] ? 1 : 0;
+  if (x->sg[q]) {
+    cudaGraphExecDestroy(x->sg[q]);
+    x->sg[q] = nullptr;
+  }
+  const int l0 = x->l;
+  const DBuf T0 = x->f[NSE_T], uT0 = x->uT;
+  if (cudaStreamBeginCapture(x->stream, cudaStreamCaptureModeRelaxed) != cudaSuccess) {
+    cudaGetLastError();
+    x->sg_off = true;
+    return 0;
+  }
+  ctx_step(x);
+  cudaGraph_t g = nullptr;
+  const cudaError_t ce = cudaStreamEndCapture(x->stream, &g);
+  cudaGraphExec_t ex = nullptr;
+  const bool ok = ce == cudaSuccess && g && cudaGraphInstantiate(&ex, g, 0) == cudaSuccess;
+  if (g) cudaGraphDestroy(g);
+  if (!ok) {
+    // nothing ran: put the host-side state back and step eagerly
+    cudaGetLastError();
+    x->l = l0;
+    x->f[NSE_T] = T0;
+    x->uT = uT0;
+    x->sg_off = true;
+    return 0;
+  }
+  if (!NSE_CUDA(cudaGraphLaunch(ex, x->stream))) {
+    cudaGraphExecDestroy(ex);
+    x->l = l0;
+    x->f[NSE_T] = T0;
+    x->uT = uT0;
+    return -1;
+  }
+  x->sg[q] = ex;
+  x->sg_t[q] = t0;
+  x->sg_T[q] = x->f[NSE_T];
+  x->sg_uT[q] = x->uT;
+  return 1;
+}
+
 int nse_step(nse_ctx* x, int nsteps) {
   if (!x || nsteps < 0) return NSE_ERR_ARG;
   for (int n = 0; n < nsteps; ++n) {
-    ctx_step(x);
+    const int r = step_replay(x);
+    if (r < 0) return status_or(NSE_ERR_CUDA);
+    if (r == 0) ctx_step(x);
     if (!NSE_CUDA(cudaGetLastError())) return status_or(NSE_ERR_CUDA);
     if (x->cfg.flags & 1) {  // check for non-finite values after every step
       double m[6];
