@@ -369,9 +369,12 @@ def test_graph_replayed_steps_match_eager_steps(prec):
     (one per temperature buffer a step starts from).  Ten steps with a mask
     change and a launch-shape change in between (each drops the graphs)
     give the same bits as the same steps run eagerly (profiled steps never
-    replay)."""
+    replay).  The library counts a replayed step's kernels like a captured
+    one's: four steps after the shape change (two captures, two replays)
+    count the same launches each (the profiled steps run the passes in order
+    on one stream, where set_bc is one launch instead of two)."""
     g, f, c1, par = make_case(64, 48, 64, seed=13)
-    out = []
+    out, nk = [], []
     for eager in (False, True):
         cfg = S.Config(g["nx"], g["ny"], g["nz"], par["dt"], par["Re"], par["Sc"], par["eta"],
                        g["xl"], g["yl"], g["zl"], y0=-1.0, ystretch=2.0,
@@ -389,11 +392,18 @@ def test_graph_replayed_steps_match_eager_steps(prec):
             ctx.upload("cellvalue", np.asfortranarray(0.5 * c1))
             ctx.step(2)
             ctx.set_shapes(2, 2)
-            ctx.step(3)
+            per = []
+            for _ in range(4):
+                n0 = S.launch_count()
+                ctx.step(1)
+                per.append(S.launch_count() - n0)
             ctx.sync()
+            nk.append(per)
             out.append({k: ctx.download(k) for k in STATE})
     for k in STATE:
         assert np.array_equal(out[0][k], out[1][k]), k
+    for per in nk:
+        assert len(set(per)) == 1 and per[0] > 0, per
 
 
 def test_levelset_leaves_the_poisson_work_field_clean():

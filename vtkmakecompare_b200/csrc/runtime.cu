@@ -164,6 +164,8 @@ bool ensure_device() {
 
 static std::atomic<long long> g_launches{0};
 void count_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
+// a graph replay launches the kernels its capture counted
+static void count_launches(long long n) { g_launches.fetch_add(n, std::memory_order_relaxed); }
 
 DBuf& arena(int slot) {
   static DBuf slots[48];
@@ -1431,6 +1433,7 @@ struct nse_ctx {
   cudaGraphExec_t sg[2] = {nullptr, nullptr};
   void* sg_t[2] = {nullptr, nullptr};
   DBuf sg_T[2], sg_uT[2];
+  long long sg_nk[2] = {0, 0};    // kernels in each graph
   unsigned long long sg_sig = 0;  // launch shapes the graphs were captured with
   void* hpin = nullptr;           // pinned staging of the masked line lists
   size_t hpin_n = 0;              // its capacity (ints)
@@ -2843,6 +2846,7 @@ static int step_replay(nse_ctx* x) {
     if (x->sg[k] && x->sg_t[k] == t0) q = k;
   if (q >= 0) {
     if (!NSE_CUDA(cudaGraphLaunch(x->sg[q], x->stream))) return -1;
+    count_launches(x->sg_nk[q]);
     x->f[NSE_T] = x->sg_T[q];
     x->uT = x->sg_uT[q];
     x->l += 1;
@@ -2860,7 +2864,9 @@ static int step_replay(nse_ctx* x) {
     x->sg_off = true;
     return 0;
   }
+  const long long k0 = g_launches.load();
   ctx_step(x);
+  const long long nk = g_launches.load() - k0;  // counted once: the launch below
   cudaGraph_t g = nullptr;
   const cudaError_t ce = cudaStreamEndCapture(x->stream, &g);
   cudaGraphExec_t ex = nullptr;
@@ -2869,6 +2875,7 @@ static int step_replay(nse_ctx* x) {
   if (!ok) {
     // nothing ran: put the host-side state back and step eagerly
     cudaGetLastError();
+    count_launches(-nk);
     x->l = l0;
     x->f[NSE_T] = T0;
     x->uT = uT0;
@@ -2877,12 +2884,14 @@ static int step_replay(nse_ctx* x) {
   }
   if (!NSE_CUDA(cudaGraphLaunch(ex, x->stream))) {
     cudaGraphExecDestroy(ex);
+    count_launches(-nk);
     x->l = l0;
     x->f[NSE_T] = T0;
     x->uT = uT0;
     return -1;
   }
   x->sg[q] = ex;
+  x->sg_nk[q] = nk;
   x->sg_t[q] = t0;
   x->sg_T[q] = x->f[NSE_T];
   x->sg_uT[q] = x->uT;
@@ -3148,6 +3157,7 @@ struct nse_ensemble {
   // form swaps it with the work buffer every step, so a replay is valid only
   // after an even number of eager steps since the capture
   std::vector<void*> tbuf;
+  long long nk = 0;  // kernels in the graph (counted once per replay)
 };
 
 namespace nse {
@@ -3182,9 +3192,12 @@ static bool ens_capture(nse_ensemble* e) {
   e->tbuf.clear();
   for (nse_ctx* x : e->cases) e->tbuf.push_back(x->f[NSE_T].p);
   if (!NSE_CUDA(cudaStreamBeginCapture(e->origin, cudaStreamCaptureModeRelaxed))) return false;
+  const long long k0 = g_launches.load();
   bool ok = ens_fork_from_origin(e);
   for (int st = 0; ok && st < 2; ++st)
     for (nse_ctx* x : e->cases) ctx_step(x);
+  e->nk = g_launches.load() - k0;
+  count_launches(-e->nk);  // counted by each replay instead
   ok = ok && ens_join_into_origin(e);
   cudaGraph_t g = nullptr;
   cudaError_t ce = cudaStreamEndCapture(e->origin, &g);
@@ -3258,6 +3271,7 @@ int nse_ensemble_step(nse_ensemble* e, int nsteps) {
     ok = ok && ens_join_into_origin(e);
     for (; ok && nsteps >= 2; nsteps -= 2) {
       ok = NSE_CUDA(cudaGraphLaunch(e->exec, e->origin));
+      if (ok) count_launches(e->nk);
       for (nse_ctx* x : e->cases) x->l += 2;
     }
     ok = ok && ens_fork_from_origin(e);
