@@ -219,7 +219,7 @@ __global__ void k_fft_fwd_x(FFTShape sh, int npair, Dims d, SpecViewT<CT> sv, Fw
 // CTA: plane index jj (0..ny-1) and columns kx0..kx0+W-1
 template <class CT>
 __global__ void k_fft_z(FFTShape sh, int W, int H, SpecViewT<CT> sv, const CT* __restrict__ tw,
-                        int inv, double nrm) {
+                        int inv, double nrm, int rmul) {
   using RT = typename CReal<CT>::T;
   extern __shared__ __align__(16) char fsm[];
   CT* smem = reinterpret_cast<CT*>(fsm);
@@ -243,7 +243,9 @@ __global__ void k_fft_z(FFTShape sh, int W, int H, SpecViewT<CT> sv, const CT* _
     int kx = kx0 + c;
     if (kx >= H) continue;
     CT v = r[c * FS + kz];
-    if (!inv) { v.x = v.x / rn; v.y = v.y / rn; }
+    // rmul: nrm is the exact reciprocal of a power of two (the same bits)
+    if (!inv && rmul) { v.x = v.x * rn; v.y = v.y * rn; }
+    if (!inv && !rmul) { v.x = v.x / rn; v.y = v.y / rn; }
     sv.base[kx + sv.sj * jj + sv.sk * kz] = v;
   }
 }
@@ -1182,9 +1184,12 @@ static void fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0 = 
   size_t sm = 2 * (size_t)W * (pp.nz + 1) * sizeof(CT);
   smem_optin((const void*)k_fft_z<CT>, sm);
   count_launch();
+  const double nrm = (double)pp.nx * (double)pp.nz;
+  int e2 = 0;
+  const bool pow2 = !inverse && frexp(nrm, &e2) == 0.5;
   k_fft_z<CT><<<grid, fft_threads(W * pp.nz), sm, s>>>(sh, W, pp.H, sv, twz_of<CT>(pp),
-                                                       inverse ? 1 : 0,
-                                                       (double)pp.nx * (double)pp.nz);
+                                                       inverse ? 1 : 0, pow2 ? 1.0 / nrm : nrm,
+                                                       pow2 ? 1 : 0);
 }
 void launch_fft_z(const PoissonPlan& pp, bool inverse, cudaStream_t s, int j0, int nj) {
   fft_z<double2>(pp, inverse, s, j0, nj);
