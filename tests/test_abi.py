@@ -39,6 +39,22 @@ def test_library_exports_every_declared_symbol():
     assert not missing, missing
 
 
+def test_config_flags_match_header():
+    """Every NSE_FLAG_* of include/nsegpu.h has the same value as the Python
+    mirror's FLAG_* constant, and the flags are distinct bits."""
+    from vtkmakecompare_b200 import solver as S
+    text = re.sub(r"/\*.*?\*/", "", open(HEADER).read(), flags=re.S)
+    flags = {m.group(1): int(m.group(2))
+             for m in re.finditer(r"\bNSE_FLAG_([A-Z0-9_]+)\s*=\s*(\d+)", text)}
+    assert len(flags) >= 14
+    for name, v in flags.items():
+        assert getattr(S, "FLAG_" + name) == v, name
+        assert v & (v - 1) == 0, name
+    assert len(set(flags.values())) == len(flags)
+    mirror = {n[5:] for n in dir(S) if n.startswith("FLAG_")}
+    assert mirror == set(flags), mirror ^ set(flags)
+
+
 def test_legacy_signature_tables_match_header():
     protos = prototypes()
     for name, sig in legacy._SIG.items():
